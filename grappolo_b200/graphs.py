@@ -1,0 +1,195 @@
+"""Seeded synthetic graphs and Grappolo's binary graph format.
+
+Every generator returns a :class:`CSRGraph` in the layout Grappolo's loaders
+produce (``DefineStructure/defs.h:85-92``): ``ptr`` int64[NV+1] row offsets,
+``tail`` int64[nnz] column ids and ``weight`` float64[nnz], undirected graphs
+stored twice (once per direction), rows sorted by tail, no duplicate entries.
+
+The generators stand in for the inputs the reference is run on (there is no
+dataset in the reference tree); each one names its shape, sizes and seed.
+"""
+from __future__ import annotations
+
+import dataclasses
+import struct
+
+import numpy as np
+
+
+@dataclasses.dataclass
+class CSRGraph:
+    ptr: np.ndarray      # int64[NV+1]
+    tail: np.ndarray     # int64[nnz]
+    weight: np.ndarray   # float64[nnz]
+
+    @property
+    def num_vertices(self) -> int:
+        return int(self.ptr.shape[0] - 1)
+
+    @property
+    def nnz(self) -> int:
+        return int(self.tail.shape[0])
+
+    @property
+    def num_edges(self) -> int:
+        """Grappolo's ``numEdges``: undirected edges, self-loops counted once."""
+        nv = self.num_vertices
+        heads = np.repeat(np.arange(nv, dtype=np.int64), np.diff(self.ptr))
+        loops = int(np.count_nonzero(heads == self.tail))
+        return (self.nnz - loops) // 2 + loops
+
+    def heads(self) -> np.ndarray:
+        return np.repeat(np.arange(self.num_vertices, dtype=np.int64), np.diff(self.ptr))
+
+
+def csr_from_undirected(nv: int, u: np.ndarray, v: np.ndarray,
+                        w: np.ndarray | None = None) -> CSRGraph:
+    """Symmetrise an undirected edge list (u, v, w) into a deduplicated CSR.
+
+    Self-loops are dropped. When a pair appears more than once the first
+    occurrence's weight is kept, so each undirected edge has one weight that is
+    stored in both directions.
+    """
+    u = np.asarray(u, dtype=np.int64)
+    v = np.asarray(v, dtype=np.int64)
+    if w is None:
+        w = np.ones(u.shape[0], dtype=np.float64)
+    keep = u != v
+    u, v, w = u[keep], v[keep], np.asarray(w, dtype=np.float64)[keep]
+    lo = np.minimum(u, v)
+    hi = np.maximum(u, v)
+    key = lo * nv + hi
+    _, first = np.unique(key, return_index=True)
+    lo, hi, w = lo[first], hi[first], w[first]
+    src = np.concatenate([lo, hi])
+    dst = np.concatenate([hi, lo])
+    ww = np.concatenate([w, w])
+    order = np.lexsort((dst, src))
+    src, dst, ww = src[order], dst[order], ww[order]
+    ptr = np.zeros(nv + 1, dtype=np.int64)
+    np.cumsum(np.bincount(src, minlength=nv), out=ptr[1:])
+    return CSRGraph(ptr, dst.astype(np.int64), ww.astype(np.float64))
+
+
+def planted_partition(num_blocks: int = 1000, block_size: int = 100,
+                      intra_degree: float = 12.0, inter_degree: float = 4.0,
+                      seed: int = 1) -> CSRGraph:
+    """Planted-partition graph with equal blocks and unit weights.
+
+    Inside a block every pair is an edge with probability
+    ``intra_degree / (block_size - 1)``; on top of that
+    ``inter_degree * NV / 2`` edges join uniform random endpoints in different
+    blocks. Default: 100,000 vertices in 1,000 blocks of 100, intra degree 12,
+    inter degree 4 (the plain-Louvain parity workload).
+    """
+    rng = np.random.default_rng(seed)
+    nv = num_blocks * block_size
+    p = intra_degree / (block_size - 1)
+    iu, ju = np.triu_indices(block_size, k=1)
+    pick = rng.random((num_blocks, iu.shape[0])) < p
+    blk, pair = np.nonzero(pick)
+    u_in = blk * block_size + iu[pair]
+    v_in = blk * block_size + ju[pair]
+    m_out = int(round(inter_degree * nv / 2))
+    uo = rng.integers(0, nv, size=m_out, dtype=np.int64)
+    vo = rng.integers(0, nv, size=m_out, dtype=np.int64)
+    cross = (uo // block_size) != (vo // block_size)
+    u = np.concatenate([u_in, uo[cross]])
+    v = np.concatenate([v_in, vo[cross]])
+    return csr_from_undirected(nv, u, v)
+
+
+def rmat(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19,
+         c: float = 0.19, seed: int = 1, weighted: bool = True) -> CSRGraph:
+    """R-MAT graph (Chakrabarti et al.) on 2**scale vertices.
+
+    ``edge_factor * 2**scale`` edges are drawn by recursive quadrant choice with
+    probabilities (a, b, c, 1-a-b-c); the result is symmetrised with self-loops
+    and duplicates removed. Weights are uniform in (0, 1] when ``weighted``.
+    Vertex ids are not permuted, so low ids are the hubs.
+    """
+    rng = np.random.default_rng(seed)
+    nv = 1 << scale
+    m = edge_factor * nv
+    u = np.zeros(m, dtype=np.int64)
+    v = np.zeros(m, dtype=np.int64)
+    ab, abc = a + b, a + b + c
+    for _ in range(scale):
+        r = rng.random(m)
+        u = (u << 1) | (r >= ab)
+        v = (v << 1) | (((r >= a) & (r < ab)) | (r >= abc))
+    w = (1.0 - rng.random(m)) if weighted else None
+    return csr_from_undirected(nv, u, v, w)
+
+
+def random_weights(g: CSRGraph, seed: int = 7) -> CSRGraph:
+    """Same topology, FP64 weights uniform in (0, 1], symmetric per edge."""
+    rng = np.random.default_rng(seed)
+    heads = g.heads()
+    lo = np.minimum(heads, g.tail)
+    hi = np.maximum(heads, g.tail)
+    key = lo * g.num_vertices + hi
+    uniq, inv = np.unique(key, return_inverse=True)
+    wu = 1.0 - rng.random(uniq.shape[0])
+    return CSRGraph(g.ptr.copy(), g.tail.copy(), wu[inv].astype(np.float64))
+
+
+def from_edges(nv: int, edges, weights=None, keep_self_loops: bool = True) -> CSRGraph:
+    """Small hand-built graphs: undirected (u, v[, w]) list, self-loops kept once."""
+    e = np.asarray(edges, dtype=np.int64).reshape(-1, 2)
+    w = np.ones(e.shape[0]) if weights is None else np.asarray(weights, dtype=np.float64)
+    loops = e[:, 0] == e[:, 1]
+    g = csr_from_undirected(nv, e[~loops, 0], e[~loops, 1], w[~loops])
+    if keep_self_loops and loops.any():
+        heads = np.concatenate([g.heads(), e[loops, 0]])
+        tails = np.concatenate([g.tail, e[loops, 1]])
+        ws = np.concatenate([g.weight, w[loops]])
+        order = np.lexsort((tails, heads))
+        ptr = np.zeros(nv + 1, dtype=np.int64)
+        np.cumsum(np.bincount(heads, minlength=nv), out=ptr[1:])
+        g = CSRGraph(ptr, tails[order], ws[order])
+    return g
+
+
+def load_metis(path: str) -> CSRGraph:
+    """Unweighted METIS adjacency file (1-based neighbour lists), as in karate.graph."""
+    with open(path) as f:
+        lines = [ln for ln in f.read().splitlines() if not ln.startswith('%')]
+    nv = int(lines[0].split()[0])
+    heads, tails = [], []
+    for i in range(nv):
+        toks = lines[1 + i].split() if 1 + i < len(lines) else []
+        for t in toks:
+            heads.append(i)
+            tails.append(int(t) - 1)
+    heads = np.asarray(heads, dtype=np.int64)
+    tails = np.asarray(tails, dtype=np.int64)
+    order = np.lexsort((tails, heads))
+    ptr = np.zeros(nv + 1, dtype=np.int64)
+    np.cumsum(np.bincount(heads, minlength=nv), out=ptr[1:])
+    return CSRGraph(ptr, tails[order], np.ones(heads.shape[0]))
+
+
+# Grappolo binary format (InputsOutput/loadBinary.cpp:6-48, writeBinary.cpp:2-29):
+# int64 NV, int64 NE, int64 weighted, int64[NV+1] offsets, then 2*NE records of
+# {int64 head, int64 tail, float64 weight}.
+_EDGE = np.dtype([('head', '<i8'), ('tail', '<i8'), ('weight', '<f8')])
+
+
+def write_binary(g: CSRGraph, path: str, weighted: int = 1) -> None:
+    rec = np.empty(g.nnz, dtype=_EDGE)
+    rec['head'] = g.heads()
+    rec['tail'] = g.tail
+    rec['weight'] = g.weight
+    with open(path, 'wb') as f:
+        f.write(struct.pack('<qqq', g.num_vertices, g.nnz // 2, weighted))
+        f.write(g.ptr.astype('<i8').tobytes())
+        f.write(rec.tobytes())
+
+
+def read_binary(path: str) -> CSRGraph:
+    with open(path, 'rb') as f:
+        nv, ne, _ = struct.unpack('<qqq', f.read(24))
+        ptr = np.frombuffer(f.read(8 * (nv + 1)), dtype='<i8').copy()
+        rec = np.frombuffer(f.read(_EDGE.itemsize * 2 * ne), dtype=_EDGE)
+    return CSRGraph(ptr, rec['tail'].astype(np.int64), rec['weight'].astype(np.float64))

@@ -1,0 +1,285 @@
+// Harness around Grappolo's own hot-path functions.
+//
+// TEST INFRASTRUCTURE ONLY.  oracle/Makefile compiles this file together with
+// the reference's unmodified sources (Utility/, Coloring/,
+// BasicCommunitiesDetection/, InputsOutput/loadMetis.cpp) into
+// oracle/_ref/libgrappolo_ref.so.  It converts the SoA CSR that the tests use
+// into the reference's `graph`/`edge` structs (DefineStructure/defs.h:78-92),
+// calls the reference function named in each wrapper, and copies results
+// back.  It is what pins the C restatement in louvain_oracle.c, generates the
+// golden fixtures, and is the CPU baseline that bench.py times.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <unistd.h>
+#include <vector>
+
+#include "defs.h"
+#include "basic_comm.h"
+#include "basic_util.h"
+#include "color_comm.h"
+#include "coloring.h"
+#include "input_output.h"
+#include "utilityClusteringFunctions.h"
+
+static int g_quiet = 0;
+static int g_saved_fd = -1;
+
+static void quiet_begin() {
+    if (!g_quiet) return;
+    fflush(stdout);
+    g_saved_fd = dup(1);
+    FILE *devnull = fopen("/dev/null", "w");
+    dup2(fileno(devnull), 1);
+    fclose(devnull);
+}
+
+static void quiet_end() {
+    if (!g_quiet || g_saved_fd < 0) return;
+    fflush(stdout);
+    dup2(g_saved_fd, 1);
+    close(g_saved_fd);
+    g_saved_fd = -1;
+}
+
+static graph *make_graph(long nv, const long *ptr, const long *tail, const double *w) {
+    graph *G = (graph *)malloc(sizeof(graph));
+    long nnz = ptr[nv];
+    G->numVertices = nv;
+    G->sVertices = nv;
+    long loops = 0;
+    G->edgeListPtrs = (long *)malloc(sizeof(long) * (nv + 1));
+    G->edgeList = (edge *)malloc(sizeof(edge) * (nnz ? nnz : 1));
+    memcpy(G->edgeListPtrs, ptr, sizeof(long) * (nv + 1));
+    for (long i = 0; i < nv; i++) {
+        for (long j = ptr[i]; j < ptr[i + 1]; j++) {
+            G->edgeList[j].head = i;
+            G->edgeList[j].tail = tail[j];
+            G->edgeList[j].weight = w[j];
+            if (tail[j] == i) loops++;
+        }
+    }
+    G->numEdges = (nnz - loops) / 2 + loops;
+    return G;
+}
+
+static void free_graph(graph *G) {
+    free(G->edgeListPtrs);
+    free(G->edgeList);
+    free(G);
+}
+
+extern "C" {
+
+void ref_set_quiet(int q) { g_quiet = q; }
+
+// Coloring/coloringDistanceOne.cpp:50 algoDistanceOneVertexColoringOpt,
+// colours initialised to -1 as runMultiPhaseColoring.cpp:61-65 does.
+int ref_color(long nv, const long *ptr, const long *tail, const double *w, int *color,
+              int nthreads, double *totTime) {
+    graph *G = make_graph(nv, ptr, tail, w);
+    for (long i = 0; i < nv; i++) color[i] = -1;
+    quiet_begin();
+    int mc = algoDistanceOneVertexColoringOpt(G, color, nthreads, totTime);
+    quiet_end();
+    free_graph(G);
+    return mc;
+}
+
+// Coloring/parallelLouvainWithColoring.cpp:47 algoLouvainWithDistOneColoring
+double ref_coloring_phase(long nv, const long *ptr, const long *tail, const double *w,
+                          long *C, int *color, int numColor, double Lower, double thresh,
+                          int nthreads, int *numItr, double *totTime) {
+    graph *G = make_graph(nv, ptr, tail, w);
+    quiet_begin();
+    double q = algoLouvainWithDistOneColoring(G, C, nthreads, color, numColor, Lower, thresh,
+                                              totTime, numItr);
+    quiet_end();
+    free_graph(G);
+    return q;
+}
+
+// BasicCommunitiesDetection/parallelLouvainMethod.cpp:65 parallelLouvianMethod
+double ref_basic_phase(long nv, const long *ptr, const long *tail, const double *w, long *C,
+                       double Lower, double thresh, int nthreads, int *numItr,
+                       double *totTime) {
+    graph *G = make_graph(nv, ptr, tail, w);
+    quiet_begin();
+    double q = parallelLouvianMethod(G, C, nthreads, Lower, thresh, totTime, numItr);
+    quiet_end();
+    free_graph(G);
+    return q;
+}
+
+// Utility/buildNextPhase.cpp:48 renumberClustersContiguously
+long ref_renumber(long *C, long n) {
+    quiet_begin();
+    long r = renumberClustersContiguously(C, n);
+    quiet_end();
+    return r;
+}
+
+// Utility/buildNextPhase.cpp:83 buildNextLevelGraphOpt.  Returns the output
+// nnz; arrays are malloc'd here and released with ref_free.  Fails (-1) if an
+// output record's head does not match its row.
+long ref_build_next_level(long nv, const long *ptr, const long *tail, const double *w,
+                          long *C, long ncl, int nthreads, long **optr, long **otail,
+                          double **ow, long *numEdges) {
+    graph *G = make_graph(nv, ptr, tail, w);
+    graph *Gout = (graph *)malloc(sizeof(graph));
+    quiet_begin();
+    buildNextLevelGraphOpt(G, Gout, C, ncl, nthreads);
+    quiet_end();
+    long onv = Gout->numVertices;
+    long onnz = Gout->edgeListPtrs[onv];
+    long *p = (long *)malloc(sizeof(long) * (onv + 1));
+    long *t = (long *)malloc(sizeof(long) * (onnz ? onnz : 1));
+    double *ww = (double *)malloc(sizeof(double) * (onnz ? onnz : 1));
+    memcpy(p, Gout->edgeListPtrs, sizeof(long) * (onv + 1));
+    long bad = 0;
+    for (long i = 0; i < onv; i++)
+        for (long j = p[i]; j < p[i + 1]; j++) {
+            t[j] = Gout->edgeList[j].tail;
+            ww[j] = Gout->edgeList[j].weight;
+            if (Gout->edgeList[j].head != i) bad++;
+        }
+    *numEdges = Gout->numEdges;
+    free_graph(Gout);
+    free_graph(G);
+    *optr = p; *otail = t; *ow = ww;
+    return bad ? -1 : onnz;
+}
+
+void ref_free(void *p) { free(p); }
+
+// Per-vertex move decision through the reference's own primitives, set up as
+// the colour sweep does (parallelLouvainWithColoring.cpp:181-188):
+// own community first with Counter 0, buildLocalMapCounter
+// (utilityClusteringFunctions.cpp:172), then max() (:226).
+void ref_decide_batch(long nv, const long *ptr, const long *tail, const double *w,
+                      const long *C, const double *vDeg, const double *cDeg,
+                      const long *cSize, double constant, long nverts, const long *verts,
+                      long *targets) {
+    graph *G = make_graph(nv, ptr, tail, w);
+    Comm *cInfo = (Comm *)malloc(sizeof(Comm) * (nv ? nv : 1));
+    for (long i = 0; i < nv; i++) { cInfo[i].size = cSize[i]; cInfo[i].degree = cDeg[i]; }
+    long *Cm = (long *)malloc(sizeof(long) * (nv ? nv : 1));
+    memcpy(Cm, C, sizeof(long) * nv);
+    for (long k = 0; k < nverts; k++) {
+        long i = verts[k];
+        long adj1 = ptr[i], adj2 = ptr[i + 1];
+        if (adj1 == adj2) { targets[k] = -1; continue; }
+        std::map<long, long> clusterLocalMap;
+        std::vector<double> Counter;
+        clusterLocalMap[Cm[i]] = 0;
+        Counter.push_back(0);
+        double selfLoop = buildLocalMapCounter(adj1, adj2, clusterLocalMap, Counter,
+                                               G->edgeList, Cm, i);
+        targets[k] = max(clusterLocalMap, Counter, selfLoop, cInfo, vDeg[i], Cm[i], constant);
+    }
+    free(Cm);
+    free(cInfo);
+    free_graph(G);
+}
+
+// Utility/utilityClusteringFunctions.cpp:70,89 sumVertexDegree +
+// calConstantForSecondTerm.
+double ref_vertex_degrees(long nv, const long *ptr, const long *tail, const double *w,
+                          double *vDeg) {
+    graph *G = make_graph(nv, ptr, tail, w);
+    Comm *cInfo = (Comm *)malloc(sizeof(Comm) * (nv ? nv : 1));
+    sumVertexDegree(G->edgeList, G->edgeListPtrs, vDeg, nv, cInfo);
+    double c = calConstantForSecondTerm(vDeg, nv);
+    free(cInfo);
+    free_graph(G);
+    return c;
+}
+
+// Coloring/runMultiPhaseColoring.cpp:51 and
+// BasicCommunitiesDetection/runMultiPhaseBasic.cpp:52.  They print their
+// results; stdout is captured into `log` (NUL-terminated, truncated to cap).
+static long run_captured(char *log, long cap, void (*fn)(void *), void *arg) {
+    fflush(stdout);
+    int saved = dup(1);
+    FILE *tmp = tmpfile();
+    dup2(fileno(tmp), 1);
+    fn(arg);
+    fflush(stdout);
+    dup2(saved, 1);
+    close(saved);
+    long n = 0;
+    if (log && cap > 0) {
+        fseek(tmp, 0, SEEK_END);
+        long size = ftell(tmp);
+        long keep = size < cap - 1 ? size : cap - 1;
+        fseek(tmp, size - keep, SEEK_SET);
+        n = (long)fread(log, 1, keep, tmp);
+        log[n] = 0;
+    }
+    fclose(tmp);
+    return n;
+}
+
+struct mp_args {
+    graph *G; long *C_orig; int coloring, numColors, replaceMap, basicOpt;
+    long minGraphSize; double threshold, C_threshold; int nthreads;
+};
+
+static void call_coloring(void *p) {
+    mp_args *a = (mp_args *)p;
+    runMultiPhaseColoring(a->G, a->C_orig, a->coloring, a->numColors, a->replaceMap,
+                          a->minGraphSize, a->threshold, a->C_threshold, a->nthreads, 1);
+}
+
+static void call_basic(void *p) {
+    mp_args *a = (mp_args *)p;
+    runMultiPhaseBasic(a->G, a->C_orig, a->basicOpt, a->minGraphSize, a->threshold,
+                       a->C_threshold, a->nthreads, 1);
+}
+
+long ref_run_multiphase_coloring(long nv, const long *ptr, const long *tail, const double *w,
+                                 long *C_orig, int coloring, int numColors, int replaceMap,
+                                 long minGraphSize, double threshold, double C_threshold,
+                                 int nthreads, char *log, long cap) {
+    mp_args a;
+    a.G = make_graph(nv, ptr, tail, w);  // freed by the reference
+    a.C_orig = C_orig; a.coloring = coloring; a.numColors = numColors;
+    a.replaceMap = replaceMap; a.basicOpt = 0; a.minGraphSize = minGraphSize;
+    a.threshold = threshold; a.C_threshold = C_threshold; a.nthreads = nthreads;
+    for (long i = 0; i < nv; i++) C_orig[i] = -1;
+    return run_captured(log, cap, call_coloring, &a);
+}
+
+long ref_run_multiphase_basic(long nv, const long *ptr, const long *tail, const double *w,
+                              long *C_orig, int basicOpt, long minGraphSize, double threshold,
+                              double C_threshold, int nthreads, char *log, long cap) {
+    mp_args a;
+    a.G = make_graph(nv, ptr, tail, w);
+    a.C_orig = C_orig; a.coloring = 0; a.numColors = 0; a.replaceMap = 0;
+    a.basicOpt = basicOpt; a.minGraphSize = minGraphSize; a.threshold = threshold;
+    a.C_threshold = C_threshold; a.nthreads = nthreads;
+    for (long i = 0; i < nv; i++) C_orig[i] = -1;
+    return run_captured(log, cap, call_basic, &a);
+}
+
+// InputsOutput/loadMetis.cpp:19 loadMetisFileFormat -> SoA CSR (malloc'd).
+long ref_load_metis(const char *path, long **optr, long **otail, double **ow) {
+    graph G;
+    quiet_begin();
+    loadMetisFileFormat(&G, path);
+    quiet_end();
+    long nv = G.numVertices;
+    long nnz = G.edgeListPtrs[nv];
+    long *p = (long *)malloc(sizeof(long) * (nv + 1));
+    long *t = (long *)malloc(sizeof(long) * (nnz ? nnz : 1));
+    double *ww = (double *)malloc(sizeof(double) * (nnz ? nnz : 1));
+    memcpy(p, G.edgeListPtrs, sizeof(long) * (nv + 1));
+    for (long j = 0; j < nnz; j++) { t[j] = G.edgeList[j].tail; ww[j] = G.edgeList[j].weight; }
+    free(G.edgeListPtrs);
+    free(G.edgeList);
+    *optr = p; *otail = t; *ow = ww;
+    return nv;
+}
+
+}  // extern "C"
