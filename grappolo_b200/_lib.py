@@ -1,0 +1,123 @@
+"""ctypes binding of libgrappolo_b200.so (the C ABI in include/grappolo_b200.h).
+
+The library is built in-tree by ``grappolo_b200.build`` (or
+``__graft_entry__.build()``).  There is no CPU fallback: if the shared library
+is missing, importing this module raises.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, 'libgrappolo_b200.so')
+
+GLV_OK = 0
+GLV_MODE_VERIFY = 0
+GLV_MODE_FAST = 1
+GLV_MAX_PHASES = 256
+
+ERRORS = {
+    1: 'invalid argument', 2: 'CUDA error', 3: 'out of memory',
+    4: 'colouring needs more than 4096 colours', 5: 'numVertices >= 2^31',
+    6: 'unsupported option', 7: 'no CUDA device', 8: 'size exceeds a fixed limit',
+}
+
+
+class GlvEdge(ct.Structure):
+    _fields_ = [('head', ct.c_long), ('tail', ct.c_long), ('weight', ct.c_double)]
+
+
+class GlvGraph(ct.Structure):
+    _fields_ = [('numVertices', ct.c_long), ('sVertices', ct.c_long), ('numEdges', ct.c_long),
+                ('edgeListPtrs', ct.POINTER(ct.c_long)), ('edgeList', ct.POINTER(GlvEdge))]
+
+
+class GlvPhaseStats(ct.Structure):
+    _fields_ = [('num_vertices', ct.c_long), ('nnz', ct.c_long), ('colored', ct.c_int),
+                ('recolored', ct.c_int), ('num_colors', ct.c_int), ('iterations', ct.c_int),
+                ('modularity', ct.c_double), ('clusters', ct.c_long),
+                ('time_sweep', ct.c_double), ('time_color', ct.c_double),
+                ('time_coarsen', ct.c_double), ('edges_swept', ct.c_double)]
+
+
+class GlvRunStats(ct.Structure):
+    _fields_ = [('phases', ct.c_int), ('total_iterations', ct.c_int),
+                ('final_clusters', ct.c_long), ('final_modularity', ct.c_double),
+                ('time_total', ct.c_double), ('time_clustering', ct.c_double),
+                ('time_coloring', ct.c_double), ('time_building', ct.c_double),
+                ('time_transfer', ct.c_double), ('edges_swept', ct.c_double),
+                ('kernel_launches', ct.c_long), ('nphase', ct.c_int),
+                ('phase', GlvPhaseStats * GLV_MAX_PHASES)]
+
+    def to_dict(self) -> dict:
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k != 'phase'}
+        d['phase'] = [{k: getattr(p, k) for k, _ in GlvPhaseStats._fields_}
+                      for p in self.phase[:self.nphase]]
+        return d
+
+
+class GrappoloError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f'grappolo_b200 error {code} ({ERRORS.get(code, "?")}): {msg}')
+        self.code = code
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f'{LIB_PATH} is missing: build it with grappolo_b200.build.build()')
+    L = ct.CDLL(LIB_PATH)
+    P = ct.POINTER
+    L.glv_version.restype = ct.c_char_p
+    L.glv_last_error.restype = ct.c_char_p
+    L.glv_kernel_launch_count.restype = ct.c_long
+    for name in ('glv_run_multiphase_coloring', 'glv_run_multiphase_basic',
+                 'glv_run_multiphase_coloring_csr', 'glv_run_multiphase_basic_csr',
+                 'glv_dev_run_multiphase', 'glv_louvain_coloring_phase',
+                 'glv_louvain_basic_phase', 'glv_distance_one_coloring',
+                 'glv_renumber_clusters', 'glv_build_next_level', 'glv_modularity',
+                 'glv_decide_batch'):
+        getattr(L, name).restype = ct.c_int
+    L.glv_run_multiphase_coloring.argtypes = [P(GlvGraph), P(ct.c_long), ct.c_int, ct.c_int,
+                                              ct.c_int, ct.c_long, ct.c_double, ct.c_double,
+                                              ct.c_int, P(GlvRunStats)]
+    L.glv_run_multiphase_basic.argtypes = [P(GlvGraph), P(ct.c_long), ct.c_int, ct.c_long,
+                                           ct.c_double, ct.c_double, ct.c_int, P(GlvRunStats)]
+    L.glv_run_multiphase_coloring_csr.argtypes = [ct.c_long, P(ct.c_long), P(ct.c_long),
+                                                  P(ct.c_double), P(ct.c_long), ct.c_long,
+                                                  ct.c_double, ct.c_double, ct.c_int,
+                                                  P(GlvRunStats)]
+    L.glv_run_multiphase_basic_csr.argtypes = [ct.c_long, P(ct.c_long), P(ct.c_long),
+                                               P(ct.c_double), P(ct.c_long), ct.c_double,
+                                               ct.c_int, P(GlvRunStats)]
+    L.glv_dev_run_multiphase.argtypes = [ct.c_long, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                         ct.c_void_p, ct.c_int, ct.c_long, ct.c_double,
+                                         ct.c_double, ct.c_int, ct.c_void_p, P(GlvRunStats)]
+    L.glv_louvain_coloring_phase.argtypes = [P(GlvGraph), P(ct.c_long), P(ct.c_int), ct.c_int,
+                                             ct.c_double, ct.c_double, ct.c_int,
+                                             P(ct.c_double), P(ct.c_int), P(ct.c_double)]
+    L.glv_louvain_basic_phase.argtypes = [P(GlvGraph), P(ct.c_long), ct.c_double, ct.c_double,
+                                          ct.c_int, P(ct.c_double), P(ct.c_int),
+                                          P(ct.c_double)]
+    L.glv_distance_one_coloring.argtypes = [P(GlvGraph), P(ct.c_int), ct.c_int, P(ct.c_int),
+                                            P(ct.c_double)]
+    L.glv_renumber_clusters.argtypes = [P(ct.c_long), ct.c_long, P(ct.c_long)]
+    L.glv_build_next_level.argtypes = [P(GlvGraph), P(GlvGraph), P(ct.c_long), ct.c_long,
+                                       ct.c_int, P(ct.c_double)]
+    L.glv_modularity.argtypes = [P(GlvGraph), P(ct.c_long), P(ct.c_double)]
+    L.glv_decide_batch.argtypes = [ct.c_long, P(ct.c_long), P(ct.c_long), P(ct.c_double),
+                                   P(ct.c_long), P(ct.c_double), P(ct.c_double), P(ct.c_long),
+                                   ct.c_double, ct.c_long, P(ct.c_long), P(ct.c_long)]
+    _lib = L
+    return L
+
+
+def check(rc: int) -> None:
+    if rc != GLV_OK:
+        raise GrappoloError(rc, lib().glv_last_error().decode(errors='replace'))

@@ -1,0 +1,118 @@
+// Grappolo's C++ entry points (include/grappolo_compat.h) over the C ABI.
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+
+#include "grappolo_b200.h"
+#include "grappolo_compat.h"
+
+static_assert(sizeof(edge) == sizeof(glv_edge), "edge layout");
+static_assert(sizeof(graph) == sizeof(glv_graph), "graph layout");
+
+static int mode_for(int nThreads) {
+  const char *env = getenv("GRAPPOLO_B200_MODE");
+  if (env && !strcmp(env, "verify")) return GLV_MODE_VERIFY;
+  if (env && !strcmp(env, "fast")) return GLV_MODE_FAST;
+  return nThreads <= 1 ? GLV_MODE_VERIFY : GLV_MODE_FAST;
+}
+
+static void die(const char *where, int rc) {
+  fprintf(stderr, "%s: grappolo_b200 error %d: %s\n", where, rc, glv_last_error());
+  exit(1);
+}
+
+static void print_summary(const glv_run_stats &s, int coloring, int numThreads) {
+  printf("********************************************\n");
+  printf("*********    Compact Summary   *************\n");
+  printf("********************************************\n");
+  printf("Number of threads              : %d\n", numThreads);
+  printf("Total number of phases         : %d\n", s.phases);
+  printf("Total number of iterations     : %d\n", s.total_iterations);
+  printf("Final number of clusters       : %ld\n", s.final_clusters);
+  printf("Final modularity               : %lf\n", s.final_modularity);
+  printf("Total time for clustering      : %lf\n", s.time_clustering);
+  printf("Total time for building phases : %lf\n", s.time_building);
+  if (coloring) printf("Total time for coloring        : %lf\n", s.time_coloring);
+  printf("********************************************\n");
+  printf("TOTAL TIME                     : %lf\n",
+         s.time_clustering + s.time_building + s.time_coloring);
+  printf("********************************************\n");
+}
+
+static void free_graph(graph *G) {
+  if (!G) return;
+  free(G->edgeListPtrs);
+  free(G->edgeList);
+  free(G);
+}
+
+void runMultiPhaseColoring(graph *G, long *C_orig, int coloring, int numColors, int replaceMap,
+                           long minGraphSize, double threshold, double C_threshold,
+                           int numThreads, int threadsOpt) {
+  (void)threadsOpt;
+  printf("Within runMultiPhaseColoring()\n");
+  glv_run_stats *s = (glv_run_stats *)calloc(1, sizeof(glv_run_stats));
+  int rc = glv_run_multiphase_coloring((const glv_graph *)G, C_orig, coloring, numColors,
+                                       replaceMap, minGraphSize, threshold, C_threshold,
+                                       mode_for(numThreads), s);
+  if (rc != GLV_OK) die("runMultiPhaseColoring", rc);
+  print_summary(*s, coloring == 1, numThreads);
+  free(s);
+  free_graph(G);  // the reference consumes G (runMultiPhaseColoring.cpp:226-232)
+}
+
+void runMultiPhaseBasic(graph *G, long *C_orig, int basicOpt, long minGraphSize,
+                        double threshold, double C_threshold, int numThreads, int threadsOpt) {
+  (void)threadsOpt;
+  glv_run_stats *s = (glv_run_stats *)calloc(1, sizeof(glv_run_stats));
+  int rc = glv_run_multiphase_basic((const glv_graph *)G, C_orig, basicOpt, minGraphSize,
+                                    threshold, C_threshold, mode_for(numThreads), s);
+  if (rc != GLV_OK) die("runMultiPhaseBasic", rc);
+  print_summary(*s, 0, numThreads);
+  free(s);
+  free_graph(G);
+}
+
+double algoLouvainWithDistOneColoring(graph *G, long *C, int nThreads, int *color, int numColor,
+                                      double Lower, double thresh, double *totTime, int *numItr) {
+  printf("Within algoLouvainWithDistOneColoring(#colors= %d)\n", numColor);
+  double q = 0;
+  int rc = glv_louvain_coloring_phase((const glv_graph *)G, C, color, numColor, Lower, thresh,
+                                      mode_for(nThreads), &q, numItr, totTime);
+  if (rc != GLV_OK) die("algoLouvainWithDistOneColoring", rc);
+  return q;
+}
+
+double parallelLouvianMethod(graph *G, long *C, int nThreads, double Lower, double thresh,
+                             double *totTime, int *numItr) {
+  printf("Within parallelLouvianMethod()\n");
+  double q = 0;
+  int rc = glv_louvain_basic_phase((const glv_graph *)G, C, Lower, thresh, mode_for(nThreads),
+                                   &q, numItr, totTime);
+  if (rc != GLV_OK) die("parallelLouvianMethod", rc);
+  return q;
+}
+
+int algoDistanceOneVertexColoringOpt(graph *G, int *vtxColor, int nThreads, double *totTime) {
+  int mc = -1;
+  int rc = glv_distance_one_coloring((const glv_graph *)G, vtxColor, mode_for(nThreads), &mc,
+                                     totTime);
+  if (rc != GLV_OK) die("algoDistanceOneVertexColoringOpt", rc);
+  return mc;
+}
+
+long renumberClustersContiguously(long *C, long size) {
+  long n = 0;
+  int rc = glv_renumber_clusters(C, size, &n);
+  if (rc != GLV_OK) die("renumberClustersContiguously", rc);
+  return n;
+}
+
+double buildNextLevelGraphOpt(graph *Gin, graph *Gout, long *C, long numUniqueClusters,
+                              int nThreads) {
+  double t = 0;
+  int rc = glv_build_next_level((const glv_graph *)Gin, (glv_graph *)Gout, C, numUniqueClusters,
+                                mode_for(nThreads), &t);
+  if (rc != GLV_OK) die("buildNextLevelGraphOpt", rc);
+  return t;
+}

@@ -1,0 +1,1341 @@
+// Host side of the B200 Louvain engine: device-resident levels, the colour /
+// degree-bin schedule, CUDA-graph-captured sweep iterations, the multiphase
+// drivers and the C ABI declared in include/grappolo_b200.h.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cub/cub.cuh>
+
+#include "phase_kernels.cuh"
+#include "sweep.cuh"
+
+namespace glv {
+
+static std::atomic<long> g_launches{0};
+static thread_local std::string g_err;
+
+static int fail(int code, const char *msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(expr)                                                                         \
+  do {                                                                                   \
+    cudaError_t e_ = (expr);                                                             \
+    if (e_ != cudaSuccess) {                                                             \
+      g_err = std::string(#expr) + ": " + cudaGetErrorString(e_);                        \
+      return e_ == cudaErrorMemoryAllocation ? GLV_ERR_OOM : GLV_ERR_CUDA;              \
+    }                                                                                    \
+  } while (0)
+
+#define TRY(expr)                 \
+  do {                            \
+    int r_ = (expr);              \
+    if (r_ != GLV_OK) return r_;  \
+  } while (0)
+
+#define LAUNCH(kernel, grid, block, smem, stream, ...)            \
+  do {                                                            \
+    kernel<<<(grid), (block), (smem), (stream)>>>(__VA_ARGS__);   \
+    ++launches_;                                                  \
+    CK(cudaGetLastError());                                       \
+  } while (0)
+
+static double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch())
+      .count();
+}
+
+static int bits_for(int64_t x) {  // bits to hold values 0..x
+  int b = 1;
+  while (b < 62 && (int64_t(1) << b) <= x) ++b;
+  return b;
+}
+
+// A device level graph.
+struct Level {
+  int64_t nv = 0, nnz = 0;
+  int64_t *ptr = nullptr;
+  int32_t *tail = nullptr;
+  double *w = nullptr;
+  bool owned = false;
+};
+
+// One (class, sublevel) step: member positions of each degree bin.
+struct Step {
+  int64_t seg[NBINS + 1];
+};
+
+struct ClassSched {
+  int64_t begin = 0, end = 0;  // member positions of the whole class
+  std::vector<Step> steps;
+};
+
+class Engine {
+ public:
+  explicit Engine(cudaStream_t s, int mode) : s_(s), mode_(mode) {}
+  ~Engine() { release(); }
+
+  int init(int64_t nv0, int64_t nnz0);
+  int upload_check(const Level &L);
+  int color(const Level &L, int *ncolors, double *secs);
+  int coloring_phase(const Level &L, int ncolors, bool stale, double lower, double thresh,
+                     double *mod, int *itr);
+  int basic_phase(const Level &L, double lower, double thresh, double *mod, int *itr);
+  int renumber(int32_t *C, int64_t n, int64_t *ncl);
+  int coarsen(const Level &in, const int32_t *C, int64_t ncl, Level *out, int64_t *num_edges);
+  int modularity_of(const Level &L, const int32_t *C, double *q);
+  int decide(const Level &L, const int32_t *verts, int64_t nverts);
+  int run_multiphase(const Level &L0, int32_t *d_C_orig, bool coloring, long min_graph_size,
+                     double threshold, double c_threshold, glv_run_stats *st);
+  void free_level(Level &L);
+
+  // state buffers (device)
+  double *vDeg = nullptr, *cDeg = nullptr, *dDeg = nullptr, *own_w = nullptr;
+  int32_t *cSize = nullptr, *dSize = nullptr;
+  int32_t *C = nullptr, *Cpast = nullptr, *Ctgt = nullptr;
+  int32_t *color_ = nullptr;
+  double *cst = nullptr;  // {constant, 2m}
+  long launches_ = 0;
+  bool integral = false;
+  double t_sweep = 0, t_color = 0, t_coarsen = 0;
+  double edges_swept = 0;
+
+ private:
+  template <class T>
+  int alloc(T **p, size_t n) {
+    CK(cudaMallocAsync((void **)p, std::max<size_t>(n, 1) * sizeof(T), s_));
+    return GLV_OK;
+  }
+  template <class T>
+  void dfree(T *&p) {
+    if (p) cudaFreeAsync(p, s_);
+    p = nullptr;
+  }
+  int temp(size_t bytes) {
+    if (bytes <= temp_bytes_) return GLV_OK;
+    dfree(temp_);
+    temp_bytes_ = bytes + (bytes >> 3) + 1024;
+    return alloc(reinterpret_cast<unsigned char **>(&temp_), temp_bytes_);
+  }
+  void release();
+  int phase_init(const Level &L, bool need_past);
+  int build_schedule(const Level &L, const int32_t *color, int ncolors, const int32_t *sub,
+                     int nsub, std::vector<ClassSched> *sched);
+  int hub_offsets(const Level &L, std::vector<ClassSched> &sched);
+  int sublevels(const Level &L, int ncolors, int32_t **d_sub, int *nsub);
+  int launch_sweep(const Level &L, const Step &st, SweepArgs a, bool ordered);
+  int launch_apply(const ClassSched &cs, bool ordered);
+  int launch_modularity(const Level &L, const int32_t *Cm, const double *ownw);
+  int grow_hub(size_t entries);
+  bool ordered() const { return mode_ == GLV_MODE_VERIFY && !integral; }
+
+  cudaStream_t s_;
+  int mode_;
+  int nsm_ = 148;
+  int64_t nv0_ = 0, nnz0_ = 0;
+  BinLimits lim_{127, 4095};
+  // schedule buffers
+  int32_t *keys_ = nullptr, *keys2_ = nullptr, *members_ = nullptr, *vals_ = nullptr;
+  int32_t *move_old_ = nullptr, *move_new_ = nullptr, *hist_ = nullptr;
+  int64_t *hub_off_ = nullptr;
+  int32_t *hub_keys_ = nullptr;
+  double *hub_vals_ = nullptr;
+  size_t hub_cap_ = 0;
+  int hist_cap_ = 0;
+  // ordered-delta buffers
+  uint64_t *dkeys_ = nullptr, *dkeys2_ = nullptr;
+  DeltaRec *drecs_ = nullptr, *drecs2_ = nullptr;
+  // modularity
+  double *part_e_ = nullptr, *part_a_ = nullptr, *mod_out_ = nullptr;
+  double *h_mod_ = nullptr;  // pinned
+  // misc
+  unsigned char *temp_ = nullptr;
+  size_t temp_bytes_ = 0;
+  int64_t max_class_ = 0;
+};
+
+constexpr int kConstParts = 1024;  // blocks of the constant's reduction
+
+static int grid_for(int64_t n, int block, int cap) {
+  int64_t g = (n + block - 1) / block;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(g, cap));
+}
+
+void Engine::release() {
+  double **dp[] = {&vDeg, &cDeg, &dDeg, &own_w, &cst, &hub_vals_, &part_e_, &part_a_, &mod_out_};
+  for (auto p : dp) dfree(*p);
+  int32_t **ip[] = {&cSize, &dSize, &C, &Cpast, &Ctgt, &color_, &keys_, &keys2_, &members_,
+                    &vals_, &move_old_, &move_new_, &hist_, &hub_keys_};
+  for (auto p : ip) dfree(*p);
+  dfree(hub_off_);
+  dfree(dkeys_); dfree(dkeys2_); dfree(drecs_); dfree(drecs2_);
+  dfree(temp_);
+  if (h_mod_) cudaFreeHost(h_mod_);
+  h_mod_ = nullptr;
+  cudaStreamSynchronize(s_);
+}
+
+int Engine::init(int64_t nv0, int64_t nnz0) {
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&nsm_, cudaDevAttrMultiProcessorCount, dev));
+  nv0_ = nv0;
+  nnz0_ = nnz0;
+  const size_t n = (size_t)nv0 + 1;
+  TRY(alloc(&vDeg, n)); TRY(alloc(&cDeg, n)); TRY(alloc(&dDeg, n)); TRY(alloc(&own_w, n));
+  TRY(alloc(&cSize, n)); TRY(alloc(&dSize, n));
+  TRY(alloc(&C, n)); TRY(alloc(&Cpast, n)); TRY(alloc(&Ctgt, n)); TRY(alloc(&color_, n));
+  TRY(alloc(&keys_, n)); TRY(alloc(&keys2_, n)); TRY(alloc(&members_, n)); TRY(alloc(&vals_, n));
+  TRY(alloc(&move_old_, n)); TRY(alloc(&move_new_, n)); TRY(alloc(&hub_off_, n));
+  TRY(alloc(&cst, 4));
+  // partials of the modularity pass (one per 256 vertices) and of the
+  // constant's reduction (kConstParts blocks) share these buffers
+  const size_t nparts = std::max<size_t>((n + kModVB - 1) / kModVB, kConstParts) + 1;
+  TRY(alloc(&part_e_, nparts)); TRY(alloc(&part_a_, nparts)); TRY(alloc(&mod_out_, 4));
+  CK(cudaMallocHost((void **)&h_mod_, 4 * sizeof(double)));
+  CK(cudaMemsetAsync(dDeg, 0, n * sizeof(double), s_));
+  CK(cudaMemsetAsync(dSize, 0, n * sizeof(int32_t), s_));
+  return GLV_OK;
+}
+
+
+// Integral-weight detection: every weight a non-negative integer and the total
+// below 2^53 -> every sum in any order is exact.
+__global__ void k_check_weights(int64_t nnz, const double *w, const int32_t *tail, int64_t nv,
+                                int32_t *flags, double *total) {
+  double s = 0.0;
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nnz;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    const double x = w[j];
+    if (!(x >= 0.0 && x == floor(x))) atomicOr(&flags[0], 1);
+    const int32_t t = tail[j];
+    if (t < 0 || t >= nv) atomicOr(&flags[1], 1);
+    s += x;
+  }
+  atomicAdd(total, s);
+}
+
+int Engine::upload_check(const Level &L) {
+  int32_t *flags;
+  double *total;
+  TRY(alloc(&flags, 2));
+  TRY(alloc(&total, 1));
+  CK(cudaMemsetAsync(flags, 0, 2 * sizeof(int32_t), s_));
+  CK(cudaMemsetAsync(total, 0, sizeof(double), s_));
+  LAUNCH(k_check_weights, grid_for(L.nnz, 256, nsm_ * 8), 256, 0, s_, L.nnz, L.w, L.tail, L.nv,
+         flags, total);
+  int32_t hf[2];
+  double ht;
+  CK(cudaMemcpyAsync(hf, flags, sizeof(hf), cudaMemcpyDeviceToHost, s_));
+  CK(cudaMemcpyAsync(&ht, total, sizeof(double), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  dfree(flags);
+  dfree(total);
+  if (hf[1]) return fail(GLV_ERR_ARG, "edge tail out of range [0, numVertices)");
+  integral = (hf[0] == 0) && (ht < 9007199254740992.0);
+  return GLV_OK;
+}
+
+int Engine::phase_init(const Level &L, bool need_past) {
+  LAUNCH(k_init_phase, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, L.ptr, L.w, vDeg, cDeg,
+         cSize, C, need_past ? Cpast : (int32_t *)nullptr);
+  if (ordered()) {
+    LAUNCH(k_constant_sequential, 1, 1, 0, s_, L.nv, vDeg, cst);
+  } else {
+    LAUNCH(k_sum_partials, kConstParts, 256, 0, s_, L.nv, vDeg, part_e_);
+    LAUNCH(k_constant_from_partials, 1, 32, 0, s_, kConstParts, part_e_, cst);
+  }
+  return GLV_OK;
+}
+
+// ----------------------------------------------------------------- colouring
+int Engine::color(const Level &L, int *ncolors, double *secs) {
+  const double t0 = now_s();
+  int32_t *pending, *f0, *f1, *fcount, *status, *maxc;
+  TRY(alloc(&pending, L.nv)); TRY(alloc(&f0, L.nv)); TRY(alloc(&f1, L.nv));
+  TRY(alloc(&fcount, 3)); TRY(alloc(&status, 2)); TRY(alloc(&maxc, 1));
+  CK(cudaMemsetAsync(fcount, 0, 3 * sizeof(int32_t), s_));
+  CK(cudaMemsetAsync(status, 0, 2 * sizeof(int32_t), s_));
+  CK(cudaMemsetAsync(maxc, 0xff, sizeof(int32_t), s_));
+  const int hashed = (mode_ == GLV_MODE_FAST) ? 1 : 0;
+  const uint32_t seed = 0x5bd1e995u;
+  LAUNCH(k_color_init, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, L.ptr, L.tail, hashed,
+         seed, pending, color_, f0, fcount);
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_color_rounds, 256, 0));
+  int grid = std::max(1, per_sm) * nsm_;
+  int64_t nv = L.nv;
+  const int64_t *ptr = L.ptr;
+  const int32_t *tail = L.tail;
+  int32_t *color = color_;
+  void *args[] = {&nv, (void *)&ptr, (void *)&tail, (void *)&hashed, (void *)&seed, &pending,
+                  &color, &f0, &f1, &fcount, &status};
+  CK(cudaLaunchCooperativeKernel((void *)k_color_rounds, grid, 256, args, 0, s_));
+  ++launches_;
+  LAUNCH(k_max_color, grid_for(L.nv, 256, nsm_ * 8), 256, 0, s_, L.nv, color_, maxc);
+  int32_t h[2], hm;
+  CK(cudaMemcpyAsync(h, status, sizeof(h), cudaMemcpyDeviceToHost, s_));
+  CK(cudaMemcpyAsync(&hm, maxc, sizeof(hm), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  dfree(pending); dfree(f0); dfree(f1); dfree(fcount); dfree(status); dfree(maxc);
+  if (h[0]) return fail(GLV_ERR_COLORS, "colouring needs more than 4096 colours");
+  *ncolors = hm + 1;
+  if (secs) *secs = now_s() - t0;
+  return GLV_OK;
+}
+
+// Improper (reused) colourings: split each class into sublevels so that a
+// vertex comes after its same-colour lower-id neighbours — the order in which
+// the reference's one-thread loop sees their in-place updates.
+int Engine::sublevels(const Level &L, int ncolors, int32_t **d_sub, int *nsub) {
+  std::vector<int64_t> ptr(L.nv + 1);
+  std::vector<int32_t> tail(L.nnz), col(L.nv);
+  CK(cudaMemcpyAsync(ptr.data(), L.ptr, (L.nv + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaMemcpyAsync(tail.data(), L.tail, L.nnz * sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaMemcpyAsync(col.data(), color_, L.nv * sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  std::vector<int32_t> sub(L.nv, 0);
+  int mx = 0;
+  for (int64_t v = 0; v < L.nv; ++v) {
+    int d = 0;
+    for (int64_t j = ptr[v]; j < ptr[v + 1]; ++j) {
+      const int32_t u = tail[j];
+      if (u < v && col[u] == col[v]) d = std::max(d, sub[u] + 1);
+    }
+    sub[v] = d;
+    mx = std::max(mx, d);
+  }
+  *nsub = mx + 1;
+  *d_sub = nullptr;
+  if (mx == 0) return GLV_OK;
+  TRY(alloc(d_sub, L.nv));
+  CK(cudaMemcpyAsync(*d_sub, sub.data(), L.nv * sizeof(int32_t), cudaMemcpyHostToDevice, s_));
+  CK(cudaStreamSynchronize(s_));
+  return GLV_OK;
+}
+
+// ------------------------------------------------------------------ schedule
+int Engine::build_schedule(const Level &L, const int32_t *color, int ncolors, const int32_t *sub,
+                           int nsub, std::vector<ClassSched> *sched) {
+  const int64_t nkeys = (int64_t)ncolors * nsub * NBINS;
+  if (nkeys + 1 > hist_cap_) {
+    dfree(hist_);
+    hist_cap_ = (int)(nkeys + 1);
+    TRY(alloc(&hist_, hist_cap_));
+  }
+  CK(cudaMemsetAsync(hist_, 0, (nkeys + 1) * sizeof(int32_t), s_));
+  LAUNCH(k_schedule_keys, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, L.ptr, color, sub,
+         nsub, lim_, keys_, vals_, hist_);
+  const int end_bit = bits_for(nkeys);
+  size_t tb = 0;
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys_, keys2_, vals_, members_, L.nv, 0,
+                                     end_bit, s_));
+  TRY(temp(tb));
+  CK(cub::DeviceRadixSort::SortPairs(temp_, tb, keys_, keys2_, vals_, members_, L.nv, 0, end_bit,
+                                     s_));
+  std::vector<int32_t> hist(nkeys);
+  CK(cudaMemcpyAsync(hist.data(), hist_, nkeys * sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  sched->clear();
+  int64_t pos = 0;
+  max_class_ = 0;
+  for (int c = 0; c < ncolors; ++c) {
+    ClassSched cs;
+    cs.begin = pos;
+    for (int sl = 0; sl < nsub; ++sl) {
+      Step st;
+      int64_t cnt = 0;
+      for (int b = 0; b < NBINS; ++b) {
+        st.seg[b] = pos;
+        pos += hist[((int64_t)c * nsub + sl) * NBINS + b];
+        cnt += hist[((int64_t)c * nsub + sl) * NBINS + b];
+      }
+      st.seg[NBINS] = pos;
+      if (cnt) cs.steps.push_back(st);
+    }
+    cs.end = pos;
+    if (cs.end > cs.begin) {
+      max_class_ = std::max(max_class_, cs.end - cs.begin);
+      sched->push_back(cs);
+    }
+  }
+  return hub_offsets(L, *sched);
+}
+
+int Engine::grow_hub(size_t entries) {
+  if (entries <= hub_cap_) return GLV_OK;
+  dfree(hub_keys_);
+  dfree(hub_vals_);
+  hub_cap_ = entries;
+  TRY(alloc(&hub_keys_, hub_cap_));
+  TRY(alloc(&hub_vals_, hub_cap_));
+  return GLV_OK;
+}
+
+// Hub tables: each hub of a step gets a region of the global scratch; steps
+// run one after another, so regions are reused across steps.
+int Engine::hub_offsets(const Level &L, std::vector<ClassSched> &sched) {
+  size_t need = 0;
+  for (auto &cs : sched)
+    for (auto &st : cs.steps) {
+      const int64_t b = st.seg[BIN_HUB], e = st.seg[BIN_HUB + 1];
+      if (e == b) continue;
+      LAUNCH(k_hub_caps, grid_for(e - b, 256, nsm_ * 4), 256, 0, s_, e - b, members_ + b, L.ptr,
+             hub_off_ + b);
+      std::vector<int64_t> off(e - b);
+      CK(cudaMemcpyAsync(off.data(), hub_off_ + b, (e - b) * sizeof(int64_t),
+                         cudaMemcpyDeviceToHost, s_));
+      CK(cudaStreamSynchronize(s_));
+      int64_t acc = 0;
+      for (int64_t k = 0; k < e - b; ++k) {
+        const int64_t c = off[k];
+        off[k] = acc;
+        acc += c;
+      }
+      need = std::max(need, (size_t)acc);
+      CK(cudaMemcpyAsync(hub_off_ + b, off.data(), (e - b) * sizeof(int64_t),
+                         cudaMemcpyHostToDevice, s_));
+      CK(cudaStreamSynchronize(s_));
+    }
+  return grow_hub(need);
+}
+
+// ------------------------------------------------------------------- sweeps
+constexpr int kWarpCap = 256;   // table_cap(127)
+constexpr int kBlockCap = 8192; // table_cap(4095)
+
+int Engine::launch_sweep(const Level &L, const Step &st, SweepArgs a, bool ordered_acc) {
+  const int cap = nsm_ * 16;
+  for (int b = 0; b < NBINS; ++b) {
+    const int64_t lo = st.seg[b], hi = st.seg[b + 1];
+    const int64_t n = hi - lo;
+    if (n <= 0) continue;
+    switch (b) {
+      case BIN_G4:
+        LAUNCH(k_sweep_small<4>, grid_for(n * 4, 256, cap), 256, 0, s_, a, lo, hi);
+        break;
+      case BIN_G8:
+        LAUNCH(k_sweep_small<8>, grid_for(n * 8, 256, cap), 256, 0, s_, a, lo, hi);
+        break;
+      case BIN_G16:
+        LAUNCH(k_sweep_small<16>, grid_for(n * 16, 256, cap), 256, 0, s_, a, lo, hi);
+        break;
+      case BIN_G32:
+        LAUNCH(k_sweep_small<32>, grid_for(n * 32, 256, cap), 256, 0, s_, a, lo, hi);
+        break;
+      case BIN_WARP: {
+        const size_t smem = 8 * kWarpCap * (sizeof(double) + sizeof(int32_t));
+        LAUNCH(k_sweep_warp<kWarpCap>, grid_for(n * 32, 256, cap), 256, smem, s_, a, lo, hi);
+        break;
+      }
+      case BIN_BLOCK: {
+        const size_t smem = (size_t)kBlockCap * (sizeof(double) + sizeof(int32_t));
+        LAUNCH(k_sweep_block, (int)std::min<int64_t>(n, nsm_ * 2), 256, smem, s_, a, lo, hi, 0,
+               ordered_acc ? 1 : 0);
+        break;
+      }
+      case BIN_HUB:
+        LAUNCH(k_sweep_block, (int)std::min<int64_t>(n, nsm_), 512, 0, s_, a, lo, hi, 1,
+               ordered_acc ? 1 : 0);
+        break;
+    }
+  }
+  return GLV_OK;
+}
+
+int Engine::launch_apply(const ClassSched &cs, bool ordered_upd) {
+  const int64_t n = cs.end - cs.begin;
+  if (!ordered_upd) {
+    LAUNCH(k_apply_deltas, grid_for(n, 256, nsm_ * 16), 256, 0, s_, cs.begin, cs.end, move_old_,
+           move_new_, dDeg, dSize, cDeg, cSize);
+    return GLV_OK;
+  }
+  const uint64_t sentinel = (uint64_t)(uint32_t)nv0_ << 32;
+  const int end_bit = 32 + bits_for(nv0_);
+  LAUNCH(k_delta_records, grid_for(n, 256, nsm_ * 16), 256, 0, s_, cs.begin, cs.end, members_,
+         move_old_, move_new_, vDeg, sentinel, dkeys_, drecs_);
+  size_t tb = 0;
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, dkeys_, dkeys2_, drecs_, drecs2_, 2 * n, 0,
+                                     end_bit, s_));
+  if (tb > temp_bytes_) return fail(GLV_ERR_CUDA, "sort scratch not reserved before capture");
+  CK(cub::DeviceRadixSort::SortPairs(temp_, tb, dkeys_, dkeys2_, drecs_, drecs2_, 2 * n, 0,
+                                     end_bit, s_));
+  LAUNCH(k_fold_deltas, grid_for(2 * n, 256, nsm_ * 16), 256, 0, s_, 2 * n, dkeys2_, drecs2_,
+         sentinel, cDeg, cSize);
+  return GLV_OK;
+}
+
+int Engine::launch_modularity(const Level &L, const int32_t *Cm, const double *ownw) {
+  const int64_t nparts = (L.nv + kModVB - 1) / kModVB;
+  LAUNCH(k_modularity_part, (int)std::max<int64_t>(1, nparts), 256, 0, s_, L.nv, L.ptr, L.tail,
+         L.w, Cm, ownw, cDeg, part_e_, part_a_);
+  LAUNCH(k_modularity_final, 1, 256, 0, s_, (int)std::max<int64_t>(1, nparts), part_e_, part_a_,
+         cst, mod_out_);
+  CK(cudaMemcpyAsync(h_mod_, mod_out_, 3 * sizeof(double), cudaMemcpyDeviceToHost, s_));
+  return GLV_OK;
+}
+
+// Captures `body` into a CUDA graph (launch count recorded), returns the exec.
+template <class F>
+static int capture(cudaStream_t s, long *launches, F body, cudaGraphExec_t *exec, long *nodes) {
+  cudaGraph_t g;
+  const long before = *launches;
+  CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+  int r = body();
+  cudaError_t e = cudaStreamEndCapture(s, &g);
+  if (r != GLV_OK) {
+    if (e == cudaSuccess) cudaGraphDestroy(g);
+    return r;
+  }
+  CK(e);
+  *nodes = *launches - before;
+  *launches = before;
+  cudaError_t ie = cudaGraphInstantiate(exec, g, 0);
+  cudaGraphDestroy(g);
+  CK(ie);
+  return GLV_OK;
+}
+
+int Engine::coloring_phase(const Level &L, int ncolors, bool stale, double lower, double thresh,
+                           double *mod, int *itr) {
+  TRY(phase_init(L, false));
+  int32_t *d_sub = nullptr;
+  int nsub = 1;
+  if (stale) TRY(sublevels(L, ncolors, &d_sub, &nsub));
+  std::vector<ClassSched> sched;
+  TRY(build_schedule(L, color_, ncolors, d_sub, nsub, &sched));
+  dfree(d_sub);
+  const bool ord = ordered();
+  if (ord) {
+    if (!dkeys_) {
+      TRY(alloc(&dkeys_, 2 * nv0_)); TRY(alloc(&dkeys2_, 2 * nv0_));
+      TRY(alloc(&drecs_, 2 * nv0_)); TRY(alloc(&drecs2_, 2 * nv0_));
+    }
+    size_t tb = 0;
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, dkeys_, dkeys2_, drecs_, drecs2_,
+                                       2 * std::max<int64_t>(max_class_, 1), 0, 64, s_));
+    TRY(temp(tb));
+  }
+  SweepArgs a{};
+  a.ptr = L.ptr; a.tail = L.tail; a.w = L.w; a.C = C; a.target = nullptr; a.own_w = nullptr;
+  a.vDeg = vDeg; a.cDeg = cDeg; a.cSize = cSize; a.members = members_;
+  a.move_old = move_old_; a.move_new = move_new_; a.dDeg = dDeg; a.dSize = dSize;
+  a.atomic_deltas = ord ? 0 : 1;
+  a.hub_keys = hub_keys_; a.hub_vals = hub_vals_; a.hub_off = hub_off_;
+  CK(cudaMemcpyAsync(&a.constant, cst, sizeof(double), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  cudaGraphExec_t exec = nullptr;
+  long nodes = 0;
+  TRY(capture(s_, &launches_, [&]() -> int {
+        for (auto &cs : sched) {
+          for (auto &st : cs.steps) TRY(launch_sweep(L, st, a, ord));
+          TRY(launch_apply(cs, ord));
+        }
+        return launch_modularity(L, C, nullptr);
+      }, &exec, &nodes));
+  double prev = lower;
+  int n = 0;
+  int rc = GLV_OK;
+  while (true) {
+    ++n;
+    const double t0 = now_s();
+    cudaError_t e = cudaGraphLaunch(exec, s_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s_);
+    t_sweep += now_s() - t0;
+    if (e != cudaSuccess) { g_err = cudaGetErrorString(e); rc = GLV_ERR_CUDA; break; }
+    launches_ += nodes;
+    edges_swept += (double)L.nnz;
+    const double q = h_mod_[0];
+    if (q - prev < thresh) break;
+    prev = q;
+  }
+  cudaGraphExecDestroy(exec);
+  *mod = prev;
+  *itr = n;
+  return rc;
+}
+
+__global__ void k_rotate(int64_t n, int32_t *past, int32_t *curr, const int32_t *tgt) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    past[i] = curr[i];
+    curr[i] = tgt[i];
+  }
+}
+
+int Engine::basic_phase(const Level &L, double lower, double thresh, double *mod, int *itr) {
+  TRY(phase_init(L, true));
+  std::vector<ClassSched> sched;
+  TRY(build_schedule(L, nullptr, 1, nullptr, 1, &sched));
+  const bool ord = ordered();
+  if (ord) {
+    if (!dkeys_) {
+      TRY(alloc(&dkeys_, 2 * nv0_)); TRY(alloc(&dkeys2_, 2 * nv0_));
+      TRY(alloc(&drecs_, 2 * nv0_)); TRY(alloc(&drecs2_, 2 * nv0_));
+    }
+    size_t tb = 0;
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, dkeys_, dkeys2_, drecs_, drecs2_,
+                                       2 * std::max<int64_t>(max_class_, 1), 0, 64, s_));
+    TRY(temp(tb));
+  }
+  SweepArgs a{};
+  a.ptr = L.ptr; a.tail = L.tail; a.w = L.w; a.C = C; a.target = Ctgt; a.own_w = own_w;
+  a.vDeg = vDeg; a.cDeg = cDeg; a.cSize = cSize; a.members = members_;
+  a.move_old = move_old_; a.move_new = move_new_; a.dDeg = dDeg; a.dSize = dSize;
+  a.atomic_deltas = ord ? 0 : 1;
+  a.hub_keys = hub_keys_; a.hub_vals = hub_vals_; a.hub_off = hub_off_;
+  CK(cudaMemcpyAsync(&a.constant, cst, sizeof(double), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  cudaGraphExec_t exec = nullptr;
+  long nodes = 0;
+  // Q is taken on the state before the moves (parallelLouvainMethod.cpp:244-255);
+  // the totals update is applied in the same graph and only matters if the
+  // loop continues.
+  TRY(capture(s_, &launches_, [&]() -> int {
+        for (auto &cs : sched) {
+          for (auto &st : cs.steps) TRY(launch_sweep(L, st, a, ord));
+        }
+        TRY(launch_modularity(L, C, own_w));
+        for (auto &cs : sched) TRY(launch_apply(cs, ord));
+        return GLV_OK;
+      }, &exec, &nodes));
+  double prev = -1.0;
+  int n = 0;
+  int rc = GLV_OK;
+  while (true) {
+    ++n;
+    const double t0 = now_s();
+    cudaError_t e = cudaGraphLaunch(exec, s_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s_);
+    t_sweep += now_s() - t0;
+    if (e != cudaSuccess) { g_err = cudaGetErrorString(e); rc = GLV_ERR_CUDA; break; }
+    launches_ += nodes;
+    edges_swept += (double)L.nnz;
+    const double q = h_mod_[0];
+    if (q - prev < thresh) break;
+    prev = q;
+    if (prev < lower) prev = lower;
+    LAUNCH(k_rotate, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, Cpast, C, Ctgt);
+  }
+  cudaGraphExecDestroy(exec);
+  // C = pastCommAss (parallelLouvainMethod.cpp:304-307)
+  CK(cudaMemcpyAsync(C, Cpast, L.nv * sizeof(int32_t), cudaMemcpyDeviceToDevice, s_));
+  CK(cudaStreamSynchronize(s_));
+  *mod = prev;
+  *itr = n;
+  return rc;
+}
+
+// Decisions for a vertex list against the state already in C/cDeg/cSize/vDeg
+// and cst[0]; targets land in Ctgt[v].
+int Engine::decide(const Level &L, const int32_t *verts, int64_t nverts) {
+  const int64_t nkeys = NBINS;
+  if (nkeys + 1 > hist_cap_) {
+    dfree(hist_);
+    hist_cap_ = (int)(nkeys + 1);
+    TRY(alloc(&hist_, hist_cap_));
+  }
+  // schedule over the given list: key = bin only
+  std::vector<int32_t> hv(nverts);
+  std::vector<int64_t> hp(L.nv + 1);
+  CK(cudaMemcpyAsync(hv.data(), verts, nverts * sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaMemcpyAsync(hp.data(), L.ptr, (L.nv + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  std::vector<std::vector<int32_t>> byb(NBINS);
+  for (int32_t v : hv) byb[degree_bin(hp[v + 1] - hp[v], lim_)].push_back(v);
+  std::vector<int32_t> mem;
+  ClassSched cs;
+  Step st;
+  for (int b = 0; b < NBINS; ++b) {
+    st.seg[b] = (int64_t)mem.size();
+    mem.insert(mem.end(), byb[b].begin(), byb[b].end());
+  }
+  st.seg[NBINS] = (int64_t)mem.size();
+  cs.begin = 0; cs.end = (int64_t)mem.size();
+  cs.steps.push_back(st);
+  CK(cudaMemcpyAsync(members_, mem.data(), mem.size() * sizeof(int32_t), cudaMemcpyHostToDevice,
+                     s_));
+  CK(cudaStreamSynchronize(s_));
+  std::vector<ClassSched> sched{cs};
+  TRY(hub_offsets(L, sched));
+  SweepArgs a{};
+  a.ptr = L.ptr; a.tail = L.tail; a.w = L.w; a.C = C; a.target = Ctgt; a.own_w = own_w;
+  a.vDeg = vDeg; a.cDeg = cDeg; a.cSize = cSize; a.members = members_;
+  a.move_old = move_old_; a.move_new = move_new_; a.dDeg = dDeg; a.dSize = dSize;
+  a.atomic_deltas = 0;
+  a.hub_keys = hub_keys_; a.hub_vals = hub_vals_; a.hub_off = hub_off_;
+  CK(cudaMemcpyAsync(&a.constant, cst, sizeof(double), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  TRY(launch_sweep(L, st, a, true));
+  CK(cudaStreamSynchronize(s_));
+  return GLV_OK;
+}
+
+// --------------------------------------------------------------- renumbering
+int Engine::renumber(int32_t *Cm, int64_t n, int64_t *ncl) {
+  if (n == 0) { *ncl = 0; return GLV_OK; }
+  int32_t *first, *flag, *scan;
+  TRY(alloc(&first, n)); TRY(alloc(&flag, n)); TRY(alloc(&scan, n));
+  const int g = grid_for(n, 256, nsm_ * 16);
+  LAUNCH(k_fill_i32, g, 256, 0, s_, n, first, INT32_MAX);
+  LAUNCH(k_first_occurrence, g, 256, 0, s_, n, Cm, first);
+  LAUNCH(k_open_flags, g, 256, 0, s_, n, Cm, first, flag);
+  size_t tb = 0;
+  CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, flag, scan, n, s_));
+  TRY(temp(tb));
+  CK(cub::DeviceScan::ExclusiveSum(temp_, tb, flag, scan, n, s_));
+  LAUNCH(k_apply_renumber, g, 256, 0, s_, n, Cm, first, scan);
+  int32_t h[2];
+  CK(cudaMemcpyAsync(&h[0], scan + n - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaMemcpyAsync(&h[1], flag + n - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  dfree(first); dfree(flag); dfree(scan);
+  *ncl = (int64_t)h[0] + h[1];
+  return GLV_OK;
+}
+
+// ----------------------------------------------------------------- coarsening
+__global__ void k_add_counts(int64_t n, const int64_t *a, const int64_t *b, int64_t *out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (i < n) ? a[i] + b[i] : 0;
+}
+
+int Engine::coarsen(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
+                    int64_t *num_edges) {
+  const int nb = bits_for(std::max<int64_t>(ncl - 1, 1));
+  const uint64_t sentinel = 1ull << (2 * nb);
+  const int end_bit = 2 * nb + 1;
+  const int64_t n = ncl + in.nnz;
+  const int g = grid_for(n, 256, nsm_ * 16);
+  uint64_t *k1, *k2;
+  double *v1, *v2;
+  TRY(alloc(&k1, n)); TRY(alloc(&k2, n)); TRY(alloc(&v1, n)); TRY(alloc(&v2, n));
+  LAUNCH(k_coarse_records, grid_for(std::max<int64_t>(in.nv, ncl), 256, nsm_ * 16), 256, 0, s_,
+         in.nv, in.ptr, in.tail, in.w, Cm, ncl, nb, sentinel, k1, v1);
+  size_t tb = 0;
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, k1, k2, v1, v2, n, 0, end_bit, s_));
+  TRY(temp(tb));
+  CK(cub::DeviceRadixSort::SortPairs(temp_, tb, k1, k2, v1, v2, n, 0, end_bit, s_));
+  dfree(k1); dfree(v1);
+  int32_t *flag;
+  int64_t *uidx;
+  TRY(alloc(&flag, n)); TRY(alloc(&uidx, n));
+  LAUNCH(k_segment_heads, g, 256, 0, s_, n, k2, sentinel, flag);
+  CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, flag, uidx, n, s_));
+  TRY(temp(tb));
+  CK(cub::DeviceScan::ExclusiveSum(temp_, tb, flag, uidx, n, s_));
+  int64_t hu;
+  int32_t hf;
+  CK(cudaMemcpyAsync(&hu, uidx + n - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaMemcpyAsync(&hf, flag + n - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  const int64_t np = hu + hf;
+  uint64_t *ukeys;
+  double *uvals;
+  TRY(alloc(&ukeys, np)); TRY(alloc(&uvals, np));
+  if (ordered()) {
+    LAUNCH(k_fold_pairs, g, 256, 0, s_, n, k2, v2, flag, uidx, sentinel, ukeys, uvals);
+  } else {
+    CK(cudaMemsetAsync(uvals, 0, np * sizeof(double), s_));
+    LAUNCH(k_scatter_pairs, g, 256, 0, s_, n, k2, v2, flag, uidx, sentinel, ukeys, uvals);
+  }
+  dfree(k2); dfree(v2); dfree(flag); dfree(uidx);
+  int64_t *lower_cnt, *upper_cnt, *ne_off, *rowc, *lower_first, *upper_first;
+  TRY(alloc(&lower_cnt, ncl)); TRY(alloc(&upper_cnt, ncl)); TRY(alloc(&ne_off, 1));
+  TRY(alloc(&rowc, ncl + 1)); TRY(alloc(&lower_first, ncl)); TRY(alloc(&upper_first, ncl));
+  CK(cudaMemsetAsync(lower_cnt, 0, ncl * sizeof(int64_t), s_));
+  CK(cudaMemsetAsync(upper_cnt, 0, ncl * sizeof(int64_t), s_));
+  CK(cudaMemsetAsync(ne_off, 0, sizeof(int64_t), s_));
+  const int gp = grid_for(np, 256, nsm_ * 16);
+  LAUNCH(k_row_counts, gp, 256, 0, s_, np, ukeys, nb, lower_cnt, upper_cnt, ne_off);
+  LAUNCH(k_add_counts, grid_for(ncl + 1, 256, nsm_ * 16), 256, 0, s_, ncl, lower_cnt, upper_cnt,
+         rowc);
+  Level o;
+  o.nv = ncl;
+  o.owned = true;
+  TRY(alloc(&o.ptr, ncl + 1));
+  CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, rowc, o.ptr, ncl + 1, s_));
+  TRY(temp(tb));
+  CK(cub::DeviceScan::ExclusiveSum(temp_, tb, rowc, o.ptr, ncl + 1, s_));
+  int64_t hne;
+  CK(cudaMemcpyAsync(&o.nnz, o.ptr + ncl, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaMemcpyAsync(&hne, ne_off, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  TRY(alloc(&o.tail, o.nnz)); TRY(alloc(&o.w, o.nnz));
+  LAUNCH(k_run_first, gp, 256, 0, s_, np, ukeys, nb, sentinel, lower_first);
+  uint64_t *tk1, *tk2;
+  double *tv1, *tv2;
+  TRY(alloc(&tk1, np)); TRY(alloc(&tk2, np)); TRY(alloc(&tv1, np)); TRY(alloc(&tv2, np));
+  LAUNCH(k_emit_lower, gp, 256, 0, s_, np, ukeys, uvals, nb, o.ptr, lower_first, o.tail, o.w, tk1,
+         tv1, sentinel);
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, tk1, tk2, tv1, tv2, np, 0, end_bit, s_));
+  TRY(temp(tb));
+  CK(cub::DeviceRadixSort::SortPairs(temp_, tb, tk1, tk2, tv1, tv2, np, 0, end_bit, s_));
+  LAUNCH(k_run_first, gp, 256, 0, s_, np, tk2, nb, sentinel, upper_first);
+  LAUNCH(k_emit_upper, gp, 256, 0, s_, np, tk2, tv2, nb, o.ptr, lower_cnt, upper_first, o.tail,
+         o.w, sentinel);
+  CK(cudaStreamSynchronize(s_));
+  dfree(tk1); dfree(tk2); dfree(tv1); dfree(tv2); dfree(ukeys); dfree(uvals);
+  dfree(lower_cnt); dfree(upper_cnt); dfree(ne_off); dfree(rowc); dfree(lower_first);
+  dfree(upper_first);
+  *out = o;
+  *num_edges = hne + ncl;
+  return GLV_OK;
+}
+
+__global__ void k_comm_degrees(int64_t nv, const int32_t *Cm, const double *vDeg, double *cDeg) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t c = Cm[i];
+    if (c >= 0) atomicAdd(&cDeg[c], vDeg[i]);
+  }
+}
+
+// Q of an arbitrary assignment Cm (ids < L.nv, -1 = none) over L.
+int Engine::modularity_of(const Level &L, const int32_t *Cm, double *q) {
+  TRY(phase_init(L, false));
+  CK(cudaMemsetAsync(cDeg, 0, L.nv * sizeof(double), s_));
+  LAUNCH(k_comm_degrees, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, Cm, vDeg, cDeg);
+  TRY(launch_modularity(L, Cm, nullptr));
+  CK(cudaStreamSynchronize(s_));
+  *q = h_mod_[0];
+  return GLV_OK;
+}
+
+void Engine::free_level(Level &L) {
+  if (L.owned) {
+    dfree(L.ptr);
+    dfree(L.tail);
+    dfree(L.w);
+  }
+  L = Level{};
+}
+
+// ------------------------------------------------------------ multiphase
+int Engine::run_multiphase(const Level &L0, int32_t *d_C_orig, bool coloring,
+                           long min_graph_size, double threshold, double c_threshold,
+                           glv_run_stats *st) {
+  Level L = L0;
+  L.owned = false;
+  int ncolors = 0;
+  bool recolored = false;
+  double tcol = 0;
+  if (coloring) {
+    TRY(color(L, &ncolors, &tcol));
+    t_color += tcol;
+    recolored = true;
+  }
+  double prev = -1, curr = -1;
+  long phase = 1;
+  bool non_color = !coloring;
+  int tot_itr = 0;
+  int64_t ncl = 0;
+  int nrec = 0;
+  const long itr_cap = coloring ? 10000 : 100000;
+  while (true) {
+    prev = curr;
+    int itr = 0;
+    const bool used_color = !non_color;
+    const double ts0 = t_sweep, es0 = edges_swept;
+    if (!non_color) {
+      TRY(coloring_phase(L, ncolors, !recolored, curr, c_threshold, &curr, &itr));
+    } else {
+      TRY(basic_phase(L, curr, threshold, &curr, &itr));
+    }
+    tot_itr += itr;
+    const double tc0 = now_s();
+    TRY(renumber(C, L.nv, &ncl));
+    LAUNCH(k_compose, grid_for(L0.nv, 256, nsm_ * 16), 256, 0, s_, L0.nv, d_C_orig, C,
+           phase == 1 ? 1 : 0);
+    CK(cudaStreamSynchronize(s_));
+    double tcoarse = now_s() - tc0;
+    const glv_phase_stats rec0{L.nv, L.nnz, used_color ? 1 : 0,
+                               used_color ? (recolored ? 1 : 0) : 0, used_color ? ncolors : 0,
+                               itr, curr, (long)ncl, t_sweep - ts0, 0.0, 0.0,
+                               edges_swept - es0};
+    glv_phase_stats rec = rec0;
+    if (used_color && nrec == 0) rec.time_color = tcol;
+    bool stop = (phase > 200) || (tot_itr > itr_cap);
+    if (!stop) {
+      if ((curr - prev) > threshold) {
+        const double tb0 = now_s();
+        Level nl;
+        int64_t ne = 0;
+        TRY(coarsen(L, C, ncl, &nl, &ne));
+        free_level(L);
+        L = nl;
+        tcoarse += now_s() - tb0;
+        ++phase;
+        recolored = false;
+        if (coloring && L.nv > min_graph_size && !non_color) {
+          TRY(color(L, &ncolors, &tcol));
+          t_color += tcol;
+          recolored = true;
+        }
+      } else {
+        if (coloring && !non_color) non_color = true;
+        else stop = true;
+      }
+    }
+    t_coarsen += tcoarse;
+    rec.time_coarsen = tcoarse;
+    if (st && nrec < GLV_MAX_PHASES) st->phase[nrec] = rec;
+    ++nrec;
+    if (stop) break;
+  }
+  free_level(L);
+  if (st) {
+    st->phases = (int)phase;
+    st->total_iterations = tot_itr;
+    st->final_clusters = (long)ncl;
+    st->final_modularity = prev;
+    st->nphase = std::min(nrec, GLV_MAX_PHASES);
+    st->time_clustering = t_sweep;
+    st->time_coloring = t_color;
+    st->time_building = t_coarsen;
+    st->edges_swept = edges_swept;
+  }
+  return GLV_OK;
+}
+
+}  // namespace glv
+
+// =========================================================================
+// C ABI (include/grappolo_b200.h)
+// =========================================================================
+namespace glv {
+
+__global__ void k_split_aos(int64_t n, const glv_edge *aos, int32_t *tail, double *w) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    tail[i] = (int32_t)aos[i].tail;
+    w[i] = aos[i].weight;
+  }
+}
+
+__global__ void k_narrow(int64_t n, const int64_t *in, int32_t *out, int32_t *bad, int64_t hi) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t x = in[i];
+    if (x < -1 || x >= hi) atomicOr(bad, 1);
+    out[i] = (int32_t)x;
+  }
+}
+
+__global__ void k_widen(int64_t n, const int32_t *in, int64_t *out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = in[i];
+}
+
+__global__ void k_fill_aos(int64_t nv, const int64_t *ptr, const int32_t *tail, const double *w,
+                           glv_edge *aos) {
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
+       v += (int64_t)gridDim.x * blockDim.x)
+    for (int64_t j = ptr[v]; j < ptr[v + 1]; ++j) aos[j] = glv_edge{(long)v, (long)tail[j], w[j]};
+}
+
+// A call's device context: stream, engine and the uploaded level-0 graph.
+struct Call {
+  cudaStream_t s = nullptr;
+  Engine *eng = nullptr;
+  Level L0;
+  long launches = 0;
+  double t_transfer = 0;
+  ~Call() {
+    if (eng) {
+      eng->free_level(L0);
+      launches += eng->launches_;
+      g_launches += eng->launches_;
+      delete eng;
+    }
+    if (s) {
+      cudaStreamSynchronize(s);
+      cudaStreamDestroy(s);
+    }
+  }
+};
+
+static int device_ready() {
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
+    return fail(GLV_ERR_NO_DEVICE, "no CUDA device");
+  static bool attrs = false;
+  if (!attrs) {
+    cudaFuncSetAttribute(k_sweep_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kBlockCap * (int)(sizeof(double) + sizeof(int32_t)));
+    attrs = true;
+  }
+  return GLV_OK;
+}
+
+static int check_ptr(long nv, const long *ptr) {
+  if (nv < 0) return fail(GLV_ERR_ARG, "numVertices < 0");
+  if (nv >= (1L << 31) - 1) return fail(GLV_ERR_TOO_LARGE, "numVertices >= 2^31");
+  if (!ptr) return fail(GLV_ERR_ARG, "edgeListPtrs is NULL");
+  if (ptr[0] != 0) return fail(GLV_ERR_ARG, "edgeListPtrs[0] != 0");
+  for (long i = 0; i < nv; ++i)
+    if (ptr[i + 1] < ptr[i]) return fail(GLV_ERR_ARG, "edgeListPtrs not non-decreasing");
+  return GLV_OK;
+}
+
+// Uploads a host CSR (either AoS `edges` or SoA `tail64`/`w`) as level 0.
+static int open_call(Call &c, int mode, long nv, const long *ptr, const glv_edge *edges,
+                     const long *tail64, const double *w) {
+  TRY(device_ready());
+  TRY(check_ptr(nv, ptr));
+  if (mode != GLV_MODE_VERIFY && mode != GLV_MODE_FAST) return fail(GLV_ERR_ARG, "bad mode");
+  const int64_t nnz = ptr[nv];
+  if (nnz > 0 && !edges && !(tail64 && w)) return fail(GLV_ERR_ARG, "edge arrays are NULL");
+  CK(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
+  c.eng = new Engine(c.s, mode);
+  TRY(c.eng->init(nv, nnz));
+  const double t0 = now_s();
+  Level &L = c.L0;
+  L.nv = nv;
+  L.nnz = nnz;
+  L.owned = true;
+  CK(cudaMallocAsync((void **)&L.ptr, (nv + 1) * sizeof(int64_t), c.s));
+  CK(cudaMallocAsync((void **)&L.tail, std::max<int64_t>(nnz, 1) * sizeof(int32_t), c.s));
+  CK(cudaMallocAsync((void **)&L.w, std::max<int64_t>(nnz, 1) * sizeof(double), c.s));
+  CK(cudaMemcpyAsync(L.ptr, ptr, (nv + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c.s));
+  // Edges move in chunks through one device staging buffer.
+  const int64_t chunk = std::min<int64_t>(std::max<int64_t>(nnz, 1), 1 << 24);
+  int nsm = 148;
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
+  if (edges) {
+    glv_edge *stage;
+    CK(cudaMallocAsync((void **)&stage, chunk * sizeof(glv_edge), c.s));
+    for (int64_t b = 0; b < nnz; b += chunk) {
+      const int64_t n = std::min(chunk, nnz - b);
+      CK(cudaMemcpyAsync(stage, edges + b, n * sizeof(glv_edge), cudaMemcpyHostToDevice, c.s));
+      k_split_aos<<<grid_for(n, 256, nsm * 8), 256, 0, c.s>>>(n, stage, L.tail + b, L.w + b);
+      ++c.launches;
+      CK(cudaGetLastError());
+    }
+    CK(cudaFreeAsync(stage, c.s));
+  } else if (nnz > 0) {
+    int64_t *stage;
+    int32_t *bad;
+    CK(cudaMallocAsync((void **)&stage, chunk * sizeof(int64_t), c.s));
+    CK(cudaMallocAsync((void **)&bad, sizeof(int32_t), c.s));
+    CK(cudaMemsetAsync(bad, 0, sizeof(int32_t), c.s));
+    for (int64_t b = 0; b < nnz; b += chunk) {
+      const int64_t n = std::min(chunk, nnz - b);
+      CK(cudaMemcpyAsync(stage, tail64 + b, n * sizeof(int64_t), cudaMemcpyHostToDevice, c.s));
+      k_narrow<<<grid_for(n, 256, nsm * 8), 256, 0, c.s>>>(n, stage, L.tail + b, bad, nv);
+      ++c.launches;
+      CK(cudaGetLastError());
+    }
+    CK(cudaMemcpyAsync(L.w, w, nnz * sizeof(double), cudaMemcpyHostToDevice, c.s));
+    CK(cudaFreeAsync(stage, c.s));
+    CK(cudaFreeAsync(bad, c.s));
+  }
+  CK(cudaStreamSynchronize(c.s));
+  c.t_transfer += now_s() - t0;
+  return c.eng->upload_check(L);
+}
+
+// int32 device ids -> caller's int64 host array.
+static int download_ids(Call &c, const int32_t *d, int64_t n, long *host) {
+  if (n == 0) return GLV_OK;
+  const double t0 = now_s();
+  int64_t *tmp;
+  CK(cudaMallocAsync((void **)&tmp, n * sizeof(int64_t), c.s));
+  k_widen<<<grid_for(n, 256, 148 * 8), 256, 0, c.s>>>(n, d, tmp);
+  ++c.launches;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(host, tmp, n * sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
+  CK(cudaFreeAsync(tmp, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  c.t_transfer += now_s() - t0;
+  return GLV_OK;
+}
+
+static int upload_ids(Call &c, const long *host, int64_t n, int32_t *d, int64_t hi) {
+  if (n == 0) return GLV_OK;
+  int64_t *tmp;
+  int32_t *bad;
+  CK(cudaMallocAsync((void **)&tmp, n * sizeof(int64_t), c.s));
+  CK(cudaMallocAsync((void **)&bad, sizeof(int32_t), c.s));
+  CK(cudaMemsetAsync(bad, 0, sizeof(int32_t), c.s));
+  CK(cudaMemcpyAsync(tmp, host, n * sizeof(int64_t), cudaMemcpyHostToDevice, c.s));
+  k_narrow<<<grid_for(n, 256, 148 * 8), 256, 0, c.s>>>(n, tmp, d, bad, hi);
+  ++c.launches;
+  CK(cudaGetLastError());
+  int32_t hb = 0;
+  CK(cudaMemcpyAsync(&hb, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, c.s));
+  CK(cudaFreeAsync(tmp, c.s));
+  CK(cudaFreeAsync(bad, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  if (hb) return fail(GLV_ERR_ARG, "id out of range");
+  return GLV_OK;
+}
+
+static int run_host(int mode, long nv, const long *ptr, const glv_edge *edges, const long *tail64,
+                    const double *w, long *C_orig, bool coloring, long min_graph_size,
+                    double threshold, double c_threshold, glv_run_stats *st) {
+  const double t0 = now_s();
+  if (!C_orig && nv > 0) return fail(GLV_ERR_ARG, "C_orig is NULL");
+  if (st) memset(st, 0, sizeof(*st));
+  Call c;
+  TRY(open_call(c, mode, nv, ptr, edges, tail64, w));
+  int32_t *dC;
+  CK(cudaMallocAsync((void **)&dC, std::max<long>(nv, 1) * sizeof(int32_t), c.s));
+  TRY(c.eng->run_multiphase(c.L0, dC, coloring, min_graph_size, threshold, c_threshold, st));
+  TRY(download_ids(c, dC, nv, C_orig));
+  CK(cudaFreeAsync(dC, c.s));
+  if (st) {
+    st->time_transfer = c.t_transfer;
+    st->kernel_launches = c.launches + c.eng->launches_;
+    st->time_total = now_s() - t0;
+  }
+  return GLV_OK;
+}
+
+}  // namespace glv
+
+using namespace glv;
+
+extern "C" {
+
+const char *glv_version(void) { return "grappolo_b200 0.1 (sm_100a)"; }
+const char *glv_last_error(void) { return g_err.c_str(); }
+long glv_kernel_launch_count(void) { return g_launches.load(); }
+
+int glv_run_multiphase_coloring(const glv_graph *G, long *C_orig, int coloring, int numColors,
+                                int replaceMap, long minGraphSize, double threshold,
+                                double C_threshold, int mode, glv_run_stats *stats) {
+  (void)numColors;  // only the incomplete colouring (coloring = 3) reads it
+  if (!G) return fail(GLV_ERR_ARG, "G is NULL");
+  if (coloring != 1) return fail(GLV_ERR_UNSUPPORTED, "only coloring = 1 is implemented");
+  if (replaceMap != 0) return fail(GLV_ERR_UNSUPPORTED, "replaceMap = 1 is not implemented");
+  return run_host(mode, G->numVertices, G->edgeListPtrs, G->edgeList, nullptr, nullptr, C_orig,
+                  true, minGraphSize, threshold, C_threshold, stats);
+}
+
+int glv_run_multiphase_basic(const glv_graph *G, long *C_orig, int basicOpt, long minGraphSize,
+                             double threshold, double C_threshold, int mode,
+                             glv_run_stats *stats) {
+  if (!G) return fail(GLV_ERR_ARG, "G is NULL");
+  if (basicOpt != 0) return fail(GLV_ERR_UNSUPPORTED, "basicOpt = 1 is not implemented");
+  return run_host(mode, G->numVertices, G->edgeListPtrs, G->edgeList, nullptr, nullptr, C_orig,
+                  false, minGraphSize, threshold, C_threshold, stats);
+}
+
+int glv_run_multiphase_coloring_csr(long nv, const long *ptr, const long *tail,
+                                    const double *weight, long *C_orig, long minGraphSize,
+                                    double threshold, double C_threshold, int mode,
+                                    glv_run_stats *stats) {
+  return run_host(mode, nv, ptr, nullptr, tail, weight, C_orig, true, minGraphSize, threshold,
+                  C_threshold, stats);
+}
+
+int glv_run_multiphase_basic_csr(long nv, const long *ptr, const long *tail, const double *weight,
+                                 long *C_orig, double threshold, int mode, glv_run_stats *stats) {
+  return run_host(mode, nv, ptr, nullptr, tail, weight, C_orig, false, 0, threshold, 0.0, stats);
+}
+
+int glv_dev_run_multiphase(long nv, const long *d_ptr, const int *d_tail, const double *d_weight,
+                           int *d_C_orig, int coloring, long minGraphSize, double threshold,
+                           double C_threshold, int mode, void *stream, glv_run_stats *stats) {
+  const double t0 = now_s();
+  TRY(device_ready());
+  if (nv < 0) return fail(GLV_ERR_ARG, "nv < 0");
+  if (nv >= (1L << 31) - 1) return fail(GLV_ERR_TOO_LARGE, "nv >= 2^31");
+  if (mode != GLV_MODE_VERIFY && mode != GLV_MODE_FAST) return fail(GLV_ERR_ARG, "bad mode");
+  if (stats) memset(stats, 0, sizeof(*stats));
+  Call c;
+  CK(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
+  if (stream) {
+    cudaEvent_t ev;
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    CK(cudaEventRecord(ev, (cudaStream_t)stream));
+    CK(cudaStreamWaitEvent(c.s, ev, 0));
+    cudaEventDestroy(ev);
+  } else {
+    CK(cudaStreamSynchronize(0));
+  }
+  int64_t nnz = 0;
+  if (nv > 0) {
+    CK(cudaMemcpyAsync(&nnz, d_ptr + nv, sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
+    CK(cudaStreamSynchronize(c.s));
+  }
+  c.eng = new Engine(c.s, mode);
+  TRY(c.eng->init(nv, nnz));
+  c.L0.nv = nv;
+  c.L0.nnz = nnz;
+  c.L0.ptr = (int64_t *)d_ptr;
+  c.L0.tail = (int32_t *)d_tail;
+  c.L0.w = (double *)d_weight;
+  c.L0.owned = false;
+  TRY(c.eng->upload_check(c.L0));
+  TRY(c.eng->run_multiphase(c.L0, d_C_orig, coloring != 0, minGraphSize, threshold, C_threshold,
+                            stats));
+  CK(cudaStreamSynchronize(c.s));
+  if (stats) {
+    stats->kernel_launches = c.launches + c.eng->launches_;
+    stats->time_total = now_s() - t0;
+  }
+  return GLV_OK;
+}
+
+int glv_louvain_coloring_phase(const glv_graph *G, long *C, const int *color, int numColor,
+                               double Lower, double thresh, int mode, double *mod, int *numItr,
+                               double *totTime) {
+  const double t0 = now_s();
+  if (!G || !C || (!color && G->numVertices > 0)) return fail(GLV_ERR_ARG, "NULL argument");
+  if (numColor < 1 || numColor > kMaxColors) return fail(GLV_ERR_ARG, "numColor out of range");
+  Call c;
+  TRY(open_call(c, mode, G->numVertices, G->edgeListPtrs, G->edgeList, nullptr, nullptr));
+  const long nv = G->numVertices;
+  for (long i = 0; i < nv; ++i)
+    if (color[i] < 0 || color[i] >= numColor) return fail(GLV_ERR_ARG, "colour out of range");
+  CK(cudaMemcpyAsync(c.eng->color_, color, nv * sizeof(int32_t), cudaMemcpyHostToDevice, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  double q = 0;
+  int itr = 0;
+  TRY(c.eng->coloring_phase(c.L0, numColor, true, Lower, thresh, &q, &itr));
+  TRY(download_ids(c, c.eng->C, nv, C));
+  if (mod) *mod = q;
+  if (numItr) *numItr = itr;
+  if (totTime) *totTime = now_s() - t0;
+  return GLV_OK;
+}
+
+int glv_louvain_basic_phase(const glv_graph *G, long *C, double Lower, double thresh, int mode,
+                            double *mod, int *numItr, double *totTime) {
+  const double t0 = now_s();
+  if (!G || !C) return fail(GLV_ERR_ARG, "NULL argument");
+  Call c;
+  TRY(open_call(c, mode, G->numVertices, G->edgeListPtrs, G->edgeList, nullptr, nullptr));
+  double q = 0;
+  int itr = 0;
+  TRY(c.eng->basic_phase(c.L0, Lower, thresh, &q, &itr));
+  TRY(download_ids(c, c.eng->C, G->numVertices, C));
+  if (mod) *mod = q;
+  if (numItr) *numItr = itr;
+  if (totTime) *totTime = now_s() - t0;
+  return GLV_OK;
+}
+
+int glv_distance_one_coloring(const glv_graph *G, int *vtxColor, int mode, int *maxColor,
+                              double *totTime) {
+  if (!G || (!vtxColor && G->numVertices > 0)) return fail(GLV_ERR_ARG, "NULL argument");
+  Call c;
+  TRY(open_call(c, mode, G->numVertices, G->edgeListPtrs, G->edgeList, nullptr, nullptr));
+  int nc = 0;
+  double secs = 0;
+  if (G->numVertices > 0) TRY(c.eng->color(c.L0, &nc, &secs));
+  CK(cudaMemcpyAsync(vtxColor, c.eng->color_, G->numVertices * sizeof(int32_t),
+                     cudaMemcpyDeviceToHost, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  if (maxColor) *maxColor = nc - 1;
+  if (totTime) *totTime = secs;
+  return GLV_OK;
+}
+
+int glv_renumber_clusters(long *C, long size, long *numClusters) {
+  if (size < 0 || (!C && size > 0)) return fail(GLV_ERR_ARG, "bad arguments");
+  if (size >= (1L << 31) - 1) return fail(GLV_ERR_TOO_LARGE, "size >= 2^31");
+  TRY(device_ready());
+  Call c;
+  CK(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
+  c.eng = new Engine(c.s, GLV_MODE_VERIFY);
+  TRY(c.eng->init(size, 0));
+  TRY(upload_ids(c, C, size, c.eng->C, size));
+  int64_t ncl = 0;
+  TRY(c.eng->renumber(c.eng->C, size, &ncl));
+  TRY(download_ids(c, c.eng->C, size, C));
+  if (numClusters) *numClusters = (long)ncl;
+  return GLV_OK;
+}
+
+int glv_build_next_level(const glv_graph *Gin, glv_graph *Gout, const long *C,
+                         long numUniqueClusters, int mode, double *totTime) {
+  const double t0 = now_s();
+  if (!Gin || !Gout || (!C && Gin->numVertices > 0)) return fail(GLV_ERR_ARG, "NULL argument");
+  if (numUniqueClusters < 1 || numUniqueClusters > Gin->numVertices)
+    return fail(GLV_ERR_ARG, "numUniqueClusters out of range");
+  Call c;
+  TRY(open_call(c, mode, Gin->numVertices, Gin->edgeListPtrs, Gin->edgeList, nullptr, nullptr));
+  TRY(upload_ids(c, C, Gin->numVertices, c.eng->C, numUniqueClusters));
+  Level out;
+  int64_t ne = 0;
+  TRY(c.eng->coarsen(c.L0, c.eng->C, numUniqueClusters, &out, &ne));
+  long *hp = (long *)malloc((numUniqueClusters + 1) * sizeof(long));
+  glv_edge *he = (glv_edge *)malloc(std::max<int64_t>(out.nnz, 1) * sizeof(glv_edge));
+  if (!hp || !he) {
+    free(hp); free(he);
+    c.eng->free_level(out);
+    return fail(GLV_ERR_OOM, "host allocation failed");
+  }
+  glv_edge *daos;
+  CK(cudaMallocAsync((void **)&daos, std::max<int64_t>(out.nnz, 1) * sizeof(glv_edge), c.s));
+  k_fill_aos<<<grid_for(out.nv, 256, 148 * 8), 256, 0, c.s>>>(out.nv, out.ptr, out.tail, out.w,
+                                                              daos);
+  ++c.launches;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(hp, out.ptr, (numUniqueClusters + 1) * sizeof(long), cudaMemcpyDeviceToHost,
+                     c.s));
+  CK(cudaMemcpyAsync(he, daos, out.nnz * sizeof(glv_edge), cudaMemcpyDeviceToHost, c.s));
+  CK(cudaFreeAsync(daos, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  c.eng->free_level(out);
+  Gout->numVertices = numUniqueClusters;
+  Gout->sVertices = numUniqueClusters;
+  Gout->numEdges = ne;
+  Gout->edgeListPtrs = hp;
+  Gout->edgeList = he;
+  if (totTime) *totTime = now_s() - t0;
+  return GLV_OK;
+}
+
+int glv_modularity(const glv_graph *G, const long *C, double *mod) {
+  if (!G || !mod || (!C && G->numVertices > 0)) return fail(GLV_ERR_ARG, "NULL argument");
+  Call c;
+  TRY(open_call(c, GLV_MODE_VERIFY, G->numVertices, G->edgeListPtrs, G->edgeList, nullptr,
+                nullptr));
+  TRY(upload_ids(c, C, G->numVertices, c.eng->Ctgt, G->numVertices));
+  return c.eng->modularity_of(c.L0, c.eng->Ctgt, mod);
+}
+
+int glv_decide_batch(long nv, const long *ptr, const long *tail, const double *weight,
+                     const long *C, const double *vDeg, const double *cDeg, const long *cSize,
+                     double constant, long nverts, const long *verts, long *targets) {
+  if (nverts < 0 || (nverts > 0 && (!verts || !targets))) return fail(GLV_ERR_ARG, "bad list");
+  for (long k = 0; k < nverts; ++k)
+    if (verts[k] < 0 || verts[k] >= nv) return fail(GLV_ERR_ARG, "vertex id out of range");
+  if (!C || !vDeg || !cDeg || !cSize) return fail(GLV_ERR_ARG, "NULL state array");
+  Call c;
+  TRY(open_call(c, GLV_MODE_VERIFY, nv, ptr, nullptr, tail, weight));
+  Engine &e = *c.eng;
+  TRY(upload_ids(c, C, nv, e.C, nv));
+  std::vector<int32_t> cs(nv);
+  for (long i = 0; i < nv; ++i) cs[i] = (int32_t)cSize[i];
+  CK(cudaMemcpyAsync(e.vDeg, vDeg, nv * sizeof(double), cudaMemcpyHostToDevice, c.s));
+  CK(cudaMemcpyAsync(e.cDeg, cDeg, nv * sizeof(double), cudaMemcpyHostToDevice, c.s));
+  CK(cudaMemcpyAsync(e.cSize, cs.data(), nv * sizeof(int32_t), cudaMemcpyHostToDevice, c.s));
+  double cst2[2] = {constant, 0.0};
+  CK(cudaMemcpyAsync(e.cst, cst2, sizeof(cst2), cudaMemcpyHostToDevice, c.s));
+  int32_t *dv;
+  CK(cudaMallocAsync((void **)&dv, std::max<long>(nverts, 1) * sizeof(int32_t), c.s));
+  TRY(upload_ids(c, verts, nverts, dv, nv));
+  CK(cudaStreamSynchronize(c.s));
+  TRY(e.decide(c.L0, dv, nverts));
+  std::vector<int32_t> tg(nv);
+  CK(cudaMemcpyAsync(tg.data(), e.Ctgt, nv * sizeof(int32_t), cudaMemcpyDeviceToHost, c.s));
+  CK(cudaFreeAsync(dv, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  for (long k = 0; k < nverts; ++k) targets[k] = tg[verts[k]];
+  return GLV_OK;
+}
+
+}  // extern "C"

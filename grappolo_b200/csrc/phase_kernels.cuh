@@ -1,0 +1,537 @@
+// Per-phase kernels around the sweep: degrees, modularity, colouring, the
+// colour/bin schedule, community-total updates, renumbering and coarsening.
+#pragma once
+
+#include <cooperative_groups.h>
+
+#include "glv_common.cuh"
+
+namespace glv {
+
+namespace cg = cooperative_groups;
+
+// ---------------------------------------------------------------------------
+// Phase init: vDeg = CSR-order row sums (Utility/utilityClusteringFunctions.cpp:70-87),
+// cInfo = {1, vDeg}, C = identity (initCommAss, :98-104).  One thread per row
+// keeps the reference's summation order.
+__global__ void k_init_phase(int64_t nv, const int64_t *ptr, const double *w, double *vDeg,
+                             double *cDeg, int32_t *cSize, int32_t *C, int32_t *C2) {
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    const int64_t e = ptr[v + 1];
+    for (int64_t j = ptr[v]; j < e; ++j) s = __dadd_rn(s, w[j]);
+    vDeg[v] = s;
+    cDeg[v] = s;
+    cSize[v] = 1;
+    C[v] = (int32_t)v;
+    if (C2) C2[v] = (int32_t)v;
+  }
+}
+
+// 1 / sequential sum (calConstantForSecondTerm, :89-96 at one thread).
+__global__ void k_constant_sequential(int64_t n, const double *x, double *out) {
+  double s = 0.0;
+  for (int64_t i = 0; i < n; ++i) s = __dadd_rn(s, x[i]);
+  out[0] = __ddiv_rn(1.0, s);
+  out[1] = s;
+}
+
+// Deterministic two-level reductions: blocks write partials, one block folds
+// them in index order.
+template <int BS>
+__device__ __forceinline__ double block_sum(double x, double *sh) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) x = __dadd_rn(x, __shfl_xor_sync(FULL, x, off));
+  if (lane == 0) sh[warp] = x;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x == 0)
+    for (int k = 0; k < BS / 32; ++k) r = __dadd_rn(r, sh[k]);
+  __syncthreads();
+  return r;  // valid in thread 0
+}
+
+__global__ void __launch_bounds__(256) k_sum_partials(int64_t n, const double *x, double *part) {
+  __shared__ double sh[8];
+  double s = 0.0;
+  const int64_t per = (n + gridDim.x - 1) / gridDim.x;
+  const int64_t b = (int64_t)blockIdx.x * per, e = min(n, b + per);
+  for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x) s = __dadd_rn(s, x[i]);
+  s = block_sum<256>(s, sh);
+  if (threadIdx.x == 0) part[blockIdx.x] = s;
+}
+
+__global__ void k_constant_from_partials(int nparts, const double *part, double *out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double s = 0.0;
+  for (int i = 0; i < nparts; ++i) s = __dadd_rn(s, part[i]);
+  out[0] = __ddiv_rn(1.0, s);
+  out[1] = s;
+}
+
+// ---------------------------------------------------------------------------
+// Modularity: e_xx = sum_i cWI[i], a2_x = sum_i cDeg[i]^2, Q = e_xx*c - a2_x*c*c
+// (Coloring/parallelLouvainWithColoring.cpp:226-249,
+//  BasicCommunitiesDetection/parallelLouvainMethod.cpp:247-255).
+// Colour phases compute cWI[i] = sum_{j: C[tail]==C[i]} w here; Jacobi phases
+// pass the per-vertex Counter[own] their sweep produced (own_w).
+// Each block takes 256 consecutive vertices and walks their edges
+// edge-parallel, so hub rows do not serialise one lane.
+constexpr int kModVB = 256;
+
+__global__ void __launch_bounds__(256) k_modularity_part(int64_t nv, const int64_t *ptr,
+                                                         const int32_t *tail, const double *w,
+                                                         const int32_t *C, const double *own_w,
+                                                         const double *cDeg, double *part_e,
+                                                         double *part_a) {
+  __shared__ int64_t s_ptr[kModVB + 1];
+  __shared__ int32_t s_c[kModVB];
+  __shared__ double sh[8];
+  const int64_t v0 = (int64_t)blockIdx.x * kModVB;
+  const int64_t v1 = min(nv, v0 + kModVB);
+  const int nvb = (int)(v1 - v0);
+  double a2 = 0.0, ex = 0.0;
+  if (threadIdx.x < nvb) {
+    const double d = cDeg[v0 + threadIdx.x];
+    a2 = __dmul_rn(d, d);
+  }
+  if (own_w) {
+    if (threadIdx.x < nvb) ex = own_w[v0 + threadIdx.x];
+  } else {
+    for (int k = threadIdx.x; k <= nvb; k += blockDim.x) s_ptr[k] = ptr[v0 + k];
+    for (int k = threadIdx.x; k < nvb; k += blockDim.x) s_c[k] = C[v0 + k];
+    __syncthreads();
+    const int64_t eb = s_ptr[0], ee = s_ptr[nvb];
+    int h = 0;
+    for (int64_t e = eb + threadIdx.x; e < ee; e += blockDim.x) {
+      while (s_ptr[h + 1] <= e) ++h;
+      if (C[tail[e]] == s_c[h]) ex = __dadd_rn(ex, w[e]);
+    }
+  }
+  ex = block_sum<256>(ex, sh);
+  a2 = block_sum<256>(a2, sh);
+  if (threadIdx.x == 0) { part_e[blockIdx.x] = ex; part_a[blockIdx.x] = a2; }
+}
+
+// out[0] = Q, out[1] = e_xx, out[2] = a2_x.  `cst` = {constant, 2m}.
+__global__ void __launch_bounds__(256) k_modularity_final(int nparts, const double *part_e,
+                                                          const double *part_a, const double *cst,
+                                                          double *out) {
+  __shared__ double sh[8];
+  double e = 0.0, a = 0.0;
+  const int per = (nparts + blockDim.x - 1) / blockDim.x;
+  const int b = threadIdx.x * per, en = min(nparts, b + per);
+  for (int i = b; i < en; ++i) { e = __dadd_rn(e, part_e[i]); a = __dadd_rn(a, part_a[i]); }
+  e = block_sum<256>(e, sh);
+  a = block_sum<256>(a, sh);
+  if (threadIdx.x == 0) {
+    const double c = cst[0];
+    out[0] = __dsub_rn(__dmul_rn(e, c), __dmul_rn(__dmul_rn(a, c), c));
+    out[1] = e;
+    out[2] = a;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Distance-1 colouring by priority order (Jones-Plassmann).  A vertex takes
+// the smallest colour not used by its higher-priority neighbours once they are
+// all coloured.  With priority "lower id first" this is exactly the
+// sequential first-fit pass of Coloring/coloringDistanceOne.cpp:137-150 at one
+// thread; with hashed priorities it is the parallel independent-set form.
+__device__ __forceinline__ bool prio_before(int32_t u, int32_t v, int hashed, uint32_t seed) {
+  if (!hashed) return u < v;
+  const uint32_t hu = mix32((uint32_t)u ^ seed), hv = mix32((uint32_t)v ^ seed);
+  return (hu < hv) || (hu == hv && u < v);
+}
+
+__global__ void k_color_init(int64_t nv, const int64_t *ptr, const int32_t *tail, int hashed,
+                             uint32_t seed, int32_t *pending, int32_t *color, int32_t *frontier,
+                             int32_t *fcount) {
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    int32_t cnt = 0;
+    for (int64_t j = ptr[v]; j < ptr[v + 1]; ++j) {
+      const int32_t u = tail[j];
+      if (u != (int32_t)v && prio_before(u, (int32_t)v, hashed, seed)) ++cnt;
+    }
+    pending[v] = cnt;
+    color[v] = -1;
+    if (cnt == 0) frontier[atomicAdd(fcount, 1)] = (int32_t)v;
+  }
+}
+
+// Persistent cooperative kernel: one grid-wide barrier per round.  fcount has
+// three counters used round-robin (read / push / reset).  Each round colours
+// at least one vertex, so the loop ends after at most nv rounds.
+__global__ void __launch_bounds__(256) k_color_rounds(int64_t nv, const int64_t *ptr,
+                                                      const int32_t *tail, int hashed,
+                                                      uint32_t seed, int32_t *pending,
+                                                      int32_t *color, int32_t *front0,
+                                                      int32_t *front1, int32_t *fcount,
+                                                      int32_t *status) {
+  cg::grid_group grid = cg::this_grid();
+  __shared__ uint32_t bm[8][kMaxColors / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  uint32_t *mybm = bm[warp];
+  for (int64_t round = 0; round <= nv; ++round) {
+    int32_t *cur = (round & 1) ? front1 : front0;
+    int32_t *nxt = (round & 1) ? front0 : front1;
+    const int32_t n = *((volatile int32_t *)&fcount[round % 3]);
+    if (n == 0) break;
+    if (blockIdx.x == 0 && threadIdx.x == 0) fcount[(round + 2) % 3] = 0;
+    for (int64_t k = wid; k < n; k += nw) {
+      const int32_t v = cur[k];
+      const int64_t rb = ptr[v], re = ptr[v + 1];
+      const int64_t deg = re - rb;
+      const int words = (int)((deg + 32) / 32 < kMaxColors / 32 ? (deg + 32) / 32 : kMaxColors / 32);
+      for (int q = lane; q < words; q += 32) mybm[q] = 0u;
+      __syncwarp();
+      for (int64_t j = rb + lane; j < re; j += 32) {
+        const int32_t u = tail[j];
+        if (u != v && prio_before(u, v, hashed, seed)) {
+          const int32_t cu = color[u];
+          if (cu >= 0 && cu < words * 32) atomicOr(&mybm[cu >> 5], 1u << (cu & 31));
+        }
+      }
+      __syncwarp();
+      int first = INT32_MAX;
+      for (int q = lane; q < words; q += 32) {
+        const uint32_t free_bits = ~mybm[q];
+        if (free_bits) { first = q * 32 + __ffs(free_bits) - 1; break; }
+      }
+      first = __reduce_min_sync(FULL, first);
+      if (first == INT32_MAX) first = words * 32;  // all marked: next colour
+      if (first >= kMaxColors) {
+        if (lane == 0) atomicExch(status, 1);
+        first = kMaxColors - 1;
+      }
+      if (lane == 0) color[v] = first;
+      __syncwarp();
+      for (int64_t j = rb + lane; j < re; j += 32) {
+        const int32_t u = tail[j];
+        if (u != v && prio_before(v, u, hashed, seed)) {
+          if (atomicSub(&pending[u], 1) == 1) nxt[atomicAdd(&fcount[(round + 1) % 3], 1)] = u;
+        }
+      }
+    }
+    grid.sync();
+  }
+}
+
+__global__ void k_max_color(int64_t nv, const int32_t *color, int32_t *out) {
+  int32_t m = -1;
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
+       v += (int64_t)gridDim.x * blockDim.x)
+    m = max(m, color[v]);
+  m = __reduce_max_sync(FULL, (unsigned)(m + 1)) - 1;
+  if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+// ---------------------------------------------------------------------------
+// Schedule: vertices sorted by key = (colour*nsub + sublevel)*NBINS + bin;
+// a stable sort keeps ascending ids inside every (class, bin) segment.
+__global__ void k_schedule_keys(int64_t nv, const int64_t *ptr, const int32_t *color,
+                                const int32_t *sub, int nsub, BinLimits lim, int32_t *keys,
+                                int32_t *vals, int32_t *hist) {
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t deg = ptr[v + 1] - ptr[v];
+    const int c = color ? color[v] : 0;
+    const int s = sub ? sub[v] : 0;
+    const int k = (c * nsub + s) * NBINS + degree_bin(deg, lim);
+    keys[v] = k;
+    vals[v] = (int32_t)v;
+    atomicAdd(&hist[k], 1);
+  }
+}
+
+// Per-member hub table offsets: prefix over table capacities within a class.
+__global__ void k_hub_caps(int64_t n, const int32_t *members, const int64_t *ptr, int64_t *cap) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t v = members[k];
+    cap[k] = table_cap(ptr[v + 1] - ptr[v]);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Community totals after a class (cInfo += cUpdate,
+// parallelLouvainWithColoring.cpp:213-217).  Atomic form: the sweep already
+// summed the deltas into dDeg/dSize; the first thread to claim a community's
+// delta adds it to the totals and clears it.
+__global__ void k_apply_deltas(int64_t begin, int64_t end, const int32_t *move_old,
+                               const int32_t *move_new, double *dDeg, int32_t *dSize,
+                               double *cDeg, int32_t *cSize) {
+  for (int64_t pos = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; pos < end;
+       pos += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t o = move_old[pos];
+    if (o < 0) continue;
+    const int32_t cs[2] = {move_new[pos], o};
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int32_t c = cs[k];
+      // Each field is claimed separately, so exactly one thread writes it.
+      const unsigned long long bits = atomicExch((unsigned long long *)&dDeg[c], 0ull);
+      if (bits != 0ull) cDeg[c] = __dadd_rn(cDeg[c], __longlong_as_double((long long)bits));
+      const int32_t s = atomicExch(&dSize[c], 0);
+      if (s != 0) cSize[c] += s;
+    }
+  }
+}
+
+// Ordered form: one record per (community, vertex) delta, sorted by
+// (community, vertex id), folded from 0.0 in member order as the reference's
+// one-thread loop accumulates cUpdate.
+struct DeltaRec {
+  double d;
+  int32_t s;
+  int32_t pad;
+};
+
+__global__ void k_delta_records(int64_t begin, int64_t end, const int32_t *members,
+                                const int32_t *move_old, const int32_t *move_new,
+                                const double *vDeg, uint64_t sentinel, uint64_t *keys,
+                                DeltaRec *recs) {
+  for (int64_t pos = begin + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; pos < end;
+       pos += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = 2 * (pos - begin);
+    const int32_t o = move_old[pos];
+    if (o < 0) {
+      keys[k] = sentinel; keys[k + 1] = sentinel;
+      recs[k] = DeltaRec{0.0, 0, 0}; recs[k + 1] = DeltaRec{0.0, 0, 0};
+      continue;
+    }
+    const int32_t v = members[pos];
+    const int32_t n = move_new[pos];
+    const double d = vDeg[v];
+    keys[k] = ((uint64_t)(uint32_t)n << 32) | (uint32_t)v;
+    recs[k] = DeltaRec{d, 1, 0};
+    keys[k + 1] = ((uint64_t)(uint32_t)o << 32) | (uint32_t)v;
+    recs[k + 1] = DeltaRec{-d, -1, 0};
+  }
+}
+
+__global__ void k_fold_deltas(int64_t n, const uint64_t *keys, const DeltaRec *recs,
+                              uint64_t sentinel, double *cDeg, int32_t *cSize) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t ki = keys[i];
+    if (ki >= sentinel) continue;
+    const uint32_t c = (uint32_t)(ki >> 32);
+    if (i > 0 && (uint32_t)(keys[i - 1] >> 32) == c) continue;
+    double s = 0.0;
+    int32_t cnt = 0;
+    for (int64_t j = i; j < n && keys[j] < sentinel && (uint32_t)(keys[j] >> 32) == c; ++j) {
+      s = __dadd_rn(s, recs[j].d);
+      cnt += recs[j].s;
+    }
+    cDeg[c] = __dadd_rn(cDeg[c], s);
+    cSize[c] += cnt;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Renumbering by first occurrence (Utility/buildNextPhase.cpp:48-79):
+// first[c] = min{i : C[i] = c}; position i opens a new id iff first[C[i]] == i;
+// new ids are the exclusive prefix count of openings.
+__global__ void k_fill_i32(int64_t n, int32_t *x, int32_t val) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = val;
+}
+
+__global__ void k_first_occurrence(int64_t n, const int32_t *C, int32_t *first) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t c = C[i];
+    if (c >= 0) atomicMin(&first[c], (int32_t)i);
+  }
+}
+
+__global__ void k_open_flags(int64_t n, const int32_t *C, const int32_t *first, int32_t *flag) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t c = C[i];
+    flag[i] = (c >= 0 && first[c] == (int32_t)i) ? 1 : 0;
+  }
+}
+
+__global__ void k_apply_renumber(int64_t n, int32_t *C, const int32_t *first,
+                                 const int32_t *scan) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t c = C[i];
+    if (c >= 0) C[i] = scan[first[c]];
+  }
+}
+
+// C_orig composition (runMultiPhaseColoring.cpp:132-144).
+__global__ void k_compose(int64_t n, int32_t *C_orig, const int32_t *C, int first_phase) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (first_phase) C_orig[i] = C[i];
+    else if (C_orig[i] >= 0) C_orig[i] = C[C_orig[i]];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Coarsening (Utility/buildNextPhase.cpp:83-255).  Records: one seed (a, a,
+// 0.0) per cluster, then one per CSR entry i->t with a = C[i] >= b = C[t], in
+// (i, j) order; others get the sentinel key.  A stable radix sort by
+// (a << nb) | b groups each pair with its entries still in (i, j) order.
+__global__ void k_coarse_records(int64_t nv, const int64_t *ptr, const int32_t *tail,
+                                 const double *w, const int32_t *C, int64_t ncl, int nb,
+                                 uint64_t sentinel, uint64_t *keys, double *vals) {
+  // seeds
+  for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < ncl;
+       a += (int64_t)gridDim.x * blockDim.x) {
+    keys[a] = ((uint64_t)a << nb) | (uint64_t)a;
+    vals[a] = 0.0;
+  }
+  // entries: block-level edge-parallel walk over 256-vertex tiles
+  __shared__ int64_t s_ptr[kModVB + 1];
+  __shared__ int32_t s_c[kModVB];
+  const int64_t ntiles = (nv + kModVB - 1) / kModVB;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t v0 = tile * kModVB, v1 = min(nv, v0 + kModVB);
+    const int nvb = (int)(v1 - v0);
+    __syncthreads();
+    for (int k = threadIdx.x; k <= nvb; k += blockDim.x) s_ptr[k] = ptr[v0 + k];
+    for (int k = threadIdx.x; k < nvb; k += blockDim.x) s_c[k] = C[v0 + k];
+    __syncthreads();
+    const int64_t eb = s_ptr[0], ee = s_ptr[nvb];
+    int h = 0;
+    for (int64_t e = eb + threadIdx.x; e < ee; e += blockDim.x) {
+      while (s_ptr[h + 1] <= e) ++h;
+      const int32_t a = s_c[h];
+      const int32_t b = C[tail[e]];
+      if (a >= b) {
+        keys[ncl + e] = ((uint64_t)a << nb) | (uint64_t)b;
+        vals[ncl + e] = w[e];
+      } else {
+        keys[ncl + e] = sentinel;
+        vals[ncl + e] = 0.0;
+      }
+    }
+  }
+}
+
+// Segment heads of the sorted records -> flags (1 at the first record of each
+// distinct key, sentinel excluded).
+__global__ void k_segment_heads(int64_t n, const uint64_t *keys, uint64_t sentinel,
+                                int32_t *flag) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    flag[i] = (k < sentinel && (i == 0 || keys[i - 1] != k)) ? 1 : 0;
+  }
+}
+
+// Fold each pair's records in order (one thread per pair): the reference's
+// map entry starts at the first weight (or 0.0 for the self seed) and adds
+// the rest in (i, j) order.
+__global__ void k_fold_pairs(int64_t n, const uint64_t *keys, const double *vals,
+                             const int32_t *flag, const int64_t *uidx, uint64_t sentinel,
+                             uint64_t *ukeys, double *uvals) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    if (!flag[i]) continue;
+    const uint64_t k = keys[i];
+    double s = vals[i];
+    for (int64_t j = i + 1; j < n && keys[j] == k; ++j) s = __dadd_rn(s, vals[j]);
+    const int64_t u = uidx[i];
+    ukeys[u] = k;
+    uvals[u] = s;
+  }
+}
+
+// Atomic form for FAST mode: every record adds into its pair's slot.
+__global__ void k_scatter_pairs(int64_t n, const uint64_t *keys, const double *vals,
+                                const int32_t *flag, const int64_t *uidx, uint64_t sentinel,
+                                uint64_t *ukeys, double *uvals) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    if (k >= sentinel) continue;
+    const int64_t u = uidx[i] - (flag[i] ? 0 : 1);
+    if (flag[i]) ukeys[u] = k;
+    atomicAdd(&uvals[u], vals[i]);
+  }
+}
+
+// Row sizes of the coarse CSR: pair (a, b) counts once in row a and, when
+// a > b, once more in row b (buildNextPhase.cpp:157-170).
+__global__ void k_row_counts(int64_t np, const uint64_t *ukeys, int nb, int64_t *lower_cnt,
+                             int64_t *upper_cnt, int64_t *ne_off) {
+  const uint64_t mask = (1ull << nb) - 1;
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t a = (int64_t)(ukeys[p] >> nb), b = (int64_t)(ukeys[p] & mask);
+    atomicAdd((unsigned long long *)&lower_cnt[a], 1ull);
+    if (a > b) {
+      atomicAdd((unsigned long long *)&upper_cnt[b], 1ull);
+      atomicAdd((unsigned long long *)ne_off, 1ull);
+    }
+  }
+}
+
+// Lower part of each row: pairs (a, b <= a) in ascending b.  Pairs are sorted
+// by (a, b), so a pair's rank inside row a is p - first pair of a; also emits
+// the transposed key (b << nb) | a of every off-diagonal pair for the mirror.
+__global__ void k_emit_lower(int64_t np, const uint64_t *ukeys, const double *uvals, int nb,
+                             const int64_t *row_ptr, const int64_t *lower_first,
+                             int32_t *otail, double *ow, uint64_t *tkeys, double *tvals,
+                             uint64_t sentinel) {
+  const uint64_t mask = (1ull << nb) - 1;
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t a = (int64_t)(ukeys[p] >> nb), b = (int64_t)(ukeys[p] & mask);
+    const int64_t at = row_ptr[a] + (p - lower_first[a]);
+    otail[at] = (int32_t)b;
+    ow[at] = uvals[p];
+    if (a > b) {
+      tkeys[p] = ((uint64_t)b << nb) | (uint64_t)a;
+      tvals[p] = uvals[p];
+    } else {
+      tkeys[p] = sentinel;
+      tvals[p] = 0.0;
+    }
+  }
+}
+
+// Mirrored part: transposed pairs sorted by (b, a) land after row b's lower
+// part, in ascending a (the order cluster a emits them at one thread,
+// buildNextPhase.cpp:205-223).
+__global__ void k_emit_upper(int64_t np, const uint64_t *tkeys, const double *tvals, int nb,
+                             const int64_t *row_ptr, const int64_t *lower_cnt,
+                             const int64_t *upper_first, int32_t *otail, double *ow,
+                             uint64_t sentinel) {
+  const uint64_t mask = (1ull << nb) - 1;
+  for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < np;
+       q += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = tkeys[q];
+    if (k >= sentinel) continue;
+    const int64_t b = (int64_t)(k >> nb), a = (int64_t)(k & mask);
+    const int64_t at = row_ptr[b] + lower_cnt[b] + (q - upper_first[b]);
+    otail[at] = (int32_t)a;
+    ow[at] = tvals[q];
+  }
+}
+
+// first index of each row's run in a sorted key array (keys >> shift = row).
+__global__ void k_run_first(int64_t n, const uint64_t *keys, int shift, uint64_t sentinel,
+                            int64_t *first) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = keys[i];
+    if (k >= sentinel) continue;
+    const uint64_t r = k >> shift;
+    if (i == 0 || (keys[i - 1] >> shift) != r) first[r] = i;
+  }
+}
+
+}  // namespace glv

@@ -1,0 +1,340 @@
+// Local-moving sweep kernels (one launch per colour class and degree bin).
+//
+// Per vertex v with community own = C[v] and weighted degree k = vDeg[v] the
+// kernels compute what Grappolo's buildLocalMapCounter + max compute
+// (Utility/utilityClusteringFunctions.cpp:172-194, 226-259):
+//   Counter[c] = sum of w(v,t) over neighbours t with C[t] = c, in CSR order,
+//   selfLoop   = sum of w(v,v) entries,
+//   eix = Counter[own] - selfLoop,  ax = cDeg[own] - k,
+//   gain(c) = 2*(Counter[c] - eix) - 2*k*(cDeg[c] - ax)*constant  (c != own),
+// and move to the strictly positive best gain (ties: lower id), with the
+// reference's swap protection for two singletons.  Every per-community sum is
+// folded in CSR order (leader lanes add their group's weights lane by lane,
+// chunks in row order), so the sums are bit-identical to the reference's.
+#pragma once
+
+#include "glv_common.cuh"
+
+namespace glv {
+
+struct SweepArgs {
+  const int64_t *ptr;
+  const int32_t *tail;
+  const double *w;
+  int32_t *C;            // communities read; colour phases also write decisions here
+  int32_t *target;       // Jacobi phases: decisions (nullptr in colour phases)
+  double *own_w;         // Jacobi phases: Counter[own] per vertex (cluster weight internal)
+  const double *vDeg;
+  const double *cDeg;
+  const int32_t *cSize;
+  double constant;
+  const int32_t *members;  // vertices ordered by (colour, bin, id)
+  int32_t *move_old;       // per member slot: old community if it moved, else -1
+  int32_t *move_new;       // per member slot: decision
+  double *dDeg;            // community-degree deltas (atomic accumulation)
+  int32_t *dSize;
+  int atomic_deltas;       // 1: accumulate deltas here; 0: ordered fold after the class
+  int32_t *hub_keys;       // BIN_HUB global tables
+  double *hub_vals;
+  const int64_t *hub_off;  // per member slot: table offset
+};
+
+// Writes the decision of vertex v (member slot pos) and its delta records.
+__device__ __forceinline__ void emit_decision(const SweepArgs &a, int64_t pos, int32_t v,
+                                              int32_t own, int32_t target, double degree,
+                                              double own_w) {
+  if (a.target) {
+    a.target[v] = target;
+    if (a.own_w) a.own_w[v] = own_w;
+  } else {
+    a.C[v] = target;
+  }
+  bool moved = (target != own) && (target != -1);
+  a.move_old[pos] = moved ? own : -1;
+  a.move_new[pos] = target;
+  if (moved && a.atomic_deltas) {
+    atomicAdd(&a.dDeg[target], degree);
+    atomicAdd(&a.dDeg[own], -degree);
+    atomicAdd(&a.dSize[target], 1);
+    atomicAdd(&a.dSize[own], -1);
+  }
+}
+
+// Final choice: best strictly positive gain or stay; swap protection
+// (utilityClusteringFunctions.cpp:254-256).
+__device__ __forceinline__ int32_t finish_choice(const SweepArgs &a, int32_t own, double best_g,
+                                                 int32_t best_c) {
+  int32_t t = (best_g > 0.0) ? best_c : own;
+  if (t != own && a.cSize[t] == 1 && a.cSize[own] == 1 && t > own) t = own;
+  return t;
+}
+
+// ---------------------------------------------------------------------------
+// Rows of at most G entries: G lanes per vertex, one entry per lane, no table.
+template <int G>
+__global__ void __launch_bounds__(256) k_sweep_small(SweepArgs a, int64_t begin, int64_t end) {
+  constexpr int VPW = 32 / G;
+  const int lane = threadIdx.x & 31;
+  const int grp = lane / G;
+  const int gl = lane & (G - 1);
+  const unsigned gmask = (G == 32) ? FULL : (((1u << G) - 1u) << (grp * G));
+  const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t base = begin + wid * VPW; base < end; base += nw * VPW) {
+    const int64_t pos = base + grp;
+    const bool valid = pos < end;
+    const int32_t v = valid ? a.members[pos] : 0;
+    const int64_t rb = valid ? a.ptr[v] : 0;
+    const int deg = valid ? (int)(a.ptr[v + 1] - rb) : 0;
+    const int32_t own = (valid && deg > 0) ? a.C[v] : -1;
+    const bool has = gl < deg;
+    const int32_t t = has ? a.tail[rb + gl] : -1;
+    const double wt = has ? a.w[rb + gl] : 0.0;
+    const int32_t c = has ? a.C[t] : -1;
+    const unsigned long long key =
+        has ? (((unsigned long long)grp << 32) | (uint32_t)c) : (0xFFFFFFFF00000000ull | lane);
+    const unsigned m = __match_any_sync(FULL, key);
+    const bool leader = has && (lane == __ffs(m) - 1);
+    // Ordered fold of each community group (lane order == CSR order).
+    unsigned rem = leader ? m : 0u;
+    const int rounds = __reduce_max_sync(FULL, (unsigned)__popc(rem));
+    double sum = 0.0;
+    for (int it = 0; it < rounds; ++it) {
+      const int src = rem ? __ffs(rem) - 1 : lane;
+      const double x = __shfl_sync(FULL, wt, src);
+      if (rem) { sum = __dadd_rn(sum, x); rem &= rem - 1; }
+    }
+    // Self-loop weight, in CSR order.
+    unsigned sm = __ballot_sync(FULL, has && t == v) & gmask;
+    const int srounds = __reduce_max_sync(FULL, (unsigned)__popc(sm));
+    double self_loop = 0.0;
+    for (int it = 0; it < srounds; ++it) {
+      const int src = sm ? __ffs(sm) - 1 : lane;
+      const double x = __shfl_sync(FULL, wt, src);
+      if (sm) { self_loop = __dadd_rn(self_loop, x); sm &= sm - 1; }
+    }
+    // Counter[own]
+    const unsigned om = __ballot_sync(FULL, leader && c == own) & gmask;
+    const double osum = __shfl_sync(FULL, sum, om ? __ffs(om) - 1 : lane);
+    const double own_w = om ? osum : 0.0;
+    const double degree = (valid && deg > 0) ? a.vDeg[v] : 0.0;
+    double g = 0.0;
+    int32_t bc = INT32_MAX;
+    if (leader && c != own) {
+      const double eix = __dsub_rn(own_w, self_loop);
+      const double ax = __dsub_rn(a.cDeg[own], degree);
+      const double gain = louvain_gain(sum, eix, degree, a.cDeg[c], ax, a.constant);
+      if (gain > 0.0) { g = gain; bc = c; }
+    }
+#pragma unroll
+    for (int off = G / 2; off >= 1; off >>= 1) {
+      const double og = __shfl_xor_sync(FULL, g, off);
+      const int32_t oc = __shfl_xor_sync(FULL, bc, off);
+      if (better(og, oc, g, bc)) { g = og; bc = oc; }
+    }
+    if (valid && gl == 0) {
+      const int32_t tgt = (deg == 0) ? -1 : finish_choice(a, own, g, bc);
+      emit_decision(a, pos, v, own, tgt, degree, own_w);
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Shared/global open-addressing table helpers.  Keys are community ids (>= 0),
+// -1 marks an empty slot; values start at 0.0.
+
+// Find or insert `key`, returning its slot.  Safe under concurrent inserts.
+__device__ __forceinline__ uint32_t table_slot(int32_t *keys, uint32_t mask, int32_t key) {
+  uint32_t s = hash_slot(key, mask);
+  while (true) {
+    int32_t k = keys[s];
+    if (k == key) return s;
+    if (k == -1) {
+      int32_t old = atomicCAS(&keys[s], -1, key);
+      if (old == -1 || old == key) return s;
+    }
+    s = (s + 1) & mask;
+  }
+}
+
+__device__ __forceinline__ uint32_t table_find(const int32_t *keys, uint32_t mask, int32_t key) {
+  uint32_t s = hash_slot(key, mask);
+  while (keys[s] != key) s = (s + 1) & mask;
+  return s;
+}
+
+// One warp accumulates row [rb, re) into the table in CSR order.  Leaders
+// fold their group's weights starting from the table value, so each
+// community's sum is the sequential CSR-order sum.  Returns the self-loop sum
+// (same value in every lane).  With `atomic_add` the group sums are added with
+// atomics instead (used when several warps share one table).
+__device__ __forceinline__ double warp_accumulate(const SweepArgs &a, int32_t v, int64_t rb,
+                                                  int64_t re, int64_t stride, int32_t *keys,
+                                                  double *vals, uint32_t mask, bool atomic_add) {
+  const int lane = threadIdx.x & 31;
+  double self_loop = 0.0;
+  for (int64_t base = rb; base < re; base += stride) {
+    const int64_t j = base + lane;
+    const bool has = j < re;
+    const int32_t t = has ? a.tail[j] : -1;
+    const double wt = has ? a.w[j] : 0.0;
+    const int32_t c = has ? a.C[t] : -1;
+    const uint32_t key = has ? (uint32_t)c : (0x80000000u | lane);
+    const unsigned m = __match_any_sync(FULL, key);
+    const bool leader = has && (lane == __ffs(m) - 1);
+    uint32_t slot = 0;
+    double acc = 0.0;
+    if (leader) {
+      slot = table_slot(keys, mask, c);
+      if (!atomic_add) acc = vals[slot];
+    }
+    unsigned rem = leader ? m : 0u;
+    const int rounds = __reduce_max_sync(FULL, (unsigned)__popc(rem));
+    for (int it = 0; it < rounds; ++it) {
+      const int src = rem ? __ffs(rem) - 1 : lane;
+      const double x = __shfl_sync(FULL, wt, src);
+      if (rem) { acc = __dadd_rn(acc, x); rem &= rem - 1; }
+    }
+    if (leader) {
+      if (atomic_add) atomicAdd(&vals[slot], acc);
+      else vals[slot] = acc;
+    }
+    unsigned sm = __ballot_sync(FULL, has && t == v);
+    while (sm) {  // warp-uniform
+      const int src = __ffs(sm) - 1;
+      self_loop = __dadd_rn(self_loop, __shfl_sync(FULL, wt, src));
+      sm &= sm - 1;
+    }
+    __syncwarp();
+  }
+  return self_loop;
+}
+
+// Best (gain, id) over table slots [first, cap) with stride.
+__device__ __forceinline__ void scan_table(const SweepArgs &a, const int32_t *keys,
+                                           const double *vals, uint32_t first, uint32_t cap,
+                                           uint32_t stride, int32_t own, double eix, double ax,
+                                           double degree, double &g, int32_t &bc) {
+  for (uint32_t s = first; s < cap; s += stride) {
+    const int32_t k = keys[s];
+    if (k >= 0 && k != own) {
+      const double gain = louvain_gain(vals[s], eix, degree, a.cDeg[k], ax, a.constant);
+      if (gain > 0.0 && better(gain, k, g, bc)) { g = gain; bc = k; }
+    }
+  }
+}
+
+__device__ __forceinline__ void warp_argmax(double &g, int32_t &bc) {
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) {
+    const double og = __shfl_xor_sync(FULL, g, off);
+    const int32_t oc = __shfl_xor_sync(FULL, bc, off);
+    if (better(og, oc, g, bc)) { g = og; bc = oc; }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Rows of 33..warp_max entries: one warp per vertex, table in shared memory.
+template <int CAP>
+__global__ void __launch_bounds__(256) k_sweep_warp(SweepArgs a, int64_t begin, int64_t end) {
+  extern __shared__ unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwb = blockDim.x >> 5;
+  double *vals = reinterpret_cast<double *>(smem_raw) + (size_t)warp * CAP;
+  int32_t *keys = reinterpret_cast<int32_t *>(reinterpret_cast<double *>(smem_raw) + (size_t)nwb * CAP) +
+                  (size_t)warp * CAP;
+  const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t pos = begin + wid; pos < end; pos += nw) {
+    const int32_t v = a.members[pos];
+    const int64_t rb = a.ptr[v], re = a.ptr[v + 1];
+    const uint32_t cap = table_cap(re - rb);
+    const uint32_t mask = cap - 1;
+    for (uint32_t s = lane; s < cap; s += 32) { keys[s] = -1; vals[s] = 0.0; }
+    __syncwarp();
+    const int32_t own = a.C[v];
+    if (lane == 0) keys[hash_slot(own, mask)] = own;
+    __syncwarp();
+    const double self_loop = warp_accumulate(a, v, rb, re, 32, keys, vals, mask, false);
+    const double degree = a.vDeg[v];
+    const double own_w = vals[hash_slot(own, mask)];
+    const double eix = __dsub_rn(own_w, self_loop);
+    const double ax = __dsub_rn(a.cDeg[own], degree);
+    double g = 0.0;
+    int32_t bc = INT32_MAX;
+    scan_table(a, keys, vals, lane, cap, 32, own, eix, ax, degree, g, bc);
+    warp_argmax(g, bc);
+    if (lane == 0) emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), degree, own_w);
+    __syncwarp();
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Large rows: one block per vertex.  BIN_BLOCK keeps the table in shared
+// memory (capacity up to `smem_cap`), BIN_HUB in global scratch at hub_off.
+// ordered = 1: warp 0 walks the whole row in CSR order (bit-exact sums);
+// ordered = 0: all warps take chunks and add group sums with atomics.
+__global__ void __launch_bounds__(512) k_sweep_block(SweepArgs a, int64_t begin, int64_t end,
+                                                     int hub, int ordered) {
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ double s_self[32];
+  __shared__ double s_g[32];
+  __shared__ int32_t s_c[32];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwb = blockDim.x >> 5;
+  for (int64_t pos = begin + blockIdx.x; pos < end; pos += gridDim.x) {
+    const int32_t v = a.members[pos];
+    const int64_t rb = a.ptr[v], re = a.ptr[v + 1];
+    const uint32_t cap = table_cap(re - rb);
+    const uint32_t mask = cap - 1;
+    int32_t *keys;
+    double *vals;
+    if (hub) {
+      keys = a.hub_keys + a.hub_off[pos];
+      vals = a.hub_vals + a.hub_off[pos];
+    } else {
+      vals = reinterpret_cast<double *>(smem_raw);
+      keys = reinterpret_cast<int32_t *>(vals + cap);
+    }
+    for (uint32_t s = threadIdx.x; s < cap; s += blockDim.x) { keys[s] = -1; vals[s] = 0.0; }
+    __syncthreads();
+    const int32_t own = a.C[v];
+    if (threadIdx.x == 0) keys[hash_slot(own, mask)] = own;
+    __syncthreads();
+    double self_loop;
+    if (ordered) {
+      if (warp == 0) {
+        double sl = warp_accumulate(a, v, rb, re, 32, keys, vals, mask, false);
+        if (lane == 0) s_self[0] = sl;
+      }
+      __syncthreads();
+      self_loop = s_self[0];
+    } else {
+      double sl = warp_accumulate(a, v, rb + 32 * warp, re, 32 * nwb, keys, vals, mask, true);
+      if (lane == 0) s_self[warp] = sl;
+      __syncthreads();
+      self_loop = 0.0;
+      for (int k = 0; k < nwb; ++k) self_loop = __dadd_rn(self_loop, s_self[k]);
+    }
+    const double degree = a.vDeg[v];
+    const double own_w = vals[hash_slot(own, mask)];
+    const double eix = __dsub_rn(own_w, self_loop);
+    const double ax = __dsub_rn(a.cDeg[own], degree);
+    double g = 0.0;
+    int32_t bc = INT32_MAX;
+    scan_table(a, keys, vals, threadIdx.x, cap, blockDim.x, own, eix, ax, degree, g, bc);
+    warp_argmax(g, bc);
+    if (lane == 0) { s_g[warp] = g; s_c[warp] = bc; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      for (int k = 1; k < nwb; ++k)
+        if (better(s_g[k], s_c[k], g, bc)) { g = s_g[k]; bc = s_c[k]; }
+      emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), degree, own_w);
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace glv

@@ -1,0 +1,230 @@
+"""Host-side mirror of Grappolo's clustering API over the B200 engine.
+
+Function names, argument meaning and return conventions follow the reference
+(DefineStructure/color_comm.h, basic_comm.h, coloring.h, basic_util.h); the
+work runs in libgrappolo_b200.so on the GPU.  Differences that a Python
+caller sees:
+
+* ``graph`` arguments are :class:`grappolo_b200.graphs.CSRGraph` (or
+  :class:`Graph`), not freed by the call;
+* results the reference returns through pointers are returned as values;
+* ``nThreads`` selects the schedule: 1 -> verify mode (the reference's
+  one-thread results, bit for bit), >1 -> fast mode (parallel colouring and
+  atomic accumulation).  ``GRAPPOLO_B200_MODE=verify|fast`` overrides it.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+import os
+
+import numpy as np
+
+from . import _lib
+from .graphs import CSRGraph
+
+_P = ct.POINTER
+
+
+def _mode(n_threads: int) -> int:
+    env = os.environ.get('GRAPPOLO_B200_MODE', '').lower()
+    if env == 'verify':
+        return _lib.GLV_MODE_VERIFY
+    if env == 'fast':
+        return _lib.GLV_MODE_FAST
+    return _lib.GLV_MODE_VERIFY if n_threads <= 1 else _lib.GLV_MODE_FAST
+
+
+class Graph:
+    """A ``graph`` struct (DefineStructure/defs.h:85-92) backed by numpy arrays."""
+
+    EDGE = np.dtype([('head', '<i8'), ('tail', '<i8'), ('weight', '<f8')])
+
+    def __init__(self, g: CSRGraph):
+        self.csr = g
+        self.ptr = np.ascontiguousarray(g.ptr, dtype=np.int64)
+        self.edges = np.empty(g.nnz, dtype=self.EDGE)
+        self.edges['head'] = g.heads()
+        self.edges['tail'] = g.tail
+        self.edges['weight'] = g.weight
+        self.struct = _lib.GlvGraph(g.num_vertices, g.num_vertices, g.num_edges,
+                                    self.ptr.ctypes.data_as(_P(ct.c_long)),
+                                    self.edges.ctypes.data_as(_P(_lib.GlvEdge)))
+
+    @property
+    def numVertices(self) -> int:
+        return self.csr.num_vertices
+
+
+def _as_graph(g) -> Graph:
+    return g if isinstance(g, Graph) else Graph(g)
+
+
+def runMultiPhaseColoring(G, C_orig=None, coloring=1, numColors=16, replaceMap=0,
+                          minGraphSize=1000, threshold=1e-6, C_threshold=1e-4, numThreads=1,
+                          threadsOpt=1, stats: bool = False):
+    """Coloring/runMultiPhaseColoring.cpp:51 — returns C_orig (int64[NV]); with
+    ``stats`` also the run statistics (phases, iterations, "Final modularity"...)."""
+    G = _as_graph(G)
+    nv = G.numVertices
+    if C_orig is None:
+        C_orig = np.full(nv, -1, dtype=np.int64)
+    st = _lib.GlvRunStats()
+    _lib.check(_lib.lib().glv_run_multiphase_coloring(
+        ct.byref(G.struct), C_orig.ctypes.data_as(_P(ct.c_long)), coloring, numColors,
+        replaceMap, minGraphSize, threshold, C_threshold, _mode(numThreads), ct.byref(st)))
+    return (C_orig, st.to_dict()) if stats else C_orig
+
+
+def runMultiPhaseBasic(G, C_orig=None, basicOpt=0, minGraphSize=1000, threshold=1e-6,
+                       C_threshold=1e-4, numThreads=1, threadsOpt=1, stats: bool = False):
+    """BasicCommunitiesDetection/runMultiPhaseBasic.cpp:52."""
+    G = _as_graph(G)
+    nv = G.numVertices
+    if C_orig is None:
+        C_orig = np.full(nv, -1, dtype=np.int64)
+    st = _lib.GlvRunStats()
+    _lib.check(_lib.lib().glv_run_multiphase_basic(
+        ct.byref(G.struct), C_orig.ctypes.data_as(_P(ct.c_long)), basicOpt, minGraphSize,
+        threshold, C_threshold, _mode(numThreads), ct.byref(st)))
+    return (C_orig, st.to_dict()) if stats else C_orig
+
+
+def algoLouvainWithDistOneColoring(G, color, numColor, Lower=-1.0, thresh=1e-4, nThreads=1):
+    """Coloring/parallelLouvainWithColoring.cpp:47 — returns (prevMod, C, numItr, totTime)."""
+    G = _as_graph(G)
+    C = np.zeros(G.numVertices, dtype=np.int64)
+    col = np.ascontiguousarray(color, dtype=np.int32)
+    q, itr, tt = ct.c_double(0), ct.c_int(0), ct.c_double(0)
+    _lib.check(_lib.lib().glv_louvain_coloring_phase(
+        ct.byref(G.struct), C.ctypes.data_as(_P(ct.c_long)), col.ctypes.data_as(_P(ct.c_int)),
+        numColor, Lower, thresh, _mode(nThreads), ct.byref(q), ct.byref(itr), ct.byref(tt)))
+    return q.value, C, itr.value, tt.value
+
+
+def parallelLouvianMethod(G, Lower=-1.0, thresh=1e-6, nThreads=1):
+    """BasicCommunitiesDetection/parallelLouvainMethod.cpp:65 — (prevMod, C, numItr, totTime)."""
+    G = _as_graph(G)
+    C = np.zeros(G.numVertices, dtype=np.int64)
+    q, itr, tt = ct.c_double(0), ct.c_int(0), ct.c_double(0)
+    _lib.check(_lib.lib().glv_louvain_basic_phase(
+        ct.byref(G.struct), C.ctypes.data_as(_P(ct.c_long)), Lower, thresh, _mode(nThreads),
+        ct.byref(q), ct.byref(itr), ct.byref(tt)))
+    return q.value, C, itr.value, tt.value
+
+
+def algoDistanceOneVertexColoringOpt(G, nThreads=1):
+    """Coloring/coloringDistanceOne.cpp:50 — returns (vtxColor int32[NV], maxColor, totTime)."""
+    G = _as_graph(G)
+    col = np.full(G.numVertices, -1, dtype=np.int32)
+    mc, tt = ct.c_int(0), ct.c_double(0)
+    _lib.check(_lib.lib().glv_distance_one_coloring(
+        ct.byref(G.struct), col.ctypes.data_as(_P(ct.c_int)), _mode(nThreads), ct.byref(mc),
+        ct.byref(tt)))
+    return col, mc.value, tt.value
+
+
+def renumberClustersContiguously(C):
+    """Utility/buildNextPhase.cpp:48 — returns (renumbered C, numUniqueClusters)."""
+    C = np.array(C, dtype=np.int64, copy=True)
+    n = ct.c_long(0)
+    _lib.check(_lib.lib().glv_renumber_clusters(C.ctypes.data_as(_P(ct.c_long)), C.shape[0],
+                                                ct.byref(n)))
+    return C, n.value
+
+
+def buildNextLevelGraphOpt(G, C, numUniqueClusters, nThreads=1):
+    """Utility/buildNextPhase.cpp:83 — returns (CSRGraph of the next level, numEdges)."""
+    G = _as_graph(G)
+    C = np.ascontiguousarray(C, dtype=np.int64)
+    out = _lib.GlvGraph()
+    tt = ct.c_double(0)
+    L = _lib.lib()
+    _lib.check(L.glv_build_next_level(ct.byref(G.struct), ct.byref(out),
+                                      C.ctypes.data_as(_P(ct.c_long)), numUniqueClusters,
+                                      _mode(nThreads), ct.byref(tt)))
+    nv = out.numVertices
+    ptr = np.ctypeslib.as_array(out.edgeListPtrs, (nv + 1,)).copy()
+    nnz = int(ptr[-1])
+    libc = ct.CDLL(None)
+    if nnz:
+        raw = np.ctypeslib.as_array(ct.cast(out.edgeList, _P(ct.c_char)), (nnz * 24,))
+        rec = np.frombuffer(raw.tobytes(), dtype=Graph.EDGE)
+        heads = rec['head'].copy()
+        tail = rec['tail'].copy()
+        w = rec['weight'].copy()
+    else:
+        heads = tail = np.zeros(0, dtype=np.int64)
+        w = np.zeros(0)
+    libc.free(ct.cast(out.edgeListPtrs, ct.c_void_p))
+    libc.free(ct.cast(out.edgeList, ct.c_void_p))
+    expect = np.repeat(np.arange(nv, dtype=np.int64), np.diff(ptr))
+    if not np.array_equal(heads, expect):
+        raise RuntimeError('coarse graph head/row mismatch')
+    return CSRGraph(ptr, tail, w), out.numEdges
+
+
+def modularity(G, C) -> float:
+    """Q of an assignment, the formula of Coloring/parallelLouvainWithColoring.cpp:226-249
+    (the reference's computeModularity is an unimplemented stub)."""
+    G = _as_graph(G)
+    C = np.ascontiguousarray(C, dtype=np.int64)
+    q = ct.c_double(0)
+    _lib.check(_lib.lib().glv_modularity(ct.byref(G.struct), C.ctypes.data_as(_P(ct.c_long)),
+                                         ct.byref(q)))
+    return q.value
+
+
+def decide_batch(g: CSRGraph, C, vDeg, cDeg, cSize, constant, verts):
+    """Move decisions for `verts` against one fixed state (buildLocalMapCounter + max,
+    Utility/utilityClusteringFunctions.cpp:172-194,226-259)."""
+    p = np.ascontiguousarray(g.ptr, dtype=np.int64)
+    t = np.ascontiguousarray(g.tail, dtype=np.int64)
+    w = np.ascontiguousarray(g.weight, dtype=np.float64)
+    C = np.ascontiguousarray(C, dtype=np.int64)
+    vd = np.ascontiguousarray(vDeg, dtype=np.float64)
+    cd = np.ascontiguousarray(cDeg, dtype=np.float64)
+    cs = np.ascontiguousarray(cSize, dtype=np.int64)
+    vs = np.ascontiguousarray(verts, dtype=np.int64)
+    out = np.zeros(vs.shape[0], dtype=np.int64)
+    lp = lambda a: a.ctypes.data_as(_P(ct.c_long))  # noqa: E731
+    dp = lambda a: a.ctypes.data_as(_P(ct.c_double))  # noqa: E731
+    _lib.check(_lib.lib().glv_decide_batch(g.num_vertices, lp(p), lp(t), dp(w), lp(C), dp(vd),
+                                           dp(cd), lp(cs), constant, vs.shape[0], lp(vs),
+                                           lp(out)))
+    return out
+
+
+def run_multiphase_csr(g: CSRGraph, coloring: bool = True, minGraphSize=1000, threshold=1e-6,
+                       C_threshold=1e-4, mode: int = _lib.GLV_MODE_VERIFY):
+    """SoA host entry (glv_run_multiphase_*_csr): returns (C_orig, stats dict)."""
+    p = np.ascontiguousarray(g.ptr, dtype=np.int64)
+    t = np.ascontiguousarray(g.tail, dtype=np.int64)
+    w = np.ascontiguousarray(g.weight, dtype=np.float64)
+    C = np.full(g.num_vertices, -1, dtype=np.int64)
+    st = _lib.GlvRunStats()
+    L = _lib.lib()
+    lp = lambda a: a.ctypes.data_as(_P(ct.c_long))  # noqa: E731
+    if coloring:
+        rc = L.glv_run_multiphase_coloring_csr(g.num_vertices, lp(p), lp(t),
+                                               w.ctypes.data_as(_P(ct.c_double)), lp(C),
+                                               minGraphSize, threshold, C_threshold, mode,
+                                               ct.byref(st))
+    else:
+        rc = L.glv_run_multiphase_basic_csr(g.num_vertices, lp(p), lp(t),
+                                            w.ctypes.data_as(_P(ct.c_double)), lp(C), threshold,
+                                            mode, ct.byref(st))
+    _lib.check(rc)
+    return C, st.to_dict()
+
+
+def run_multiphase_device(nv, d_ptr, d_tail, d_weight, d_C_orig, coloring=True,
+                          minGraphSize=1000, threshold=1e-6, C_threshold=1e-4,
+                          mode: int = _lib.GLV_MODE_FAST, stream=0):
+    """Device-resident entry (glv_dev_run_multiphase): pointers are ints (e.g.
+    torch ``tensor.data_ptr()``): ptr int64[nv+1], tail int32, weight f64, C_orig int32."""
+    st = _lib.GlvRunStats()
+    _lib.check(_lib.lib().glv_dev_run_multiphase(nv, d_ptr, d_tail, d_weight, d_C_orig,
+                                                 1 if coloring else 0, minGraphSize, threshold,
+                                                 C_threshold, mode, stream or None,
+                                                 ct.byref(st)))
+    return st.to_dict()

@@ -1,0 +1,181 @@
+/*
+ * grappolo_b200 — C ABI of the B200 Louvain engine.
+ *
+ * Plain pointers and sizes only; every entry point returns a status code
+ * (GLV_OK on success) and never aborts the process.  Host-buffer entry points
+ * copy their inputs to the GPU and their results back before returning; the
+ * glv_dev_* entry points take device pointers and run on the given CUDA stream.
+ *
+ * Each entry point names the reference interface it replaces
+ * (Grappolo, DefineStructure/*.h).  The reference's C++ signatures themselves
+ * are exported by the same library (include/grappolo_compat.h) as thin
+ * wrappers over these functions.
+ */
+#ifndef GRAPPOLO_B200_H
+#define GRAPPOLO_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Same layout as Grappolo's `edge` and `graph` (DefineStructure/defs.h:78-92). */
+typedef struct glv_edge {
+  long head;
+  long tail;
+  double weight;
+} glv_edge;
+
+typedef struct glv_graph {
+  long numVertices;
+  long sVertices;
+  long numEdges;       /* undirected edges, self-loops counted once */
+  long *edgeListPtrs;  /* [numVertices+1] row offsets */
+  glv_edge *edgeList;  /* [edgeListPtrs[numVertices]] entries */
+} glv_graph;
+
+enum {
+  GLV_OK = 0,
+  GLV_ERR_ARG = 1,        /* invalid argument (sizes, ids out of range, NULL) */
+  GLV_ERR_CUDA = 2,       /* a CUDA call failed */
+  GLV_ERR_OOM = 3,        /* device or host allocation failed */
+  GLV_ERR_COLORS = 4,     /* a colouring needed >= 4096 colours (coloringUtils.cpp:57-60) */
+  GLV_ERR_TOO_LARGE = 5,  /* numVertices >= 2^31 (ids are int32 on the device) */
+  GLV_ERR_UNSUPPORTED = 6,/* option outside this engine's scope (e.g. coloring 2/3, replaceMap) */
+  GLV_ERR_NO_DEVICE = 7,  /* no CUDA device */
+  GLV_ERR_LIMIT = 8       /* a size exceeds a fixed limit of the entry point */
+};
+
+/* Execution modes.
+ * GLV_MODE_VERIFY reproduces the reference's one-thread schedule: sequential
+ *   greedy colouring in vertex order, community totals and coarse weights
+ *   folded in the reference's order.  Results are bit-identical to the
+ *   reference run with OMP_NUM_THREADS=1.
+ * GLV_MODE_FAST uses hash-priority colouring and atomic accumulation, like the
+ *   reference run with many threads: results are valid Louvain results but not
+ *   bit-identical (final modularity agrees to about 1e-3).
+ * With integral edge weights (total < 2^53) every accumulation is exact in any
+ * order, so the modes differ only in the colouring. */
+enum { GLV_MODE_VERIFY = 0, GLV_MODE_FAST = 1 };
+
+#define GLV_MAX_PHASES 256
+
+typedef struct glv_phase_stats {
+  long num_vertices;   /* level graph */
+  long nnz;            /* CSR entries of the level graph */
+  int colored;         /* 1: colour-class sweep phase, 0: Jacobi phase */
+  int recolored;       /* colouring computed for this level (0: reused) */
+  int num_colors;
+  int iterations;
+  double modularity;   /* value the phase returned */
+  long clusters;       /* after renumbering */
+  double time_sweep;   /* s, local moving + modularity */
+  double time_color;   /* s */
+  double time_coarsen; /* s, renumbering + next-level build */
+  double edges_swept;  /* CSR entries evaluated by local moving */
+} glv_phase_stats;
+
+typedef struct glv_run_stats {
+  int phases;               /* reference's phase counter at exit */
+  int total_iterations;
+  long final_clusters;      /* reference's "Final number of clusters" */
+  double final_modularity;  /* reference's "Final modularity" (prevMod at exit) */
+  double time_total;        /* s, whole call incl. transfers */
+  double time_clustering;   /* s */
+  double time_coloring;     /* s */
+  double time_building;     /* s */
+  double time_transfer;     /* s, host<->device copies */
+  double edges_swept;       /* sum over phases */
+  long kernel_launches;     /* kernels this call launched */
+  int nphase;               /* entries filled in phase[] */
+  glv_phase_stats phase[GLV_MAX_PHASES];
+} glv_run_stats;
+
+/* ---- multiphase drivers ------------------------------------------------- */
+
+/* Replaces runMultiPhaseColoring (Coloring/runMultiPhaseColoring.cpp:51-238,
+ * declared DefineStructure/color_comm.h:7-8).  coloring must be 1 (distance-1
+ * colouring); replaceMap must be 0.  C_orig[numVertices] receives the final
+ * community of every input vertex (-1 for isolated vertices).  Unlike the
+ * reference, G is not freed.  `stats` may be NULL. */
+int glv_run_multiphase_coloring(const glv_graph *G, long *C_orig, int coloring, int numColors,
+                                int replaceMap, long minGraphSize, double threshold,
+                                double C_threshold, int mode, glv_run_stats *stats);
+
+/* Replaces runMultiPhaseBasic (BasicCommunitiesDetection/runMultiPhaseBasic.cpp:52-170,
+ * basic_comm.h:5-6) for basicOpt = 0. */
+int glv_run_multiphase_basic(const glv_graph *G, long *C_orig, int basicOpt, long minGraphSize,
+                             double threshold, double C_threshold, int mode,
+                             glv_run_stats *stats);
+
+/* Struct-of-arrays host variant of glv_run_multiphase_coloring: ptr int64[nv+1],
+ * tail int64[nnz], weight f64[nnz]. */
+int glv_run_multiphase_coloring_csr(long nv, const long *ptr, const long *tail,
+                                    const double *weight, long *C_orig, long minGraphSize,
+                                    double threshold, double C_threshold, int mode,
+                                    glv_run_stats *stats);
+
+int glv_run_multiphase_basic_csr(long nv, const long *ptr, const long *tail, const double *weight,
+                                 long *C_orig, double threshold, int mode, glv_run_stats *stats);
+
+/* Device-resident variant: d_ptr int64[nv+1], d_tail int32[nnz], d_weight
+ * f64[nnz] and d_C_orig int32[nv] are device pointers; `stream` is a
+ * cudaStream_t (NULL = legacy default stream).  The input graph is not
+ * modified.  `coloring` = 1 runs the colouring driver, 0 the basic one. */
+int glv_dev_run_multiphase(long nv, const long *d_ptr, const int *d_tail, const double *d_weight,
+                           int *d_C_orig, int coloring, long minGraphSize, double threshold,
+                           double C_threshold, int mode, void *stream, glv_run_stats *stats);
+
+/* ---- single phases and primitives (host buffers) ------------------------ */
+
+/* Replaces algoLouvainWithDistOneColoring (Coloring/parallelLouvainWithColoring.cpp:47-286,
+ * color_comm.h:10-11).  C[numVertices] is overwritten with the state after the
+ * last sweep; *mod receives the returned prevMod. */
+int glv_louvain_coloring_phase(const glv_graph *G, long *C, const int *color, int numColor,
+                               double Lower, double thresh, int mode, double *mod, int *numItr,
+                               double *totTime);
+
+/* Replaces parallelLouvianMethod (BasicCommunitiesDetection/parallelLouvainMethod.cpp:65-326,
+ * basic_comm.h:21-22). */
+int glv_louvain_basic_phase(const glv_graph *G, long *C, double Lower, double thresh, int mode,
+                            double *mod, int *numItr, double *totTime);
+
+/* Replaces algoDistanceOneVertexColoringOpt (Coloring/coloringDistanceOne.cpp:50-233,
+ * coloring.h:8).  *maxColor receives the largest colour (the reference's
+ * return value). */
+int glv_distance_one_coloring(const glv_graph *G, int *vtxColor, int mode, int *maxColor,
+                              double *totTime);
+
+/* Replaces renumberClustersContiguously (Utility/buildNextPhase.cpp:48-79,
+ * basic_util.h:5). */
+int glv_renumber_clusters(long *C, long size, long *numClusters);
+
+/* Replaces buildNextLevelGraphOpt (Utility/buildNextPhase.cpp:83-255,
+ * basic_util.h:6).  Gout->edgeListPtrs and Gout->edgeList are malloc'd and
+ * owned by the caller (release with free()). */
+int glv_build_next_level(const glv_graph *Gin, glv_graph *Gout, const long *C,
+                         long numUniqueClusters, int mode, double *totTime);
+
+/* Modularity of an assignment over a graph: the formula of
+ * Coloring/parallelLouvainWithColoring.cpp:226-249, standing in for the
+ * unimplemented computeModularity (Utility/utilityClusterComparisonMetrics.cpp:409-411). */
+int glv_modularity(const glv_graph *G, const long *C, double *mod);
+
+/* Move decisions of a vertex list against one fixed state — the unit
+ * buildLocalMapCounter + max compute for one vertex
+ * (Utility/utilityClusteringFunctions.cpp:172-194,226-259).  Host buffers
+ * (SoA CSR, int64 ids).  targets[k] receives the decision for verts[k]. */
+int glv_decide_batch(long nv, const long *ptr, const long *tail, const double *weight,
+                     const long *C, const double *vDeg, const double *cDeg, const long *cSize,
+                     double constant, long nverts, const long *verts, long *targets);
+
+/* ---- library information ------------------------------------------------ */
+const char *glv_version(void);
+const char *glv_last_error(void);
+/* Kernel launches issued by this library since load (all entry points). */
+long glv_kernel_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GRAPPOLO_B200_H */

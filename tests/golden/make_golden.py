@@ -1,0 +1,125 @@
+"""Generate the golden fixtures from Grappolo's own code (oracle/_ref, one thread).
+
+Run from the repository root after ``make -C oracle``:
+
+    python tests/golden/make_golden.py [/path/to/grappolo]
+
+Each fixture ``<case>.npz`` holds an input CSR and what the reference's
+functions return for it at OMP_NUM_THREADS=1: the distance-1 colouring, one
+colour phase, one Jacobi phase, renumbering, the next-level graph, the move
+decisions of a seeded state, and both multiphase drivers (C_orig plus the
+printed summary).  ``pins.json`` records the 100k-vertex planted-partition
+run (too large to store) as a digest of C_orig and its summary.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from grappolo_b200 import graphs  # noqa: E402
+from oracle import Reference  # noqa: E402
+
+
+def edge_cases():
+    cases = {}
+    cases['pair'] = graphs.from_edges(2, [(0, 1)])
+    cases['loops_isolated'] = graphs.from_edges(
+        9, [(0, 1), (1, 2), (2, 0), (2, 2), (3, 4), (4, 4), (5, 6), (6, 7), (7, 5), (0, 0)],
+        weights=[1, 2, 1, 3, 1, 2, 1, 1, 1, 0.5])
+    cases['cycle4_ties'] = graphs.from_edges(4, [(0, 1), (1, 2), (2, 3), (3, 0)])
+    rng = np.random.default_rng(11)
+    # hub of degree 5000 (global-table bin) and one of degree 400 (block bin)
+    nv = 5402
+    e = [(0, i) for i in range(1, 5001)] + [(5001, 5001 + i) for i in range(1, 401)]
+    e += [tuple(x) for x in rng.integers(1, 5001, size=(3000, 2))]
+    e += [(0, 5001)]
+    cases['hubs'] = graphs.from_edges(nv, e)
+    cases['hubs_w'] = graphs.random_weights(cases['hubs'], seed=5)
+    return cases
+
+
+def all_cases(ref_root):
+    cases = {}
+    cases['karate'] = Reference().load_metis(os.path.join(ref_root, 'karate.graph'))
+    cases['pp1000'] = graphs.planted_partition(num_blocks=20, block_size=50, intra_degree=10,
+                                               inter_degree=3, seed=2)
+    cases['pp1000_w'] = graphs.random_weights(cases['pp1000'], seed=3)
+    cases['rmat10'] = graphs.rmat(10, seed=4)
+    cases.update(edge_cases())
+    return cases
+
+
+def seeded_state(g, rng):
+    """A community state reachable by moves: random merges of neighbours."""
+    nv = g.num_vertices
+    C = np.arange(nv, dtype=np.int64)
+    heads = g.heads()
+    pick = rng.random(g.nnz) < 0.3
+    for h, t in zip(heads[pick], g.tail[pick]):
+        C[t] = C[h]
+    vdeg = np.array([g.weight[g.ptr[i]:g.ptr[i + 1]].sum() for i in range(nv)])
+    cdeg = np.zeros(nv)
+    csize = np.zeros(nv, dtype=np.int64)
+    for i in range(nv):
+        cdeg[C[i]] += vdeg[i]
+        csize[C[i]] += 1
+    return C, vdeg, cdeg, csize
+
+
+def make_case(R, g, rng):
+    out = dict(ptr=g.ptr, tail=g.tail, weight=g.weight)
+    col, mc, _ = R.color(g)
+    out.update(color=col, max_color=mc)
+    q, C, itr, _ = R.coloring_phase(g, col, mc + 1, -1.0, 1e-4)
+    out.update(cphase_mod=q, cphase_C=C, cphase_itr=itr)
+    q, Cb, itr, _ = R.basic_phase(g, -1.0, 1e-6)
+    out.update(bphase_mod=q, bphase_C=Cb, bphase_itr=itr)
+    Cr, ncl = R.renumber(C)
+    out.update(renum_C=Cr, renum_n=ncl)
+    cg, ne = R.build_next_level(g, Cr, ncl)
+    out.update(coarse_ptr=cg.ptr, coarse_tail=cg.tail, coarse_weight=cg.weight, coarse_ne=ne)
+    Cs, vdeg, cdeg, csize = seeded_state(g, rng)
+    _, const = R.vertex_degrees(g)
+    verts = np.arange(g.num_vertices, dtype=np.int64)
+    tg = R.decide_batch(g, Cs, vdeg, cdeg, csize, const, verts)
+    out.update(state_C=Cs, state_vdeg=vdeg, state_cdeg=cdeg, state_csize=csize,
+               state_const=const, state_targets=tg)
+    Co, s, _ = R.run_multiphase_coloring(g, 1000, 1e-6, 1e-4)
+    out.update(mpc_C=Co, mpc_phases=s['phases'], mpc_itr=s['total_iterations'],
+               mpc_clusters=s['final_clusters'], mpc_mod=s['final_mod'])
+    Cb2, s2, _ = R.run_multiphase_basic(g, 1e-6)
+    out.update(mpb_C=Cb2, mpb_phases=s2['phases'], mpb_itr=s2['total_iterations'],
+               mpb_clusters=s2['final_clusters'], mpb_mod=s2['final_mod'])
+    return out
+
+
+def main():
+    ref_root = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+    R = Reference()
+    rng = np.random.default_rng(2024)
+    for name, g in all_cases(ref_root).items():
+        np.savez_compressed(os.path.join(HERE, f'{name}.npz'), **make_case(R, g, rng))
+        print('wrote', name, g.num_vertices, g.nnz)
+    pins = {}
+    for name, g in [('planted_100k', graphs.planted_partition()),
+                    ('planted_100k_w', graphs.random_weights(graphs.planted_partition()))]:
+        Co, s, _ = R.run_multiphase_coloring(g, 1000, 1e-6, 1e-4)
+        pins[name] = dict(c_orig_sha256=hashlib.sha256(Co.astype('<i8').tobytes()).hexdigest(),
+                          phases=s['phases'], total_iterations=s['total_iterations'],
+                          final_clusters=s['final_clusters'], final_mod=s['final_mod'],
+                          colors=s['colors_per_phase'], clusters=s['clusters_per_phase'])
+        print('pinned', name, pins[name])
+    with open(os.path.join(HERE, 'pins.json'), 'w') as f:
+        json.dump(pins, f, indent=1)
+
+
+if __name__ == '__main__':
+    main()

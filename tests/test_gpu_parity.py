@@ -1,0 +1,177 @@
+"""GPU path vs the reference (golden fixtures) and the oracle, through the C ABI.
+
+Verify mode (nThreads=1) must be bit-identical to the reference run at one
+thread: colourings, move decisions, phase results, renumbering, coarse graphs
+and the multiphase community arrays.  Fast mode must give a proper colouring
+and a final modularity within 1e-3 (absolute) of the reference's.
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+from grappolo_b200 import graphs, louvain
+from _golden import CASES, load, pins
+
+pytestmark = pytest.mark.gpu
+
+FAST_Q_TOL = 1e-3       # fast mode: |Q_gpu - Q_ref| (absolute)
+MOD_REL_TOL = 1e-9      # verify mode Q on non-integral weights (reduction order)
+
+
+def _proper(g, col):
+    heads = g.heads()
+    off = heads != g.tail
+    return not np.any(col[heads[off]] == col[g.tail[off]])
+
+
+@pytest.mark.parametrize('name', CASES)
+def test_coloring_verify(name):
+    g, z = load(name)
+    col, mc, _ = louvain.algoDistanceOneVertexColoringOpt(g, nThreads=1)
+    assert mc == z['max_color']
+    assert np.array_equal(col, z['color'])
+
+
+@pytest.mark.parametrize('name', CASES)
+def test_coloring_fast_is_proper(name):
+    g, _ = load(name)
+    col, mc, _ = louvain.algoDistanceOneVertexColoringOpt(g, nThreads=8)
+    assert col.min() >= 0 and col.max() == mc
+    assert _proper(g, col)
+
+
+@pytest.mark.parametrize('name', CASES)
+def test_decisions(name):
+    g, z = load(name)
+    verts = np.arange(g.num_vertices)
+    tg = louvain.decide_batch(g, z['state_C'], z['state_vdeg'], z['state_cdeg'],
+                              z['state_csize'], float(z['state_const']), verts)
+    assert np.array_equal(tg, z['state_targets'])
+
+
+@pytest.mark.parametrize('name', CASES)
+def test_coloring_phase(name):
+    g, z = load(name)
+    q, C, itr, _ = louvain.algoLouvainWithDistOneColoring(g, z['color'], int(z['max_color']) + 1,
+                                                          -1.0, 1e-4, nThreads=1)
+    assert itr == z['cphase_itr']
+    assert np.array_equal(C, z['cphase_C'])
+    assert q == pytest.approx(float(z['cphase_mod']), rel=MOD_REL_TOL, abs=1e-15)
+
+
+@pytest.mark.parametrize('name', CASES)
+def test_basic_phase(name):
+    g, z = load(name)
+    q, C, itr, _ = louvain.parallelLouvianMethod(g, -1.0, 1e-6, nThreads=1)
+    assert itr == z['bphase_itr']
+    assert np.array_equal(C, z['bphase_C'])
+    assert q == pytest.approx(float(z['bphase_mod']), rel=MOD_REL_TOL, abs=1e-15)
+
+
+@pytest.mark.parametrize('name', CASES)
+def test_renumber(name):
+    _, z = load(name)
+    Cr, n = louvain.renumberClustersContiguously(z['cphase_C'])
+    assert n == z['renum_n']
+    assert np.array_equal(Cr, z['renum_C'])
+
+
+@pytest.mark.parametrize('name', CASES)
+def test_coarsen(name):
+    g, z = load(name)
+    cg, ne = louvain.buildNextLevelGraphOpt(g, z['renum_C'], int(z['renum_n']), nThreads=1)
+    assert ne == z['coarse_ne']
+    assert np.array_equal(cg.ptr, z['coarse_ptr'])
+    assert np.array_equal(cg.tail, z['coarse_tail'])
+    assert np.array_equal(cg.weight, z['coarse_weight'])
+
+
+@pytest.mark.parametrize('name', CASES)
+def test_multiphase_coloring_verify(name):
+    g, z = load(name)
+    C, st = louvain.runMultiPhaseColoring(g, numThreads=1, stats=True)
+    assert np.array_equal(C, z['mpc_C'])
+    assert (st['phases'], st['total_iterations'], st['final_clusters']) == \
+        (z['mpc_phases'], z['mpc_itr'], z['mpc_clusters'])
+    assert abs(st['final_modularity'] - z['mpc_mod']) <= 5e-7  # reference prints %lf
+    assert st['kernel_launches'] > 0
+
+
+@pytest.mark.parametrize('name', CASES)
+def test_multiphase_basic_verify(name):
+    g, z = load(name)
+    C, st = louvain.runMultiPhaseBasic(g, numThreads=1, stats=True)
+    assert np.array_equal(C, z['mpb_C'])
+    assert (st['phases'], st['total_iterations'], st['final_clusters']) == \
+        (z['mpb_phases'], z['mpb_itr'], z['mpb_clusters'])
+    assert abs(st['final_modularity'] - z['mpb_mod']) <= 5e-7
+
+
+@pytest.mark.parametrize('name', ['planted_100k', 'planted_100k_w'])
+def test_pinned_100k(name, oracle):
+    g = graphs.planted_partition()
+    if name.endswith('_w'):
+        g = graphs.random_weights(g)
+    pin = pins()[name]
+    C, st = louvain.runMultiPhaseColoring(g, numThreads=1, stats=True)
+    assert hashlib.sha256(C.astype('<i8').tobytes()).hexdigest() == pin['c_orig_sha256']
+    assert st['phases'] == pin['phases'] and st['total_iterations'] == pin['total_iterations']
+    assert [p['clusters'] for p in st['phase']] == pin['clusters']
+    Co, so, _ = oracle.run_multiphase_coloring(g)
+    assert st['final_modularity'] == pytest.approx(so['final_mod'], rel=MOD_REL_TOL)
+
+
+@pytest.mark.parametrize('seed', [1, 2])
+def test_fast_mode_modularity(seed, oracle):
+    g = graphs.planted_partition(seed=seed)
+    C, st = louvain.runMultiPhaseColoring(g, numThreads=8, stats=True)
+    _, so, _ = oracle.run_multiphase_coloring(g)
+    assert abs(st['final_modularity'] - so['final_mod']) <= FAST_Q_TOL
+    q_gpu = oracle.modularity(g, C)
+    q_ref = oracle.modularity(g, oracle.run_multiphase_coloring(g)[0])
+    assert abs(q_gpu - q_ref) <= FAST_Q_TOL
+
+
+def test_rmat_verify_vs_oracle(oracle):
+    g = graphs.rmat(14, seed=9)
+    C, st = louvain.runMultiPhaseColoring(g, numThreads=1, stats=True)
+    Co, so, recs = oracle.run_multiphase_coloring(g)
+    assert np.array_equal(C, Co)
+    assert st['total_iterations'] == so['total_iterations']
+    assert [p['clusters'] for p in st['phase']] == [r.clusters for r in recs]
+
+
+def test_soa_entry_matches_aos():
+    g = graphs.rmat(12, seed=5)
+    C1 = louvain.runMultiPhaseColoring(g, numThreads=1)
+    C2, _ = louvain.run_multiphase_csr(g, coloring=True)
+    assert np.array_equal(C1, C2)
+    C3 = louvain.runMultiPhaseBasic(g, numThreads=1)
+    C4, _ = louvain.run_multiphase_csr(g, coloring=False)
+    assert np.array_equal(C3, C4)
+
+
+def test_device_entry_matches_host():
+    import torch
+    g = graphs.rmat(12, seed=6)
+    dev = torch.device('cuda:0')
+    ptr = torch.from_numpy(g.ptr).to(dev)
+    tail = torch.from_numpy(g.tail.astype(np.int32)).to(dev)
+    w = torch.from_numpy(g.weight).to(dev)
+    C = torch.full((g.num_vertices,), -1, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+    st = louvain.run_multiphase_device(g.num_vertices, ptr.data_ptr(), tail.data_ptr(),
+                                       w.data_ptr(), C.data_ptr(), coloring=True,
+                                       mode=0)
+    torch.cuda.synchronize()
+    C_host = louvain.runMultiPhaseColoring(g, numThreads=1)
+    assert np.array_equal(C.cpu().numpy().astype(np.int64), C_host)
+    assert st['phases'] >= 1
+
+
+def test_modularity_matches_oracle(oracle):
+    for name in ['karate', 'pp1000_w', 'rmat10']:
+        g, z = load(name)
+        q = louvain.modularity(g, z['mpc_C'])
+        assert q == pytest.approx(oracle.modularity(g, z['mpc_C']), rel=MOD_REL_TOL, abs=1e-15)

@@ -1,0 +1,86 @@
+"""The C oracle against the golden fixtures generated by the reference itself."""
+import hashlib
+
+import numpy as np
+import pytest
+
+from grappolo_b200 import graphs
+from _golden import CASES, load, pins
+
+
+@pytest.mark.parametrize('name', CASES)
+def test_coloring(oracle, name):
+    g, z = load(name)
+    col, mc = oracle.color_greedy(g)
+    assert mc == z['max_color']
+    assert np.array_equal(col, z['color'])
+
+
+@pytest.mark.parametrize('name', CASES)
+def test_coloring_phase(oracle, name):
+    g, z = load(name)
+    q, C, itr, _ = oracle.coloring_phase(g, z['color'], int(z['max_color']) + 1, -1.0, 1e-4)
+    assert itr == z['cphase_itr']
+    assert q == z['cphase_mod']
+    assert np.array_equal(C, z['cphase_C'])
+
+
+@pytest.mark.parametrize('name', CASES)
+def test_basic_phase(oracle, name):
+    g, z = load(name)
+    q, C, itr, _ = oracle.basic_phase(g, -1.0, 1e-6)
+    assert itr == z['bphase_itr']
+    assert q == z['bphase_mod']
+    assert np.array_equal(C, z['bphase_C'])
+
+
+@pytest.mark.parametrize('name', CASES)
+def test_renumber_and_coarsen(oracle, name):
+    g, z = load(name)
+    Cr, n = oracle.renumber(z['cphase_C'])
+    assert n == z['renum_n']
+    assert np.array_equal(Cr, z['renum_C'])
+    cg, ne = oracle.build_next_level(g, Cr, n)
+    assert ne == z['coarse_ne']
+    assert np.array_equal(cg.ptr, z['coarse_ptr'])
+    assert np.array_equal(cg.tail, z['coarse_tail'])
+    assert np.array_equal(cg.weight, z['coarse_weight'])  # bit-exact FP64
+
+
+@pytest.mark.parametrize('name', CASES)
+def test_decisions(oracle, name):
+    g, z = load(name)
+    verts = np.arange(g.num_vertices)
+    tg = oracle.decide_batch(g, z['state_C'], z['state_vdeg'], z['state_cdeg'], z['state_csize'],
+                             float(z['state_const']), verts)
+    assert np.array_equal(tg, z['state_targets'])
+
+
+@pytest.mark.parametrize('name', CASES)
+def test_multiphase(oracle, name):
+    g, z = load(name)
+    C, s, _ = oracle.run_multiphase_coloring(g, 1000, 1e-6, 1e-4)
+    assert np.array_equal(C, z['mpc_C'])
+    assert (s['phases'], s['total_iterations'], s['final_clusters']) == \
+        (z['mpc_phases'], z['mpc_itr'], z['mpc_clusters'])
+    assert abs(s['final_mod'] - z['mpc_mod']) <= 5e-7  # printed with %lf
+    C, s, _ = oracle.run_multiphase_basic(g, 1e-6)
+    assert np.array_equal(C, z['mpb_C'])
+    assert (s['phases'], s['total_iterations'], s['final_clusters']) == \
+        (z['mpb_phases'], z['mpb_itr'], z['mpb_clusters'])
+    assert abs(s['final_mod'] - z['mpb_mod']) <= 5e-7
+
+
+@pytest.mark.parametrize('name', ['planted_100k', 'planted_100k_w'])
+def test_pinned_100k(oracle, name):
+    g = graphs.planted_partition()
+    if name.endswith('_w'):
+        g = graphs.random_weights(g)
+    pin = pins()[name]
+    C, s, recs = oracle.run_multiphase_coloring(g, 1000, 1e-6, 1e-4)
+    assert hashlib.sha256(C.astype('<i8').tobytes()).hexdigest() == pin['c_orig_sha256']
+    assert s['phases'] == pin['phases'] and s['total_iterations'] == pin['total_iterations']
+    assert s['final_clusters'] == pin['final_clusters']
+    assert abs(s['final_mod'] - pin['final_mod']) <= 5e-7
+    assert [r.num_colors for r in recs if r.colored] == pin['colors']
+    assert [r.clusters for r in recs] == pin['clusters']
