@@ -1,0 +1,341 @@
+#!/usr/bin/env python
+"""Benchmark: plain multiphase Louvain (distance-1 colouring) on an R-MAT graph.
+
+Workload: R-MAT scale 24 (16.7M vertices, edge factor 16, a=.57 b=.19 c=.19),
+symmetrised, self-loops and duplicates removed, FP64 weights uniform in (0,1],
+seeded and generated on the device; coloring=1, threshold 1e-6, C_thresh 1e-4,
+minGraphSize 1000 (the reference's runMultiPhaseColoring configuration).
+
+A step is one full multiphase run (colouring, colour-class sweeps, modularity,
+renumbering, coarsening, every phase) with the graph resident in HBM.  The
+metric is local-move edges/s: CSR entries evaluated by the local-moving sweeps
+over the whole run, divided by the run's device time.  The graph (several GB)
+is larger than L2, so no flush is needed between steps.
+
+--impl reference times Grappolo's own OpenMP code (oracle/_ref, compiled from
+its sources with its shipped flags) on all host cores for the same metric,
+one sweep iteration of phase 1 per step (a bounded sample of the workload).
+
+Multi-GPU (torchrun): the single-graph path does not shard, so every rank runs
+an independent replica (weak scaling); value = all ranks' edges / max time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = 'local-move edges/s'
+UNIT = 'edges/s'
+
+
+def parse_args():
+    p = argparse.ArgumentParser()
+    p.add_argument('--gpus', type=int, default=1)
+    p.add_argument('--steps', type=int, default=5)
+    p.add_argument('--warmup', type=int, default=3)
+    p.add_argument('--impl', choices=['ours', 'reference'], default='ours')
+    p.add_argument('--scale', type=int, default=24)
+    p.add_argument('--mode', choices=['fast', 'verify'], default='fast')
+    p.add_argument('--no-e2e', action='store_true')
+    p.add_argument('--no-cpu-baseline', action='store_true')
+    p.add_argument('--profile-level', type=int, default=1,
+                   help='1: time each class sweep (roofline); 2: time every launch by kind')
+    return p.parse_args()
+
+
+def workload_config(args, nv, nnz, extra=None):
+    cfg = {'workload': f'plain multiphase Louvain (coloring=1) on R-MAT scale {args.scale}',
+           'graph': f'R-MAT scale {args.scale}, edge factor 16, a=0.57 b=0.19 c=0.19, '
+                    f'symmetrised, dedup, no self-loops, FP64 weights U(0,1], seed 1',
+           'num_vertices': nv, 'nnz': nnz, 'threshold': 1e-6, 'C_threshold': 1e-4,
+           'minGraphSize': 1000, 'parallelism': f'replicas x{args.gpus}',
+           'l2': 'inputs larger than L2 (no flush)'}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int):
+        self.f = tempfile.NamedTemporaryFile('w+', suffix='.csv', delete=False)
+        q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+             'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+             'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+        try:
+            self.p = subprocess.Popen(['nvidia-smi', f'--query-gpu={q}', '--format=csv,noheader,nounits',
+                                       '-i', str(index), '-lms', '200'], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['nvidia-smi unavailable']}
+        self.p.terminate()
+        self.p.wait()
+        self.f.seek(0)
+        rows = [r.split(',') for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], None, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+            except (ValueError, IndexError):
+                continue
+            for name, val in zip(names, r[5:9]):
+                if val.lower() == 'active':
+                    reasons.add(name)
+        return {'sm_mhz': statistics.median(sm) if sm else None, 'sm_max_mhz': mx,
+                'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    try:
+        with open(path) as f:
+            return float(json.load(f)['hbm_gbs']), 'measured'
+    except (OSError, KeyError, ValueError):
+        return 6650.0, 'fallback'
+
+
+def profiled_traffic_ratio():
+    """DRAM bytes per algorithmic byte of the sweep kernels, from the committed ncu summary."""
+    path = os.path.join(ROOT, 'profiles', 'sweep_kernels_rmat.txt')
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith('traffic_per_algorithmic_byte'):
+                    return float(line.split('=')[1])
+    except OSError:
+        pass
+    return None
+
+
+# --------------------------------------------------------------------- reference arm
+def run_reference(args, rank):
+    if rank != 0:
+        return 0
+    import numpy as np
+    import torch
+    from grappolo_b200 import graphs
+    from oracle import Reference
+    dev = torch.device('cuda:0') if torch.cuda.is_available() else torch.device('cpu')
+    ptr, tail, w = graphs.rmat_device(args.scale, device=dev)
+    g = graphs.CSRGraph(ptr.cpu().numpy(), tail.cpu().numpy().astype(np.int64), w.cpu().numpy())
+    del ptr, tail, w
+    if dev.type == 'cuda':
+        torch.cuda.empty_cache()
+    cores = os.cpu_count() or 1
+    R = Reference(fast=True)
+    h = R.graph(g)
+    col, mc, tcol = R.color_g(h, g.num_vertices, cores)
+    vals = []
+    for k in range(args.warmup + args.steps):
+        _, _, itr, tt = R.coloring_phase_g(h, g.num_vertices, col, mc + 1, -1.0, float('inf'),
+                                           cores)
+        if k >= args.warmup:
+            vals.append(g.nnz * itr / tt)
+    R.free_graph(h)
+    value = statistics.median(vals)
+    sample = (f'phase-1 colour-class sweep iteration (+modularity) of the reference '
+              f'algoLouvainWithDistOneColoring on the full graph, {cores} OpenMP threads, '
+              f'-Ofast build; its own iteration timer; colouring ({mc + 1} colours, '
+              f'{tcol:.2f} s) done once before')
+    line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'impl': 'reference',
+            'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': 1e3 * g.nnz / value, 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+            'config': workload_config(args, g.num_vertices, g.nnz),
+            'cpu_baseline': {'value': value, 'unit': UNIT, 'cores': cores, 'kind': 'reference',
+                             'sample': sample},
+            'e2e': {'value': value, 'unit': UNIT, 'h2d_bytes_per_step': 0,
+                    'd2h_bytes_per_step': 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------------------- our arm
+def main():
+    args = parse_args()
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if args.impl == 'reference':
+        return run_reference(args, rank)
+    import numpy as np
+    import torch
+    from grappolo_b200 import graphs, louvain, _lib
+    torch.cuda.set_device(local)
+    dev = torch.device('cuda', local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=600),
+                                device_id=dev)
+    L = _lib.lib()
+    mode = _lib.GLV_MODE_FAST if args.mode == 'fast' else _lib.GLV_MODE_VERIFY
+
+    ptr, tail, w = graphs.rmat_device(args.scale, device=dev)
+    nv, nnz = ptr.numel() - 1, tail.numel()
+    C = torch.empty(nv, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+
+    def step(profile=False):
+        L.glv_set_profiling(args.profile_level if profile else 0)
+        st = louvain.run_multiphase_device(nv, ptr.data_ptr(), tail.data_ptr(), w.data_ptr(),
+                                           C.data_ptr(), coloring=True, mode=mode,
+                                           stream=torch.cuda.current_stream().cuda_stream)
+        L.glv_set_profiling(0)
+        return st
+
+    for _ in range(args.warmup):
+        step()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    ev0.record()
+    for _ in range(args.steps):
+        stats.append(step(profile=True))
+    ev1.record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    t = ev0.elapsed_time(ev1) * 1e-3
+    edges = sum(s['edges_swept'] for s in stats)
+    launches = sum(s['kernel_launches'] for s in stats)
+    sweep_t = sum(s['sweep_kernel_time'] for s in stats)
+    sweep_b = sum(s['sweep_bytes'] for s in stats)
+    if dist:
+        tt = torch.tensor([t], dtype=torch.float64, device=dev)
+        ee = torch.tensor([edges], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        dist.all_reduce(ee, op=dist.ReduceOp.SUM)
+        t, edges_all = float(tt), float(ee)
+    else:
+        edges_all = edges
+    value = edges_all / t
+
+    # end to end through the reference-facing API: host AoS graph (pinned),
+    # host->device copy and C_orig read-back inside every step
+    e2e = None
+    if not args.no_e2e:
+        heads = torch.repeat_interleave(torch.arange(nv, device=dev, dtype=torch.int64),
+                                        ptr[1:] - ptr[:-1])
+        aos = torch.empty((nnz, 3), dtype=torch.int64, pin_memory=True)
+        dev_aos = torch.stack([heads, tail.to(torch.int64), w.view(torch.int64)], dim=1)
+        aos.copy_(dev_aos)
+        del dev_aos, heads
+        hptr = ptr.cpu().pin_memory()
+        hC = torch.empty(nv, dtype=torch.int64, pin_memory=True)
+        import ctypes as ct
+        gstruct = _lib.GlvGraph(nv, nv, nnz // 2, ct.cast(hptr.data_ptr(), ct.POINTER(ct.c_long)),
+                                ct.cast(aos.data_ptr(), ct.POINTER(_lib.GlvEdge)))
+
+        def e2e_step():
+            st = _lib.GlvRunStats()
+            _lib.check(L.glv_run_multiphase_coloring(
+                ct.byref(gstruct), ct.cast(hC.data_ptr(), ct.POINTER(ct.c_long)), 1, 16, 0,
+                1000, 1e-6, 1e-4, mode, ct.byref(st)))
+            return st.to_dict()
+
+        e2e_step()
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = time.perf_counter()
+        est = [e2e_step() for _ in range(args.steps)]
+        et = time.perf_counter() - e0
+        ee = sum(s['edges_swept'] for s in est)
+        if dist:
+            tt = torch.tensor([et], dtype=torch.float64, device=dev)
+            eet = torch.tensor([ee], dtype=torch.float64, device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            dist.all_reduce(eet, op=dist.ReduceOp.SUM)
+            et, ee = float(tt), float(eet)
+        e2e = {'value': ee / et, 'unit': UNIT, 'h2d_bytes_per_step': 24 * nnz + 8 * (nv + 1),
+               'd2h_bytes_per_step': 8 * nv,
+               'seconds_per_step': et / args.steps,
+               'transfer_s_per_step': statistics.mean(s['time_transfer'] for s in est)}
+        del aos, hptr, hC
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(ptr, tail, w)
+
+    peak, peak_kind = measured_peak()
+    achieved = (sweep_b / sweep_t) / 1e9 if sweep_t > 0 else None
+    ratio = profiled_traffic_ratio()
+    steps_timed = sum(s['sweep_steps'] for s in stats)
+    roofline = {'bound': 'hbm', 'kernel': 'k_sweep_* (degree-binned local moving, all bins)',
+                'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
+                'frac': (achieved / peak) if achieved else None, 'peak_kind': peak_kind,
+                'traffic': (ratio * sweep_b / steps_timed) if (ratio and steps_timed) else None,
+                'algorithmic_bytes_per_launch': sweep_b / steps_timed if steps_timed else None,
+                'avg_launch_s': sweep_t / steps_timed if steps_timed else None}
+    s0 = stats[-1]
+    extra = {'final_modularity': s0['final_modularity'], 'phases': s0['phases'],
+             'iterations': s0['total_iterations'], 'final_clusters': s0['final_clusters'],
+             'colors_phase1': s0['phase'][0]['num_colors'] if s0['phase'] else None,
+             'mode': args.mode, 'time_to_modularity_s': t / args.steps,
+             'kernel_time_per_step_s': dict(zip(
+                 ['bin_deg0-4', 'bin_deg5-8', 'bin_deg9-16', 'bin_deg17-32', 'bin_warp_table',
+                  'bin_block_table', 'bin_hub_table', 'apply', 'modularity'],
+                 [sum(s['kernel_time'][k] for s in stats) / args.steps for k in range(9)]))
+             if args.profile_level >= 2 else None,
+             'time_split_s': {'sweep+modularity': s0['time_clustering'],
+                              'coloring': s0['time_coloring'],
+                              'renumber+coarsen': s0['time_building']}}
+    line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': 1e3 * t / args.steps,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
+            'data': 'synthetic (seeded R-MAT generated on the device)',
+            'config': workload_config(args, nv, nnz, extra), 'roofline': roofline,
+            'cpu_baseline': cpu, 'e2e': e2e, 'gpu_launches': launches, 'clocks': clk}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def cpu_baseline(ptr, tail, w):
+    """The reference (oracle/_ref, shipped -Ofast flags) on all host cores: one phase-1
+    colour sweep iteration of the same graph (a bounded sample)."""
+    import numpy as np
+    from grappolo_b200 import graphs
+    from oracle import Reference
+    g = graphs.CSRGraph(ptr.cpu().numpy(), tail.cpu().numpy().astype(np.int64), w.cpu().numpy())
+    cores = os.cpu_count() or 1
+    R = Reference(fast=True)
+    h = R.graph(g)
+    col, mc, tcol = R.color_g(h, g.num_vertices, cores)
+    _, _, itr, tt = R.coloring_phase_g(h, g.num_vertices, col, mc + 1, -1.0, float('inf'), cores)
+    R.free_graph(h)
+    return {'value': g.nnz * itr / tt, 'unit': UNIT, 'cores': cores, 'kind': 'reference',
+            'sample': f'one phase-1 colour-class sweep iteration (+modularity) of the '
+                      f'reference algoLouvainWithDistOneColoring on the same graph '
+                      f'({g.nnz} CSR entries, {mc + 1} colours), {cores} OpenMP threads, '
+                      f'-Ofast build, its own iteration timer ({tt:.2f} s)'}
+
+
+if __name__ == '__main__':
+    sys.exit(main())

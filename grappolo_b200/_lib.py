@@ -47,11 +47,14 @@ class GlvRunStats(ct.Structure):
                 ('time_total', ct.c_double), ('time_clustering', ct.c_double),
                 ('time_coloring', ct.c_double), ('time_building', ct.c_double),
                 ('time_transfer', ct.c_double), ('edges_swept', ct.c_double),
-                ('kernel_launches', ct.c_long), ('nphase', ct.c_int),
+                ('kernel_launches', ct.c_long), ('sweep_kernel_time', ct.c_double),
+                ('sweep_bytes', ct.c_double), ('sweep_steps', ct.c_long),
+                ('kernel_time', ct.c_double * 9), ('nphase', ct.c_int),
                 ('phase', GlvPhaseStats * GLV_MAX_PHASES)]
 
     def to_dict(self) -> dict:
-        d = {k: getattr(self, k) for k, _ in self._fields_ if k != 'phase'}
+        d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ('phase', 'kernel_time')}
+        d['kernel_time'] = list(self.kernel_time)
         d['phase'] = [{k: getattr(p, k) for k, _ in GlvPhaseStats._fields_}
                       for p in self.phase[:self.nphase]]
         return d
@@ -77,6 +80,7 @@ def lib():
     L.glv_version.restype = ct.c_char_p
     L.glv_last_error.restype = ct.c_char_p
     L.glv_kernel_launch_count.restype = ct.c_long
+    L.glv_set_profiling.argtypes = [ct.c_int]
     for name in ('glv_run_multiphase_coloring', 'glv_run_multiphase_basic',
                  'glv_run_multiphase_coloring_csr', 'glv_run_multiphase_basic_csr',
                  'glv_dev_run_multiphase', 'glv_louvain_coloring_phase',

@@ -17,6 +17,7 @@
 namespace glv {
 
 static std::atomic<long> g_launches{0};
+static std::atomic<int> g_profile{0};  // 0 off, 1 per-class sweep, 2 per launch
 static thread_local std::string g_err;
 
 static int fail(int code, const char *msg) {
@@ -76,6 +77,56 @@ struct ClassSched {
   std::vector<Step> steps;
 };
 
+// CUDA-event pairs captured into the phase graph as event-record nodes.
+// Level 1 brackets each class's sweep launches; level 2 brackets every launch
+// (slots: degree bins, then apply, then modularity).
+constexpr int kSlotApply = NBINS, kSlotModularity = NBINS + 1, kSlots = NBINS + 2;
+
+struct Probes {
+  int level = 0;
+  std::vector<int> slot;
+  std::vector<cudaEvent_t> b, e;
+  double slot_s[kSlots] = {0};
+  double sweep_s = 0;
+  long sweep_pairs = 0;
+  ~Probes() {
+    for (auto x : b) cudaEventDestroy(x);
+    for (auto x : e) cudaEventDestroy(x);
+  }
+  // Opens a pair for `sl` (-1: a whole class's sweep); returns its index or -1.
+  int begin(int sl, int need_level, cudaStream_t s, int *idx) {
+    *idx = -1;
+    if (level < need_level) return GLV_OK;
+    cudaEvent_t x, y;
+    CK(cudaEventCreate(&x));
+    CK(cudaEventCreate(&y));
+    b.push_back(x);
+    e.push_back(y);
+    slot.push_back(sl);
+    *idx = (int)b.size() - 1;
+    // During capture only the External flag turns a record into a graph node.
+    CK(cudaEventRecordWithFlags(x, s, cudaEventRecordExternal));
+    return GLV_OK;
+  }
+  int end(int idx, cudaStream_t s) {
+    if (idx >= 0) CK(cudaEventRecordWithFlags(e[idx], s, cudaEventRecordExternal));
+    return GLV_OK;
+  }
+  // Adds one replay's elapsed times.
+  void collect() {
+    for (size_t k = 0; k < b.size(); ++k) {
+      float ms = 0;
+      if (cudaEventElapsedTime(&ms, b[k], e[k]) != cudaSuccess) {
+        cudaGetLastError();  // keep a failed query from surfacing at the next launch
+        continue;
+      }
+      const double t = ms * 1e-3;
+      if (slot[k] < 0) { sweep_s += t; ++sweep_pairs; }
+      else slot_s[slot[k]] += t;
+    }
+  }
+};
+
 class Engine {
  public:
   explicit Engine(cudaStream_t s, int mode) : s_(s), mode_(mode) {}
@@ -105,6 +156,9 @@ class Engine {
   bool integral = false;
   double t_sweep = 0, t_color = 0, t_coarsen = 0;
   double edges_swept = 0;
+  double sweep_kernel_s = 0, sweep_bytes = 0;
+  long sweep_steps = 0;
+  double slot_s[kSlots] = {0};
 
  private:
   template <class T>
@@ -129,11 +183,25 @@ class Engine {
                      int nsub, std::vector<ClassSched> *sched);
   int hub_offsets(const Level &L, std::vector<ClassSched> &sched);
   int sublevels(const Level &L, int ncolors, int32_t **d_sub, int *nsub);
-  int launch_sweep(const Level &L, const Step &st, SweepArgs a, bool ordered);
+  int launch_sweep(const Level &L, const Step &st, SweepArgs a, bool ordered, Probes *pr);
   int launch_apply(const ClassSched &cs, bool ordered);
   int launch_modularity(const Level &L, const int32_t *Cm, const double *ownw);
+  int color_jp(const Level &L, int *ncolors);
+  int color_spec(const Level &L, int *ncolors);
   int grow_hub(size_t entries);
   bool ordered() const { return mode_ == GLV_MODE_VERIFY && !integral; }
+  void account(Probes &pr, const Level &L) {
+    if (pr.b.empty()) return;
+    const double s0 = pr.sweep_s;
+    const long p0 = pr.sweep_pairs;
+    double before[kSlots];
+    for (int k = 0; k < kSlots; ++k) before[k] = pr.slot_s[k];
+    pr.collect();
+    sweep_kernel_s += pr.sweep_s - s0;
+    sweep_steps += pr.sweep_pairs - p0;
+    for (int k = 0; k < kSlots; ++k) slot_s[k] += pr.slot_s[k] - before[k];
+    sweep_bytes += 16.0 * (double)L.nnz + 36.0 * (double)L.nv;
+  }
 
   cudaStream_t s_;
   int mode_;
@@ -257,6 +325,18 @@ int Engine::phase_init(const Level &L, bool need_past) {
 // ----------------------------------------------------------------- colouring
 int Engine::color(const Level &L, int *ncolors, double *secs) {
   const double t0 = now_s();
+  if (L.nv == 0) {
+    *ncolors = 0;
+    return GLV_OK;
+  }
+  TRY(mode_ == GLV_MODE_FAST ? color_spec(L, ncolors) : color_jp(L, ncolors));
+  if (secs) *secs = now_s() - t0;
+  return GLV_OK;
+}
+
+// Verify mode: Jones-Plassmann in vertex-id priority = the reference's
+// one-thread sequential first-fit.
+int Engine::color_jp(const Level &L, int *ncolors) {
   int32_t *pending, *f0, *f1, *fcount, *status, *maxc;
   TRY(alloc(&pending, L.nv)); TRY(alloc(&f0, L.nv)); TRY(alloc(&f1, L.nv));
   TRY(alloc(&fcount, 3)); TRY(alloc(&status, 2)); TRY(alloc(&maxc, 1));
@@ -286,7 +366,55 @@ int Engine::color(const Level &L, int *ncolors, double *secs) {
   dfree(pending); dfree(f0); dfree(f1); dfree(fcount); dfree(status); dfree(maxc);
   if (h[0]) return fail(GLV_ERR_COLORS, "colouring needs more than 4096 colours");
   *ncolors = hm + 1;
-  if (secs) *secs = now_s() - t0;
+  return GLV_OK;
+}
+
+// Fast mode: speculative first-fit rounds with hashed-priority conflicts.
+constexpr int64_t kSpecBlockDeg = 2048;
+
+int Engine::color_spec(const Level &L, int *ncolors) {
+  int32_t *wl, *bl, *nx, *cnt, *status, *maxc;
+  TRY(alloc(&wl, L.nv)); TRY(alloc(&bl, L.nv)); TRY(alloc(&nx, L.nv));
+  TRY(alloc(&cnt, 4)); TRY(alloc(&status, 1)); TRY(alloc(&maxc, 1));
+  CK(cudaMemsetAsync(cnt, 0, 4 * sizeof(int32_t), s_));
+  CK(cudaMemsetAsync(status, 0, sizeof(int32_t), s_));
+  CK(cudaMemsetAsync(maxc, 0xff, sizeof(int32_t), s_));
+  const uint32_t seed = 0x5bd1e995u;
+  LAUNCH(k_spec_init, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, L.ptr, L.tail,
+         kSpecBlockDeg, color_, wl, cnt, bl, cnt + 1);
+  int32_t h[3];
+  CK(cudaMemcpyAsync(h, cnt, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  int rounds = 0;
+  while (h[0] + h[1] > 0) {
+    if (++rounds > 100000) return fail(GLV_ERR_CUDA, "speculative colouring did not settle");
+    const int64_t nw = h[0], nb = h[1];
+    if (nw) LAUNCH(k_spec_assign_warp, grid_for(nw * 32, 256, nsm_ * 16), 256, 0, s_, nw, wl,
+                   L.ptr, L.tail, color_, status);
+    if (nb) LAUNCH(k_spec_assign_block, (int)std::min<int64_t>(nb, nsm_ * 4), 512, 0, s_, nb, bl,
+                   L.ptr, L.tail, color_, status);
+    CK(cudaMemsetAsync(cnt + 2, 0, sizeof(int32_t), s_));
+    if (nw) LAUNCH(k_spec_conflicts, grid_for(nw * 32, 256, nsm_ * 16), 256, 0, s_, nw, wl,
+                   L.ptr, L.tail, seed, color_, nx, cnt + 2);
+    if (nb) LAUNCH(k_spec_conflicts, grid_for(nb * 32, 256, nsm_ * 16), 256, 0, s_, nb, bl,
+                   L.ptr, L.tail, seed, color_, nx, cnt + 2);
+    CK(cudaMemcpyAsync(&h[2], cnt + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
+    CK(cudaStreamSynchronize(s_));
+    if (h[2] == 0) break;
+    CK(cudaMemsetAsync(cnt, 0, 2 * sizeof(int32_t), s_));
+    LAUNCH(k_spec_split, grid_for(h[2], 256, nsm_ * 16), 256, 0, s_, (int64_t)h[2], nx, L.ptr,
+           kSpecBlockDeg, wl, cnt, bl, cnt + 1);
+    CK(cudaMemcpyAsync(h, cnt, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
+    CK(cudaStreamSynchronize(s_));
+  }
+  LAUNCH(k_max_color, grid_for(L.nv, 256, nsm_ * 8), 256, 0, s_, L.nv, color_, maxc);
+  int32_t hs, hm;
+  CK(cudaMemcpyAsync(&hs, status, sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaMemcpyAsync(&hm, maxc, sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  dfree(wl); dfree(bl); dfree(nx); dfree(cnt); dfree(status); dfree(maxc);
+  if (hs) return fail(GLV_ERR_COLORS, "colouring needs more than 4096 colours");
+  *ncolors = hm + 1;
   return GLV_OK;
 }
 
@@ -410,12 +538,15 @@ int Engine::hub_offsets(const Level &L, std::vector<ClassSched> &sched) {
 constexpr int kWarpCap = 256;   // table_cap(127)
 constexpr int kBlockCap = 8192; // table_cap(4095)
 
-int Engine::launch_sweep(const Level &L, const Step &st, SweepArgs a, bool ordered_acc) {
+int Engine::launch_sweep(const Level &L, const Step &st, SweepArgs a, bool ordered_acc,
+                         Probes *pr) {
   const int cap = nsm_ * 16;
   for (int b = 0; b < NBINS; ++b) {
     const int64_t lo = st.seg[b], hi = st.seg[b + 1];
     const int64_t n = hi - lo;
     if (n <= 0) continue;
+    int pidx = -1;
+    if (pr) TRY(pr->begin(b, 2, s_, &pidx));
     switch (b) {
       case BIN_G4:
         LAUNCH(k_sweep_small<4>, grid_for(n * 4, 256, cap), 256, 0, s_, a, lo, hi);
@@ -445,6 +576,7 @@ int Engine::launch_sweep(const Level &L, const Step &st, SweepArgs a, bool order
                ordered_acc ? 1 : 0);
         break;
     }
+    if (pr) TRY(pr->end(pidx, s_));
   }
   return GLV_OK;
 }
@@ -532,12 +664,23 @@ int Engine::coloring_phase(const Level &L, int ncolors, bool stale, double lower
   CK(cudaStreamSynchronize(s_));
   cudaGraphExec_t exec = nullptr;
   long nodes = 0;
+  Probes pr;
+  pr.level = g_profile.load();
   TRY(capture(s_, &launches_, [&]() -> int {
         for (auto &cs : sched) {
-          for (auto &st : cs.steps) TRY(launch_sweep(L, st, a, ord));
+          int k;
+          TRY(pr.begin(-1, 1, s_, &k));
+          for (auto &st : cs.steps) TRY(launch_sweep(L, st, a, ord, &pr));
+          TRY(pr.end(k, s_));
+          int q;
+          TRY(pr.begin(kSlotApply, 2, s_, &q));
           TRY(launch_apply(cs, ord));
+          TRY(pr.end(q, s_));
         }
-        return launch_modularity(L, C, nullptr);
+        int q;
+        TRY(pr.begin(kSlotModularity, 2, s_, &q));
+        TRY(launch_modularity(L, C, nullptr));
+        return pr.end(q, s_);
       }, &exec, &nodes));
   double prev = lower;
   int n = 0;
@@ -551,6 +694,7 @@ int Engine::coloring_phase(const Level &L, int ncolors, bool stale, double lower
     if (e != cudaSuccess) { g_err = cudaGetErrorString(e); rc = GLV_ERR_CUDA; break; }
     launches_ += nodes;
     edges_swept += (double)L.nnz;
+    account(pr, L);
     const double q = h_mod_[0];
     if (q - prev < thresh) break;
     prev = q;
@@ -597,10 +741,15 @@ int Engine::basic_phase(const Level &L, double lower, double thresh, double *mod
   // Q is taken on the state before the moves (parallelLouvainMethod.cpp:244-255);
   // the totals update is applied in the same graph and only matters if the
   // loop continues.
+  Probes pr;
+  pr.level = g_profile.load();
   TRY(capture(s_, &launches_, [&]() -> int {
+        int k;
+        TRY(pr.begin(-1, 1, s_, &k));
         for (auto &cs : sched) {
-          for (auto &st : cs.steps) TRY(launch_sweep(L, st, a, ord));
+          for (auto &st : cs.steps) TRY(launch_sweep(L, st, a, ord, &pr));
         }
+        TRY(pr.end(k, s_));
         TRY(launch_modularity(L, C, own_w));
         for (auto &cs : sched) TRY(launch_apply(cs, ord));
         return GLV_OK;
@@ -617,6 +766,7 @@ int Engine::basic_phase(const Level &L, double lower, double thresh, double *mod
     if (e != cudaSuccess) { g_err = cudaGetErrorString(e); rc = GLV_ERR_CUDA; break; }
     launches_ += nodes;
     edges_swept += (double)L.nnz;
+    account(pr, L);
     const double q = h_mod_[0];
     if (q - prev < thresh) break;
     prev = q;
@@ -672,7 +822,7 @@ int Engine::decide(const Level &L, const int32_t *verts, int64_t nverts) {
   a.hub_keys = hub_keys_; a.hub_vals = hub_vals_; a.hub_off = hub_off_;
   CK(cudaMemcpyAsync(&a.constant, cst, sizeof(double), cudaMemcpyDeviceToHost, s_));
   CK(cudaStreamSynchronize(s_));
-  TRY(launch_sweep(L, st, a, true));
+  TRY(launch_sweep(L, st, a, true, nullptr));
   CK(cudaStreamSynchronize(s_));
   return GLV_OK;
 }
@@ -901,6 +1051,10 @@ int Engine::run_multiphase(const Level &L0, int32_t *d_C_orig, bool coloring,
     st->time_coloring = t_color;
     st->time_building = t_coarsen;
     st->edges_swept = edges_swept;
+    st->sweep_kernel_time = sweep_kernel_s;
+    st->sweep_bytes = sweep_bytes;
+    st->sweep_steps = sweep_steps;
+    for (int k = 0; k < kSlots; ++k) st->kernel_time[k] = slot_s[k];
   }
   return GLV_OK;
 }
@@ -1109,6 +1263,7 @@ extern "C" {
 const char *glv_version(void) { return "grappolo_b200 0.1 (sm_100a)"; }
 const char *glv_last_error(void) { return g_err.c_str(); }
 long glv_kernel_launch_count(void) { return g_launches.load(); }
+void glv_set_profiling(int on) { g_profile = on < 0 ? 0 : (on > 2 ? 2 : on); }
 
 int glv_run_multiphase_coloring(const glv_graph *G, long *C_orig, int coloring, int numColors,
                                 int replaceMap, long minGraphSize, double threshold,

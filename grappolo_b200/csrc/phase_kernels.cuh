@@ -535,3 +535,149 @@ __global__ void k_run_first(int64_t n, const uint64_t *keys, int shift, uint64_t
 }
 
 }  // namespace glv
+
+namespace glv {
+
+// ---------------------------------------------------------------------------
+// Fast-mode colouring: speculative first-fit with priority conflict
+// resolution (the parallel form of Coloring/coloringDistanceOne.cpp:129-188,
+// with hashed priorities in place of its RngStream values).  Each round every
+// uncoloured vertex takes the smallest colour not seen on its neighbours;
+// then a vertex that shares its colour with a higher-priority neighbour gives
+// it up and joins the next round.  The highest-priority vertex of every
+// conflict keeps its colour, so each round colours at least one vertex.
+
+// First free colour over the neighbours of v (self-loops skipped); `bm` is a
+// bitmap of kMaxColors bits shared by the `team` threads calling this.
+template <int TEAM>
+__device__ __forceinline__ int first_free_color(const int64_t *ptr, const int32_t *tail,
+                                                const int32_t *color, int32_t v, uint32_t *bm,
+                                                int tid) {
+  const int64_t rb = ptr[v], re = ptr[v + 1];
+  const int64_t deg = re - rb;
+  const int words = (int)((deg + 32) / 32 < kMaxColors / 32 ? (deg + 32) / 32 : kMaxColors / 32);
+  for (int q = tid; q < words; q += TEAM) bm[q] = 0u;
+  if (TEAM == 32) __syncwarp(); else __syncthreads();
+  for (int64_t j = rb + tid; j < re; j += TEAM) {
+    const int32_t u = tail[j];
+    if (u != v) {
+      const int32_t cu = color[u];
+      if (cu >= 0 && cu < words * 32) atomicOr(&bm[cu >> 5], 1u << (cu & 31));
+    }
+  }
+  if (TEAM == 32) __syncwarp(); else __syncthreads();
+  int first = INT32_MAX;
+  for (int q = tid; q < words; q += TEAM) {
+    const uint32_t free_bits = ~bm[q];
+    if (free_bits) { first = q * 32 + __ffs(free_bits) - 1; break; }
+  }
+  return first;  // per-thread candidate; caller reduces (min)
+}
+
+// Warp per vertex (rows below kSpecBlockDeg entries).
+__global__ void __launch_bounds__(256) k_spec_assign_warp(int64_t n, const int32_t *list,
+                                                          const int64_t *ptr, const int32_t *tail,
+                                                          int32_t *color, int32_t *status) {
+  __shared__ uint32_t bm[8][kMaxColors / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t k = wid; k < n; k += nw) {
+    const int32_t v = list[k];
+    int first = first_free_color<32>(ptr, tail, color, v, bm[warp], lane);
+    first = __reduce_min_sync(FULL, first);
+    if (first == INT32_MAX) {
+      const int64_t deg = ptr[v + 1] - ptr[v];
+      first = (int)((deg + 32) / 32 < kMaxColors / 32 ? (deg + 32) / 32 : kMaxColors / 32) * 32;
+    }
+    if (first >= kMaxColors) {
+      if (lane == 0) atomicExch(status, 1);
+      first = kMaxColors - 1;
+    }
+    if (lane == 0) color[v] = first;
+    __syncwarp();
+  }
+}
+
+// Block per vertex (hubs).
+__global__ void __launch_bounds__(512) k_spec_assign_block(int64_t n, const int32_t *list,
+                                                           const int64_t *ptr,
+                                                           const int32_t *tail, int32_t *color,
+                                                           int32_t *status) {
+  __shared__ uint32_t bm[kMaxColors / 32];
+  __shared__ int s_min[16];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int64_t k = blockIdx.x; k < n; k += gridDim.x) {
+    const int32_t v = list[k];
+    int first = first_free_color<512>(ptr, tail, color, v, bm, threadIdx.x);
+    first = __reduce_min_sync(FULL, first);
+    if (lane == 0) s_min[warp] = first;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int f = s_min[0];
+      for (int q = 1; q < 16; ++q) f = min(f, s_min[q]);
+      if (f == INT32_MAX) {
+        const int64_t deg = ptr[v + 1] - ptr[v];
+        f = (int)((deg + 32) / 32 < kMaxColors / 32 ? (deg + 32) / 32 : kMaxColors / 32) * 32;
+      }
+      if (f >= kMaxColors) { atomicExch(status, 1); f = kMaxColors - 1; }
+      color[v] = f;
+    }
+    __syncthreads();
+  }
+}
+
+// A vertex that shares its colour with a higher-priority neighbour resets
+// and goes to the next round's list.  Warp per vertex.
+__global__ void __launch_bounds__(256) k_spec_conflicts(int64_t n, const int32_t *list,
+                                                        const int64_t *ptr, const int32_t *tail,
+                                                        uint32_t seed, int32_t *color,
+                                                        int32_t *next, int32_t *next_count) {
+  const int lane = threadIdx.x & 31;
+  const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t k = wid; k < n; k += nw) {
+    const int32_t v = list[k];
+    const int32_t cv = color[v];
+    bool lose = false;
+    for (int64_t j = ptr[v] + lane; j < ptr[v + 1] && !lose; j += 32) {
+      const int32_t u = tail[j];
+      if (u != v && color[u] == cv && prio_before(u, v, 1, seed)) lose = true;
+    }
+    if (__any_sync(FULL, lose) && lane == 0) {
+      color[v] = -1;
+      next[atomicAdd(next_count, 1)] = v;
+    }
+  }
+}
+
+// Initial lists: rows with no neighbour but themselves take colour 0; the
+// rest go to the warp or block list by degree.
+__global__ void k_spec_init(int64_t nv, const int64_t *ptr, const int32_t *tail,
+                            int64_t block_deg, int32_t *color, int32_t *wl, int32_t *wcount,
+                            int32_t *bl, int32_t *bcount) {
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t rb = ptr[v], re = ptr[v + 1];
+    bool any = false;
+    for (int64_t j = rb; j < re && !any; ++j) any = tail[j] != (int32_t)v;
+    color[v] = any ? -1 : 0;
+    if (!any) continue;
+    if (re - rb >= block_deg) bl[atomicAdd(bcount, 1)] = (int32_t)v;
+    else wl[atomicAdd(wcount, 1)] = (int32_t)v;
+  }
+}
+
+// Split a list by degree (next round's lists).
+__global__ void k_spec_split(int64_t n, const int32_t *list, const int64_t *ptr,
+                             int64_t block_deg, int32_t *wl, int32_t *wcount, int32_t *bl,
+                             int32_t *bcount) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t v = list[k];
+    if (ptr[v + 1] - ptr[v] >= block_deg) bl[atomicAdd(bcount, 1)] = v;
+    else wl[atomicAdd(wcount, 1)] = v;
+  }
+}
+
+}  // namespace glv

@@ -193,3 +193,49 @@ def read_binary(path: str) -> CSRGraph:
         ptr = np.frombuffer(f.read(8 * (nv + 1)), dtype='<i8').copy()
         rec = np.frombuffer(f.read(_EDGE.itemsize * 2 * ne), dtype=_EDGE)
     return CSRGraph(ptr, rec['tail'].astype(np.int64), rec['weight'].astype(np.float64))
+
+
+def rmat_device(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19,
+                c: float = 0.19, seed: int = 1, device='cuda', weighted: bool = True):
+    """R-MAT graph built directly in device memory with torch (large inputs).
+
+    Same construction as :func:`rmat` (recursive quadrant choice, symmetrised,
+    self-loops and duplicates removed, weights uniform in (0, 1]) but drawn from
+    torch's device generator, so the graph differs from the numpy one of the
+    same seed.  Returns device tensors (ptr int64[NV+1], tail int32[nnz],
+    weight float64[nnz]).
+    """
+    import torch
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    nv = 1 << scale
+    m = edge_factor * nv
+    u = torch.zeros(m, dtype=torch.int64, device=device)
+    v = torch.zeros(m, dtype=torch.int64, device=device)
+    ab, abc = a + b, a + b + c
+    for _ in range(scale):
+        r = torch.rand(m, generator=gen, device=device)
+        u = (u << 1) | (r >= ab).to(torch.int64)
+        v = (v << 1) | (((r >= a) & (r < ab)) | (r >= abc)).to(torch.int64)
+        del r
+    keep = u != v
+    u, v = u[keep], v[keep]
+    key = torch.minimum(u, v) * nv + torch.maximum(u, v)
+    del u, v, keep
+    key = torch.unique(key)
+    lo, hi = key // nv, key % nv
+    del key
+    if weighted:
+        w = 1.0 - torch.rand(lo.numel(), generator=gen, device=device, dtype=torch.float64)
+    else:
+        w = torch.ones(lo.numel(), device=device, dtype=torch.float64)
+    src = torch.cat([lo, hi])
+    dst = torch.cat([hi, lo])
+    ww = torch.cat([w, w])
+    del lo, hi, w
+    order = torch.argsort(src * nv + dst)
+    src, dst, ww = src[order], dst[order], ww[order]
+    del order
+    ptr = torch.zeros(nv + 1, dtype=torch.int64, device=device)
+    ptr[1:] = torch.cumsum(torch.bincount(src, minlength=nv), 0)
+    return ptr, dst.to(torch.int32), ww

@@ -86,6 +86,17 @@ typedef struct glv_run_stats {
   double time_transfer;     /* s, host<->device copies */
   double edges_swept;       /* sum over phases */
   long kernel_launches;     /* kernels this call launched */
+  /* With glv_set_profiling(1): device time of the local-moving sweep kernels
+   * (CUDA events around every class's sweep launches, on the engine's stream)
+   * and their algorithmic bytes, 16 B per CSR entry + 36 B per vertex
+   * (tail 4 + weight 8 + C[tail] 4; offset 8 + C 4 + degree 8 + own total 8
+   * + member id 4 + decision 4) per full sweep. */
+  double sweep_kernel_time; /* s */
+  double sweep_bytes;
+  long sweep_steps;         /* (class, sublevel) steps timed */
+  /* With glv_set_profiling(2): device time per launch kind — the seven degree
+   * bins of the sweep, the community-total update, the modularity pass. */
+  double kernel_time[9];    /* s */
   int nphase;               /* entries filled in phase[] */
   glv_phase_stats phase[GLV_MAX_PHASES];
 } glv_run_stats;
@@ -169,6 +180,10 @@ int glv_decide_batch(long nv, const long *ptr, const long *tail, const double *w
                      double constant, long nverts, const long *verts, long *targets);
 
 /* ---- library information ------------------------------------------------ */
+/* Process-wide switch for the following calls: 0 off; 1 time each colour
+ * class's sweep with CUDA events (sweep_kernel_time / sweep_bytes); 2 also
+ * time every launch by kind (kernel_time). */
+void glv_set_profiling(int on);
 const char *glv_version(void);
 const char *glv_last_error(void);
 /* Kernel launches issued by this library since load (all entry points). */

@@ -230,6 +230,14 @@ class Reference:
         L.ref_run_multiphase_coloring.restype = ct.c_long
         L.ref_run_multiphase_basic.restype = ct.c_long
         L.ref_load_metis.restype = ct.c_long
+        L.ref_graph_create.restype = ct.c_void_p
+        L.ref_graph_free.argtypes = [ct.c_void_p]
+        L.ref_color_g.restype = ct.c_int
+        L.ref_color_g.argtypes = [ct.c_void_p, _c_int_p, ct.c_int, _c_double_p]
+        L.ref_coloring_phase_g.restype = ct.c_double
+        L.ref_coloring_phase_g.argtypes = [ct.c_void_p, _c_long_p, _c_int_p, ct.c_int,
+                                           ct.c_double, ct.c_double, ct.c_int, _c_int_p,
+                                           _c_double_p]
         L.ref_set_quiet(ct.c_int(1 if quiet else 0))
 
     def color(self, g, nthreads=1):
@@ -326,6 +334,29 @@ class Reference:
                                         ct.c_int(nthreads), buf, ct.c_long(1 << 22))
         text = buf.value.decode(errors='replace')
         return C, parse_reference_log(text), text
+
+    def graph(self, g):
+        """A persistent reference `graph` (AoS) for repeated calls; free with free_graph."""
+        p, t, w = _csr(g)
+        return self.L.ref_graph_create(ct.c_long(g.num_vertices), _lp(p), _lp(t), _dp(w))
+
+    def free_graph(self, handle):
+        self.L.ref_graph_free(handle)
+
+    def color_g(self, handle, nv, nthreads):
+        col = np.full(nv, -1, dtype=np.int32)
+        tt = ct.c_double(0)
+        mc = self.L.ref_color_g(handle, _ip(col), ct.c_int(nthreads), ct.byref(tt))
+        return col, mc, tt.value
+
+    def coloring_phase_g(self, handle, nv, colors, num_colors, lower, thresh, nthreads):
+        C = np.zeros(nv, dtype=np.int64)
+        col = np.array(colors, dtype=np.int32, copy=True)
+        itr, tt = ct.c_int(0), ct.c_double(0)
+        q = self.L.ref_coloring_phase_g(handle, _lp(C), _ip(col), ct.c_int(num_colors),
+                                        ct.c_double(lower), ct.c_double(thresh),
+                                        ct.c_int(nthreads), ct.byref(itr), ct.byref(tt))
+        return q, C, itr.value, tt.value
 
     def load_metis(self, path):
         from grappolo_b200.graphs import CSRGraph

@@ -52,6 +52,7 @@ static graph *make_graph(long nv, const long *ptr, const long *tail, const doubl
     G->edgeListPtrs = (long *)malloc(sizeof(long) * (nv + 1));
     G->edgeList = (edge *)malloc(sizeof(edge) * (nnz ? nnz : 1));
     memcpy(G->edgeListPtrs, ptr, sizeof(long) * (nv + 1));
+#pragma omp parallel for schedule(dynamic, 4096) reduction(+ : loops)
     for (long i = 0; i < nv; i++) {
         for (long j = ptr[i]; j < ptr[i + 1]; j++) {
             G->edgeList[j].head = i;
@@ -152,6 +153,32 @@ long ref_build_next_level(long nv, const long *ptr, const long *tail, const doub
 }
 
 void ref_free(void *p) { free(p); }
+
+// Persistent graphs for repeated timing of one input (the AoS copy is built
+// once, in parallel).
+void *ref_graph_create(long nv, const long *ptr, const long *tail, const double *w) {
+  return make_graph(nv, ptr, tail, w);
+}
+
+void ref_graph_free(void *G) { free_graph((graph *)G); }
+
+int ref_color_g(void *Gv, int *color, int nthreads, double *totTime) {
+  graph *G = (graph *)Gv;
+  for (long i = 0; i < G->numVertices; i++) color[i] = -1;
+  quiet_begin();
+  int mc = algoDistanceOneVertexColoringOpt(G, color, nthreads, totTime);
+  quiet_end();
+  return mc;
+}
+
+double ref_coloring_phase_g(void *Gv, long *C, int *color, int numColor, double Lower,
+                            double thresh, int nthreads, int *numItr, double *totTime) {
+  quiet_begin();
+  double q = algoLouvainWithDistOneColoring((graph *)Gv, C, nthreads, color, numColor, Lower,
+                                            thresh, totTime, numItr);
+  quiet_end();
+  return q;
+}
 
 // Per-vertex move decision through the reference's own primitives, set up as
 // the colour sweep does (parallelLouvainWithColoring.cpp:181-188):
