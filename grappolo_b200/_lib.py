@@ -86,7 +86,7 @@ def lib():
                  'glv_dev_run_multiphase', 'glv_louvain_coloring_phase',
                  'glv_louvain_basic_phase', 'glv_distance_one_coloring',
                  'glv_renumber_clusters', 'glv_build_next_level', 'glv_modularity',
-                 'glv_decide_batch'):
+                 'glv_decide_batch', 'glv_dev_modularity_static'):
         getattr(L, name).restype = ct.c_int
     L.glv_run_multiphase_coloring.argtypes = [P(GlvGraph), P(ct.c_long), ct.c_int, ct.c_int,
                                               ct.c_int, ct.c_long, ct.c_double, ct.c_double,
@@ -118,6 +118,9 @@ def lib():
     L.glv_decide_batch.argtypes = [ct.c_long, P(ct.c_long), P(ct.c_long), P(ct.c_double),
                                    P(ct.c_long), P(ct.c_double), P(ct.c_double), P(ct.c_long),
                                    ct.c_double, ct.c_long, P(ct.c_long), P(ct.c_long)]
+    L.glv_dev_modularity_static.argtypes = [ct.c_long, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                            ct.c_void_p, ct.c_void_p, ct.c_double, ct.c_void_p,
+                                            ct.c_void_p]
     _lib = L
     return L
 

@@ -1494,3 +1494,89 @@ int glv_decide_batch(long nv, const long *ptr, const long *tail, const double *w
 }
 
 }  // extern "C"
+
+// =========================================================================
+// Modularity without allocation (glv_dev_modularity_static)
+// =========================================================================
+#include <mutex>
+
+namespace glv {
+
+// Largest vertex count the static scratch covers: one partial pair per 256
+// vertices, 65,536 pairs -> 16,777,216 vertices, 1 MiB of device memory that
+// every GPU which loads this library keeps until the process exits.
+constexpr int64_t kStaticModParts = 65536;
+constexpr int64_t kStaticModMaxVertices = kStaticModParts * kModVB;
+
+// Block partials of e_xx (first half) and a2_x (second half).  Shared by every
+// call on a device: concurrent calls on that device race on it.
+static __device__ __align__(256) double g_mod_scratch[2 * kStaticModParts];
+
+static std::mutex g_mod_scratch_mu;
+static double *g_mod_scratch_addr[128];  // device address of g_mod_scratch, per device
+
+// The fold of k_modularity_final with the constant passed by value, so the
+// call needs no device copy of it.
+__global__ void __launch_bounds__(256) k_modularity_final_value(int nparts, const double *part_e,
+                                                                const double *part_a,
+                                                                double constant, double *out) {
+  __shared__ double sh[8];
+  double e = 0.0, a = 0.0;
+  const int per = (nparts + blockDim.x - 1) / blockDim.x;
+  const int b = threadIdx.x * per, en = min(nparts, b + per);
+  for (int i = b; i < en; ++i) { e = __dadd_rn(e, part_e[i]); a = __dadd_rn(a, part_a[i]); }
+  e = block_sum<256>(e, sh);
+  a = block_sum<256>(a, sh);
+  if (threadIdx.x == 0) {
+    out[0] = __dsub_rn(__dmul_rn(e, constant), __dmul_rn(__dmul_rn(a, constant), constant));
+    out[1] = e;
+    out[2] = a;
+  }
+}
+
+}  // namespace glv
+
+extern "C" int glv_dev_modularity_static(long nv, const long *d_ptr, const int *d_tail,
+                                         const double *d_weight, const int *d_C,
+                                         const double *d_cDeg, double constant, double *d_out,
+                                         void *stream) {
+  using namespace glv;
+  if (nv < 1) return fail(GLV_ERR_ARG, "glv_dev_modularity_static: numVertices < 1");
+  if (nv > kStaticModMaxVertices)
+    return fail(GLV_ERR_LIMIT,
+                "glv_dev_modularity_static: numVertices exceeds 16,777,216, the size its "
+                "static scratch covers; use the allocating entry points");
+  if (!d_ptr || !d_tail || !d_weight || !d_C || !d_cDeg || !d_out)
+    return fail(GLV_ERR_ARG, "glv_dev_modularity_static: NULL pointer");
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) return fail(GLV_ERR_ARG, "glv_dev_modularity_static: device id");
+  double *scratch = nullptr;
+  {
+    // First call on a device: look up the array's device address with that
+    // device current.
+    std::lock_guard<std::mutex> lock(g_mod_scratch_mu);
+    if (!g_mod_scratch_addr[dev]) {
+      void *p = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&p, g_mod_scratch);
+      if (e != cudaSuccess || !p) {
+        g_err = std::string("glv_dev_modularity_static: cudaGetSymbolAddress: ") +
+                cudaGetErrorString(e);
+        return GLV_ERR_CUDA;
+      }
+      g_mod_scratch_addr[dev] = static_cast<double *>(p);
+    }
+    scratch = g_mod_scratch_addr[dev];
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int nparts = (int)((nv + kModVB - 1) / kModVB);
+  double *part_e = scratch, *part_a = scratch + kStaticModParts;
+  // Every partial read below is written first by this call's k_modularity_part,
+  // so nothing in the scratch needs clearing.
+  k_modularity_part<<<nparts, 256, 0, s>>>(nv, (const int64_t *)d_ptr, d_tail, d_weight, d_C,
+                                           nullptr, d_cDeg, part_e, part_a);
+  k_modularity_final_value<<<1, 256, 0, s>>>(nparts, part_e, part_a, constant, d_out);
+  g_launches += 2;
+  CK(cudaGetLastError());
+  return GLV_OK;
+}

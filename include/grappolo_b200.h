@@ -179,6 +179,30 @@ int glv_decide_batch(long nv, const long *ptr, const long *tail, const double *w
                      const long *C, const double *vDeg, const double *cDeg, const long *cSize,
                      double constant, long nverts, const long *verts, long *targets);
 
+/* Modularity of an assignment on the device without allocating anything.
+ * No counterpart in the reference.  For callers that cannot call cudaMalloc
+ * during their run: code whose device memory is all handed out by a host
+ * framework's caching allocator (a foreign cudaMalloc can fail on a
+ * fragmented or full device and implicitly synchronises it), or code running
+ * under a memory budget fixed at start-up.  Inputs and the output are the
+ * caller's device buffers: d_ptr int64[nv+1], d_tail int32[nnz],
+ * d_weight f64[nnz], d_C int32[nv] (-1 = none), d_cDeg f64[nv] (total weighted
+ * degree of each community id), `constant` = 1 / (sum of all weighted degrees);
+ * d_out f64[3] receives {Q, e_xx, a2_x} with Q = e_xx*constant -
+ * a2_x*constant^2 (the formula of Coloring/parallelLouvainWithColoring.cpp:226-249).
+ * Scratch is a 1 MiB static device array compiled into the library, which
+ * bounds nv to 16,777,216 (larger nv returns GLV_ERR_LIMIT without touching the
+ * GPU).  Every GPU that loads the library holds that array until the process
+ * exits.  The first call on a device looks up the array's address (once per
+ * device, with that device current); make that first call before any stream
+ * capture.  The work is queued on `stream` (cudaStream_t, NULL = legacy
+ * default stream) and is complete when the stream reaches it.  All calls on a
+ * device share the one array: calls that overlap on the GPU (other streams,
+ * other host threads) race and must be serialised by the caller. */
+int glv_dev_modularity_static(long nv, const long *d_ptr, const int *d_tail,
+                              const double *d_weight, const int *d_C, const double *d_cDeg,
+                              double constant, double *d_out, void *stream);
+
 /* ---- library information ------------------------------------------------ */
 /* Process-wide switch for the following calls: 0 off; 1 time each colour
  * class's sweep with CUDA events (sweep_kernel_time / sweep_bytes); 2 also
