@@ -297,9 +297,10 @@ def main():
              'colors_phase1': s0['phase'][0]['num_colors'] if s0['phase'] else None,
              'mode': args.mode, 'time_to_modularity_s': t / args.steps,
              'kernel_time_per_step_s': dict(zip(
-                 ['bin_deg0-4', 'bin_deg5-8', 'bin_deg9-16', 'bin_deg17-32', 'bin_warp_table',
-                  'bin_block_table', 'bin_hub_table', 'apply', 'modularity'],
-                 [sum(s['kernel_time'][k] for s in stats) / args.steps for k in range(9)]))
+                 ['bin_deg0-4', 'bin_deg5-8', 'bin_deg9-16', 'bin_deg17-32', 'bin_deg33-127',
+                  'bin_deg128-511', 'bin_deg512-1023', 'bin_deg1024-2047', 'bin_hubs', 'apply',
+                  'modularity'],
+                 [sum(s['kernel_time'][k] for s in stats) / args.steps for k in range(11)]))
              if args.profile_level >= 2 else None,
              'time_split_s': {'sweep+modularity': s0['time_clustering'],
                               'coloring': s0['time_coloring'],

@@ -16,6 +16,7 @@ GLV_OK = 0
 GLV_MODE_VERIFY = 0
 GLV_MODE_FAST = 1
 GLV_MAX_PHASES = 256
+GLV_KERNEL_SLOTS = 11
 
 ERRORS = {
     1: 'invalid argument', 2: 'CUDA error', 3: 'out of memory',
@@ -49,7 +50,7 @@ class GlvRunStats(ct.Structure):
                 ('time_transfer', ct.c_double), ('edges_swept', ct.c_double),
                 ('kernel_launches', ct.c_long), ('sweep_kernel_time', ct.c_double),
                 ('sweep_bytes', ct.c_double), ('sweep_steps', ct.c_long),
-                ('kernel_time', ct.c_double * 9), ('nphase', ct.c_int),
+                ('kernel_time', ct.c_double * GLV_KERNEL_SLOTS), ('nphase', ct.c_int),
                 ('phase', GlvPhaseStats * GLV_MAX_PHASES)]
 
     def to_dict(self) -> dict:

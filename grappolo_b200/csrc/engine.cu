@@ -9,14 +9,42 @@
 #include <string>
 #include <vector>
 
+#include <mutex>
+
 #include <cub/cub.cuh>
 
+#include "persist.cuh"
 #include "phase_kernels.cuh"
 #include "sweep.cuh"
 
 namespace glv {
 
 static std::atomic<long> g_launches{0};
+
+// Library-owned stream-ordered memory pool per device.  Freed blocks stay
+// cached in the pool (release threshold = max), so the large per-phase buffers
+// of one run (and of the next run) do not go back to the driver at every
+// synchronisation; glv_release_cached_memory() returns them.
+static std::mutex g_pool_mu;
+static cudaMemPool_t g_pool[128];
+
+static cudaMemPool_t engine_pool() {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return nullptr;
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  if (!g_pool[dev]) {
+    cudaMemPoolProps props = {};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t p = nullptr;
+    if (cudaMemPoolCreate(&p, &props) != cudaSuccess) return nullptr;
+    uint64_t keep = UINT64_MAX;
+    cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+    g_pool[dev] = p;
+  }
+  return g_pool[dev];
+}
 static std::atomic<int> g_profile{0};  // 0 off, 1 per-class sweep, 2 per launch
 static thread_local std::string g_err;
 
@@ -70,6 +98,8 @@ struct Level {
 // One (class, sublevel) step: member positions of each degree bin.
 struct Step {
   int64_t seg[NBINS + 1];
+  int64_t hub_chunk[2] = {0, 0};  // k_hub_accum work items
+  int64_t hub_segs[2] = {0, 0};   // k_hub_scan work items
 };
 
 struct ClassSched {
@@ -81,6 +111,7 @@ struct ClassSched {
 // Level 1 brackets each class's sweep launches; level 2 brackets every launch
 // (slots: degree bins, then apply, then modularity).
 constexpr int kSlotApply = NBINS, kSlotModularity = NBINS + 1, kSlots = NBINS + 2;
+static_assert(kSlots == GLV_KERNEL_SLOTS, "glv_run_stats.kernel_time must hold every slot");
 
 struct Probes {
   int level = 0;
@@ -163,7 +194,9 @@ class Engine {
  private:
   template <class T>
   int alloc(T **p, size_t n) {
-    CK(cudaMallocAsync((void **)p, std::max<size_t>(n, 1) * sizeof(T), s_));
+    if (!pool_) pool_ = engine_pool();
+    if (!pool_) return fail(GLV_ERR_CUDA, "could not create the device memory pool");
+    CK(cudaMallocFromPoolAsync((void **)p, std::max<size_t>(n, 1) * sizeof(T), pool_, s_));
     return GLV_OK;
   }
   template <class T>
@@ -187,6 +220,12 @@ class Engine {
   int launch_apply(const ClassSched &cs, bool ordered);
   int launch_modularity(const Level &L, const int32_t *Cm, const double *ownw);
   int color_jp(const Level &L, int *ncolors);
+  int run_persistent(const Level &L, const std::vector<ClassSched> &sched, SweepArgs a,
+                     bool jacobi, double lower, double thresh, double *mod, int *itr);
+  bool persistent() const {
+    const char *e = getenv("GRAPPOLO_B200_PERSISTENT");
+    return !ordered() && !(e && e[0] == '0');
+  }
   int color_spec(const Level &L, int *ncolors);
   int grow_hub(size_t entries);
   bool ordered() const { return mode_ == GLV_MODE_VERIFY && !integral; }
@@ -204,10 +243,11 @@ class Engine {
   }
 
   cudaStream_t s_;
+  cudaMemPool_t pool_ = nullptr;
   int mode_;
   int nsm_ = 148;
   int64_t nv0_ = 0, nnz0_ = 0;
-  BinLimits lim_{127, 4095};
+  BinLimits lim_{127, 2047};
   // schedule buffers
   int32_t *keys_ = nullptr, *keys2_ = nullptr, *members_ = nullptr, *vals_ = nullptr;
   int32_t *move_old_ = nullptr, *move_new_ = nullptr, *hist_ = nullptr;
@@ -215,6 +255,22 @@ class Engine {
   int32_t *hub_keys_ = nullptr;
   double *hub_vals_ = nullptr;
   size_t hub_cap_ = 0;
+  // parallel hub path (per member slot arrays, work lists, filled-slot lists)
+  int64_t *hub_occ_off_ = nullptr, *hub_seg_beg_ = nullptr, *hub_seg_end_ = nullptr;
+  int32_t *hub_cnt_ = nullptr;
+  double *hub_self_ = nullptr, *hub_ownw_ = nullptr;
+  int32_t *hub_occ_ = nullptr;
+  size_t hub_occ_cap_ = 0;
+  int32_t *chunk_pos_ = nullptr, *seg_pos_ = nullptr, *part_c_ = nullptr;
+  int64_t *chunk_beg_ = nullptr, *chunk_end_ = nullptr, *seg_beg_ = nullptr, *seg_end_ = nullptr;
+  double *part_g_ = nullptr;
+  size_t chunk_cap_ = 0, seg_cap_ = 0;
+  bool hub_tables_clean_ = false;
+  HubWork hub_work() const {
+    return HubWork{hub_keys_, hub_vals_, hub_off_, hub_occ_, hub_occ_off_, hub_cnt_, hub_self_,
+                   hub_ownw_, chunk_pos_, chunk_beg_, chunk_end_, seg_pos_, seg_beg_, seg_end_,
+                   part_g_, part_c_, hub_seg_beg_, hub_seg_end_};
+  }
   int hist_cap_ = 0;
   // ordered-delta buffers
   uint64_t *dkeys_ = nullptr, *dkeys2_ = nullptr;
@@ -242,6 +298,10 @@ void Engine::release() {
                     &vals_, &move_old_, &move_new_, &hist_, &hub_keys_};
   for (auto p : ip) dfree(*p);
   dfree(hub_off_);
+  dfree(hub_occ_off_); dfree(hub_seg_beg_); dfree(hub_seg_end_); dfree(hub_cnt_);
+  dfree(hub_self_); dfree(hub_ownw_); dfree(hub_occ_); dfree(chunk_pos_); dfree(seg_pos_);
+  dfree(part_c_); dfree(chunk_beg_); dfree(chunk_end_); dfree(seg_beg_); dfree(seg_end_);
+  dfree(part_g_);
   dfree(dkeys_); dfree(dkeys2_); dfree(drecs_); dfree(drecs2_);
   dfree(temp_);
   if (h_mod_) cudaFreeHost(h_mod_);
@@ -261,6 +321,15 @@ int Engine::init(int64_t nv0, int64_t nnz0) {
   TRY(alloc(&C, n)); TRY(alloc(&Cpast, n)); TRY(alloc(&Ctgt, n)); TRY(alloc(&color_, n));
   TRY(alloc(&keys_, n)); TRY(alloc(&keys2_, n)); TRY(alloc(&members_, n)); TRY(alloc(&vals_, n));
   TRY(alloc(&move_old_, n)); TRY(alloc(&move_new_, n)); TRY(alloc(&hub_off_, n));
+  TRY(alloc(&hub_occ_off_, n)); TRY(alloc(&hub_seg_beg_, n)); TRY(alloc(&hub_seg_end_, n));
+  TRY(alloc(&hub_cnt_, n)); TRY(alloc(&hub_self_, n)); TRY(alloc(&hub_ownw_, n));
+  CK(cudaMemsetAsync(hub_cnt_, 0, n * sizeof(int32_t), s_));
+  CK(cudaMemsetAsync(hub_self_, 0, n * sizeof(double), s_));
+  CK(cudaMemsetAsync(hub_ownw_, 0, n * sizeof(double), s_));
+  if (const char *bm = getenv("GRAPPOLO_B200_BLOCK_MAX")) {
+    const int v = atoi(bm);
+    if (v >= lim_.warp_max && v <= 2047) lim_.block_max = v;
+  }
   TRY(alloc(&cst, 4));
   // partials of the modularity pass (one per 256 vertices) and of the
   // constant's reduction (kConstParts blocks) share these buffers
@@ -407,6 +476,8 @@ int Engine::color_spec(const Level &L, int *ncolors) {
     CK(cudaMemcpyAsync(h, cnt, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
     CK(cudaStreamSynchronize(s_));
   }
+  if (getenv("GRAPPOLO_B200_DEBUG"))
+    fprintf(stderr, "grappolo_b200: speculative colouring nv=%ld rounds=%d\n", (long)L.nv, rounds);
   LAUNCH(k_max_color, grid_for(L.nv, 256, nsm_ * 8), 256, 0, s_, L.nv, color_, maxc);
   int32_t hs, hm;
   CK(cudaMemcpyAsync(&hs, status, sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
@@ -506,32 +577,133 @@ int Engine::grow_hub(size_t entries) {
   return GLV_OK;
 }
 
-// Hub tables: each hub of a step gets a region of the global scratch; steps
-// run one after another, so regions are reused across steps.
+__global__ void k_row_bounds(int64_t n, const int32_t *members, const int64_t *ptr,
+                             int64_t *out) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t v = members[k];
+    out[2 * k] = ptr[v];
+    out[2 * k + 1] = ptr[v + 1];
+  }
+}
+
+template <class T>
+static int upload(cudaStream_t s, T *dst, const std::vector<T> &src) {
+  if (src.empty()) return GLV_OK;
+  CK(cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+  return GLV_OK;
+}
+
+// Hub tables and work lists.  Ordered accumulation (verify mode, non-integral
+// weights) walks each hub with one warp and reuses one table region per step;
+// the parallel path gives every hub of the schedule a private table, cut its
+// row into kHubChunk-entry chunks and its filled-slot list into kHubSeg
+// segments.
 int Engine::hub_offsets(const Level &L, std::vector<ClassSched> &sched) {
-  size_t need = 0;
+  const bool parallel = !ordered();
+  std::vector<int64_t> tab_off, occ_off, seg_b, seg_e;
+  std::vector<int32_t> c_pos, s_pos;
+  std::vector<int64_t> c_beg, c_end, s_beg, s_end;
+  std::vector<int64_t> hub_pos_all;
+  size_t need_tab = 0, tab_acc = 0, occ_acc = 0;
+  int64_t *bounds = nullptr;
   for (auto &cs : sched)
     for (auto &st : cs.steps) {
       const int64_t b = st.seg[BIN_HUB], e = st.seg[BIN_HUB + 1];
+      st.hub_chunk[0] = st.hub_chunk[1] = (int64_t)c_pos.size();
+      st.hub_segs[0] = st.hub_segs[1] = (int64_t)s_pos.size();
       if (e == b) continue;
-      LAUNCH(k_hub_caps, grid_for(e - b, 256, nsm_ * 4), 256, 0, s_, e - b, members_ + b, L.ptr,
-             hub_off_ + b);
-      std::vector<int64_t> off(e - b);
-      CK(cudaMemcpyAsync(off.data(), hub_off_ + b, (e - b) * sizeof(int64_t),
-                         cudaMemcpyDeviceToHost, s_));
+      dfree(bounds);
+      TRY(alloc(&bounds, 2 * (e - b)));
+      LAUNCH(k_row_bounds, grid_for(e - b, 256, nsm_ * 4), 256, 0, s_, e - b, members_ + b, L.ptr,
+             bounds);
+      std::vector<int64_t> hb(2 * (e - b));
+      CK(cudaMemcpyAsync(hb.data(), bounds, hb.size() * sizeof(int64_t), cudaMemcpyDeviceToHost,
+                         s_));
       CK(cudaStreamSynchronize(s_));
-      int64_t acc = 0;
+      size_t step_tab = 0;
       for (int64_t k = 0; k < e - b; ++k) {
-        const int64_t c = off[k];
-        off[k] = acc;
-        acc += c;
+        const int64_t rb = hb[2 * k], re = hb[2 * k + 1], deg = re - rb;
+        const int64_t pos = b + k;
+        if (!parallel) {
+          tab_off.push_back((int64_t)step_tab);
+          step_tab += table_cap(deg);
+          continue;
+        }
+        tab_off.push_back((int64_t)tab_acc);
+        tab_acc += table_cap(deg);
+        occ_off.push_back((int64_t)occ_acc);
+        occ_acc += (size_t)deg + 1;
+        for (int64_t x = rb; x < re; x += kHubChunk) {
+          c_pos.push_back((int32_t)pos);
+          c_beg.push_back(x);
+          c_end.push_back(std::min<int64_t>(re, x + kHubChunk));
+        }
+        seg_b.push_back((int64_t)s_pos.size());
+        for (int64_t x = 0; x < deg + 1; x += kHubSeg) {
+          s_pos.push_back((int32_t)pos);
+          s_beg.push_back(x);
+          s_end.push_back(std::min<int64_t>(deg + 1, x + kHubSeg));
+        }
+        seg_e.push_back((int64_t)s_pos.size());
       }
-      need = std::max(need, (size_t)acc);
-      CK(cudaMemcpyAsync(hub_off_ + b, off.data(), (e - b) * sizeof(int64_t),
-                         cudaMemcpyHostToDevice, s_));
-      CK(cudaStreamSynchronize(s_));
+      need_tab = std::max(need_tab, step_tab);
+      st.hub_chunk[1] = (int64_t)c_pos.size();
+      st.hub_segs[1] = (int64_t)s_pos.size();
+      hub_pos_all.push_back(b);
+      hub_pos_all.push_back(e);
     }
-  return grow_hub(need);
+  dfree(bounds);
+  if (!parallel) {
+    TRY(grow_hub(need_tab));
+    size_t k = 0;
+    for (size_t q = 0; q < hub_pos_all.size(); q += 2) {
+      const int64_t b = hub_pos_all[q], e = hub_pos_all[q + 1];
+      std::vector<int64_t> part(tab_off.begin() + k, tab_off.begin() + k + (e - b));
+      TRY(upload(s_, hub_off_ + b, part));
+      k += e - b;
+    }
+    CK(cudaStreamSynchronize(s_));
+    return GLV_OK;
+  }
+  if (tab_acc > 0 && (tab_acc > hub_cap_ || !hub_tables_clean_)) {
+    TRY(grow_hub(tab_acc));
+    CK(cudaMemsetAsync(hub_keys_, 0xff, std::max<size_t>(hub_cap_, 1) * sizeof(int32_t), s_));
+    CK(cudaMemsetAsync(hub_vals_, 0, std::max<size_t>(hub_cap_, 1) * sizeof(double), s_));
+    hub_tables_clean_ = true;
+  }
+  if (occ_acc > hub_occ_cap_) {
+    dfree(hub_occ_);
+    hub_occ_cap_ = occ_acc;
+    TRY(alloc(&hub_occ_, hub_occ_cap_));
+  }
+  if (c_pos.size() > chunk_cap_) {
+    dfree(chunk_pos_); dfree(chunk_beg_); dfree(chunk_end_);
+    chunk_cap_ = c_pos.size();
+    TRY(alloc(&chunk_pos_, chunk_cap_)); TRY(alloc(&chunk_beg_, chunk_cap_));
+    TRY(alloc(&chunk_end_, chunk_cap_));
+  }
+  if (s_pos.size() > seg_cap_) {
+    dfree(seg_pos_); dfree(seg_beg_); dfree(seg_end_); dfree(part_g_); dfree(part_c_);
+    seg_cap_ = s_pos.size();
+    TRY(alloc(&seg_pos_, seg_cap_)); TRY(alloc(&seg_beg_, seg_cap_));
+    TRY(alloc(&seg_end_, seg_cap_)); TRY(alloc(&part_g_, seg_cap_)); TRY(alloc(&part_c_, seg_cap_));
+  }
+  TRY(upload(s_, chunk_pos_, c_pos)); TRY(upload(s_, chunk_beg_, c_beg));
+  TRY(upload(s_, chunk_end_, c_end)); TRY(upload(s_, seg_pos_, s_pos));
+  TRY(upload(s_, seg_beg_, s_beg)); TRY(upload(s_, seg_end_, s_end));
+  size_t k = 0;
+  for (size_t q = 0; q < hub_pos_all.size(); q += 2) {
+    const int64_t b = hub_pos_all[q], e = hub_pos_all[q + 1];
+    const size_t n = (size_t)(e - b);
+    TRY(upload(s_, hub_off_ + b, std::vector<int64_t>(tab_off.begin() + k, tab_off.begin() + k + n)));
+    TRY(upload(s_, hub_occ_off_ + b, std::vector<int64_t>(occ_off.begin() + k, occ_off.begin() + k + n)));
+    TRY(upload(s_, hub_seg_beg_ + b, std::vector<int64_t>(seg_b.begin() + k, seg_b.begin() + k + n)));
+    TRY(upload(s_, hub_seg_end_ + b, std::vector<int64_t>(seg_e.begin() + k, seg_e.begin() + k + n)));
+    k += n;
+  }
+  CK(cudaStreamSynchronize(s_));
+  return GLV_OK;
 }
 
 // ------------------------------------------------------------------- sweeps
@@ -565,6 +737,8 @@ int Engine::launch_sweep(const Level &L, const Step &st, SweepArgs a, bool order
         LAUNCH(k_sweep_warp<kWarpCap>, grid_for(n * 32, 256, cap), 256, smem, s_, a, lo, hi);
         break;
       }
+      case BIN_T128:
+      case BIN_T256:
       case BIN_BLOCK: {
         const size_t smem = (size_t)kBlockCap * (sizeof(double) + sizeof(int32_t));
         LAUNCH(k_sweep_block, (int)std::min<int64_t>(n, nsm_ * 2), 256, smem, s_, a, lo, hi, 0,
@@ -572,8 +746,19 @@ int Engine::launch_sweep(const Level &L, const Step &st, SweepArgs a, bool order
         break;
       }
       case BIN_HUB:
-        LAUNCH(k_sweep_block, (int)std::min<int64_t>(n, nsm_), 512, 0, s_, a, lo, hi, 1,
-               ordered_acc ? 1 : 0);
+        if (ordered_acc) {
+          LAUNCH(k_sweep_block, (int)std::min<int64_t>(n, nsm_), 512, 0, s_, a, lo, hi, 1, 1);
+        } else {
+          const HubWork hw = hub_work();
+          const int64_t nc = st.hub_chunk[1] - st.hub_chunk[0];
+          const int64_t ns = st.hub_segs[1] - st.hub_segs[0];
+          LAUNCH(k_hub_accum, (int)std::min<int64_t>(nc, nsm_ * 4), 512,
+                 kHubStageCap * (sizeof(double) + sizeof(int32_t)), s_, a, hw, st.hub_chunk[0],
+                 st.hub_chunk[1]);
+          LAUNCH(k_hub_scan, (int)std::min<int64_t>(ns, nsm_ * 8), 256, 0, s_, a, hw,
+                 st.hub_segs[0], st.hub_segs[1]);
+          LAUNCH(k_hub_final, grid_for(n * 32, 256, nsm_ * 4), 256, 0, s_, a, hw, lo, hi);
+        }
         break;
     }
     if (pr) TRY(pr->end(pidx, s_));
@@ -662,6 +847,7 @@ int Engine::coloring_phase(const Level &L, int ncolors, bool stale, double lower
   a.hub_keys = hub_keys_; a.hub_vals = hub_vals_; a.hub_off = hub_off_;
   CK(cudaMemcpyAsync(&a.constant, cst, sizeof(double), cudaMemcpyDeviceToHost, s_));
   CK(cudaStreamSynchronize(s_));
+  if (persistent()) return run_persistent(L, sched, a, false, lower, thresh, mod, itr);
   cudaGraphExec_t exec = nullptr;
   long nodes = 0;
   Probes pr;
@@ -736,6 +922,13 @@ int Engine::basic_phase(const Level &L, double lower, double thresh, double *mod
   a.hub_keys = hub_keys_; a.hub_vals = hub_vals_; a.hub_off = hub_off_;
   CK(cudaMemcpyAsync(&a.constant, cst, sizeof(double), cudaMemcpyDeviceToHost, s_));
   CK(cudaStreamSynchronize(s_));
+  if (persistent()) {
+    TRY(run_persistent(L, sched, a, true, lower, thresh, mod, itr));
+    // C = pastCommAss (parallelLouvainMethod.cpp:304-307)
+    CK(cudaMemcpyAsync(C, Cpast, L.nv * sizeof(int32_t), cudaMemcpyDeviceToDevice, s_));
+    CK(cudaStreamSynchronize(s_));
+    return GLV_OK;
+  }
   cudaGraphExec_t exec = nullptr;
   long nodes = 0;
   // Q is taken on the state before the moves (parallelLouvainMethod.cpp:244-255);
@@ -827,6 +1020,172 @@ int Engine::decide(const Level &L, const int32_t *verts, int64_t nverts) {
   return GLV_OK;
 }
 
+// One cooperative launch per iteration (persist.cuh).  Colour phases: C is
+// updated in place and Q is taken after the sweep; Jacobi phases: targets go
+// to Ctgt, Q is taken on the state before the moves, and the loop rotates
+// past <- curr <- target after an accepted iteration.
+int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched, SweepArgs a,
+                           bool jacobi, double lower, double thresh, double *mod, int *itr) {
+  std::vector<StepDesc> steps;
+  for (auto &cs : sched)
+    for (size_t k = 0; k < cs.steps.size(); ++k) {
+      const Step &st = cs.steps[k];
+      StepDesc d;
+      for (int b = 0; b <= NBINS; ++b) d.seg[b] = st.seg[b];
+      d.hub_chunk[0] = st.hub_chunk[0]; d.hub_chunk[1] = st.hub_chunk[1];
+      d.hub_segs[0] = st.hub_segs[0]; d.hub_segs[1] = st.hub_segs[1];
+      const bool last = (k + 1 == cs.steps.size());
+      d.apply[0] = last ? cs.begin : 0;
+      d.apply[1] = last ? cs.end : 0;
+      steps.push_back(d);
+    }
+  StepDesc *d_steps = nullptr;
+  int64_t *d_ctr = nullptr;
+  TRY(alloc(&d_steps, steps.size()));
+  TRY(alloc(&d_ctr, steps.size()));
+  TRY(upload(s_, d_steps, steps));
+  IterArgs p{};
+  p.a = a;
+  p.h = hub_work();
+  p.steps = d_steps;
+  p.nsteps = (int)steps.size();
+  p.jacobi = jacobi ? 1 : 0;
+  p.nv = L.nv;
+  p.C_mod = C;
+  p.own_w_mod = jacobi ? own_w : nullptr;
+  p.part_e = part_e_;
+  p.part_a = part_a_;
+  p.cst = cst;
+  p.mod_out = mod_out_;
+  p.cDeg = cDeg;
+  p.cSize = cSize;
+  p.task_ctr = d_ctr;
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_iteration, kPersistThreads,
+                                                   kPersistSmem));
+  if (per_sm < 1) return fail(GLV_ERR_CUDA, "persistent sweep kernel does not fit on an SM");
+  const int grid = per_sm * nsm_;
+  void *args[] = {&p};
+  const bool debug = getenv("GRAPPOLO_B200_DEBUG") != nullptr;
+  uint64_t *d_trace = nullptr;
+  std::vector<uint64_t> h_trace;
+  if (debug) {
+    TRY(alloc(&d_trace, 4 * steps.size() + 2));
+    CK(cudaMemsetAsync(d_trace, 0, (4 * steps.size() + 2) * sizeof(uint64_t), s_));
+    h_trace.resize(4 * steps.size() + 2);
+    p.trace = d_trace;
+  }
+  const int level = g_profile.load();
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (level > 0) {
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+  }
+  double prev = jacobi ? -1.0 : lower;
+  int n = 0;
+  int rc = GLV_OK;
+  while (true) {
+    ++n;
+    const double t0 = now_s();
+    cudaError_t e = cudaMemsetAsync(d_ctr, 0, steps.size() * sizeof(int64_t), s_);
+    if (e0) cudaEventRecord(e0, s_);
+    if (e == cudaSuccess)
+      e = cudaLaunchCooperativeKernel((void *)k_sweep_iteration, grid, kPersistThreads, args,
+                                      kPersistSmem, s_);
+    if (e1) cudaEventRecord(e1, s_);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(h_mod_, mod_out_, 3 * sizeof(double), cudaMemcpyDeviceToHost, s_);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s_);
+    t_sweep += now_s() - t0;
+    if (e != cudaSuccess) { g_err = cudaGetErrorString(e); rc = GLV_ERR_CUDA; break; }
+    ++launches_;
+    edges_swept += (double)L.nnz;
+    if (e0) {
+      float ms = 0;
+      if (cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) sweep_kernel_s += ms * 1e-3;
+      sweep_bytes += 32.0 * (double)L.nnz + 48.0 * (double)L.nv;
+      ++sweep_steps;
+    }
+    if (debug) {
+      CK(cudaMemcpy(h_trace.data(), d_trace, h_trace.size() * sizeof(uint64_t),
+                    cudaMemcpyDeviceToHost));
+      // per step: stage-1 time (from the previous barrier), hub stages, apply
+      const size_t ns = steps.size();
+      uint64_t last = h_trace[4 * ns];
+      double st1 = 0, st23 = 0, st4 = 0, worst = 0;
+      size_t worst_k = 0;
+      for (size_t k = 0; k < ns; ++k) {
+        const double a1 = (h_trace[4 * k] - last) * 1e-9;
+        st1 += a1;
+        const uint64_t t1 = h_trace[4 * k];
+        uint64_t t = t1;
+        if (steps[k].hub_segs[1] > steps[k].hub_segs[0]) { st23 += (h_trace[4 * k + 2] - t) * 1e-9; t = h_trace[4 * k + 2]; }
+        if (steps[k].apply[1] > steps[k].apply[0]) { st4 += (h_trace[4 * k + 3] - t) * 1e-9; t = h_trace[4 * k + 3]; }
+        const double tot = (t - last) * 1e-9;
+        if (tot > worst) { worst = tot; worst_k = k; }
+        last = t;
+      }
+      const double tm = (h_trace[4 * ns + 1] - last) * 1e-9;
+      if (n == 1 || n == 2) {
+        // ten slowest steps with their composition
+        std::vector<std::pair<double, size_t>> per;
+        uint64_t prevt = h_trace[4 * ns];
+        for (size_t k = 0; k < ns; ++k) {
+          uint64_t t = h_trace[4 * k];
+          if (steps[k].hub_segs[1] > steps[k].hub_segs[0]) t = h_trace[4 * k + 2];
+          if (steps[k].apply[1] > steps[k].apply[0]) t = h_trace[4 * k + 3];
+          per.push_back({(t - prevt) * 1e-9, k});
+          prevt = t;
+        }
+        std::sort(per.begin(), per.end(), [](auto &x, auto &y) { return x.first > y.first; });
+        for (size_t q = 0; q < std::min<size_t>(10, per.size()); ++q) {
+          const StepDesc &d = steps[per[q].second];
+          fprintf(stderr, "   step %zu: %.1f us bins", per[q].second, per[q].first * 1e6);
+          for (int b = 0; b < NBINS; ++b) fprintf(stderr, " %ld", (long)(d.seg[b + 1] - d.seg[b]));
+          fprintf(stderr, " hub_chunks %ld hub_segs %ld\n", (long)(d.hub_chunk[1] - d.hub_chunk[0]),
+                  (long)(d.hub_segs[1] - d.hub_segs[0]));
+        }
+        for (double qf : {0.25, 0.5, 0.75, 0.9}) {
+          const auto &x = per[(size_t)(qf * (per.size() - 1))];
+          const StepDesc &d = steps[x.second];
+          int64_t edges = 0;
+          fprintf(stderr, "   q%.2f step %zu: %.1f us bins", qf, x.second, x.first * 1e6);
+          for (int b = 0; b < NBINS; ++b) fprintf(stderr, " %ld", (long)(d.seg[b + 1] - d.seg[b]));
+          (void)edges;
+          fprintf(stderr, " hub_chunks %ld hub_segs %ld\n", (long)(d.hub_chunk[1] - d.hub_chunk[0]),
+                  (long)(d.hub_segs[1] - d.hub_segs[0]));
+        }
+        std::vector<double> t_only;
+        for (auto &x : per) t_only.push_back(x.first);
+        std::sort(t_only.begin(), t_only.end());
+        fprintf(stderr, "   step time median %.1f us p90 %.1f us\n", t_only[t_only.size() / 2] * 1e6,
+                t_only[t_only.size() * 9 / 10] * 1e6);
+      }
+      fprintf(stderr,
+              "grappolo_b200: iter %d nv=%ld steps=%zu stage1=%.4f hubs=%.4f apply=%.4f "
+              "modularity=%.4f worst step %zu (%.5f s, %ld members, %ld hub chunks)\n",
+              n, (long)L.nv, ns, st1, st23, st4, tm, worst_k, worst,
+              (long)(steps[worst_k].seg[NBINS] - steps[worst_k].seg[0]),
+              (long)(steps[worst_k].hub_chunk[1] - steps[worst_k].hub_chunk[0]));
+    }
+    const double q = h_mod_[0];
+    if (q - prev < thresh) break;
+    prev = q;
+    if (jacobi) {
+      if (prev < lower) prev = lower;
+      LAUNCH(k_rotate, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, Cpast, C, Ctgt);
+    }
+  }
+  dfree(d_trace);
+  dfree(d_ctr);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  dfree(d_steps);
+  *mod = prev;
+  *itr = n;
+  return rc;
+}
+
 // --------------------------------------------------------------- renumbering
 int Engine::renumber(int32_t *Cm, int64_t n, int64_t *ncl) {
   if (n == 0) { *ncl = 0; return GLV_OK; }
@@ -859,6 +1218,15 @@ __global__ void k_add_counts(int64_t n, const int64_t *a, const int64_t *b, int6
 
 int Engine::coarsen(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
                     int64_t *num_edges) {
+  const bool debug = getenv("GRAPPOLO_B200_DEBUG") != nullptr;
+  double tdbg = now_s();
+  auto mark = [&](const char *what) {
+    if (!debug) return;
+    cudaStreamSynchronize(s_);
+    const double t = now_s();
+    fprintf(stderr, "grappolo_b200: coarsen %s %.4f s\n", what, t - tdbg);
+    tdbg = t;
+  };
   const int nb = bits_for(std::max<int64_t>(ncl - 1, 1));
   const uint64_t sentinel = 1ull << (2 * nb);
   const int end_bit = 2 * nb + 1;
@@ -872,31 +1240,53 @@ int Engine::coarsen(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
   size_t tb = 0;
   CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, k1, k2, v1, v2, n, 0, end_bit, s_));
   TRY(temp(tb));
+  mark("records");
   CK(cub::DeviceRadixSort::SortPairs(temp_, tb, k1, k2, v1, v2, n, 0, end_bit, s_));
+  mark("sort");
   dfree(k1); dfree(v1);
-  int32_t *flag;
-  int64_t *uidx;
-  TRY(alloc(&flag, n)); TRY(alloc(&uidx, n));
-  LAUNCH(k_segment_heads, g, 256, 0, s_, n, k2, sentinel, flag);
-  CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, flag, uidx, n, s_));
-  TRY(temp(tb));
-  CK(cub::DeviceScan::ExclusiveSum(temp_, tb, flag, uidx, n, s_));
-  int64_t hu;
-  int32_t hf;
-  CK(cudaMemcpyAsync(&hu, uidx + n - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
-  CK(cudaMemcpyAsync(&hf, flag + n - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
-  CK(cudaStreamSynchronize(s_));
-  const int64_t np = hu + hf;
   uint64_t *ukeys;
   double *uvals;
-  TRY(alloc(&ukeys, np)); TRY(alloc(&uvals, np));
+  int64_t np = 0;
   if (ordered()) {
+    // one thread folds each pair's records in (i, j) order
+    int32_t *flag;
+    int64_t *uidx;
+    TRY(alloc(&flag, n)); TRY(alloc(&uidx, n));
+    LAUNCH(k_segment_heads, g, 256, 0, s_, n, k2, sentinel, flag);
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, flag, uidx, n, s_));
+    TRY(temp(tb));
+    CK(cub::DeviceScan::ExclusiveSum(temp_, tb, flag, uidx, n, s_));
+    int64_t hu;
+    int32_t hf;
+    CK(cudaMemcpyAsync(&hu, uidx + n - 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
+    CK(cudaMemcpyAsync(&hf, flag + n - 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
+    CK(cudaStreamSynchronize(s_));
+    np = hu + hf;
+    TRY(alloc(&ukeys, np)); TRY(alloc(&uvals, np));
     LAUNCH(k_fold_pairs, g, 256, 0, s_, n, k2, v2, flag, uidx, sentinel, ukeys, uvals);
+    dfree(flag); dfree(uidx);
   } else {
-    CK(cudaMemsetAsync(uvals, 0, np * sizeof(double), s_));
-    LAUNCH(k_scatter_pairs, g, 256, 0, s_, n, k2, v2, flag, uidx, sentinel, ukeys, uvals);
+    // reduce-by-key over the sorted records (the sentinel run is dropped by
+    // counting only keys below it)
+    int64_t *d_np;
+    TRY(alloc(&ukeys, n)); TRY(alloc(&uvals, n)); TRY(alloc(&d_np, 1));
+    CK(cub::DeviceReduce::ReduceByKey(nullptr, tb, k2, ukeys, v2, uvals, d_np, cuda::std::plus<>{},
+                                      n, s_));
+    TRY(temp(tb));
+    CK(cub::DeviceReduce::ReduceByKey(temp_, tb, k2, ukeys, v2, uvals, d_np, cuda::std::plus<>{},
+                                      n, s_));
+    CK(cudaMemcpyAsync(&np, d_np, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
+    CK(cudaStreamSynchronize(s_));
+    dfree(d_np);
+    uint64_t last = 0;
+    if (np > 0) {
+      CK(cudaMemcpyAsync(&last, ukeys + np - 1, sizeof(uint64_t), cudaMemcpyDeviceToHost, s_));
+      CK(cudaStreamSynchronize(s_));
+      if (last >= sentinel) --np;
+    }
   }
-  dfree(k2); dfree(v2); dfree(flag); dfree(uidx);
+  dfree(k2); dfree(v2);
+  mark("fold");
   int64_t *lower_cnt, *upper_cnt, *ne_off, *rowc, *lower_first, *upper_first;
   TRY(alloc(&lower_cnt, ncl)); TRY(alloc(&upper_cnt, ncl)); TRY(alloc(&ne_off, 1));
   TRY(alloc(&rowc, ncl + 1)); TRY(alloc(&lower_first, ncl)); TRY(alloc(&upper_first, ncl));
@@ -932,6 +1322,7 @@ int Engine::coarsen(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
   LAUNCH(k_emit_upper, gp, 256, 0, s_, np, tk2, tv2, nb, o.ptr, lower_cnt, upper_first, o.tail,
          o.w, sentinel);
   CK(cudaStreamSynchronize(s_));
+  mark("emit");
   dfree(tk1); dfree(tk2); dfree(tv1); dfree(tv2); dfree(ukeys); dfree(uvals);
   dfree(lower_cnt); dfree(upper_cnt); dfree(ne_off); dfree(rowc); dfree(lower_first);
   dfree(upper_first);
@@ -1125,6 +1516,8 @@ static int device_ready() {
   if (!attrs) {
     cudaFuncSetAttribute(k_sweep_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          kBlockCap * (int)(sizeof(double) + sizeof(int32_t)));
+    cudaFuncSetAttribute(k_sweep_iteration, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kPersistSmem);
     attrs = true;
   }
   return GLV_OK;
@@ -1156,9 +1549,13 @@ static int open_call(Call &c, int mode, long nv, const long *ptr, const glv_edge
   L.nv = nv;
   L.nnz = nnz;
   L.owned = true;
-  CK(cudaMallocAsync((void **)&L.ptr, (nv + 1) * sizeof(int64_t), c.s));
-  CK(cudaMallocAsync((void **)&L.tail, std::max<int64_t>(nnz, 1) * sizeof(int32_t), c.s));
-  CK(cudaMallocAsync((void **)&L.w, std::max<int64_t>(nnz, 1) * sizeof(double), c.s));
+  cudaMemPool_t pool = engine_pool();
+  if (!pool) return fail(GLV_ERR_CUDA, "could not create the device memory pool");
+  CK(cudaMallocFromPoolAsync((void **)&L.ptr, (nv + 1) * sizeof(int64_t), pool, c.s));
+  CK(cudaMallocFromPoolAsync((void **)&L.tail, std::max<int64_t>(nnz, 1) * sizeof(int32_t), pool,
+                             c.s));
+  CK(cudaMallocFromPoolAsync((void **)&L.w, std::max<int64_t>(nnz, 1) * sizeof(double), pool,
+                             c.s));
   CK(cudaMemcpyAsync(L.ptr, ptr, (nv + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c.s));
   // Edges move in chunks through one device staging buffer.
   const int64_t chunk = std::min<int64_t>(std::max<int64_t>(nnz, 1), 1 << 24);
@@ -1166,7 +1563,7 @@ static int open_call(Call &c, int mode, long nv, const long *ptr, const glv_edge
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
   if (edges) {
     glv_edge *stage;
-    CK(cudaMallocAsync((void **)&stage, chunk * sizeof(glv_edge), c.s));
+    CK(cudaMallocFromPoolAsync((void **)&stage, chunk * sizeof(glv_edge), engine_pool(), c.s));
     for (int64_t b = 0; b < nnz; b += chunk) {
       const int64_t n = std::min(chunk, nnz - b);
       CK(cudaMemcpyAsync(stage, edges + b, n * sizeof(glv_edge), cudaMemcpyHostToDevice, c.s));
@@ -1178,8 +1575,8 @@ static int open_call(Call &c, int mode, long nv, const long *ptr, const glv_edge
   } else if (nnz > 0) {
     int64_t *stage;
     int32_t *bad;
-    CK(cudaMallocAsync((void **)&stage, chunk * sizeof(int64_t), c.s));
-    CK(cudaMallocAsync((void **)&bad, sizeof(int32_t), c.s));
+    CK(cudaMallocFromPoolAsync((void **)&stage, chunk * sizeof(int64_t), engine_pool(), c.s));
+    CK(cudaMallocFromPoolAsync((void **)&bad, sizeof(int32_t), engine_pool(), c.s));
     CK(cudaMemsetAsync(bad, 0, sizeof(int32_t), c.s));
     for (int64_t b = 0; b < nnz; b += chunk) {
       const int64_t n = std::min(chunk, nnz - b);
@@ -1202,7 +1599,7 @@ static int download_ids(Call &c, const int32_t *d, int64_t n, long *host) {
   if (n == 0) return GLV_OK;
   const double t0 = now_s();
   int64_t *tmp;
-  CK(cudaMallocAsync((void **)&tmp, n * sizeof(int64_t), c.s));
+  CK(cudaMallocFromPoolAsync((void **)&tmp, n * sizeof(int64_t), engine_pool(), c.s));
   k_widen<<<grid_for(n, 256, 148 * 8), 256, 0, c.s>>>(n, d, tmp);
   ++c.launches;
   CK(cudaGetLastError());
@@ -1217,8 +1614,8 @@ static int upload_ids(Call &c, const long *host, int64_t n, int32_t *d, int64_t 
   if (n == 0) return GLV_OK;
   int64_t *tmp;
   int32_t *bad;
-  CK(cudaMallocAsync((void **)&tmp, n * sizeof(int64_t), c.s));
-  CK(cudaMallocAsync((void **)&bad, sizeof(int32_t), c.s));
+  CK(cudaMallocFromPoolAsync((void **)&tmp, n * sizeof(int64_t), engine_pool(), c.s));
+  CK(cudaMallocFromPoolAsync((void **)&bad, sizeof(int32_t), engine_pool(), c.s));
   CK(cudaMemsetAsync(bad, 0, sizeof(int32_t), c.s));
   CK(cudaMemcpyAsync(tmp, host, n * sizeof(int64_t), cudaMemcpyHostToDevice, c.s));
   k_narrow<<<grid_for(n, 256, 148 * 8), 256, 0, c.s>>>(n, tmp, d, bad, hi);
@@ -1242,7 +1639,7 @@ static int run_host(int mode, long nv, const long *ptr, const glv_edge *edges, c
   Call c;
   TRY(open_call(c, mode, nv, ptr, edges, tail64, w));
   int32_t *dC;
-  CK(cudaMallocAsync((void **)&dC, std::max<long>(nv, 1) * sizeof(int32_t), c.s));
+  CK(cudaMallocFromPoolAsync((void **)&dC, std::max<long>(nv, 1) * sizeof(int32_t), engine_pool(), c.s));
   TRY(c.eng->run_multiphase(c.L0, dC, coloring, min_graph_size, threshold, c_threshold, st));
   TRY(download_ids(c, dC, nv, C_orig));
   CK(cudaFreeAsync(dC, c.s));
@@ -1263,6 +1660,11 @@ extern "C" {
 const char *glv_version(void) { return "grappolo_b200 0.1 (sm_100a)"; }
 const char *glv_last_error(void) { return g_err.c_str(); }
 long glv_kernel_launch_count(void) { return g_launches.load(); }
+void glv_release_cached_memory(void) {
+  std::lock_guard<std::mutex> lock(g_pool_mu);
+  for (auto &p : g_pool)
+    if (p) cudaMemPoolTrimTo(p, 0);
+}
 void glv_set_profiling(int on) { g_profile = on < 0 ? 0 : (on > 2 ? 2 : on); }
 
 int glv_run_multiphase_coloring(const glv_graph *G, long *C_orig, int coloring, int numColors,
@@ -1433,7 +1835,7 @@ int glv_build_next_level(const glv_graph *Gin, glv_graph *Gout, const long *C,
     return fail(GLV_ERR_OOM, "host allocation failed");
   }
   glv_edge *daos;
-  CK(cudaMallocAsync((void **)&daos, std::max<int64_t>(out.nnz, 1) * sizeof(glv_edge), c.s));
+  CK(cudaMallocFromPoolAsync((void **)&daos, std::max<int64_t>(out.nnz, 1) * sizeof(glv_edge), engine_pool(), c.s));
   k_fill_aos<<<grid_for(out.nv, 256, 148 * 8), 256, 0, c.s>>>(out.nv, out.ptr, out.tail, out.w,
                                                               daos);
   ++c.launches;
@@ -1481,7 +1883,7 @@ int glv_decide_batch(long nv, const long *ptr, const long *tail, const double *w
   double cst2[2] = {constant, 0.0};
   CK(cudaMemcpyAsync(e.cst, cst2, sizeof(cst2), cudaMemcpyHostToDevice, c.s));
   int32_t *dv;
-  CK(cudaMallocAsync((void **)&dv, std::max<long>(nverts, 1) * sizeof(int32_t), c.s));
+  CK(cudaMallocFromPoolAsync((void **)&dv, std::max<long>(nverts, 1) * sizeof(int32_t), engine_pool(), c.s));
   TRY(upload_ids(c, verts, nverts, dv, nv));
   CK(cudaStreamSynchronize(c.s));
   TRY(e.decide(c.L0, dv, nverts));

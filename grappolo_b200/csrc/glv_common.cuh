@@ -19,10 +19,12 @@ enum Bin : int {
   BIN_G8 = 1,      // 5..8             : 8 lanes per vertex
   BIN_G16 = 2,     // 9..16            : 16 lanes per vertex
   BIN_G32 = 3,     // 17..32           : one warp per vertex
-  BIN_WARP = 4,    // 33..kWarpMax     : one warp, shared-memory hash table
-  BIN_BLOCK = 5,   // ..kBlockMax      : one block, shared-memory hash table
-  BIN_HUB = 6,     // > kBlockMax      : one block, global-memory hash table
-  NBINS = 7
+  BIN_WARP = 4,    // 33..127          : one warp, shared-memory table (<= 256 slots)
+  BIN_T128 = 5,    // 128..511         : 128-thread team, shared table (<= 1024 slots)
+  BIN_T256 = 6,    // 512..1023        : 256-thread team, shared table (<= 2048 slots)
+  BIN_BLOCK = 7,   // 1024..block_max  : 512-thread block, shared table (<= 4096 slots)
+  BIN_HUB = 8,     // > block_max      : whole grid per row, global-memory table
+  NBINS = 9
 };
 
 struct BinLimits {
@@ -36,8 +38,10 @@ __host__ __device__ inline int degree_bin(int64_t deg, BinLimits lim) {
   if (deg <= 16) return BIN_G16;
   if (deg <= 32) return BIN_G32;
   if (deg <= lim.warp_max) return BIN_WARP;
-  if (deg <= lim.block_max) return BIN_BLOCK;
-  return BIN_HUB;
+  if (deg > lim.block_max) return BIN_HUB;
+  if (deg <= 511) return BIN_T128;
+  if (deg <= 1023) return BIN_T256;
+  return BIN_BLOCK;
 }
 
 __host__ __device__ inline uint32_t next_pow2(uint32_t x) {
@@ -51,8 +55,13 @@ __host__ __device__ inline uint32_t table_cap(int64_t deg) {
   return next_pow2((uint32_t)(2 * (deg + 1)));
 }
 
+// Table slot of a community id.  The product's high bits are folded into the
+// low ones: the low bits of key * odd depend only on the key's low bits, and
+// vertex ids of R-MAT-like graphs share long runs of zero bits, which would
+// pile them into a few slots.
 __device__ __forceinline__ uint32_t hash_slot(int32_t key, uint32_t mask) {
-  return ((uint32_t)key * 0x9E3779B1u) & mask;
+  const uint32_t h = (uint32_t)key * 0x9E3779B1u;
+  return (h ^ (h >> 15)) & mask;
 }
 
 // 32-bit integer mixer (Wang/Jenkins style) used for colouring priorities.

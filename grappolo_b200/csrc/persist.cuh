@@ -1,0 +1,248 @@
+// One Louvain iteration in one cooperative launch (parallel-accumulation modes).
+//
+// The colour classes of an iteration depend on each other (a class decides
+// against the community totals left by the classes before it), and R-MAT-like
+// graphs need hundreds of classes, most of them small and made of high-degree
+// vertices.  Launching a few kernels per class leaves the GPU waiting on
+// launches and on the single largest row of each class.  Here every block of
+// a persistent grid takes part in every class:
+//   stage 1  hub chunks (global tables); rows of 1024..2047 entries per
+//            block, 512..1023 per 256-thread team, 128..511 per 128-thread
+//            team (shared tables); then warp items (rows <= 32 entries, and
+//            33..127-entry rows with a per-warp shared table)  -> grid barrier
+//   stage 2  hub table segments -> partial arg-maxes            -> grid barrier
+//   stage 3  one warp per hub folds its partials                -> grid barrier
+//   stage 4  community totals += the class's deltas             -> grid barrier
+// (stages 2-3 only for classes with hubs; stage 4 after the class's last
+// sublevel), then the modularity pass of the iteration.
+#pragma once
+
+#include <cooperative_groups.h>
+
+#include "phase_kernels.cuh"
+#include "sweep.cuh"
+
+namespace glv {
+
+struct StepDesc {
+  int64_t seg[NBINS + 1];  // member positions of each degree bin
+  int64_t hub_chunk[2];    // hub accumulation work items
+  int64_t hub_segs[2];     // hub scan work items
+  int64_t apply[2];        // member range whose deltas are applied after this step
+};
+
+struct IterArgs {
+  SweepArgs a;
+  HubWork h;
+  const StepDesc *steps;
+  int nsteps;
+  int jacobi;              // 1: Q on the state before the moves, totals updated after
+  int64_t nv;
+  const int32_t *C_mod;    // communities the modularity pass compares (colour phases)
+  const double *own_w_mod; // Jacobi phases: Counter[own] per vertex
+  double *part_e, *part_a; // per 256-vertex tile partials
+  const double *cst;       // {constant, 2m}
+  double *mod_out;         // {Q, e_xx, a2_x}
+  double *cDeg;
+  int32_t *cSize;
+  uint64_t *trace;         // optional: globaltimer at each barrier, 4 per step + 2
+  int64_t *task_ctr;       // per step: next stage-1 task (zero at launch)
+};
+
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+#define GLV_TRACE(slot)                                                  \
+  do {                                                                   \
+    if (p.trace && blockIdx.x == 0 && threadIdx.x == 0) p.trace[slot] = global_ns(); \
+  } while (0)
+
+constexpr int kPersistThreads = 512;
+constexpr int kPersistTableCap = 4096;  // BIN_BLOCK rows: degree <= 2047
+constexpr int kPersistWarpCap = 256;    // warp-table rows: degree <= 127
+constexpr size_t kPersistSmem = (size_t)kPersistTableCap * (sizeof(double) + sizeof(int32_t));
+static_assert(kPersistSmem >= (size_t)(kPersistThreads / 32) * kPersistWarpCap *
+                                  (sizeof(double) + sizeof(int32_t)),
+              "warp tables must fit in the block-table region");
+
+// Community totals += the deltas the sweep accumulated (see k_apply_deltas).
+__device__ __forceinline__ void apply_deltas_range(const IterArgs &p, int64_t b, int64_t e,
+                                                   int64_t gt, int64_t ngt) {
+  for (int64_t pos = b + gt; pos < e; pos += ngt) {
+    const int32_t o = p.a.move_old[pos];
+    if (o < 0) continue;
+    const int32_t cs[2] = {p.a.move_new[pos], o};
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+      const int32_t c = cs[k];
+      const unsigned long long bits = atomicExch((unsigned long long *)&p.a.dDeg[c], 0ull);
+      if (bits != 0ull) p.cDeg[c] = __dadd_rn(p.cDeg[c], __longlong_as_double((long long)bits));
+      const int32_t s = atomicExch(&p.a.dSize[c], 0);
+      if (s != 0) p.cSize[c] += s;
+    }
+  }
+}
+
+// Modularity partials of one 256-vertex tile (all threads of the block call).
+__device__ __forceinline__ void modularity_tile(const IterArgs &p, int64_t tile, int64_t *s_ptr,
+                                                int32_t *s_cc, double *sh) {
+  const int64_t v0 = tile * kModVB, v1 = min(p.nv, v0 + kModVB);
+  const int nvb = (int)(v1 - v0);
+  double a2 = 0.0, ex = 0.0;
+  if (threadIdx.x < nvb) {
+    const double d = p.cDeg[v0 + threadIdx.x];
+    a2 = __dmul_rn(d, d);
+  }
+  if (p.own_w_mod) {
+    if (threadIdx.x < nvb) ex = p.own_w_mod[v0 + threadIdx.x];
+  } else {
+    for (int k = threadIdx.x; k <= nvb; k += blockDim.x) s_ptr[k] = p.a.ptr[v0 + k];
+    for (int k = threadIdx.x; k < nvb; k += blockDim.x) s_cc[k] = p.C_mod[v0 + k];
+    __syncthreads();
+    const int64_t eb = s_ptr[0], ee = s_ptr[nvb];
+    int hh = 0;
+    for (int64_t e = eb + threadIdx.x; e < ee; e += blockDim.x) {
+      while (s_ptr[hh + 1] <= e) ++hh;
+      if (p.C_mod[p.a.tail[e]] == s_cc[hh]) ex = __dadd_rn(ex, p.a.w[e]);
+    }
+  }
+  ex = block_sum<kPersistThreads>(ex, sh);
+  a2 = block_sum<kPersistThreads>(a2, sh);
+  if (threadIdx.x == 0) { p.part_e[tile] = ex; p.part_a[tile] = a2; }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void modularity_fold(const IterArgs &p, int64_t ntiles, double *sh) {
+  double e = 0.0, a = 0.0;
+  const int64_t per = (ntiles + blockDim.x - 1) / blockDim.x;
+  const int64_t b = threadIdx.x * per, en = min(ntiles, b + per);
+  for (int64_t i = b; i < en; ++i) { e = __dadd_rn(e, p.part_e[i]); a = __dadd_rn(a, p.part_a[i]); }
+  e = block_sum<kPersistThreads>(e, sh);
+  a = block_sum<kPersistThreads>(a, sh);
+  if (threadIdx.x == 0) {
+    const double c = p.cst[0];
+    p.mod_out[0] = __dsub_rn(__dmul_rn(e, c), __dmul_rn(__dmul_rn(a, c), c));
+    p.mod_out[1] = e;
+    p.mod_out[2] = a;
+  }
+}
+
+__global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs p) {
+  cg::grid_group grid = cg::this_grid();
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ double s_self[32], s_g[32], sh[32];
+  __shared__ int32_t s_c[32];
+  __shared__ int64_t s_ptr[kModVB + 1];
+  __shared__ int32_t s_cc[kModVB];
+  const int warp = threadIdx.x >> 5, nwb = blockDim.x >> 5;
+  const int64_t gw = (int64_t)blockIdx.x * nwb + warp, ngw = (int64_t)gridDim.x * nwb;
+  const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t ngt = (int64_t)gridDim.x * blockDim.x;
+  double *tvals = reinterpret_cast<double *>(smem_raw);
+  double *wvals = tvals + (size_t)warp * kPersistWarpCap;
+  int32_t *wkeys = reinterpret_cast<int32_t *>(tvals + (size_t)nwb * kPersistWarpCap) +
+                   (size_t)warp * kPersistWarpCap;
+  GLV_TRACE(4 * p.nsteps);
+  __shared__ int64_t s_task;
+  for (int s = 0; s < p.nsteps; ++s) {
+    const StepDesc &st = p.steps[s];
+    // Stage 1 as a task queue: blocks take the next task of any kind, the
+    // heaviest kinds first, so no block serialises several kinds.
+    const int64_t n4 = st.seg[1] - st.seg[0], n8 = st.seg[2] - st.seg[1];
+    const int64_t n16 = st.seg[3] - st.seg[2], n32 = st.seg[4] - st.seg[3];
+    const int64_t nw = st.seg[5] - st.seg[4];
+    const int64_t i4 = (n4 + 7) / 8, i8 = (n8 + 3) / 4, i16 = (n16 + 1) / 2;
+    const int64_t witems = i4 + i8 + i16 + n32 + nw;
+    const int64_t t_hub = st.hub_chunk[1] - st.hub_chunk[0];
+    const int64_t t_blk = st.seg[BIN_BLOCK + 1] - st.seg[BIN_BLOCK];
+    const int64_t t_256 = (st.seg[BIN_T256 + 1] - st.seg[BIN_T256] + 1) / 2;
+    const int64_t t_128 = (st.seg[BIN_T128 + 1] - st.seg[BIN_T128] + 3) / 4;
+    const int64_t t_w = (witems + nwb - 1) / nwb;
+    const int64_t ntask = t_hub + t_blk + t_256 + t_128 + t_w;
+    while (true) {
+      if (threadIdx.x == 0) s_task = atomicAdd((unsigned long long *)&p.task_ctr[s], 1ull);
+      __syncthreads();
+      int64_t t = s_task;
+      __syncthreads();
+      if (t >= ntask) break;
+      if (t < t_hub) {
+        hub_accum_chunk(p.a, p.h, st.hub_chunk[0] + t, reinterpret_cast<int32_t *>(tvals + 4096),
+                        tvals, s_self);
+        continue;
+      }
+      t -= t_hub;
+      if (t < t_blk) {
+        team_vertex<512>(p.a, st.seg[BIN_BLOCK] + t, reinterpret_cast<int32_t *>(tvals + 4096),
+                         tvals, 0, s_self, s_g, s_c);
+        continue;
+      }
+      t -= t_blk;
+      if (t < t_256) {
+        // two 256-thread teams, tables of 2048 slots
+        const int team = threadIdx.x / 256;
+        const int64_t pos = st.seg[BIN_T256] + 2 * t + team;
+        if (pos < st.seg[BIN_T256 + 1])
+          team_vertex<256>(p.a, pos, reinterpret_cast<int32_t *>(tvals + 4096) + team * 2048,
+                           tvals + team * 2048, team, s_self + 8 * team, s_g + 8 * team,
+                           s_c + 8 * team);
+        continue;
+      }
+      t -= t_256;
+      if (t < t_128) {
+        // four 128-thread teams, tables of 1024 slots
+        const int team = threadIdx.x / 128;
+        const int64_t pos = st.seg[BIN_T128] + 4 * t + team;
+        if (pos < st.seg[BIN_T128 + 1])
+          team_vertex<128>(p.a, pos, reinterpret_cast<int32_t *>(tvals + 4096) + team * 1024,
+                           tvals + team * 1024, team, s_self + 4 * team, s_g + 4 * team,
+                           s_c + 4 * team);
+        continue;
+      }
+      t -= t_128;
+      // one warp item per warp of the block (per-warp shared tables)
+      int64_t k = t * nwb + warp;
+      if (k >= witems) continue;
+      if (k < i4) { small_item<4>(p.a, st.seg[0] + 8 * k, st.seg[1]); continue; }
+      k -= i4;
+      if (k < i8) { small_item<8>(p.a, st.seg[1] + 4 * k, st.seg[2]); continue; }
+      k -= i8;
+      if (k < i16) { small_item<16>(p.a, st.seg[2] + 2 * k, st.seg[3]); continue; }
+      k -= i16;
+      if (k < n32) { small_item<32>(p.a, st.seg[3] + k, st.seg[4]); continue; }
+      k -= n32;
+      warp_table_vertex(p.a, st.seg[4] + k, wkeys, wvals);
+    }
+    grid.sync();
+    GLV_TRACE(4 * s);
+    if (st.hub_segs[1] > st.hub_segs[0]) {
+      for (int64_t si = st.hub_segs[0] + blockIdx.x; si < st.hub_segs[1]; si += gridDim.x)
+        hub_scan_segment(p.a, p.h, si, s_g, s_c);
+      grid.sync();
+      GLV_TRACE(4 * s + 1);
+      for (int64_t pos = st.seg[BIN_HUB] + gw; pos < st.seg[BIN_HUB + 1]; pos += ngw)
+        hub_final(p.a, p.h, pos);
+      grid.sync();
+      GLV_TRACE(4 * s + 2);
+    }
+    if (!p.jacobi && st.apply[1] > st.apply[0]) {
+      apply_deltas_range(p, st.apply[0], st.apply[1], gt, ngt);
+      grid.sync();
+      GLV_TRACE(4 * s + 3);
+    }
+  }
+  const int64_t ntiles = (p.nv + kModVB - 1) / kModVB;
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+    modularity_tile(p, tile, s_ptr, s_cc, sh);
+  grid.sync();
+  GLV_TRACE(4 * p.nsteps + 1);
+  if (blockIdx.x == 0) modularity_fold(p, ntiles, sh);
+  if (p.jacobi && p.nsteps > 0) {
+    // Q above used the totals before the moves; now take the moves' deltas.
+    apply_deltas_range(p, p.steps[0].apply[0], p.steps[p.nsteps - 1].apply[1], gt, ngt);
+  }
+}
+
+}  // namespace glv

@@ -71,72 +71,77 @@ __device__ __forceinline__ int32_t finish_choice(const SweepArgs &a, int32_t own
 
 // ---------------------------------------------------------------------------
 // Rows of at most G entries: G lanes per vertex, one entry per lane, no table.
+// One warp handles the 32/G member slots starting at `base` (all lanes call).
 template <int G>
-__global__ void __launch_bounds__(256) k_sweep_small(SweepArgs a, int64_t begin, int64_t end) {
-  constexpr int VPW = 32 / G;
+__device__ __forceinline__ void small_item(const SweepArgs &a, int64_t base, int64_t end) {
   const int lane = threadIdx.x & 31;
   const int grp = lane / G;
   const int gl = lane & (G - 1);
   const unsigned gmask = (G == 32) ? FULL : (((1u << G) - 1u) << (grp * G));
+  const int64_t pos = base + grp;
+  const bool valid = pos < end;
+  const int32_t v = valid ? a.members[pos] : 0;
+  const int64_t rb = valid ? a.ptr[v] : 0;
+  const int deg = valid ? (int)(a.ptr[v + 1] - rb) : 0;
+  const int32_t own = (valid && deg > 0) ? a.C[v] : -1;
+  const bool has = gl < deg;
+  const int32_t t = has ? a.tail[rb + gl] : -1;
+  const double wt = has ? a.w[rb + gl] : 0.0;
+  const int32_t c = has ? a.C[t] : -1;
+  const unsigned long long key =
+      has ? (((unsigned long long)grp << 32) | (uint32_t)c) : (0xFFFFFFFF00000000ull | lane);
+  const unsigned m = __match_any_sync(FULL, key);
+  const bool leader = has && (lane == __ffs(m) - 1);
+  // Ordered fold of each community group (lane order == CSR order).
+  unsigned rem = leader ? m : 0u;
+  const int rounds = __reduce_max_sync(FULL, (unsigned)__popc(rem));
+  double sum = 0.0;
+  for (int it = 0; it < rounds; ++it) {
+    const int src = rem ? __ffs(rem) - 1 : lane;
+    const double x = __shfl_sync(FULL, wt, src);
+    if (rem) { sum = __dadd_rn(sum, x); rem &= rem - 1; }
+  }
+  // Self-loop weight, in CSR order.
+  unsigned sm = __ballot_sync(FULL, has && t == v) & gmask;
+  const int srounds = __reduce_max_sync(FULL, (unsigned)__popc(sm));
+  double self_loop = 0.0;
+  for (int it = 0; it < srounds; ++it) {
+    const int src = sm ? __ffs(sm) - 1 : lane;
+    const double x = __shfl_sync(FULL, wt, src);
+    if (sm) { self_loop = __dadd_rn(self_loop, x); sm &= sm - 1; }
+  }
+  // Counter[own]
+  const unsigned om = __ballot_sync(FULL, leader && c == own) & gmask;
+  const double osum = __shfl_sync(FULL, sum, om ? __ffs(om) - 1 : lane);
+  const double own_w = om ? osum : 0.0;
+  const double degree = (valid && deg > 0) ? a.vDeg[v] : 0.0;
+  double g = 0.0;
+  int32_t bc = INT32_MAX;
+  if (leader && c != own) {
+    const double eix = __dsub_rn(own_w, self_loop);
+    const double ax = __dsub_rn(a.cDeg[own], degree);
+    const double gain = louvain_gain(sum, eix, degree, a.cDeg[c], ax, a.constant);
+    if (gain > 0.0) { g = gain; bc = c; }
+  }
+#pragma unroll
+  for (int off = G / 2; off >= 1; off >>= 1) {
+    const double og = __shfl_xor_sync(FULL, g, off);
+    const int32_t oc = __shfl_xor_sync(FULL, bc, off);
+    if (better(og, oc, g, bc)) { g = og; bc = oc; }
+  }
+  if (valid && gl == 0) {
+    const int32_t tgt = (deg == 0) ? -1 : finish_choice(a, own, g, bc);
+    emit_decision(a, pos, v, own, tgt, degree, own_w);
+  }
+
+}
+
+template <int G>
+__global__ void __launch_bounds__(256) k_sweep_small(SweepArgs a, int64_t begin, int64_t end) {
+  constexpr int VPW = 32 / G;
   const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t base = begin + wid * VPW; base < end; base += nw * VPW) {
-    const int64_t pos = base + grp;
-    const bool valid = pos < end;
-    const int32_t v = valid ? a.members[pos] : 0;
-    const int64_t rb = valid ? a.ptr[v] : 0;
-    const int deg = valid ? (int)(a.ptr[v + 1] - rb) : 0;
-    const int32_t own = (valid && deg > 0) ? a.C[v] : -1;
-    const bool has = gl < deg;
-    const int32_t t = has ? a.tail[rb + gl] : -1;
-    const double wt = has ? a.w[rb + gl] : 0.0;
-    const int32_t c = has ? a.C[t] : -1;
-    const unsigned long long key =
-        has ? (((unsigned long long)grp << 32) | (uint32_t)c) : (0xFFFFFFFF00000000ull | lane);
-    const unsigned m = __match_any_sync(FULL, key);
-    const bool leader = has && (lane == __ffs(m) - 1);
-    // Ordered fold of each community group (lane order == CSR order).
-    unsigned rem = leader ? m : 0u;
-    const int rounds = __reduce_max_sync(FULL, (unsigned)__popc(rem));
-    double sum = 0.0;
-    for (int it = 0; it < rounds; ++it) {
-      const int src = rem ? __ffs(rem) - 1 : lane;
-      const double x = __shfl_sync(FULL, wt, src);
-      if (rem) { sum = __dadd_rn(sum, x); rem &= rem - 1; }
-    }
-    // Self-loop weight, in CSR order.
-    unsigned sm = __ballot_sync(FULL, has && t == v) & gmask;
-    const int srounds = __reduce_max_sync(FULL, (unsigned)__popc(sm));
-    double self_loop = 0.0;
-    for (int it = 0; it < srounds; ++it) {
-      const int src = sm ? __ffs(sm) - 1 : lane;
-      const double x = __shfl_sync(FULL, wt, src);
-      if (sm) { self_loop = __dadd_rn(self_loop, x); sm &= sm - 1; }
-    }
-    // Counter[own]
-    const unsigned om = __ballot_sync(FULL, leader && c == own) & gmask;
-    const double osum = __shfl_sync(FULL, sum, om ? __ffs(om) - 1 : lane);
-    const double own_w = om ? osum : 0.0;
-    const double degree = (valid && deg > 0) ? a.vDeg[v] : 0.0;
-    double g = 0.0;
-    int32_t bc = INT32_MAX;
-    if (leader && c != own) {
-      const double eix = __dsub_rn(own_w, self_loop);
-      const double ax = __dsub_rn(a.cDeg[own], degree);
-      const double gain = louvain_gain(sum, eix, degree, a.cDeg[c], ax, a.constant);
-      if (gain > 0.0) { g = gain; bc = c; }
-    }
-#pragma unroll
-    for (int off = G / 2; off >= 1; off >>= 1) {
-      const double og = __shfl_xor_sync(FULL, g, off);
-      const int32_t oc = __shfl_xor_sync(FULL, bc, off);
-      if (better(og, oc, g, bc)) { g = og; bc = oc; }
-    }
-    if (valid && gl == 0) {
-      const int32_t tgt = (deg == 0) ? -1 : finish_choice(a, own, g, bc);
-      emit_decision(a, pos, v, own, tgt, degree, own_w);
-    }
-  }
+  for (int64_t base = begin + wid * VPW; base < end; base += nw * VPW) small_item<G>(a, base, end);
 }
 
 // ---------------------------------------------------------------------------
@@ -234,11 +239,36 @@ __device__ __forceinline__ void warp_argmax(double &g, int32_t &bc) {
 }
 
 // ---------------------------------------------------------------------------
-// Rows of 33..warp_max entries: one warp per vertex, table in shared memory.
+// Rows of 33..warp_max entries: one warp per vertex, table (capacity <= 256)
+// in the warp's slice of shared memory.
+__device__ __forceinline__ void warp_table_vertex(const SweepArgs &a, int64_t pos, int32_t *keys,
+                                                  double *vals) {
+  const int lane = threadIdx.x & 31;
+  const int32_t v = a.members[pos];
+  const int64_t rb = a.ptr[v], re = a.ptr[v + 1];
+  const uint32_t cap = table_cap(re - rb);
+  const uint32_t mask = cap - 1;
+  for (uint32_t s = lane; s < cap; s += 32) { keys[s] = -1; vals[s] = 0.0; }
+  __syncwarp();
+  const int32_t own = a.C[v];
+  if (lane == 0) keys[hash_slot(own, mask)] = own;
+  __syncwarp();
+  const double self_loop = warp_accumulate(a, v, rb, re, 32, keys, vals, mask, false);
+  const double degree = a.vDeg[v];
+  const double own_w = vals[hash_slot(own, mask)];
+  const double eix = __dsub_rn(own_w, self_loop);
+  const double ax = __dsub_rn(a.cDeg[own], degree);
+  double g = 0.0;
+  int32_t bc = INT32_MAX;
+  scan_table(a, keys, vals, lane, cap, 32, own, eix, ax, degree, g, bc);
+  warp_argmax(g, bc);
+  if (lane == 0) emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), degree, own_w);
+  __syncwarp();
+}
+
 template <int CAP>
 __global__ void __launch_bounds__(256) k_sweep_warp(SweepArgs a, int64_t begin, int64_t end) {
   extern __shared__ unsigned char smem_raw[];
-  const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int nwb = blockDim.x >> 5;
   double *vals = reinterpret_cast<double *>(smem_raw) + (size_t)warp * CAP;
@@ -246,95 +276,299 @@ __global__ void __launch_bounds__(256) k_sweep_warp(SweepArgs a, int64_t begin, 
                   (size_t)warp * CAP;
   const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t pos = begin + wid; pos < end; pos += nw) {
-    const int32_t v = a.members[pos];
-    const int64_t rb = a.ptr[v], re = a.ptr[v + 1];
-    const uint32_t cap = table_cap(re - rb);
-    const uint32_t mask = cap - 1;
-    for (uint32_t s = lane; s < cap; s += 32) { keys[s] = -1; vals[s] = 0.0; }
-    __syncwarp();
-    const int32_t own = a.C[v];
-    if (lane == 0) keys[hash_slot(own, mask)] = own;
-    __syncwarp();
-    const double self_loop = warp_accumulate(a, v, rb, re, 32, keys, vals, mask, false);
-    const double degree = a.vDeg[v];
-    const double own_w = vals[hash_slot(own, mask)];
-    const double eix = __dsub_rn(own_w, self_loop);
-    const double ax = __dsub_rn(a.cDeg[own], degree);
-    double g = 0.0;
-    int32_t bc = INT32_MAX;
-    scan_table(a, keys, vals, lane, cap, 32, own, eix, ax, degree, g, bc);
-    warp_argmax(g, bc);
-    if (lane == 0) emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), degree, own_w);
-    __syncwarp();
-  }
+  for (int64_t pos = begin + wid; pos < end; pos += nw) warp_table_vertex(a, pos, keys, vals);
 }
 
 // ---------------------------------------------------------------------------
-// Large rows: one block per vertex.  BIN_BLOCK keeps the table in shared
-// memory (capacity up to `smem_cap`), BIN_HUB in global scratch at hub_off.
-// ordered = 1: warp 0 walks the whole row in CSR order (bit-exact sums);
-// ordered = 0: all warps take chunks and add group sums with atomics.
+// Large rows: one block per vertex; the table is `keys`/`vals` (shared memory
+// or a global region).  ordered = 1: warp 0 walks the whole row in CSR order
+// (bit-exact sums); ordered = 0: all warps take chunks and add group sums with
+// atomics.  `red` is block scratch of 3 x 32 words.  All threads call.
+__device__ __forceinline__ void block_vertex(const SweepArgs &a, int64_t pos, int32_t *keys,
+                                             double *vals, int ordered, double *s_self,
+                                             double *s_g, int32_t *s_c) {
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nwb = blockDim.x >> 5;
+  const int32_t v = a.members[pos];
+  const int64_t rb = a.ptr[v], re = a.ptr[v + 1];
+  const uint32_t cap = table_cap(re - rb);
+  const uint32_t mask = cap - 1;
+  for (uint32_t s = threadIdx.x; s < cap; s += blockDim.x) { keys[s] = -1; vals[s] = 0.0; }
+  __syncthreads();
+  const int32_t own = a.C[v];
+  if (threadIdx.x == 0) keys[hash_slot(own, mask)] = own;
+  __syncthreads();
+  double self_loop;
+  if (ordered) {
+    if (warp == 0) {
+      double sl = warp_accumulate(a, v, rb, re, 32, keys, vals, mask, false);
+      if (lane == 0) s_self[0] = sl;
+    }
+    __syncthreads();
+    self_loop = s_self[0];
+  } else {
+    double sl = warp_accumulate(a, v, rb + 32 * warp, re, 32 * nwb, keys, vals, mask, true);
+    if (lane == 0) s_self[warp] = sl;
+    __syncthreads();
+    self_loop = 0.0;
+    for (int k = 0; k < nwb; ++k) self_loop = __dadd_rn(self_loop, s_self[k]);
+  }
+  const double degree = a.vDeg[v];
+  const double own_w = vals[hash_slot(own, mask)];
+  const double eix = __dsub_rn(own_w, self_loop);
+  const double ax = __dsub_rn(a.cDeg[own], degree);
+  double g = 0.0;
+  int32_t bc = INT32_MAX;
+  scan_table(a, keys, vals, threadIdx.x, cap, blockDim.x, own, eix, ax, degree, g, bc);
+  warp_argmax(g, bc);
+  if (lane == 0) { s_g[warp] = g; s_c[warp] = bc; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < nwb; ++k)
+      if (better(s_g[k], s_c[k], g, bc)) { g = s_g[k]; bc = s_c[k]; }
+    emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), degree, own_w);
+  }
+  __syncthreads();
+}
+
+// Team of T threads (T/32 warps; T == blockDim.x or a named-barrier slice of
+// the block) handles one row with the table in `keys`/`vals`; parallel
+// accumulation only.  `red` arrays have one entry per warp of the team.
+template <int T>
+__device__ __forceinline__ void team_sync(int team) {
+  if (T == 512) __syncthreads();
+  else asm volatile("bar.sync %0, %1;" ::"r"(team + 1), "r"(T) : "memory");
+}
+
+template <int T>
+__device__ __forceinline__ void team_vertex(const SweepArgs &a, int64_t pos, int32_t *keys,
+                                            double *vals, int team, double *s_self, double *s_g,
+                                            int32_t *s_c) {
+  constexpr int NW = T / 32;
+  const int tt = threadIdx.x % T;
+  const int lane = tt & 31, tw = tt >> 5;
+  const int32_t v = a.members[pos];
+  const int64_t rb = a.ptr[v], re = a.ptr[v + 1];
+  const uint32_t cap = table_cap(re - rb);
+  const uint32_t mask = cap - 1;
+  for (uint32_t s = tt; s < cap; s += T) { keys[s] = -1; vals[s] = 0.0; }
+  team_sync<T>(team);
+  const int32_t own = a.C[v];
+  if (tt == 0) keys[hash_slot(own, mask)] = own;
+  team_sync<T>(team);
+  const double sl = warp_accumulate(a, v, rb + 32 * tw, re, 32 * NW, keys, vals, mask, true);
+  if (lane == 0) s_self[tw] = sl;
+  team_sync<T>(team);
+  double self_loop = 0.0;
+  for (int k = 0; k < NW; ++k) self_loop = __dadd_rn(self_loop, s_self[k]);
+  const double degree = a.vDeg[v];
+  const double own_w = vals[hash_slot(own, mask)];
+  const double eix = __dsub_rn(own_w, self_loop);
+  const double ax = __dsub_rn(a.cDeg[own], degree);
+  double g = 0.0;
+  int32_t bc = INT32_MAX;
+  scan_table(a, keys, vals, tt, cap, T, own, eix, ax, degree, g, bc);
+  warp_argmax(g, bc);
+  if (lane == 0) { s_g[tw] = g; s_c[tw] = bc; }
+  team_sync<T>(team);
+  if (tt == 0) {
+    for (int k = 1; k < NW; ++k)
+      if (better(s_g[k], s_c[k], g, bc)) { g = s_g[k]; bc = s_c[k]; }
+    emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), degree, own_w);
+  }
+  team_sync<T>(team);
+}
+
+// BIN_T128/T256/BLOCK keep the table in shared memory (capacity up to 8192),
+// BIN_HUB in global scratch at hub_off.
 __global__ void __launch_bounds__(512) k_sweep_block(SweepArgs a, int64_t begin, int64_t end,
                                                      int hub, int ordered) {
   extern __shared__ unsigned char smem_raw[];
   __shared__ double s_self[32];
   __shared__ double s_g[32];
   __shared__ int32_t s_c[32];
-  const int lane = threadIdx.x & 31;
-  const int warp = threadIdx.x >> 5;
-  const int nwb = blockDim.x >> 5;
   for (int64_t pos = begin + blockIdx.x; pos < end; pos += gridDim.x) {
-    const int32_t v = a.members[pos];
-    const int64_t rb = a.ptr[v], re = a.ptr[v + 1];
-    const uint32_t cap = table_cap(re - rb);
-    const uint32_t mask = cap - 1;
     int32_t *keys;
     double *vals;
     if (hub) {
       keys = a.hub_keys + a.hub_off[pos];
       vals = a.hub_vals + a.hub_off[pos];
     } else {
+      const int32_t v = a.members[pos];
+      const uint32_t cap = table_cap(a.ptr[v + 1] - a.ptr[v]);
       vals = reinterpret_cast<double *>(smem_raw);
       keys = reinterpret_cast<int32_t *>(vals + cap);
     }
-    for (uint32_t s = threadIdx.x; s < cap; s += blockDim.x) { keys[s] = -1; vals[s] = 0.0; }
-    __syncthreads();
-    const int32_t own = a.C[v];
-    if (threadIdx.x == 0) keys[hash_slot(own, mask)] = own;
-    __syncthreads();
-    double self_loop;
-    if (ordered) {
-      if (warp == 0) {
-        double sl = warp_accumulate(a, v, rb, re, 32, keys, vals, mask, false);
-        if (lane == 0) s_self[0] = sl;
-      }
-      __syncthreads();
-      self_loop = s_self[0];
-    } else {
-      double sl = warp_accumulate(a, v, rb + 32 * warp, re, 32 * nwb, keys, vals, mask, true);
-      if (lane == 0) s_self[warp] = sl;
-      __syncthreads();
-      self_loop = 0.0;
-      for (int k = 0; k < nwb; ++k) self_loop = __dadd_rn(self_loop, s_self[k]);
-    }
-    const double degree = a.vDeg[v];
-    const double own_w = vals[hash_slot(own, mask)];
-    const double eix = __dsub_rn(own_w, self_loop);
-    const double ax = __dsub_rn(a.cDeg[own], degree);
-    double g = 0.0;
-    int32_t bc = INT32_MAX;
-    scan_table(a, keys, vals, threadIdx.x, cap, blockDim.x, own, eix, ax, degree, g, bc);
-    warp_argmax(g, bc);
-    if (lane == 0) { s_g[warp] = g; s_c[warp] = bc; }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      for (int k = 1; k < nwb; ++k)
-        if (better(s_g[k], s_c[k], g, bc)) { g = s_g[k]; bc = s_c[k]; }
-      emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), degree, own_w);
-    }
-    __syncthreads();
+    block_vertex(a, pos, keys, vals, ordered, s_self, s_g, s_c);
   }
+}
+
+// ---------------------------------------------------------------------------
+// Hubs in the parallel-accumulation modes: each hub's row is cut into chunks
+// that all blocks share (hub_accum_chunk), its table is scanned in segments of
+// the slots that were filled (hub_scan_segment), and one warp per hub folds
+// the segments' partial arg-maxes (hub_final).  Every table is left empty
+// again by the scan, so tables are cleared only when allocated.
+struct HubWork {
+  int32_t *keys;            // tables (keys -1 = empty)
+  double *vals;
+  const int64_t *tab_off;   // per member slot: table offset
+  int32_t *occ;             // filled-slot lists
+  const int64_t *occ_off;   // per member slot: list offset
+  int32_t *cnt;             // per member slot: filled slots
+  double *self_w;           // per member slot: self-loop weight
+  double *own_w;            // per member slot: Counter[own]
+  const int32_t *chunk_pos; // chunk -> member slot
+  const int64_t *chunk_beg, *chunk_end;  // CSR range
+  const int32_t *seg_pos;   // segment -> member slot
+  const int64_t *seg_beg, *seg_end;      // range in the filled-slot list
+  double *part_g;           // per segment: best gain
+  int32_t *part_c;          //              and its community
+  const int64_t *hub_seg_beg, *hub_seg_end;  // per member slot: its segments
+};
+
+constexpr int kHubChunk = 2048;     // CSR entries per accumulation work item
+constexpr int kHubSeg = 2048;       // filled slots per scan work item
+constexpr int kHubStageCap = 4096;  // block-local staging table of one chunk
+
+// All threads of the block call.  The chunk is first folded into a
+// block-local shared table (`skeys`/`svals`, kHubStageCap slots; at most
+// kHubChunk distinct keys), then each distinct community is added to the
+// hub's global table once — a hub's neighbours concentrate on a few
+// communities, and per-warp global atomics on those slots would serialise.
+__device__ __forceinline__ void hub_accum_chunk(const SweepArgs &a, const HubWork &h, int64_t ci,
+                                                int32_t *skeys, double *svals, double *s_self) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwb = blockDim.x >> 5;
+  const int32_t pos = h.chunk_pos[ci];
+  const int64_t eb = h.chunk_beg[ci], ee = h.chunk_end[ci];
+  const int32_t v = a.members[pos];
+  const uint32_t smask = kHubStageCap - 1;
+  for (uint32_t q = threadIdx.x; q < kHubStageCap; q += blockDim.x) { skeys[q] = -1; svals[q] = 0.0; }
+  if (threadIdx.x == 0) s_self[0] = 0.0;
+  __syncthreads();
+  double sl = warp_accumulate(a, v, eb + 32 * warp, ee, 32 * nwb, skeys, svals, smask, true);
+  if (lane == 0 && sl != 0.0) atomicAdd(&s_self[0], sl);
+  __syncthreads();
+  const uint32_t mask = table_cap(a.ptr[v + 1] - a.ptr[v]) - 1;
+  int32_t *keys = h.keys + h.tab_off[pos];
+  double *vals = h.vals + h.tab_off[pos];
+  int32_t *occ = h.occ + h.occ_off[pos];
+  const int32_t own = a.C[v];
+  for (uint32_t q0 = 0; q0 < kHubStageCap; q0 += blockDim.x) {
+    const uint32_t q = q0 + threadIdx.x;  // blockDim divides kHubStageCap: warp-uniform loop
+    const int32_t c = skeys[q];
+    const double val = svals[q];
+    uint32_t s = 0;
+    bool inserted = false;
+    if (c >= 0) {
+      s = hash_slot(c, mask);
+      while (true) {
+        const int32_t k = keys[s];
+        if (k == c) break;
+        if (k == -1) {
+          const int32_t old = atomicCAS(&keys[s], -1, c);
+          if (old == -1) { inserted = true; break; }
+          if (old == c) break;
+        }
+        s = (s + 1) & mask;
+      }
+    }
+    // one counter update per warp for the slots it filled
+    const unsigned ins = __ballot_sync(FULL, inserted);
+    int obase = 0;
+    if (lane == __ffs(ins) - 1) obase = atomicAdd(&h.cnt[pos], __popc(ins));
+    obase = __shfl_sync(FULL, obase, ins ? __ffs(ins) - 1 : 0);
+    if (inserted) occ[obase + __popc(ins & ((1u << lane) - 1u))] = (int32_t)s;
+    if (c >= 0) {
+      atomicAdd(&vals[s], val);
+      if (c == own) atomicAdd(&h.own_w[pos], val);
+    }
+  }
+  if (threadIdx.x == 0 && s_self[0] != 0.0) atomicAdd(&h.self_w[pos], s_self[0]);
+  __syncthreads();
+}
+
+// All threads of the block call; s_g/s_c are 32-entry block scratch.
+__device__ __forceinline__ void hub_scan_segment(const SweepArgs &a, const HubWork &h, int64_t si,
+                                                 double *s_g, int32_t *s_c) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwb = blockDim.x >> 5;
+  const int32_t pos = h.seg_pos[si];
+  const int32_t v = a.members[pos];
+  const int32_t own = a.C[v];
+  const double degree = a.vDeg[v];
+  const double eix = __dsub_rn(h.own_w[pos], h.self_w[pos]);
+  const double ax = __dsub_rn(a.cDeg[own], degree);
+  int32_t *keys = h.keys + h.tab_off[pos];
+  double *vals = h.vals + h.tab_off[pos];
+  const int32_t *occ = h.occ + h.occ_off[pos];
+  const int64_t ob = h.seg_beg[si];
+  const int64_t oe = min(h.seg_end[si], (int64_t)h.cnt[pos]);
+  double g = 0.0;
+  int32_t bc = INT32_MAX;
+  for (int64_t k = ob + threadIdx.x; k < oe; k += blockDim.x) {
+    const int32_t s = occ[k];
+    const int32_t c = keys[s];
+    const double val = vals[s];
+    if (c != own) {
+      const double gain = louvain_gain(val, eix, degree, a.cDeg[c], ax, a.constant);
+      if (gain > 0.0 && better(gain, c, g, bc)) { g = gain; bc = c; }
+    }
+    keys[s] = -1;  // leave the table empty for its next use
+    vals[s] = 0.0;
+  }
+  warp_argmax(g, bc);
+  if (lane == 0) { s_g[warp] = g; s_c[warp] = bc; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < nwb; ++k)
+      if (better(s_g[k], s_c[k], g, bc)) { g = s_g[k]; bc = s_c[k]; }
+    h.part_g[si] = g;
+    h.part_c[si] = bc;
+  }
+  __syncthreads();
+}
+
+// One warp per hub (all lanes call).
+__device__ __forceinline__ void hub_final(const SweepArgs &a, const HubWork &h, int64_t pos) {
+  const int lane = threadIdx.x & 31;
+  double g = 0.0;
+  int32_t bc = INT32_MAX;
+  for (int64_t si = h.hub_seg_beg[pos] + lane; si < h.hub_seg_end[pos]; si += 32)
+    if (better(h.part_g[si], h.part_c[si], g, bc)) { g = h.part_g[si]; bc = h.part_c[si]; }
+  warp_argmax(g, bc);
+  if (lane == 0) {
+    const int32_t v = a.members[pos];
+    const int32_t own = a.C[v];
+    emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), a.vDeg[v], h.own_w[pos]);
+    h.cnt[pos] = 0;
+    h.self_w[pos] = 0.0;
+    h.own_w[pos] = 0.0;
+  }
+}
+
+__global__ void __launch_bounds__(512) k_hub_accum(SweepArgs a, HubWork h, int64_t cb,
+                                                   int64_t ce) {
+  extern __shared__ unsigned char smem_raw[];
+  __shared__ double s_self[1];
+  double *svals = reinterpret_cast<double *>(smem_raw);
+  int32_t *skeys = reinterpret_cast<int32_t *>(svals + kHubStageCap);
+  for (int64_t ci = cb + blockIdx.x; ci < ce; ci += gridDim.x)
+    hub_accum_chunk(a, h, ci, skeys, svals, s_self);
+}
+
+__global__ void __launch_bounds__(256) k_hub_scan(SweepArgs a, HubWork h, int64_t sb,
+                                                  int64_t se) {
+  __shared__ double s_g[32];
+  __shared__ int32_t s_c[32];
+  for (int64_t si = sb + blockIdx.x; si < se; si += gridDim.x) hub_scan_segment(a, h, si, s_g, s_c);
+}
+
+__global__ void __launch_bounds__(256) k_hub_final(SweepArgs a, HubWork h, int64_t b,
+                                                   int64_t e) {
+  const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t pos = b + wid; pos < e; pos += nw) hub_final(a, h, pos);
 }
 
 }  // namespace glv

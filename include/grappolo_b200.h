@@ -58,6 +58,7 @@ enum {
 enum { GLV_MODE_VERIFY = 0, GLV_MODE_FAST = 1 };
 
 #define GLV_MAX_PHASES 256
+#define GLV_KERNEL_SLOTS 11
 
 typedef struct glv_phase_stats {
   long num_vertices;   /* level graph */
@@ -94,9 +95,11 @@ typedef struct glv_run_stats {
   double sweep_kernel_time; /* s */
   double sweep_bytes;
   long sweep_steps;         /* (class, sublevel) steps timed */
-  /* With glv_set_profiling(2): device time per launch kind — the seven degree
-   * bins of the sweep, the community-total update, the modularity pass. */
-  double kernel_time[9];    /* s */
+  /* With glv_set_profiling(2) and the per-class launch schedule: device time
+   * per launch kind — the nine degree bins of the sweep (rows of 0-4, 5-8,
+   * 9-16, 17-32, 33-127, 128-511, 512-1023, 1024-2047 entries and larger hubs),
+   * the community-total update, the modularity pass. */
+  double kernel_time[GLV_KERNEL_SLOTS]; /* s */
   int nphase;               /* entries filled in phase[] */
   glv_phase_stats phase[GLV_MAX_PHASES];
 } glv_run_stats;
@@ -202,6 +205,11 @@ int glv_decide_batch(long nv, const long *ptr, const long *tail, const double *w
 int glv_dev_modularity_static(long nv, const long *d_ptr, const int *d_tail,
                               const double *d_weight, const int *d_C, const double *d_cDeg,
                               double constant, double *d_out, void *stream);
+
+/* Device memory: the engine allocates from its own stream-ordered pool per
+ * device and keeps freed blocks cached for later calls.  This returns the
+ * cached blocks to the driver. */
+void glv_release_cached_memory(void);
 
 /* ---- library information ------------------------------------------------ */
 /* Process-wide switch for the following calls: 0 off; 1 time each colour
