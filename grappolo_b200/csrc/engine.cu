@@ -192,11 +192,20 @@ class Engine {
   double slot_s[kSlots] = {0};
 
  private:
+  // Requests above 1 MiB are rounded up to quarter-octave size classes so that
+  // repeated runs, whose level sizes differ slightly, reuse the pool's blocks.
+  static size_t size_class(size_t bytes) {
+    if (bytes <= (1u << 20)) return bytes;
+    int e = 63 - __builtin_clzll(bytes);
+    const size_t step = (size_t(1) << e) >> 2;
+    return (bytes + step - 1) / step * step;
+  }
   template <class T>
   int alloc(T **p, size_t n) {
     if (!pool_) pool_ = engine_pool();
     if (!pool_) return fail(GLV_ERR_CUDA, "could not create the device memory pool");
-    CK(cudaMallocFromPoolAsync((void **)p, std::max<size_t>(n, 1) * sizeof(T), pool_, s_));
+    CK(cudaMallocFromPoolAsync((void **)p, size_class(std::max<size_t>(n, 1) * sizeof(T)), pool_,
+                               s_));
     return GLV_OK;
   }
   template <class T>
@@ -282,6 +291,10 @@ class Engine {
   unsigned char *temp_ = nullptr;
   size_t temp_bytes_ = 0;
   int64_t max_class_ = 0;
+  // coarsening records, sized for level 0 and reused by every level
+  uint64_t *ck1_ = nullptr, *ck2_ = nullptr;
+  double *cv1_ = nullptr, *cv2_ = nullptr;
+  int64_t crec_cap_ = 0;
 };
 
 constexpr int kConstParts = 1024;  // blocks of the constant's reduction
@@ -303,6 +316,7 @@ void Engine::release() {
   dfree(part_c_); dfree(chunk_beg_); dfree(chunk_end_); dfree(seg_beg_); dfree(seg_end_);
   dfree(part_g_);
   dfree(dkeys_); dfree(dkeys2_); dfree(drecs_); dfree(drecs2_);
+  dfree(ck1_); dfree(ck2_); dfree(cv1_); dfree(cv2_);
   dfree(temp_);
   if (h_mod_) cudaFreeHost(h_mod_);
   h_mod_ = nullptr;
@@ -380,8 +394,13 @@ int Engine::upload_check(const Level &L) {
 }
 
 int Engine::phase_init(const Level &L, bool need_past) {
-  LAUNCH(k_init_phase, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, L.ptr, L.w, vDeg, cDeg,
-         cSize, C, need_past ? Cpast : (int32_t *)nullptr);
+  if (ordered()) {
+    LAUNCH(k_init_phase, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, L.ptr, L.w, vDeg, cDeg,
+           cSize, C, need_past ? Cpast : (int32_t *)nullptr);
+  } else {
+    LAUNCH(k_init_phase_warp, grid_for(L.nv * 32, 256, nsm_ * 16), 256, 0, s_, L.nv, L.ptr, L.w,
+           vDeg, cDeg, cSize, C, need_past ? Cpast : (int32_t *)nullptr);
+  }
   if (ordered()) {
     LAUNCH(k_constant_sequential, 1, 1, 0, s_, L.nv, vDeg, cst);
   } else {
@@ -465,8 +484,8 @@ int Engine::color_spec(const Level &L, int *ncolors) {
     CK(cudaMemsetAsync(cnt + 2, 0, sizeof(int32_t), s_));
     if (nw) LAUNCH(k_spec_conflicts, grid_for(nw * 32, 256, nsm_ * 16), 256, 0, s_, nw, wl,
                    L.ptr, L.tail, seed, color_, nx, cnt + 2);
-    if (nb) LAUNCH(k_spec_conflicts, grid_for(nb * 32, 256, nsm_ * 16), 256, 0, s_, nb, bl,
-                   L.ptr, L.tail, seed, color_, nx, cnt + 2);
+    if (nb) LAUNCH(k_spec_conflicts_block, (int)std::min<int64_t>(nb, nsm_ * 4), 512, 0, s_, nb,
+                   bl, L.ptr, L.tail, seed, color_, nx, cnt + 2);
     CK(cudaMemcpyAsync(&h[2], cnt + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
     CK(cudaStreamSynchronize(s_));
     if (h[2] == 0) break;
@@ -522,6 +541,8 @@ int Engine::sublevels(const Level &L, int ncolors, int32_t **d_sub, int *nsub) {
 // ------------------------------------------------------------------ schedule
 int Engine::build_schedule(const Level &L, const int32_t *color, int ncolors, const int32_t *sub,
                            int nsub, std::vector<ClassSched> *sched) {
+  const bool debug = getenv("GRAPPOLO_B200_DEBUG") != nullptr;
+  const double tsd = now_s();
   const int64_t nkeys = (int64_t)ncolors * nsub * NBINS;
   if (nkeys + 1 > hist_cap_) {
     dfree(hist_);
@@ -564,6 +585,7 @@ int Engine::build_schedule(const Level &L, const int32_t *color, int ncolors, co
       sched->push_back(cs);
     }
   }
+  if (debug) fprintf(stderr, "grappolo_b200: schedule sort+hist %.4f s\n", now_s() - tsd);
   return hub_offsets(L, *sched);
 }
 
@@ -577,11 +599,17 @@ int Engine::grow_hub(size_t entries) {
   return GLV_OK;
 }
 
-__global__ void k_row_bounds(int64_t n, const int32_t *members, const int64_t *ptr,
-                             int64_t *out) {
+__global__ void k_scatter_i64(int64_t n, const int32_t *pos, const int64_t *val, int64_t *out) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x)
+    out[pos[k]] = val[k];
+}
+
+__global__ void k_row_bounds_at(int64_t n, const int32_t *pos, const int32_t *members,
+                                const int64_t *ptr, int64_t *out) {
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
        k += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t v = members[k];
+    const int32_t v = members[pos[k]];
     out[2 * k] = ptr[v];
     out[2 * k + 1] = ptr[v + 1];
   }
@@ -606,34 +634,48 @@ int Engine::hub_offsets(const Level &L, std::vector<ClassSched> &sched) {
   std::vector<int64_t> c_beg, c_end, s_beg, s_end;
   std::vector<int64_t> hub_pos_all;
   size_t need_tab = 0, tab_acc = 0, occ_acc = 0;
-  int64_t *bounds = nullptr;
+  // row bounds of every hub of the schedule, in one gather
+  std::vector<int32_t> hpos;
+  for (auto &cs : sched)
+    for (auto &st : cs.steps)
+      for (int64_t k = st.seg[BIN_HUB]; k < st.seg[BIN_HUB + 1]; ++k) hpos.push_back((int32_t)k);
+  std::vector<int64_t> hb_all(2 * hpos.size());
+  if (!hpos.empty()) {
+    int32_t *d_pos;
+    int64_t *bounds;
+    TRY(alloc(&d_pos, hpos.size()));
+    TRY(alloc(&bounds, 2 * hpos.size()));
+    TRY(upload(s_, d_pos, hpos));
+    LAUNCH(k_row_bounds_at, grid_for((int64_t)hpos.size(), 256, nsm_ * 4), 256, 0, s_,
+           (int64_t)hpos.size(), d_pos, members_, L.ptr, bounds);
+    CK(cudaMemcpyAsync(hb_all.data(), bounds, hb_all.size() * sizeof(int64_t),
+                       cudaMemcpyDeviceToHost, s_));
+    CK(cudaStreamSynchronize(s_));
+    dfree(d_pos);
+    dfree(bounds);
+  }
+  size_t hcur = 0;
+  size_t need_occ = 0;
   for (auto &cs : sched)
     for (auto &st : cs.steps) {
       const int64_t b = st.seg[BIN_HUB], e = st.seg[BIN_HUB + 1];
       st.hub_chunk[0] = st.hub_chunk[1] = (int64_t)c_pos.size();
       st.hub_segs[0] = st.hub_segs[1] = (int64_t)s_pos.size();
       if (e == b) continue;
-      dfree(bounds);
-      TRY(alloc(&bounds, 2 * (e - b)));
-      LAUNCH(k_row_bounds, grid_for(e - b, 256, nsm_ * 4), 256, 0, s_, e - b, members_ + b, L.ptr,
-             bounds);
-      std::vector<int64_t> hb(2 * (e - b));
-      CK(cudaMemcpyAsync(hb.data(), bounds, hb.size() * sizeof(int64_t), cudaMemcpyDeviceToHost,
-                         s_));
-      CK(cudaStreamSynchronize(s_));
-      size_t step_tab = 0;
+      const int64_t *hb = hb_all.data() + 2 * hcur;
+      hcur += (size_t)(e - b);
+      // a step's tables and filled-slot lists are empty again when it ends
+      // (the scan clears the slots it visits, the finalisation the counters),
+      // so every step starts its regions at offset 0
+      size_t step_tab = 0, step_occ = 0;
       for (int64_t k = 0; k < e - b; ++k) {
         const int64_t rb = hb[2 * k], re = hb[2 * k + 1], deg = re - rb;
         const int64_t pos = b + k;
-        if (!parallel) {
-          tab_off.push_back((int64_t)step_tab);
-          step_tab += table_cap(deg);
-          continue;
-        }
-        tab_off.push_back((int64_t)tab_acc);
-        tab_acc += table_cap(deg);
-        occ_off.push_back((int64_t)occ_acc);
-        occ_acc += (size_t)deg + 1;
+        tab_off.push_back((int64_t)step_tab);
+        step_tab += table_cap(deg);
+        if (!parallel) continue;
+        occ_off.push_back((int64_t)step_occ);
+        step_occ += (size_t)deg + 1;
         for (int64_t x = rb; x < re; x += kHubChunk) {
           c_pos.push_back((int32_t)pos);
           c_beg.push_back(x);
@@ -648,61 +690,68 @@ int Engine::hub_offsets(const Level &L, std::vector<ClassSched> &sched) {
         seg_e.push_back((int64_t)s_pos.size());
       }
       need_tab = std::max(need_tab, step_tab);
+      need_occ = std::max(need_occ, step_occ);
       st.hub_chunk[1] = (int64_t)c_pos.size();
       st.hub_segs[1] = (int64_t)s_pos.size();
-      hub_pos_all.push_back(b);
-      hub_pos_all.push_back(e);
     }
-  dfree(bounds);
-  if (!parallel) {
+  (void)tab_acc;
+  (void)occ_acc;
+  (void)hub_pos_all;
+  if (hpos.empty()) return GLV_OK;
+  if (need_tab > hub_cap_ || (parallel && !hub_tables_clean_)) {
     TRY(grow_hub(need_tab));
-    size_t k = 0;
-    for (size_t q = 0; q < hub_pos_all.size(); q += 2) {
-      const int64_t b = hub_pos_all[q], e = hub_pos_all[q + 1];
-      std::vector<int64_t> part(tab_off.begin() + k, tab_off.begin() + k + (e - b));
-      TRY(upload(s_, hub_off_ + b, part));
-      k += e - b;
+    if (parallel) {
+      CK(cudaMemsetAsync(hub_keys_, 0xff, hub_cap_ * sizeof(int32_t), s_));
+      CK(cudaMemsetAsync(hub_vals_, 0, hub_cap_ * sizeof(double), s_));
+      hub_tables_clean_ = true;
     }
-    CK(cudaStreamSynchronize(s_));
-    return GLV_OK;
   }
-  if (tab_acc > 0 && (tab_acc > hub_cap_ || !hub_tables_clean_)) {
-    TRY(grow_hub(tab_acc));
-    CK(cudaMemsetAsync(hub_keys_, 0xff, std::max<size_t>(hub_cap_, 1) * sizeof(int32_t), s_));
-    CK(cudaMemsetAsync(hub_vals_, 0, std::max<size_t>(hub_cap_, 1) * sizeof(double), s_));
-    hub_tables_clean_ = true;
-  }
-  if (occ_acc > hub_occ_cap_) {
-    dfree(hub_occ_);
-    hub_occ_cap_ = occ_acc;
-    TRY(alloc(&hub_occ_, hub_occ_cap_));
-  }
-  if (c_pos.size() > chunk_cap_) {
-    dfree(chunk_pos_); dfree(chunk_beg_); dfree(chunk_end_);
-    chunk_cap_ = c_pos.size();
-    TRY(alloc(&chunk_pos_, chunk_cap_)); TRY(alloc(&chunk_beg_, chunk_cap_));
-    TRY(alloc(&chunk_end_, chunk_cap_));
-  }
-  if (s_pos.size() > seg_cap_) {
-    dfree(seg_pos_); dfree(seg_beg_); dfree(seg_end_); dfree(part_g_); dfree(part_c_);
-    seg_cap_ = s_pos.size();
-    TRY(alloc(&seg_pos_, seg_cap_)); TRY(alloc(&seg_beg_, seg_cap_));
-    TRY(alloc(&seg_end_, seg_cap_)); TRY(alloc(&part_g_, seg_cap_)); TRY(alloc(&part_c_, seg_cap_));
-  }
-  TRY(upload(s_, chunk_pos_, c_pos)); TRY(upload(s_, chunk_beg_, c_beg));
-  TRY(upload(s_, chunk_end_, c_end)); TRY(upload(s_, seg_pos_, s_pos));
-  TRY(upload(s_, seg_beg_, s_beg)); TRY(upload(s_, seg_end_, s_end));
-  size_t k = 0;
-  for (size_t q = 0; q < hub_pos_all.size(); q += 2) {
-    const int64_t b = hub_pos_all[q], e = hub_pos_all[q + 1];
-    const size_t n = (size_t)(e - b);
-    TRY(upload(s_, hub_off_ + b, std::vector<int64_t>(tab_off.begin() + k, tab_off.begin() + k + n)));
-    TRY(upload(s_, hub_occ_off_ + b, std::vector<int64_t>(occ_off.begin() + k, occ_off.begin() + k + n)));
-    TRY(upload(s_, hub_seg_beg_ + b, std::vector<int64_t>(seg_b.begin() + k, seg_b.begin() + k + n)));
-    TRY(upload(s_, hub_seg_end_ + b, std::vector<int64_t>(seg_e.begin() + k, seg_e.begin() + k + n)));
-    k += n;
+  // per-hub values, aligned with hpos, scattered to their member slots
+  int32_t *d_pos;
+  int64_t *d_vals;
+  const int64_t nh = (int64_t)hpos.size();
+  TRY(alloc(&d_pos, nh));
+  TRY(upload(s_, d_pos, hpos));
+  TRY(alloc(&d_vals, 4 * nh));
+  TRY(upload(s_, d_vals, tab_off));
+  LAUNCH(k_scatter_i64, grid_for(nh, 256, nsm_ * 4), 256, 0, s_, nh, d_pos, d_vals, hub_off_);
+  if (parallel) {
+    if (need_occ > hub_occ_cap_) {
+      dfree(hub_occ_);
+      hub_occ_cap_ = need_occ;
+      TRY(alloc(&hub_occ_, hub_occ_cap_));
+    }
+    if (c_pos.size() > chunk_cap_) {
+      dfree(chunk_pos_); dfree(chunk_beg_); dfree(chunk_end_);
+      chunk_cap_ = c_pos.size();
+      TRY(alloc(&chunk_pos_, chunk_cap_)); TRY(alloc(&chunk_beg_, chunk_cap_));
+      TRY(alloc(&chunk_end_, chunk_cap_));
+    }
+    if (s_pos.size() > seg_cap_) {
+      dfree(seg_pos_); dfree(seg_beg_); dfree(seg_end_); dfree(part_g_); dfree(part_c_);
+      seg_cap_ = s_pos.size();
+      TRY(alloc(&seg_pos_, seg_cap_)); TRY(alloc(&seg_beg_, seg_cap_));
+      TRY(alloc(&seg_end_, seg_cap_)); TRY(alloc(&part_g_, seg_cap_)); TRY(alloc(&part_c_, seg_cap_));
+    }
+    TRY(upload(s_, chunk_pos_, c_pos)); TRY(upload(s_, chunk_beg_, c_beg));
+    TRY(upload(s_, chunk_end_, c_end)); TRY(upload(s_, seg_pos_, s_pos));
+    TRY(upload(s_, seg_beg_, s_beg)); TRY(upload(s_, seg_end_, s_end));
+    std::vector<int64_t> packed;
+    packed.reserve(3 * nh);
+    packed.insert(packed.end(), occ_off.begin(), occ_off.end());
+    packed.insert(packed.end(), seg_b.begin(), seg_b.end());
+    packed.insert(packed.end(), seg_e.begin(), seg_e.end());
+    TRY(upload(s_, d_vals + nh, packed));
+    LAUNCH(k_scatter_i64, grid_for(nh, 256, nsm_ * 4), 256, 0, s_, nh, d_pos, d_vals + nh,
+           hub_occ_off_);
+    LAUNCH(k_scatter_i64, grid_for(nh, 256, nsm_ * 4), 256, 0, s_, nh, d_pos, d_vals + 2 * nh,
+           hub_seg_beg_);
+    LAUNCH(k_scatter_i64, grid_for(nh, 256, nsm_ * 4), 256, 0, s_, nh, d_pos, d_vals + 3 * nh,
+           hub_seg_end_);
   }
   CK(cudaStreamSynchronize(s_));
+  dfree(d_pos);
+  dfree(d_vals);
   return GLV_OK;
 }
 
@@ -821,12 +870,16 @@ static int capture(cudaStream_t s, long *launches, F body, cudaGraphExec_t *exec
 
 int Engine::coloring_phase(const Level &L, int ncolors, bool stale, double lower, double thresh,
                            double *mod, int *itr) {
+  const bool debug = getenv("GRAPPOLO_B200_DEBUG") != nullptr;
+  double td = now_s();
   TRY(phase_init(L, false));
   int32_t *d_sub = nullptr;
   int nsub = 1;
   if (stale) TRY(sublevels(L, ncolors, &d_sub, &nsub));
+  if (debug) { cudaStreamSynchronize(s_); fprintf(stderr, "grappolo_b200: phase init %.4f s\n", now_s() - td); td = now_s(); }
   std::vector<ClassSched> sched;
   TRY(build_schedule(L, color_, ncolors, d_sub, nsub, &sched));
+  if (debug) { cudaStreamSynchronize(s_); fprintf(stderr, "grappolo_b200: schedule %.4f s\n", now_s() - td); }
   dfree(d_sub);
   const bool ord = ordered();
   if (ord) {
@@ -1232,9 +1285,14 @@ int Engine::coarsen(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
   const int end_bit = 2 * nb + 1;
   const int64_t n = ncl + in.nnz;
   const int g = grid_for(n, 256, nsm_ * 16);
-  uint64_t *k1, *k2;
-  double *v1, *v2;
-  TRY(alloc(&k1, n)); TRY(alloc(&k2, n)); TRY(alloc(&v1, n)); TRY(alloc(&v2, n));
+  if (n > crec_cap_) {
+    dfree(ck1_); dfree(ck2_); dfree(cv1_); dfree(cv2_);
+    crec_cap_ = std::max<int64_t>(n, nnz0_ + nv0_);
+    TRY(alloc(&ck1_, crec_cap_)); TRY(alloc(&ck2_, crec_cap_));
+    TRY(alloc(&cv1_, crec_cap_)); TRY(alloc(&cv2_, crec_cap_));
+  }
+  uint64_t *k1 = ck1_, *k2 = ck2_;
+  double *v1 = cv1_, *v2 = cv2_;
   LAUNCH(k_coarse_records, grid_for(std::max<int64_t>(in.nv, ncl), 256, nsm_ * 16), 256, 0, s_,
          in.nv, in.ptr, in.tail, in.w, Cm, ncl, nb, sentinel, k1, v1);
   size_t tb = 0;
@@ -1243,7 +1301,6 @@ int Engine::coarsen(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
   mark("records");
   CK(cub::DeviceRadixSort::SortPairs(temp_, tb, k1, k2, v1, v2, n, 0, end_bit, s_));
   mark("sort");
-  dfree(k1); dfree(v1);
   uint64_t *ukeys;
   double *uvals;
   int64_t np = 0;
@@ -1269,7 +1326,9 @@ int Engine::coarsen(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
     // reduce-by-key over the sorted records (the sentinel run is dropped by
     // counting only keys below it)
     int64_t *d_np;
-    TRY(alloc(&ukeys, n)); TRY(alloc(&uvals, n)); TRY(alloc(&d_np, 1));
+    ukeys = k1;
+    uvals = v1;
+    TRY(alloc(&d_np, 1));
     CK(cub::DeviceReduce::ReduceByKey(nullptr, tb, k2, ukeys, v2, uvals, d_np, cuda::std::plus<>{},
                                       n, s_));
     TRY(temp(tb));
@@ -1285,7 +1344,6 @@ int Engine::coarsen(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
       if (last >= sentinel) --np;
     }
   }
-  dfree(k2); dfree(v2);
   mark("fold");
   int64_t *lower_cnt, *upper_cnt, *ne_off, *rowc, *lower_first, *upper_first;
   TRY(alloc(&lower_cnt, ncl)); TRY(alloc(&upper_cnt, ncl)); TRY(alloc(&ne_off, 1));
@@ -1310,9 +1368,9 @@ int Engine::coarsen(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
   CK(cudaStreamSynchronize(s_));
   TRY(alloc(&o.tail, o.nnz)); TRY(alloc(&o.w, o.nnz));
   LAUNCH(k_run_first, gp, 256, 0, s_, np, ukeys, nb, sentinel, lower_first);
-  uint64_t *tk1, *tk2;
-  double *tv1, *tv2;
-  TRY(alloc(&tk1, np)); TRY(alloc(&tk2, np)); TRY(alloc(&tv1, np)); TRY(alloc(&tv2, np));
+  uint64_t *tk1 = k2, *tk2;
+  double *tv1 = v2, *tv2;
+  TRY(alloc(&tk2, np)); TRY(alloc(&tv2, np));
   LAUNCH(k_emit_lower, gp, 256, 0, s_, np, ukeys, uvals, nb, o.ptr, lower_first, o.tail, o.w, tk1,
          tv1, sentinel);
   CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, tk1, tk2, tv1, tv2, np, 0, end_bit, s_));
@@ -1323,7 +1381,8 @@ int Engine::coarsen(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
          o.w, sentinel);
   CK(cudaStreamSynchronize(s_));
   mark("emit");
-  dfree(tk1); dfree(tk2); dfree(tv1); dfree(tv2); dfree(ukeys); dfree(uvals);
+  dfree(tk2); dfree(tv2);
+  if (ukeys != k1) { dfree(ukeys); dfree(uvals); }
   dfree(lower_cnt); dfree(upper_cnt); dfree(ne_off); dfree(rowc); dfree(lower_first);
   dfree(upper_first);
   *out = o;

@@ -29,6 +29,29 @@ __global__ void k_init_phase(int64_t nv, const int64_t *ptr, const double *w, do
   }
 }
 
+// Same results when every summation order is exact (integral weights) or when
+// bit-exactness is not asked for: one warp per row.
+__global__ void k_init_phase_warp(int64_t nv, const int64_t *ptr, const double *w, double *vDeg,
+                                  double *cDeg, int32_t *cSize, int32_t *C, int32_t *C2) {
+  const int lane = threadIdx.x & 31;
+  const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t v = wid; v < nv; v += nw) {
+    double s = 0.0;
+    const int64_t e = ptr[v + 1];
+    for (int64_t j = ptr[v] + lane; j < e; j += 32) s = __dadd_rn(s, w[j]);
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) s = __dadd_rn(s, __shfl_xor_sync(FULL, s, off));
+    if (lane == 0) {
+      vDeg[v] = s;
+      cDeg[v] = s;
+      cSize[v] = 1;
+      C[v] = (int32_t)v;
+      if (C2) C2[v] = (int32_t)v;
+    }
+  }
+}
+
 // 1 / sequential sum (calConstantForSecondTerm, :89-96 at one thread).
 __global__ void k_constant_sequential(int64_t n, const double *x, double *out) {
   double s = 0.0;
@@ -627,6 +650,16 @@ __global__ void __launch_bounds__(512) k_spec_assign_block(int64_t n, const int3
   }
 }
 
+// Conflict priority of the speculative colouring: larger degree first (the
+// dense core of a skewed graph settles early, which keeps the colour count
+// near the largest-first greedy one), then a hash of the id, then the id.
+__device__ __forceinline__ bool spec_wins(int32_t u, int32_t v, const int64_t *ptr,
+                                          uint32_t seed) {
+  const int64_t du = ptr[u + 1] - ptr[u], dv = ptr[v + 1] - ptr[v];
+  if (du != dv) return du > dv;
+  return prio_before(v, u, 1, seed);
+}
+
 // A vertex that shares its colour with a higher-priority neighbour resets
 // and goes to the next round's list.  Warp per vertex.
 __global__ void __launch_bounds__(256) k_spec_conflicts(int64_t n, const int32_t *list,
@@ -642,12 +675,38 @@ __global__ void __launch_bounds__(256) k_spec_conflicts(int64_t n, const int32_t
     bool lose = false;
     for (int64_t j = ptr[v] + lane; j < ptr[v + 1] && !lose; j += 32) {
       const int32_t u = tail[j];
-      if (u != v && color[u] == cv && prio_before(u, v, 1, seed)) lose = true;
+      if (u != v && color[u] == cv && spec_wins(u, v, ptr, seed)) lose = true;
     }
     if (__any_sync(FULL, lose) && lane == 0) {
       color[v] = -1;
       next[atomicAdd(next_count, 1)] = v;
     }
+  }
+}
+
+// Same, one block per vertex (rows of at least kSpecBlockDeg entries).
+__global__ void __launch_bounds__(512) k_spec_conflicts_block(int64_t n, const int32_t *list,
+                                                              const int64_t *ptr,
+                                                              const int32_t *tail, uint32_t seed,
+                                                              int32_t *color, int32_t *next,
+                                                              int32_t *next_count) {
+  __shared__ int s_lose;
+  for (int64_t k = blockIdx.x; k < n; k += gridDim.x) {
+    const int32_t v = list[k];
+    if (threadIdx.x == 0) s_lose = 0;
+    __syncthreads();
+    const int32_t cv = color[v];
+    for (int64_t j = ptr[v] + threadIdx.x; j < ptr[v + 1]; j += blockDim.x) {
+      if (*((volatile int *)&s_lose)) break;
+      const int32_t u = tail[j];
+      if (u != v && color[u] == cv && spec_wins(u, v, ptr, seed)) s_lose = 1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && s_lose) {
+      color[v] = -1;
+      next[atomicAdd(next_count, 1)] = v;
+    }
+    __syncthreads();
   }
 }
 
