@@ -114,7 +114,7 @@ def measured_peak():
 
 def profiled_traffic_ratio():
     """DRAM bytes per algorithmic byte of the sweep kernels, from the committed ncu summary."""
-    path = os.path.join(ROOT, 'profiles', 'sweep_kernels_rmat.txt')
+    path = os.path.join(ROOT, 'profiles', 'sweep_iteration_rmat22.txt')
     try:
         with open(path) as f:
             for line in f:
@@ -285,10 +285,14 @@ def main():
     achieved = (sweep_b / sweep_t) / 1e9 if sweep_t > 0 else None
     ratio = profiled_traffic_ratio()
     steps_timed = sum(s['sweep_steps'] for s in stats)
-    roofline = {'bound': 'hbm', 'kernel': 'k_sweep_* (degree-binned local moving, all bins)',
+    roofline = {'bound': 'hbm',
+                'kernel': 'k_sweep_iteration (one Louvain iteration: every colour class and the '
+                          'modularity pass; 32 B per CSR entry + 48 B per vertex)',
                 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                 'frac': (achieved / peak) if achieved else None, 'peak_kind': peak_kind,
                 'traffic': (ratio * sweep_b / steps_timed) if (ratio and steps_timed) else None,
+                'traffic_source': 'ncu DRAM bytes / algorithmic bytes of the R-MAT scale-22 capture '
+                                  '(profiles/sweep_iteration_rmat22.md) times this launch\'s bytes',
                 'algorithmic_bytes_per_launch': sweep_b / steps_timed if steps_timed else None,
                 'avg_launch_s': sweep_t / steps_timed if steps_timed else None}
     s0 = stats[-1]
