@@ -125,6 +125,18 @@ def profiled_traffic_ratio():
     return None
 
 
+def aggregate(seconds, edges, dist=None, device=None):
+    """Whole-job figures over replicas: max time over ranks, edges summed."""
+    if dist is None or not dist.is_initialized():
+        return seconds, edges
+    import torch
+    t = torch.tensor([seconds], dtype=torch.float64, device=device)
+    e = torch.tensor([edges], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(e, op=dist.ReduceOp.SUM)
+    return float(t), float(e)
+
+
 # --------------------------------------------------------------------- reference arm
 def run_reference(args, rank):
     if rank != 0:
@@ -224,14 +236,7 @@ def main():
     launches = sum(s['kernel_launches'] for s in stats)
     sweep_t = sum(s['sweep_kernel_time'] for s in stats)
     sweep_b = sum(s['sweep_bytes'] for s in stats)
-    if dist:
-        tt = torch.tensor([t], dtype=torch.float64, device=dev)
-        ee = torch.tensor([edges], dtype=torch.float64, device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        dist.all_reduce(ee, op=dist.ReduceOp.SUM)
-        t, edges_all = float(tt), float(ee)
-    else:
-        edges_all = edges
+    t, edges_all = aggregate(t, edges, dist, dev)
     value = edges_all / t
 
     # end to end through the reference-facing API: host AoS graph (pinned),
@@ -264,13 +269,7 @@ def main():
         e0 = time.perf_counter()
         est = [e2e_step() for _ in range(args.steps)]
         et = time.perf_counter() - e0
-        ee = sum(s['edges_swept'] for s in est)
-        if dist:
-            tt = torch.tensor([et], dtype=torch.float64, device=dev)
-            eet = torch.tensor([ee], dtype=torch.float64, device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            dist.all_reduce(eet, op=dist.ReduceOp.SUM)
-            et, ee = float(tt), float(eet)
+        et, ee = aggregate(et, sum(s['edges_swept'] for s in est), dist, dev)
         e2e = {'value': ee / et, 'unit': UNIT, 'h2d_bytes_per_step': 24 * nnz + 8 * (nv + 1),
                'd2h_bytes_per_step': 8 * nv,
                'seconds_per_step': et / args.steps,

@@ -266,7 +266,7 @@ class Engine {
   size_t hub_cap_ = 0;
   // parallel hub path (per member slot arrays, work lists, filled-slot lists)
   int64_t *hub_occ_off_ = nullptr, *hub_seg_beg_ = nullptr, *hub_seg_end_ = nullptr;
-  int32_t *hub_cnt_ = nullptr;
+  int32_t *hub_cnt_ = nullptr, *hub_left_ = nullptr, *hub_big_ = nullptr, *step_big_ = nullptr;
   double *hub_self_ = nullptr, *hub_ownw_ = nullptr;
   int32_t *hub_occ_ = nullptr;
   size_t hub_occ_cap_ = 0;
@@ -278,7 +278,7 @@ class Engine {
   HubWork hub_work() const {
     return HubWork{hub_keys_, hub_vals_, hub_off_, hub_occ_, hub_occ_off_, hub_cnt_, hub_self_,
                    hub_ownw_, chunk_pos_, chunk_beg_, chunk_end_, seg_pos_, seg_beg_, seg_end_,
-                   part_g_, part_c_, hub_seg_beg_, hub_seg_end_};
+                   part_g_, part_c_, hub_seg_beg_, hub_seg_end_, hub_left_, hub_big_, step_big_};
   }
   int hist_cap_ = 0;
   // ordered-delta buffers
@@ -312,7 +312,8 @@ void Engine::release() {
   for (auto p : ip) dfree(*p);
   dfree(hub_off_);
   dfree(hub_occ_off_); dfree(hub_seg_beg_); dfree(hub_seg_end_); dfree(hub_cnt_);
-  dfree(hub_self_); dfree(hub_ownw_); dfree(hub_occ_); dfree(chunk_pos_); dfree(seg_pos_);
+  dfree(hub_self_); dfree(hub_ownw_); dfree(hub_occ_); dfree(hub_left_); dfree(hub_big_);
+  dfree(step_big_); dfree(chunk_pos_); dfree(seg_pos_);
   dfree(part_c_); dfree(chunk_beg_); dfree(chunk_end_); dfree(seg_beg_); dfree(seg_end_);
   dfree(part_g_);
   dfree(dkeys_); dfree(dkeys2_); dfree(drecs_); dfree(drecs2_);
@@ -337,7 +338,9 @@ int Engine::init(int64_t nv0, int64_t nnz0) {
   TRY(alloc(&move_old_, n)); TRY(alloc(&move_new_, n)); TRY(alloc(&hub_off_, n));
   TRY(alloc(&hub_occ_off_, n)); TRY(alloc(&hub_seg_beg_, n)); TRY(alloc(&hub_seg_end_, n));
   TRY(alloc(&hub_cnt_, n)); TRY(alloc(&hub_self_, n)); TRY(alloc(&hub_ownw_, n));
+  TRY(alloc(&hub_left_, n)); TRY(alloc(&hub_big_, n));
   CK(cudaMemsetAsync(hub_cnt_, 0, n * sizeof(int32_t), s_));
+  CK(cudaMemsetAsync(hub_big_, 0, n * sizeof(int32_t), s_));
   CK(cudaMemsetAsync(hub_self_, 0, n * sizeof(double), s_));
   CK(cudaMemsetAsync(hub_ownw_, 0, n * sizeof(double), s_));
   if (const char *bm = getenv("GRAPPOLO_B200_BLOCK_MAX")) {
@@ -605,6 +608,15 @@ __global__ void k_scatter_i64(int64_t n, const int32_t *pos, const int64_t *val,
     out[pos[k]] = val[k];
 }
 
+__global__ void k_hub_chunk_counts(int64_t n, const int32_t *pos, const int32_t *members,
+                                   const int64_t *ptr, int32_t *left) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t v = members[pos[k]];
+    left[pos[k]] = (int32_t)((ptr[v + 1] - ptr[v] + kHubChunk - 1) / kHubChunk);
+  }
+}
+
 __global__ void k_row_bounds_at(int64_t n, const int32_t *pos, const int32_t *members,
                                 const int64_t *ptr, int64_t *out) {
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
@@ -748,6 +760,8 @@ int Engine::hub_offsets(const Level &L, std::vector<ClassSched> &sched) {
            hub_seg_beg_);
     LAUNCH(k_scatter_i64, grid_for(nh, 256, nsm_ * 4), 256, 0, s_, nh, d_pos, d_vals + 3 * nh,
            hub_seg_end_);
+    LAUNCH(k_hub_chunk_counts, grid_for(nh, 256, nsm_ * 4), 256, 0, s_, nh, d_pos, members_, L.ptr,
+           hub_left_);
   }
   CK(cudaStreamSynchronize(s_));
   dfree(d_pos);
@@ -1096,10 +1110,12 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
   int64_t *d_ctr = nullptr;
   TRY(alloc(&d_steps, steps.size()));
   TRY(alloc(&d_ctr, steps.size()));
+  dfree(step_big_);
+  TRY(alloc(&step_big_, steps.size()));
   TRY(upload(s_, d_steps, steps));
   IterArgs p{};
   p.a = a;
-  p.h = hub_work();
+  p.h = hub_work();  // after step_big_ exists
   p.steps = d_steps;
   p.nsteps = (int)steps.size();
   p.jacobi = jacobi ? 1 : 0;
@@ -1141,6 +1157,7 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
     ++n;
     const double t0 = now_s();
     cudaError_t e = cudaMemsetAsync(d_ctr, 0, steps.size() * sizeof(int64_t), s_);
+    if (e == cudaSuccess) e = cudaMemsetAsync(step_big_, 0, steps.size() * sizeof(int32_t), s_);
     if (e0) cudaEventRecord(e0, s_);
     if (e == cudaSuccess)
       e = cudaLaunchCooperativeKernel((void *)k_sweep_iteration, grid, kPersistThreads, args,
@@ -1162,6 +1179,7 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
     if (debug) {
       CK(cudaMemcpy(h_trace.data(), d_trace, h_trace.size() * sizeof(uint64_t),
                     cudaMemcpyDeviceToHost));
+      CK(cudaMemsetAsync(d_trace, 0, h_trace.size() * sizeof(uint64_t), s_));
       // per step: stage-1 time (from the previous barrier), hub stages, apply
       const size_t ns = steps.size();
       uint64_t last = h_trace[4 * ns];
@@ -1172,7 +1190,7 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
         st1 += a1;
         const uint64_t t1 = h_trace[4 * k];
         uint64_t t = t1;
-        if (steps[k].hub_segs[1] > steps[k].hub_segs[0]) { st23 += (h_trace[4 * k + 2] - t) * 1e-9; t = h_trace[4 * k + 2]; }
+        if (steps[k].hub_segs[1] > steps[k].hub_segs[0] && h_trace[4 * k + 2] > t) { st23 += (h_trace[4 * k + 2] - t) * 1e-9; t = h_trace[4 * k + 2]; }
         if (steps[k].apply[1] > steps[k].apply[0]) { st4 += (h_trace[4 * k + 3] - t) * 1e-9; t = h_trace[4 * k + 3]; }
         const double tot = (t - last) * 1e-9;
         if (tot > worst) { worst = tot; worst_k = k; }
@@ -1185,7 +1203,7 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
         uint64_t prevt = h_trace[4 * ns];
         for (size_t k = 0; k < ns; ++k) {
           uint64_t t = h_trace[4 * k];
-          if (steps[k].hub_segs[1] > steps[k].hub_segs[0]) t = h_trace[4 * k + 2];
+          if (steps[k].hub_segs[1] > steps[k].hub_segs[0] && h_trace[4 * k + 2] > t) t = h_trace[4 * k + 2];
           if (steps[k].apply[1] > steps[k].apply[0]) t = h_trace[4 * k + 3];
           per.push_back({(t - prevt) * 1e-9, k});
           prevt = t;

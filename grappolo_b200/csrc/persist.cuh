@@ -147,6 +147,7 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
                    (size_t)warp * kPersistWarpCap;
   GLV_TRACE(4 * p.nsteps);
   __shared__ int64_t s_task;
+  __shared__ int s_flag;
   for (int s = 0; s < p.nsteps; ++s) {
     const StepDesc &st = p.steps[s];
     // Stage 1 as a task queue: blocks take the next task of any kind, the
@@ -170,7 +171,7 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
       if (t >= ntask) break;
       if (t < t_hub) {
         hub_accum_chunk(p.a, p.h, st.hub_chunk[0] + t, reinterpret_cast<int32_t *>(tvals + 4096),
-                        tvals, s_self);
+                        tvals, s_self, s_g, s_c, &s_flag, s);
         continue;
       }
       t -= t_hub;
@@ -217,7 +218,7 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
     }
     grid.sync();
     GLV_TRACE(4 * s);
-    if (st.hub_segs[1] > st.hub_segs[0]) {
+    if (st.hub_segs[1] > st.hub_segs[0] && __ldcg(&p.h.step_big[s])) {
       for (int64_t si = st.hub_segs[0] + blockIdx.x; si < st.hub_segs[1]; si += gridDim.x)
         hub_scan_segment(p.a, p.h, si, s_g, s_c);
       grid.sync();

@@ -426,11 +426,15 @@ struct HubWork {
   double *part_g;           // per segment: best gain
   int32_t *part_c;          //              and its community
   const int64_t *hub_seg_beg, *hub_seg_end;  // per member slot: its segments
+  int32_t *chunks_left;     // per member slot: chunks still accumulating
+  int32_t *big;             // per member slot: 1 = decided by the segment scan
+  int32_t *step_big;        // per step: some hub of the step is big (persistent kernel)
 };
 
-constexpr int kHubChunk = 2048;     // CSR entries per accumulation work item
-constexpr int kHubSeg = 2048;       // filled slots per scan work item
-constexpr int kHubStageCap = 4096;  // block-local staging table of one chunk
+constexpr int kHubChunk = 1024;      // CSR entries per accumulation work item
+constexpr int kHubSeg = 2048;        // filled slots per scan work item
+constexpr int kHubStageCap = 2048;   // block-local staging table of one chunk
+constexpr int kHubInlineCap = 4096;  // filled slots the last chunk's block scans itself
 
 // All threads of the block call.  The chunk is first folded into a
 // block-local shared table (`skeys`/`svals`, kHubStageCap slots; at most
@@ -438,7 +442,8 @@ constexpr int kHubStageCap = 4096;  // block-local staging table of one chunk
 // hub's global table once — a hub's neighbours concentrate on a few
 // communities, and per-warp global atomics on those slots would serialise.
 __device__ __forceinline__ void hub_accum_chunk(const SweepArgs &a, const HubWork &h, int64_t ci,
-                                                int32_t *skeys, double *svals, double *s_self) {
+                                                int32_t *skeys, double *svals, double *s_self,
+                                                double *s_g, int32_t *s_c, int *s_flag, int step) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwb = blockDim.x >> 5;
   const int32_t pos = h.chunk_pos[ci];
   const int64_t eb = h.chunk_beg[ci], ee = h.chunk_end[ci];
@@ -486,6 +491,53 @@ __device__ __forceinline__ void hub_accum_chunk(const SweepArgs &a, const HubWor
     }
   }
   if (threadIdx.x == 0 && s_self[0] != 0.0) atomicAdd(&h.self_w[pos], s_self[0]);
+  // The block that finishes a hub's last chunk decides it when the hub has
+  // few distinct communities; otherwise it marks the hub for the segment scan.
+  // Every thread publishes its table and list writes before the countdown.
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) s_flag[0] = (atomicSub(&h.chunks_left[pos], 1) == 1) ? 1 : 0;
+  __syncthreads();
+  if (!s_flag[0]) return;
+  __threadfence();
+  const int32_t nfill = __ldcg(&h.cnt[pos]);
+  if (nfill > kHubInlineCap) {
+    if (threadIdx.x == 0) {
+      h.big[pos] = 1;
+      if (step >= 0) atomicOr(&h.step_big[step], 1);
+    }
+    __syncthreads();
+    return;
+  }
+  const double degree = a.vDeg[v];
+  const double own_w = __ldcg(&h.own_w[pos]);
+  const double eix = __dsub_rn(own_w, __ldcg(&h.self_w[pos]));
+  const double ax = __dsub_rn(a.cDeg[own], degree);
+  double g = 0.0;
+  int32_t bc = INT32_MAX;
+  for (int k = threadIdx.x; k < nfill; k += blockDim.x) {
+    const int32_t s = __ldcg(&occ[k]);
+    const int32_t c = __ldcg(&keys[s]);
+    const double val = __ldcg(&vals[s]);
+    if (c != own) {
+      const double gain = louvain_gain(val, eix, degree, a.cDeg[c], ax, a.constant);
+      if (gain > 0.0 && better(gain, c, g, bc)) { g = gain; bc = c; }
+    }
+    keys[s] = -1;
+    vals[s] = 0.0;
+  }
+  warp_argmax(g, bc);
+  if (lane == 0) { s_g[warp] = g; s_c[warp] = bc; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < nwb; ++k)
+      if (better(s_g[k], s_c[k], g, bc)) { g = s_g[k]; bc = s_c[k]; }
+    emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), degree, own_w);
+    h.cnt[pos] = 0;
+    h.self_w[pos] = 0.0;
+    h.own_w[pos] = 0.0;
+    h.chunks_left[pos] = (int32_t)((a.ptr[v + 1] - a.ptr[v] + kHubChunk - 1) / kHubChunk);
+  }
   __syncthreads();
 }
 
@@ -494,6 +546,7 @@ __device__ __forceinline__ void hub_scan_segment(const SweepArgs &a, const HubWo
                                                  double *s_g, int32_t *s_c) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwb = blockDim.x >> 5;
   const int32_t pos = h.seg_pos[si];
+  if (!h.big[pos]) return;  // decided when its last chunk finished (block-uniform)
   const int32_t v = a.members[pos];
   const int32_t own = a.C[v];
   const double degree = a.vDeg[v];
@@ -532,6 +585,7 @@ __device__ __forceinline__ void hub_scan_segment(const SweepArgs &a, const HubWo
 // One warp per hub (all lanes call).
 __device__ __forceinline__ void hub_final(const SweepArgs &a, const HubWork &h, int64_t pos) {
   const int lane = threadIdx.x & 31;
+  if (!h.big[pos]) return;
   double g = 0.0;
   int32_t bc = INT32_MAX;
   for (int64_t si = h.hub_seg_beg[pos] + lane; si < h.hub_seg_end[pos]; si += 32)
@@ -544,17 +598,21 @@ __device__ __forceinline__ void hub_final(const SweepArgs &a, const HubWork &h, 
     h.cnt[pos] = 0;
     h.self_w[pos] = 0.0;
     h.own_w[pos] = 0.0;
+    h.big[pos] = 0;
+    h.chunks_left[pos] = (int32_t)((a.ptr[v + 1] - a.ptr[v] + kHubChunk - 1) / kHubChunk);
   }
 }
 
 __global__ void __launch_bounds__(512) k_hub_accum(SweepArgs a, HubWork h, int64_t cb,
                                                    int64_t ce) {
   extern __shared__ unsigned char smem_raw[];
-  __shared__ double s_self[1];
+  __shared__ double s_self[1], s_g[32];
+  __shared__ int32_t s_c[32];
+  __shared__ int s_flag[1];
   double *svals = reinterpret_cast<double *>(smem_raw);
   int32_t *skeys = reinterpret_cast<int32_t *>(svals + kHubStageCap);
   for (int64_t ci = cb + blockIdx.x; ci < ce; ci += gridDim.x)
-    hub_accum_chunk(a, h, ci, skeys, svals, s_self);
+    hub_accum_chunk(a, h, ci, skeys, svals, s_self, s_g, s_c, s_flag, -1);
 }
 
 __global__ void __launch_bounds__(256) k_hub_scan(SweepArgs a, HubWork h, int64_t sb,

@@ -1,0 +1,60 @@
+"""The C restatement against Grappolo's own code (compiled from its sources),
+bit for bit, on graphs that are not in the golden set."""
+import numpy as np
+import pytest
+
+from grappolo_b200 import graphs
+
+
+def _graphs():
+    yield 'pp', graphs.planted_partition(num_blocks=30, block_size=60, intra_degree=9,
+                                         inter_degree=3, seed=11)
+    yield 'pp_w', graphs.random_weights(graphs.planted_partition(num_blocks=30, block_size=60,
+                                                                 seed=12), seed=13)
+    yield 'rmat11', graphs.rmat(11, seed=14)
+    yield 'rmat11_unit', graphs.rmat(11, seed=15, weighted=False)
+
+
+@pytest.mark.parametrize('name,g', list(_graphs()))
+def test_primitives(oracle, reference, name, g):
+    col_o, mc_o = oracle.color_greedy(g)
+    col_r, mc_r, _ = reference.color(g)
+    assert mc_o == mc_r and np.array_equal(col_o, col_r)
+    qo, Co, io, _ = oracle.coloring_phase(g, col_o, mc_o + 1)
+    qr, Cr, ir, _ = reference.coloring_phase(g, col_r, mc_r + 1)
+    assert (qo, io) == (qr, ir) and np.array_equal(Co, Cr)
+    qo, Co, io, _ = oracle.basic_phase(g)
+    qr, Cr, ir, _ = reference.basic_phase(g)
+    assert (qo, io) == (qr, ir) and np.array_equal(Co, Cr)
+    Cn, n = oracle.renumber(Cr)
+    Cn2, n2 = reference.renumber(Cr)
+    assert n == n2 and np.array_equal(Cn, Cn2)
+    go, neo = oracle.build_next_level(g, Cn, n)
+    gr, ner = reference.build_next_level(g, Cn, n)
+    assert neo == ner
+    for a, b in ((go.ptr, gr.ptr), (go.tail, gr.tail), (go.weight, gr.weight)):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize('name,g', list(_graphs()))
+def test_multiphase(oracle, reference, name, g):
+    Co, so, _ = oracle.run_multiphase_coloring(g)
+    Cr, sr, _ = reference.run_multiphase_coloring(g)
+    assert np.array_equal(Co, Cr)
+    assert so['phases'] == sr['phases'] and so['total_iterations'] == sr['total_iterations']
+    assert abs(so['final_mod'] - sr['final_mod']) <= 5e-7
+    Co, so, _ = oracle.run_multiphase_basic(g)
+    Cr, sr, _ = reference.run_multiphase_basic(g)
+    assert np.array_equal(Co, Cr)
+    assert so['phases'] == sr['phases']
+
+
+def test_decisions_with_ties_and_singletons(oracle, reference):
+    # a state with many equal gains and singleton pairs
+    g = graphs.from_edges(8, [(i, (i + 1) % 8) for i in range(8)] + [(0, 4), (2, 6)])
+    C = np.arange(8)
+    vdeg, const = oracle.vertex_degrees(g)
+    verts = np.arange(8)
+    t_o = oracle.decide_batch(g, C, vdeg, vdeg, np.ones(8, dtype=np.int64), const, verts)
+    t_r = reference.decide_batch(g, C, vdeg, vdeg, np.ones(8, dtype=np.int64), const, verts)
+    assert np.array_equal(t_o, t_r)
