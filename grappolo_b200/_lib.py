@@ -15,6 +15,9 @@ LIB_PATH = os.path.join(HERE, 'libgrappolo_b200.so')
 GLV_OK = 0
 GLV_MODE_VERIFY = 0
 GLV_MODE_FAST = 1
+GLV_MODE_LEARNED = 2
+GLV_GATE_PARAMS = 4673
+GLV_GATE_FEATURES = 6
 GLV_MAX_PHASES = 256
 GLV_KERNEL_SLOTS = 11
 
@@ -87,7 +90,9 @@ def lib():
                  'glv_dev_run_multiphase', 'glv_louvain_coloring_phase',
                  'glv_louvain_basic_phase', 'glv_distance_one_coloring',
                  'glv_renumber_clusters', 'glv_build_next_level', 'glv_modularity',
-                 'glv_decide_batch', 'glv_dev_modularity_static'):
+                 'glv_decide_batch', 'glv_dev_modularity_static', 'glv_gate_set',
+                 'glv_gate_infer', 'glv_gate_grad', 'glv_gate_train', 'glv_trace_begin',
+                 'glv_trace_end'):
         getattr(L, name).restype = ct.c_int
     L.glv_run_multiphase_coloring.argtypes = [P(GlvGraph), P(ct.c_long), ct.c_int, ct.c_int,
                                               ct.c_int, ct.c_long, ct.c_double, ct.c_double,
@@ -122,6 +127,15 @@ def lib():
     L.glv_dev_modularity_static.argtypes = [ct.c_long, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                             ct.c_void_p, ct.c_void_p, ct.c_double, ct.c_void_p,
                                             ct.c_void_p]
+    fp = P(ct.c_float)
+    L.glv_gate_set.argtypes = [fp, ct.c_float]
+    L.glv_gate_infer.argtypes = [ct.c_long, ct.c_void_p, ct.c_void_p, ct.c_void_p]
+    L.glv_gate_grad.argtypes = [ct.c_long, fp, fp, fp, fp, fp, P(ct.c_double)]
+    L.glv_gate_train.argtypes = [ct.c_long, fp, fp, fp, ct.c_int, ct.c_long, ct.c_float,
+                                 ct.c_uint, fp, P(ct.c_double)]
+    L.glv_trace_begin.argtypes = [ct.c_long, ct.c_double]
+    L.glv_trace_fetch.restype = ct.c_long
+    L.glv_trace_fetch.argtypes = [fp, fp, ct.c_long]
     _lib = L
     return L
 

@@ -13,6 +13,7 @@
 
 #include <cub/cub.cuh>
 
+#include "gate.cuh"
 #include "persist.cuh"
 #include "phase_kernels.cuh"
 #include "sweep.cuh"
@@ -46,6 +47,23 @@ static cudaMemPool_t engine_pool() {
   return g_pool[dev];
 }
 static std::atomic<int> g_profile{0};  // 0 off, 1 per-class sweep, 2 per launch
+
+// Learned gate (process-wide): parameters and keep threshold.
+static std::mutex g_gate_mu;
+static std::vector<float> g_gate_params;
+static float g_gate_tau = 0.5f;
+
+// Trace capture for training: (features, moved) rows of plain colour sweeps.
+struct TraceSink {
+  bool on = false;
+  double rate = 1.0;
+  int64_t cap = 0;
+  int device = -1;
+  float *x = nullptr;      // [cap][6]
+  float *y = nullptr;      // [cap]
+  unsigned long long *n = nullptr;
+};
+static TraceSink g_trace;
 static thread_local std::string g_err;
 
 static int fail(int code, const char *msg) {
@@ -189,7 +207,17 @@ class Engine {
   double edges_swept = 0;
   double sweep_kernel_s = 0, sweep_bytes = 0;
   long sweep_steps = 0;
+  long gated_iterations_ = 0;
   double slot_s[kSlots] = {0};
+  // learned gate state
+  double *rec_own_ = nullptr;
+  float *rec_gain_ = nullptr, *feat_ = nullptr, *gate_p_ = nullptr;
+  int32_t *last_move_ = nullptr;
+  uint8_t *skip_ = nullptr;
+  unsigned long long *evald_ = nullptr;
+  int phase_index_ = 0;
+  bool learned() const { return mode_ == GLV_MODE_LEARNED; }
+  int gate_init();
 
  private:
   // Requests above 1 MiB are rounded up to quarter-octave size classes so that
@@ -318,6 +346,8 @@ void Engine::release() {
   dfree(part_g_);
   dfree(dkeys_); dfree(dkeys2_); dfree(drecs_); dfree(drecs2_);
   dfree(ck1_); dfree(ck2_); dfree(cv1_); dfree(cv2_);
+  dfree(rec_own_); dfree(rec_gain_); dfree(feat_); dfree(gate_p_); dfree(last_move_);
+  dfree(skip_); dfree(evald_);
   dfree(temp_);
   if (h_mod_) cudaFreeHost(h_mod_);
   h_mod_ = nullptr;
@@ -420,7 +450,7 @@ int Engine::color(const Level &L, int *ncolors, double *secs) {
     *ncolors = 0;
     return GLV_OK;
   }
-  TRY(mode_ == GLV_MODE_FAST ? color_spec(L, ncolors) : color_jp(L, ncolors));
+  TRY(mode_ != GLV_MODE_VERIFY ? color_spec(L, ncolors) : color_jp(L, ncolors));
   if (secs) *secs = now_s() - t0;
   return GLV_OK;
 }
@@ -434,7 +464,7 @@ int Engine::color_jp(const Level &L, int *ncolors) {
   CK(cudaMemsetAsync(fcount, 0, 3 * sizeof(int32_t), s_));
   CK(cudaMemsetAsync(status, 0, 2 * sizeof(int32_t), s_));
   CK(cudaMemsetAsync(maxc, 0xff, sizeof(int32_t), s_));
-  const int hashed = (mode_ == GLV_MODE_FAST) ? 1 : 0;
+  const int hashed = (mode_ != GLV_MODE_VERIFY) ? 1 : 0;
   const uint32_t seed = 0x5bd1e995u;
   LAUNCH(k_color_init, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, L.ptr, L.tail, hashed,
          seed, pending, color_, f0, fcount);
@@ -1087,6 +1117,38 @@ int Engine::decide(const Level &L, const int32_t *verts, int64_t nverts) {
   return GLV_OK;
 }
 
+__global__ void k_trace_append(int64_t nv, const int64_t *ptr, const float *feat,
+                               const int32_t *last_move, int32_t iter, uint32_t keep_below,
+                               uint32_t salt, float *tx, float *ty, unsigned long long *tn,
+                               int64_t cap) {
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    if (ptr[v + 1] == ptr[v]) continue;
+    if (mix32((uint32_t)v ^ salt) > keep_below) continue;
+    const unsigned long long k = atomicAdd(tn, 1ull);
+    if ((int64_t)k >= cap) continue;
+    for (int i = 0; i < kGateIn; ++i) tx[k * kGateIn + i] = feat[(size_t)v * kGateIn + i];
+    ty[k] = (last_move[v] == iter) ? 1.0f : 0.0f;
+  }
+}
+
+int Engine::gate_init() {
+  if (rec_own_) return GLV_OK;
+  const size_t n = (size_t)nv0_ + 1;
+  TRY(alloc(&rec_own_, n)); TRY(alloc(&rec_gain_, n)); TRY(alloc(&last_move_, n));
+  TRY(alloc(&skip_, n)); TRY(alloc(&feat_, n * kGateIn)); TRY(alloc(&gate_p_, kGateParams));
+  TRY(alloc(&evald_, 1));
+  if (learned()) {
+    std::lock_guard<std::mutex> lock(g_gate_mu);
+    if ((int)g_gate_params.size() != kGateParams)
+      return fail(GLV_ERR_ARG, "learned mode needs gate parameters (glv_gate_set)");
+    CK(cudaMemcpyAsync(gate_p_, g_gate_params.data(), kGateParams * sizeof(float),
+                       cudaMemcpyHostToDevice, s_));
+    CK(cudaStreamSynchronize(s_));
+  }
+  return GLV_OK;
+}
+
 // One cooperative launch per iteration (persist.cuh).  Colour phases: C is
 // updated in place and Q is taken after the sweep; Jacobi phases: targets go
 // to Ctgt, Q is taken on the state before the moves, and the loop rotates
@@ -1094,10 +1156,14 @@ int Engine::decide(const Level &L, const int32_t *verts, int64_t nverts) {
 int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched, SweepArgs a,
                            bool jacobi, double lower, double thresh, double *mod, int *itr) {
   std::vector<StepDesc> steps;
-  for (auto &cs : sched)
+  std::vector<int64_t> cls_b, cls_e;
+  for (auto &cs : sched) {
+    cls_b.push_back(cs.begin);
+    cls_e.push_back(cs.end);
     for (size_t k = 0; k < cs.steps.size(); ++k) {
       const Step &st = cs.steps[k];
       StepDesc d;
+      d.cls = (int64_t)cls_b.size() - 1;
       for (int b = 0; b <= NBINS; ++b) d.seg[b] = st.seg[b];
       d.hub_chunk[0] = st.hub_chunk[0]; d.hub_chunk[1] = st.hub_chunk[1];
       d.hub_segs[0] = st.hub_segs[0]; d.hub_segs[1] = st.hub_segs[1];
@@ -1106,6 +1172,7 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
       d.apply[1] = last ? cs.end : 0;
       steps.push_back(d);
     }
+  }
   StepDesc *d_steps = nullptr;
   int64_t *d_ctr = nullptr;
   TRY(alloc(&d_steps, steps.size()));
@@ -1113,6 +1180,14 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
   dfree(step_big_);
   TRY(alloc(&step_big_, steps.size()));
   TRY(upload(s_, d_steps, steps));
+  int64_t *d_cls_b = nullptr, *d_cls_e = nullptr;
+  int32_t *d_kept = nullptr;
+  const int nclass = (int)cls_b.size();
+  if (!jacobi && learned()) {
+    TRY(alloc(&d_cls_b, nclass)); TRY(alloc(&d_cls_e, nclass)); TRY(alloc(&d_kept, nclass));
+    TRY(upload(s_, d_cls_b, cls_b));
+    TRY(upload(s_, d_cls_e, cls_e));
+  }
   IterArgs p{};
   p.a = a;
   p.h = hub_work();  // after step_big_ exists
@@ -1153,9 +1228,45 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
   double prev = jacobi ? -1.0 : lower;
   int n = 0;
   int rc = GLV_OK;
+  // learned gate / trace capture (colour phases only)
+  const bool tracing = !jacobi && g_trace.on;
+  const bool gating = !jacobi && learned();
+  if (gating || tracing) {
+    TRY(gate_init());
+    CK(cudaMemsetAsync(last_move_, 0, L.nv * sizeof(int32_t), s_));
+    CK(cudaMemsetAsync(rec_own_, 0, L.nv * sizeof(double), s_));
+    CK(cudaMemsetAsync(rec_gain_, 0, L.nv * sizeof(float), s_));
+    p.a.rec_own = rec_own_;
+    p.a.rec_gain = rec_gain_;
+    p.a.last_move = last_move_;
+  }
+  bool force_full = true;  // the first sweep of a phase is always a full one
+  float tau = 0.5f;
+  {
+    std::lock_guard<std::mutex> lock(g_gate_mu);
+    tau = g_gate_tau;
+  }
   while (true) {
     ++n;
     const double t0 = now_s();
+    p.a.iter = n;
+    bool gated_now = false;
+    if (gating || tracing) {
+      if (n >= 2)
+        LAUNCH(k_gate_features, grid_for(L.nv, 256, nsm_ * 8), 256, 0, s_, L.nv, L.ptr, vDeg,
+               rec_own_, rec_gain_, last_move_, n, phase_index_, feat_);
+      gated_now = gating && !force_full && n >= 2;
+      p.a.skip = nullptr;
+      if (gated_now) {
+        CK(cudaMemsetAsync(evald_, 0, sizeof(unsigned long long), s_));
+        LAUNCH(k_gate_infer, std::max(1, (int)std::min<int64_t>((L.nv + 127) / 128, nsm_ * 8)), 256, 0,
+               s_, L.nv, feat_, gate_p_, tau, L.ptr, (float *)nullptr, skip_, evald_);
+        LAUNCH(k_class_kept, std::max(1, std::min(nclass, nsm_ * 4)), 256, 0, s_, nclass, d_cls_b,
+               d_cls_e, members_, skip_, d_kept);
+        p.a.skip = skip_;
+      }
+      p.class_kept = gated_now ? d_kept : nullptr;
+    }
     cudaError_t e = cudaMemsetAsync(d_ctr, 0, steps.size() * sizeof(int64_t), s_);
     if (e == cudaSuccess) e = cudaMemsetAsync(step_big_, 0, steps.size() * sizeof(int32_t), s_);
     if (e0) cudaEventRecord(e0, s_);
@@ -1169,7 +1280,20 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
     t_sweep += now_s() - t0;
     if (e != cudaSuccess) { g_err = cudaGetErrorString(e); rc = GLV_ERR_CUDA; break; }
     ++launches_;
-    edges_swept += (double)L.nnz;
+    if (gated_now) {
+      unsigned long long ev = 0;
+      CK(cudaMemcpy(&ev, evald_, sizeof(ev), cudaMemcpyDeviceToHost));
+      edges_swept += (double)ev;
+      ++gated_iterations_;
+    } else {
+      edges_swept += (double)L.nnz;
+    }
+    if (tracing && n >= 2) {
+      const uint32_t keep = (uint32_t)std::min(4294967295.0, g_trace.rate * 4294967296.0);
+      LAUNCH(k_trace_append, grid_for(L.nv, 256, nsm_ * 8), 256, 0, s_, L.nv, L.ptr, feat_,
+             last_move_, n, keep, (uint32_t)(n * 7919 + phase_index_ * 104729), g_trace.x,
+             g_trace.y, g_trace.n, g_trace.cap);
+    }
     if (e0) {
       float ms = 0;
       if (cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) sweep_kernel_s += ms * 1e-3;
@@ -1240,8 +1364,15 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
               (long)(steps[worst_k].hub_chunk[1] - steps[worst_k].hub_chunk[0]));
     }
     const double q = h_mod_[0];
-    if (q - prev < thresh) break;
+    if (q - prev < thresh) {
+      // A phase ends only after a full (ungated) sweep gains less than thresh.
+      if (!gated_now) break;
+      if (q > prev) prev = q;
+      force_full = true;
+      continue;
+    }
     prev = q;
+    force_full = false;
     if (jacobi) {
       if (prev < lower) prev = lower;
       LAUNCH(k_rotate, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, Cpast, C, Ctgt);
@@ -1249,6 +1380,9 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
   }
   dfree(d_trace);
   dfree(d_ctr);
+  dfree(d_cls_b);
+  dfree(d_cls_e);
+  dfree(d_kept);
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
   dfree(d_steps);
@@ -1462,6 +1596,7 @@ int Engine::run_multiphase(const Level &L0, int32_t *d_C_orig, bool coloring,
     int itr = 0;
     const bool used_color = !non_color;
     const double ts0 = t_sweep, es0 = edges_swept;
+    phase_index_ = (int)phase - 1;
     if (!non_color) {
       TRY(coloring_phase(L, ncolors, !recolored, curr, c_threshold, &curr, &itr));
     } else {
@@ -1615,7 +1750,7 @@ static int open_call(Call &c, int mode, long nv, const long *ptr, const glv_edge
                      const long *tail64, const double *w) {
   TRY(device_ready());
   TRY(check_ptr(nv, ptr));
-  if (mode != GLV_MODE_VERIFY && mode != GLV_MODE_FAST) return fail(GLV_ERR_ARG, "bad mode");
+  if (mode < GLV_MODE_VERIFY || mode > GLV_MODE_LEARNED) return fail(GLV_ERR_ARG, "bad mode");
   const int64_t nnz = ptr[nv];
   if (nnz > 0 && !edges && !(tail64 && w)) return fail(GLV_ERR_ARG, "edge arrays are NULL");
   CK(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
@@ -1784,7 +1919,7 @@ int glv_dev_run_multiphase(long nv, const long *d_ptr, const int *d_tail, const 
   TRY(device_ready());
   if (nv < 0) return fail(GLV_ERR_ARG, "nv < 0");
   if (nv >= (1L << 31) - 1) return fail(GLV_ERR_TOO_LARGE, "nv >= 2^31");
-  if (mode != GLV_MODE_VERIFY && mode != GLV_MODE_FAST) return fail(GLV_ERR_ARG, "bad mode");
+  if (mode < GLV_MODE_VERIFY || mode > GLV_MODE_LEARNED) return fail(GLV_ERR_ARG, "bad mode");
   if (stats) memset(stats, 0, sizeof(*stats));
   Call c;
   CK(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
@@ -2059,3 +2194,200 @@ extern "C" int glv_dev_modularity_static(long nv, const long *d_ptr, const int *
   CK(cudaGetLastError());
   return GLV_OK;
 }
+
+// =========================================================================
+// Learned gate and trace capture (C ABI)
+// =========================================================================
+namespace glv {
+
+struct DevBuf {
+  void *p = nullptr;
+  ~DevBuf() {
+    if (p) cudaFree(p);
+  }
+};
+
+static int upload_floats(const float *h, size_t n, DevBuf &d) {
+  CK(cudaMalloc(&d.p, std::max<size_t>(n, 1) * sizeof(float)));
+  if (n) CK(cudaMemcpy(d.p, h, n * sizeof(float), cudaMemcpyHostToDevice));
+  return GLV_OK;
+}
+
+// Forward/backward and gradient reduction for rows [0, n) of x/y/w (device),
+// parameters `dp` (device, FP32); gradients into dg (zeroed here).
+static int gate_grad_device(cudaStream_t s, int64_t n, const float *x, const float *y,
+                            const float *w, const float *dp, float *dg, float *work,
+                            double *dloss) {
+  float *h1 = work, *h2 = h1 + n * kGateHid, *dz1 = h2 + n * kGateHid, *dz2 = dz1 + n * kGateHid,
+        *dz3 = dz2 + n * kGateHid;
+  CK(cudaMemsetAsync(dg, 0, kGateParams * sizeof(float), s));
+  CK(cudaMemsetAsync(dloss, 0, sizeof(double), s));
+  const int gb = (int)std::max<int64_t>(1, std::min<int64_t>((n + 127) / 128, 148 * 8));
+  k_gate_fwd_bwd<<<gb, 128, 0, s>>>(n, x, y, w, dp, h1, h2, dz1, dz2, dz3, dloss);
+  const int ga = (int)std::max<int64_t>(1, std::min<int64_t>((n + 1023) / 1024, 148 * 4));
+  k_outer_accum<<<ga, 256, 0, s>>>(n, kGateHid, kGateIn, dz1, kGateHid, x, kGateIn, dg + kGateW1);
+  k_outer_accum<<<ga, 256, 0, s>>>(n, kGateHid, 1, dz1, kGateHid, nullptr, 1, dg + kGateB1);
+  k_outer_accum<<<ga, 256, 0, s>>>(n, kGateHid, kGateHid, dz2, kGateHid, h1, kGateHid, dg + kGateW2);
+  k_outer_accum<<<ga, 256, 0, s>>>(n, kGateHid, 1, dz2, kGateHid, nullptr, 1, dg + kGateB2);
+  k_outer_accum<<<ga, 256, 0, s>>>(n, 1, kGateHid, dz3, 1, h2, kGateHid, dg + kGateW3);
+  k_outer_accum<<<ga, 256, 0, s>>>(n, 1, 1, dz3, 1, nullptr, 1, dg + kGateB3);
+  g_launches += 7;
+  CK(cudaGetLastError());
+  return GLV_OK;
+}
+
+}  // namespace glv
+
+extern "C" {
+
+int glv_gate_set(const float *params, float tau) {
+  if (!params) return fail(GLV_ERR_ARG, "params is NULL");
+  if (!(tau >= 0.0f && tau <= 1.0f)) return fail(GLV_ERR_ARG, "tau must be in [0, 1]");
+  std::lock_guard<std::mutex> lock(g_gate_mu);
+  g_gate_params.assign(params, params + kGateParams);
+  g_gate_tau = tau;
+  return GLV_OK;
+}
+
+int glv_gate_infer(long n, const float *d_feat, float *d_prob, void *stream) {
+  TRY(device_ready());
+  if (n < 0 || (n > 0 && (!d_feat || !d_prob))) return fail(GLV_ERR_ARG, "bad arguments");
+  std::vector<float> hp;
+  {
+    std::lock_guard<std::mutex> lock(g_gate_mu);
+    if ((int)g_gate_params.size() != kGateParams) return fail(GLV_ERR_ARG, "no gate parameters");
+    hp = g_gate_params;
+  }
+  DevBuf dp;
+  TRY(upload_floats(hp.data(), hp.size(), dp));
+  cudaStream_t s = (cudaStream_t)stream;
+  if (n > 0) {
+    k_gate_infer<<<(int)std::max<long>(1, std::min<long>((n + 127) / 128, 148 * 8)), 256, 0, s>>>(
+        n, d_feat, (const float *)dp.p, 0.5f, nullptr, d_prob, nullptr, nullptr);
+    ++g_launches;
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(s));
+  return GLV_OK;
+}
+
+int glv_gate_grad(long n, const float *x, const float *y, const float *w, const float *params,
+                  float *grad, double *loss) {
+  TRY(device_ready());
+  if (n < 1 || !x || !y || !w || !params || !grad) return fail(GLV_ERR_ARG, "bad arguments");
+  DevBuf dx, dy, dw, dp, dg, work, dl;
+  TRY(upload_floats(x, (size_t)n * kGateIn, dx));
+  TRY(upload_floats(y, n, dy));
+  TRY(upload_floats(w, n, dw));
+  TRY(upload_floats(params, kGateParams, dp));
+  CK(cudaMalloc(&dg.p, kGateParams * sizeof(float)));
+  CK(cudaMalloc(&work.p, (size_t)n * (4 * kGateHid + 1) * sizeof(float)));
+  CK(cudaMalloc(&dl.p, sizeof(double)));
+  TRY(gate_grad_device(0, n, (float *)dx.p, (float *)dy.p, (float *)dw.p, (float *)dp.p,
+                       (float *)dg.p, (float *)work.p, (double *)dl.p));
+  CK(cudaMemcpy(grad, dg.p, kGateParams * sizeof(float), cudaMemcpyDeviceToHost));
+  double l = 0;
+  CK(cudaMemcpy(&l, dl.p, sizeof(double), cudaMemcpyDeviceToHost));
+  if (loss) *loss = l / (double)n;
+  return GLV_OK;
+}
+
+int glv_gate_train(long n, const float *x, const float *y, const float *w, int epochs,
+                   long batch, float lr, unsigned seed, float *params, double *loss) {
+  TRY(device_ready());
+  if (n < 1 || batch < 1 || epochs < 1 || !x || !y || !w || !params)
+    return fail(GLV_ERR_ARG, "bad arguments");
+  // shuffle rows once on the host (seeded), then walk mini-batches per epoch
+  std::vector<long> order(n);
+  for (long i = 0; i < n; ++i) order[i] = i;
+  uint32_t st = seed * 2654435761u + 12345u;
+  for (long i = n - 1; i > 0; --i) {
+    st = mix32(st + (uint32_t)i);
+    std::swap(order[i], order[st % (uint32_t)(i + 1)]);
+  }
+  std::vector<float> hx((size_t)n * kGateIn), hy(n), hw(n);
+  for (long i = 0; i < n; ++i) {
+    for (int k = 0; k < kGateIn; ++k) hx[i * kGateIn + k] = x[order[i] * kGateIn + k];
+    hy[i] = y[order[i]];
+    hw[i] = w[order[i]];
+  }
+  const long bs = std::min(batch, n);
+  DevBuf dx, dy, dw, dp, dg, dm, dv, work, dl;
+  TRY(upload_floats(hx.data(), hx.size(), dx));
+  TRY(upload_floats(hy.data(), n, dy));
+  TRY(upload_floats(hw.data(), n, dw));
+  TRY(upload_floats(params, kGateParams, dp));
+  CK(cudaMalloc(&dg.p, kGateParams * sizeof(float)));
+  CK(cudaMalloc(&dm.p, kGateParams * sizeof(float)));
+  CK(cudaMalloc(&dv.p, kGateParams * sizeof(float)));
+  CK(cudaMemset(dm.p, 0, kGateParams * sizeof(float)));
+  CK(cudaMemset(dv.p, 0, kGateParams * sizeof(float)));
+  CK(cudaMalloc(&work.p, (size_t)bs * (4 * kGateHid + 1) * sizeof(float)));
+  CK(cudaMalloc(&dl.p, sizeof(double)));
+  const float b1 = 0.9f, b2 = 0.999f;
+  long t = 0;
+  double epoch_loss = 0;
+  for (int e = 0; e < epochs; ++e) {
+    epoch_loss = 0;
+    for (long b = 0; b < n; b += bs) {
+      const long m = std::min(bs, n - b);
+      TRY(gate_grad_device(0, m, (float *)dx.p + b * kGateIn, (float *)dy.p + b,
+                           (float *)dw.p + b, (float *)dp.p, (float *)dg.p, (float *)work.p,
+                           (double *)dl.p));
+      ++t;
+      const float c1 = 1.0f - std::pow(b1, (float)t), c2 = 1.0f - std::pow(b2, (float)t);
+      k_adam<<<(kGateParams + 255) / 256, 256>>>(kGateParams, (float *)dp.p, (float *)dg.p,
+                                                  (float *)dm.p, (float *)dv.p, lr, b1, b2, 1e-8f,
+                                                  c1, c2);
+      ++g_launches;
+      CK(cudaGetLastError());
+      double l = 0;
+      CK(cudaMemcpy(&l, dl.p, sizeof(double), cudaMemcpyDeviceToHost));
+      epoch_loss += l;
+    }
+    epoch_loss /= (double)n;
+  }
+  CK(cudaMemcpy(params, dp.p, kGateParams * sizeof(float), cudaMemcpyDeviceToHost));
+  if (loss) *loss = epoch_loss;
+  return GLV_OK;
+}
+
+int glv_trace_begin(long capacity, double rate) {
+  TRY(device_ready());
+  if (capacity < 1 || !(rate > 0.0 && rate <= 1.0)) return fail(GLV_ERR_ARG, "bad arguments");
+  glv_trace_end();
+  CK(cudaGetDevice(&g_trace.device));
+  CK(cudaMalloc((void **)&g_trace.x, (size_t)capacity * kGateIn * sizeof(float)));
+  CK(cudaMalloc((void **)&g_trace.y, (size_t)capacity * sizeof(float)));
+  CK(cudaMalloc((void **)&g_trace.n, sizeof(unsigned long long)));
+  CK(cudaMemset(g_trace.n, 0, sizeof(unsigned long long)));
+  g_trace.cap = capacity;
+  g_trace.rate = rate;
+  g_trace.on = true;
+  return GLV_OK;
+}
+
+long glv_trace_fetch(float *x, float *y, long cap) {
+  if (!g_trace.on) return 0;
+  unsigned long long n = 0;
+  if (cudaMemcpy(&n, g_trace.n, sizeof(n), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+  const long held = (long)std::min<unsigned long long>(n, (unsigned long long)g_trace.cap);
+  const long k = std::min(held, cap);
+  if (k > 0 && x && y) {
+    if (cudaMemcpy(x, g_trace.x, (size_t)k * kGateIn * sizeof(float), cudaMemcpyDeviceToHost) !=
+            cudaSuccess ||
+        cudaMemcpy(y, g_trace.y, (size_t)k * sizeof(float), cudaMemcpyDeviceToHost) != cudaSuccess)
+      return -1;
+  }
+  return held;
+}
+
+int glv_trace_end(void) {
+  if (g_trace.x) cudaFree(g_trace.x);
+  if (g_trace.y) cudaFree(g_trace.y);
+  if (g_trace.n) cudaFree(g_trace.n);
+  g_trace = TraceSink{};
+  return GLV_OK;
+}
+
+}  // extern "C"

@@ -29,6 +29,7 @@ struct StepDesc {
   int64_t hub_chunk[2];    // hub accumulation work items
   int64_t hub_segs[2];     // hub scan work items
   int64_t apply[2];        // member range whose deltas are applied after this step
+  int64_t cls;             // colour class of the step
 };
 
 struct IterArgs {
@@ -47,7 +48,25 @@ struct IterArgs {
   int32_t *cSize;
   uint64_t *trace;         // optional: globaltimer at each barrier, 4 per step + 2
   int64_t *task_ctr;       // per step: next stage-1 task (zero at launch)
+  const int32_t *class_kept;  // gated sweeps: vertices the gate kept per class (NULL = all)
 };
+
+// Gated sweeps: how many vertices of each colour class the gate kept.
+__global__ void k_class_kept(int nclass, const int64_t *cls_begin, const int64_t *cls_end,
+                             const int32_t *members, const uint8_t *skip, int32_t *kept) {
+  __shared__ int s_cnt;
+  for (int c = blockIdx.x; c < nclass; c += gridDim.x) {
+    if (threadIdx.x == 0) s_cnt = 0;
+    __syncthreads();
+    int local = 0;
+    for (int64_t pos = cls_begin[c] + threadIdx.x; pos < cls_end[c]; pos += blockDim.x)
+      local += skip[members[pos]] ? 0 : 1;
+    if (local) atomicAdd(&s_cnt, local);
+    __syncthreads();
+    if (threadIdx.x == 0) kept[c] = s_cnt;
+    __syncthreads();
+  }
+}
 
 __device__ __forceinline__ uint64_t global_ns() {
   uint64_t t;
@@ -150,6 +169,8 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
   __shared__ int s_flag;
   for (int s = 0; s < p.nsteps; ++s) {
     const StepDesc &st = p.steps[s];
+    // a class the gate emptied is skipped whole (no work, no barrier)
+    if (p.class_kept && p.class_kept[st.cls] == 0) continue;
     // Stage 1 as a task queue: blocks take the next task of any kind, the
     // heaviest kinds first, so no block serialises several kinds.
     const int64_t n4 = st.seg[1] - st.seg[0], n8 = st.seg[2] - st.seg[1];

@@ -37,12 +37,34 @@ struct SweepArgs {
   int32_t *hub_keys;       // BIN_HUB global tables
   double *hub_vals;
   const int64_t *hub_off;  // per member slot: table offset
+  // learned gating (colour phases of the persistent path; nullptr = off)
+  const uint8_t *skip;     // per vertex: 1 = not evaluated this sweep (stays)
+  double *rec_own;         // per vertex: Counter[own] of its last evaluation
+  float *rec_gain;         // per vertex: best positive gain of its last evaluation
+  int32_t *last_move;      // per vertex: iteration of its last move
+  int32_t iter;            // this sweep's iteration number within the phase
 };
+
+__device__ __forceinline__ bool skipped(const SweepArgs &a, int32_t v) {
+  return a.skip && a.skip[v];
+}
+
+// A vertex the gate left out keeps its community and moves nothing.
+__device__ __forceinline__ void emit_stay(const SweepArgs &a, int64_t pos, int32_t v,
+                                          int32_t own) {
+  if (a.target) a.target[v] = own;
+  a.move_old[pos] = -1;
+  a.move_new[pos] = own;
+}
 
 // Writes the decision of vertex v (member slot pos) and its delta records.
 __device__ __forceinline__ void emit_decision(const SweepArgs &a, int64_t pos, int32_t v,
                                               int32_t own, int32_t target, double degree,
-                                              double own_w) {
+                                              double own_w, double best_g = 0.0) {
+  if (a.rec_own) {
+    a.rec_own[v] = own_w;
+    a.rec_gain[v] = (float)best_g;
+  }
   if (a.target) {
     a.target[v] = target;
     if (a.own_w) a.own_w[v] = own_w;
@@ -52,6 +74,7 @@ __device__ __forceinline__ void emit_decision(const SweepArgs &a, int64_t pos, i
   bool moved = (target != own) && (target != -1);
   a.move_old[pos] = moved ? own : -1;
   a.move_new[pos] = target;
+  if (moved && a.last_move) a.last_move[v] = a.iter;
   if (moved && a.atomic_deltas) {
     atomicAdd(&a.dDeg[target], degree);
     atomicAdd(&a.dDeg[own], -degree);
@@ -84,7 +107,8 @@ __device__ __forceinline__ void small_item(const SweepArgs &a, int64_t base, int
   const int64_t rb = valid ? a.ptr[v] : 0;
   const int deg = valid ? (int)(a.ptr[v + 1] - rb) : 0;
   const int32_t own = (valid && deg > 0) ? a.C[v] : -1;
-  const bool has = gl < deg;
+  const bool skip = valid && deg > 0 && skipped(a, v);
+  const bool has = !skip && gl < deg;
   const int32_t t = has ? a.tail[rb + gl] : -1;
   const double wt = has ? a.w[rb + gl] : 0.0;
   const int32_t c = has ? a.C[t] : -1;
@@ -130,8 +154,12 @@ __device__ __forceinline__ void small_item(const SweepArgs &a, int64_t base, int
     if (better(og, oc, g, bc)) { g = og; bc = oc; }
   }
   if (valid && gl == 0) {
-    const int32_t tgt = (deg == 0) ? -1 : finish_choice(a, own, g, bc);
-    emit_decision(a, pos, v, own, tgt, degree, own_w);
+    if (skip) {
+      emit_stay(a, pos, v, own);
+    } else {
+      const int32_t tgt = (deg == 0) ? -1 : finish_choice(a, own, g, bc);
+      emit_decision(a, pos, v, own, tgt, degree, own_w, g);
+    }
   }
 
 }
@@ -245,6 +273,10 @@ __device__ __forceinline__ void warp_table_vertex(const SweepArgs &a, int64_t po
                                                   double *vals) {
   const int lane = threadIdx.x & 31;
   const int32_t v = a.members[pos];
+  if (skipped(a, v)) {
+    if (lane == 0) emit_stay(a, pos, v, a.C[v]);
+    return;
+  }
   const int64_t rb = a.ptr[v], re = a.ptr[v + 1];
   const uint32_t cap = table_cap(re - rb);
   const uint32_t mask = cap - 1;
@@ -262,7 +294,7 @@ __device__ __forceinline__ void warp_table_vertex(const SweepArgs &a, int64_t po
   int32_t bc = INT32_MAX;
   scan_table(a, keys, vals, lane, cap, 32, own, eix, ax, degree, g, bc);
   warp_argmax(g, bc);
-  if (lane == 0) emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), degree, own_w);
+  if (lane == 0) emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), degree, own_w, g);
   __syncwarp();
 }
 
@@ -349,6 +381,10 @@ __device__ __forceinline__ void team_vertex(const SweepArgs &a, int64_t pos, int
   const int tt = threadIdx.x % T;
   const int lane = tt & 31, tw = tt >> 5;
   const int32_t v = a.members[pos];
+  if (skipped(a, v)) {  // team-uniform
+    if (tt == 0) emit_stay(a, pos, v, a.C[v]);
+    return;
+  }
   const int64_t rb = a.ptr[v], re = a.ptr[v + 1];
   const uint32_t cap = table_cap(re - rb);
   const uint32_t mask = cap - 1;
@@ -375,7 +411,7 @@ __device__ __forceinline__ void team_vertex(const SweepArgs &a, int64_t pos, int
   if (tt == 0) {
     for (int k = 1; k < NW; ++k)
       if (better(s_g[k], s_c[k], g, bc)) { g = s_g[k]; bc = s_c[k]; }
-    emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), degree, own_w);
+    emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), degree, own_w, g);
   }
   team_sync<T>(team);
 }
@@ -448,7 +484,9 @@ __device__ __forceinline__ void hub_accum_chunk(const SweepArgs &a, const HubWor
   const int32_t pos = h.chunk_pos[ci];
   const int64_t eb = h.chunk_beg[ci], ee = h.chunk_end[ci];
   const int32_t v = a.members[pos];
+  const bool skip = skipped(a, v);  // block-uniform
   const uint32_t smask = kHubStageCap - 1;
+  if (!skip) {
   for (uint32_t q = threadIdx.x; q < kHubStageCap; q += blockDim.x) { skeys[q] = -1; svals[q] = 0.0; }
   if (threadIdx.x == 0) s_self[0] = 0.0;
   __syncthreads();
@@ -491,6 +529,7 @@ __device__ __forceinline__ void hub_accum_chunk(const SweepArgs &a, const HubWor
     }
   }
   if (threadIdx.x == 0 && s_self[0] != 0.0) atomicAdd(&h.self_w[pos], s_self[0]);
+  }  // !skip
   // The block that finishes a hub's last chunk decides it when the hub has
   // few distinct communities; otherwise it marks the hub for the segment scan.
   // Every thread publishes its table and list writes before the countdown.
@@ -500,6 +539,19 @@ __device__ __forceinline__ void hub_accum_chunk(const SweepArgs &a, const HubWor
   __syncthreads();
   if (!s_flag[0]) return;
   __threadfence();
+  if (skip) {
+    if (threadIdx.x == 0) {
+      emit_stay(a, pos, v, a.C[v]);
+      h.chunks_left[pos] = (int32_t)((a.ptr[v + 1] - a.ptr[v] + kHubChunk - 1) / kHubChunk);
+    }
+    __syncthreads();
+    return;
+  }
+  const uint32_t mask = table_cap(a.ptr[v + 1] - a.ptr[v]) - 1;
+  int32_t *keys = h.keys + h.tab_off[pos];
+  double *vals = h.vals + h.tab_off[pos];
+  int32_t *occ = h.occ + h.occ_off[pos];
+  const int32_t own = a.C[v];
   const int32_t nfill = __ldcg(&h.cnt[pos]);
   if (nfill > kHubInlineCap) {
     if (threadIdx.x == 0) {
@@ -532,7 +584,7 @@ __device__ __forceinline__ void hub_accum_chunk(const SweepArgs &a, const HubWor
   if (threadIdx.x == 0) {
     for (int k = 1; k < nwb; ++k)
       if (better(s_g[k], s_c[k], g, bc)) { g = s_g[k]; bc = s_c[k]; }
-    emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), degree, own_w);
+    emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), degree, own_w, g);
     h.cnt[pos] = 0;
     h.self_w[pos] = 0.0;
     h.own_w[pos] = 0.0;
@@ -594,7 +646,7 @@ __device__ __forceinline__ void hub_final(const SweepArgs &a, const HubWork &h, 
   if (lane == 0) {
     const int32_t v = a.members[pos];
     const int32_t own = a.C[v];
-    emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), a.vDeg[v], h.own_w[pos]);
+    emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), a.vDeg[v], h.own_w[pos], g);
     h.cnt[pos] = 0;
     h.self_w[pos] = 0.0;
     h.own_w[pos] = 0.0;

@@ -239,3 +239,89 @@ def rmat_device(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0
     ptr = torch.zeros(nv + 1, dtype=torch.int64, device=device)
     ptr[1:] = torch.cumsum(torch.bincount(src, minlength=nv), 0)
     return ptr, dst.to(torch.int32), ww
+
+
+def planted_partition_mixed(nv: int, block_size: int, mu: float, mean_degree: float,
+                            seed: int = 1) -> CSRGraph:
+    """Planted partition with mixing fraction `mu` and expected degree `mean_degree`.
+
+    Vertices fall into consecutive blocks of `block_size` (the last may be
+    smaller).  Each block gets (1-mu)*d*|B|/2 uniform intra pairs and the graph
+    mu*d*NV/2 uniform pairs between different blocks; duplicates and
+    self-loops are dropped.  Unit weights.  This is the graph family of the
+    batched workload (sizes, block sizes, mu and degree drawn per graph).
+    """
+    rng = np.random.default_rng(seed)
+    block = np.arange(nv, dtype=np.int64) // block_size
+    starts = np.arange(0, nv, block_size, dtype=np.int64)
+    sizes = np.minimum(block_size, nv - starts)
+    m_in = rng.poisson((1.0 - mu) * mean_degree * sizes / 2.0)
+    bidx = np.repeat(np.arange(starts.shape[0]), m_in)
+    u = starts[bidx] + (rng.random(bidx.shape[0]) * sizes[bidx]).astype(np.int64)
+    v = starts[bidx] + (rng.random(bidx.shape[0]) * sizes[bidx]).astype(np.int64)
+    m_out = int(rng.poisson(mu * mean_degree * nv / 2.0))
+    uo = rng.integers(0, nv, size=m_out, dtype=np.int64)
+    vo = rng.integers(0, nv, size=m_out, dtype=np.int64)
+    cross = block[uo] != block[vo]
+    return csr_from_undirected(nv, np.concatenate([u, uo[cross]]), np.concatenate([v, vo[cross]]))
+
+
+def _powerlaw_ints(rng, n, exponent, lo, hi):
+    """n integers from a discrete power law p(k) ~ k^-exponent on [lo, hi]."""
+    a = 1.0 - exponent
+    r = rng.random(n)
+    x = ((hi ** a - lo ** a) * r + lo ** a) ** (1.0 / a)
+    return np.clip(np.floor(x).astype(np.int64), lo, hi)
+
+
+def planted_powerlaw(nv: int, degree_exp: float = 2.5, mean_degree: float = 20.0,
+                     max_degree: int = 5000, community_exp: float = 1.5, community_min: int = 20,
+                     community_max: int = 20000, mu: float = 0.3, seed: int = 1) -> CSRGraph:
+    """Planted power-law community graph (LFR-style benchmark shape).
+
+    Community sizes follow a power law (exponent `community_exp`, sizes in
+    [community_min, community_max]); degrees a power law (exponent
+    `degree_exp`, at most `max_degree`) whose lower cut-off is chosen to give
+    `mean_degree`.  A vertex keeps a fraction 1-mu of its stubs inside its
+    community and mu outside; stubs are paired at random (configuration model)
+    within communities and across the graph, then duplicates, self-loops and
+    intra-community pairs among the outside stubs are dropped.  Unit weights.
+    """
+    rng = np.random.default_rng(seed)
+    sizes = []
+    total = 0
+    while total < nv:
+        s = int(_powerlaw_ints(rng, 1, community_exp, community_min, community_max)[0])
+        s = min(s, nv - total)
+        sizes.append(s)
+        total += s
+    sizes = np.asarray(sizes, dtype=np.int64)
+    comm = np.repeat(np.arange(sizes.shape[0]), sizes)
+    rng.shuffle(comm)
+    # lower degree cut-off giving the requested mean
+    lo = 1
+    for cand in range(1, 200):
+        d = _powerlaw_ints(np.random.default_rng(seed + 1), 200000, degree_exp, cand, max_degree)
+        if d.mean() >= mean_degree:
+            lo = cand
+            break
+    deg = _powerlaw_ints(rng, nv, degree_exp, lo, max_degree)
+    csize = sizes[comm]
+    k_in = np.minimum(np.rint((1.0 - mu) * deg).astype(np.int64), csize - 1)
+    k_out = deg - k_in
+    # intra-community stubs: sort by (community, random) and pair neighbours
+    su = np.repeat(np.arange(nv, dtype=np.int64), k_in)
+    key = comm[su].astype(np.float64) + rng.random(su.shape[0])
+    su = su[np.argsort(key, kind='stable')]
+    cs = comm[su]
+    even = su.shape[0] - (su.shape[0] % 2)
+    pu, pv = su[0:even:2], su[1:even:2]
+    same = cs[0:even:2] == cs[1:even:2]
+    # outside stubs: global random pairing, intra pairs dropped
+    so = np.repeat(np.arange(nv, dtype=np.int64), k_out)
+    rng.shuffle(so)
+    even2 = so.shape[0] - (so.shape[0] % 2)
+    qu, qv = so[0:even2:2], so[1:even2:2]
+    cross = comm[qu] != comm[qv]
+    return csr_from_undirected(nv, np.concatenate([pu[same], qu[cross]]),
+                               np.concatenate([pv[same], qv[cross]]))

@@ -55,7 +55,14 @@ enum {
  *   bit-identical (final modularity agrees to about 1e-3).
  * With integral edge weights (total < 2^53) every accumulation is exact in any
  * order, so the modes differ only in the colouring. */
-enum { GLV_MODE_VERIFY = 0, GLV_MODE_FAST = 1 };
+enum { GLV_MODE_VERIFY = 0, GLV_MODE_FAST = 1, GLV_MODE_LEARNED = 2 };
+/* GLV_MODE_LEARNED is GLV_MODE_FAST plus the learned move gate in the colour
+ * phases: from the second sweep of a phase on, a small MLP (glv_gate_set)
+ * predicts from the previous sweep which vertices will move and only those
+ * are evaluated.  A phase still ends only after a full, ungated sweep gains
+ * less than its threshold.  No counterpart in the reference (it replaces the
+ * early-termination heuristic of
+ * FullSyncOptimization/parallelLouvainMethodEarlyTerminate.cpp:116-195). */
 
 #define GLV_MAX_PHASES 256
 #define GLV_KERNEL_SLOTS 11
@@ -210,6 +217,40 @@ int glv_dev_modularity_static(long nv, const long *d_ptr, const int *d_tail,
  * device and keeps freed blocks cached for later calls.  This returns the
  * cached blocks to the driver. */
 void glv_release_cached_memory(void);
+
+/* ---- learned move gate (no counterpart in the reference) ---------------- */
+#define GLV_GATE_PARAMS 4673   /* W1[64][6] b1[64] W2[64][64] b2[64] W3[64] b3 */
+#define GLV_GATE_FEATURES 6
+
+/* Process-wide gate used by GLV_MODE_LEARNED: FP32 master parameters (rounded
+ * to BF16 on the device) and the keep threshold on the predicted move
+ * probability. */
+int glv_gate_set(const float *params, float tau);
+
+/* Move probabilities of n feature rows (device pointers d_feat[n][6],
+ * d_prob[n]) with the parameters of glv_gate_set; runs the tensor-core
+ * inference kernel on `stream` and synchronises it. */
+int glv_gate_infer(long n, const float *d_feat, float *d_prob, void *stream);
+
+/* One forward/backward pass of the weighted binary cross-entropy (mean over
+ * the rows) on host arrays x[n][6], y[n] (0/1), w[n]; grad[GLV_GATE_PARAMS]
+ * and *loss receive the result.  The gradient-check entry point. */
+int glv_gate_grad(long n, const float *x, const float *y, const float *w, const float *params,
+                  float *grad, double *loss);
+
+/* Adam training on host arrays (copied to the device once): `epochs` passes
+ * in mini-batches of `batch` rows, learning rate `lr`; params is read as the
+ * initial value and receives the result; *loss the last epoch's mean loss. */
+int glv_gate_train(long n, const float *x, const float *y, const float *w, int epochs,
+                   long batch, float lr, unsigned seed, float *params, double *loss);
+
+/* Trace capture for training: while on, every plain colour sweep from the
+ * second of a phase appends (features before the sweep, moved 0/1) for a
+ * hashed sample `rate` of the non-isolated vertices, up to `capacity` rows. */
+int glv_trace_begin(long capacity, double rate);
+/* Copies up to cap rows (x[cap][6], y[cap]) to the host; returns rows held. */
+long glv_trace_fetch(float *x, float *y, long cap);
+int glv_trace_end(void);
 
 /* ---- library information ------------------------------------------------ */
 /* Process-wide switch for the following calls: 0 off; 1 time each colour
