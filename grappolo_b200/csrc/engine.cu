@@ -249,6 +249,7 @@ class Engine {
   }
   void release();
   int phase_init(const Level &L, bool need_past);
+  int merge_splits(const Level &L);
   int build_schedule(const Level &L, const int32_t *color, int ncolors, const int32_t *sub,
                      int nsub, std::vector<ClassSched> *sched);
   int hub_offsets(const Level &L, std::vector<ClassSched> &sched);
@@ -314,6 +315,8 @@ class Engine {
   DeltaRec *drecs_ = nullptr, *drecs2_ = nullptr;
   // modularity
   double *part_e_ = nullptr, *part_a_ = nullptr, *mod_out_ = nullptr;
+  int64_t *split_row_ = nullptr;  // merge-path tiles of the current level
+  int64_t split_cap_ = 0;
   double *h_mod_ = nullptr;  // pinned
   // misc
   unsigned char *temp_ = nullptr;
@@ -348,6 +351,8 @@ void Engine::release() {
   dfree(ck1_); dfree(ck2_); dfree(cv1_); dfree(cv2_);
   dfree(rec_own_); dfree(rec_gain_); dfree(feat_); dfree(gate_p_); dfree(last_move_);
   dfree(skip_); dfree(evald_);
+  dfree(split_row_);
+  split_cap_ = 0;
   dfree(temp_);
   if (h_mod_) cudaFreeHost(h_mod_);
   h_mod_ = nullptr;
@@ -426,7 +431,21 @@ int Engine::upload_check(const Level &L) {
   return GLV_OK;
 }
 
+// split_row_ <- the merge-path tile boundaries of L.
+int Engine::merge_splits(const Level &L) {
+  const int64_t nt = merge_tiles(L.nv, L.nnz);
+  if (nt + 1 > split_cap_) {
+    dfree(split_row_);
+    split_cap_ = nt + 1;
+    TRY(alloc(&split_row_, split_cap_));
+  }
+  LAUNCH(k_merge_splits, grid_for(nt + 1, 256, nsm_ * 16), 256, 0, s_, L.nv, L.nnz, L.ptr, nt,
+         split_row_);
+  return GLV_OK;
+}
+
 int Engine::phase_init(const Level &L, bool need_past) {
+  TRY(merge_splits(L));
   if (ordered()) {
     LAUNCH(k_init_phase, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, L.ptr, L.w, vDeg, cDeg,
            cSize, C, need_past ? Cpast : (int32_t *)nullptr);
@@ -675,7 +694,7 @@ int Engine::hub_offsets(const Level &L, std::vector<ClassSched> &sched) {
   std::vector<int32_t> c_pos, s_pos;
   std::vector<int64_t> c_beg, c_end, s_beg, s_end;
   std::vector<int64_t> hub_pos_all;
-  size_t need_tab = 0, tab_acc = 0, occ_acc = 0;
+  size_t need_tab = 0;
   // row bounds of every hub of the schedule, in one gather
   std::vector<int32_t> hpos;
   for (auto &cs : sched)
@@ -736,8 +755,6 @@ int Engine::hub_offsets(const Level &L, std::vector<ClassSched> &sched) {
       st.hub_chunk[1] = (int64_t)c_pos.size();
       st.hub_segs[1] = (int64_t)s_pos.size();
     }
-  (void)tab_acc;
-  (void)occ_acc;
   (void)hub_pos_all;
   if (hpos.empty()) return GLV_OK;
   if (need_tab > hub_cap_ || (parallel && !hub_tables_clean_)) {
@@ -882,11 +899,12 @@ int Engine::launch_apply(const ClassSched &cs, bool ordered_upd) {
 }
 
 int Engine::launch_modularity(const Level &L, const int32_t *Cm, const double *ownw) {
-  const int64_t nparts = (L.nv + kModVB - 1) / kModVB;
-  LAUNCH(k_modularity_part, (int)std::max<int64_t>(1, nparts), 256, 0, s_, L.nv, L.ptr, L.tail,
-         L.w, Cm, ownw, cDeg, part_e_, part_a_);
-  LAUNCH(k_modularity_final, 1, 256, 0, s_, (int)std::max<int64_t>(1, nparts), part_e_, part_a_,
-         cst, mod_out_);
+  // one partial pair per block (part_e_ holds at least kConstParts)
+  const int nparts = (int)std::max<int64_t>(1, std::min<int64_t>(merge_tiles(L.nv, L.nnz),
+                                                                  kConstParts));
+  LAUNCH(k_modularity_merge, nparts, 256, 0, s_, L.nv, L.nnz, L.ptr, L.tail, L.w, Cm, ownw, cDeg,
+         split_row_, part_e_, part_a_);
+  LAUNCH(k_modularity_final, 1, 256, 0, s_, nparts, part_e_, part_a_, cst, mod_out_);
   CK(cudaMemcpyAsync(h_mod_, mod_out_, 3 * sizeof(double), cudaMemcpyDeviceToHost, s_));
   return GLV_OK;
 }
@@ -1204,6 +1222,8 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
   p.cDeg = cDeg;
   p.cSize = cSize;
   p.task_ctr = d_ctr;
+  p.nnz = L.nnz;
+  p.split_row = split_row_;
   int per_sm = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_iteration, kPersistThreads,
                                                    kPersistSmem));
@@ -1343,10 +1363,8 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
         for (double qf : {0.25, 0.5, 0.75, 0.9}) {
           const auto &x = per[(size_t)(qf * (per.size() - 1))];
           const StepDesc &d = steps[x.second];
-          int64_t edges = 0;
           fprintf(stderr, "   q%.2f step %zu: %.1f us bins", qf, x.second, x.first * 1e6);
           for (int b = 0; b < NBINS; ++b) fprintf(stderr, " %ld", (long)(d.seg[b + 1] - d.seg[b]));
-          (void)edges;
           fprintf(stderr, " hub_chunks %ld hub_segs %ld\n", (long)(d.hub_chunk[1] - d.hub_chunk[0]),
                   (long)(d.hub_segs[1] - d.hub_segs[0]));
         }
@@ -1364,6 +1382,9 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
               (long)(steps[worst_k].hub_chunk[1] - steps[worst_k].hub_chunk[0]));
     }
     const double q = h_mod_[0];
+    if (debug)
+      fprintf(stderr, "grappolo_b200: iter %d gated %d q %.9f gain %.3e edges %.0f time %.5f\n", n,
+              (int)gated_now, q, q - prev, edges_swept, now_s() - t0);
     if (q - prev < thresh) {
       // A phase ends only after a full (ungated) sweep gains less than thresh.
       if (!gated_now) break;
@@ -1445,8 +1466,11 @@ int Engine::coarsen(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
   }
   uint64_t *k1 = ck1_, *k2 = ck2_;
   double *v1 = cv1_, *v2 = cv2_;
-  LAUNCH(k_coarse_records, grid_for(std::max<int64_t>(in.nv, ncl), 256, nsm_ * 16), 256, 0, s_,
-         in.nv, in.ptr, in.tail, in.w, Cm, ncl, nb, sentinel, k1, v1);
+  TRY(merge_splits(in));
+  LAUNCH(k_coarse_records, std::max(1, (int)std::min<int64_t>(merge_tiles(in.nv, in.nnz),
+                                                               nsm_ * 8)),
+         256, 0, s_, in.nv, in.nnz, in.ptr, in.tail, in.w, Cm, ncl, nb, sentinel, split_row_, k1,
+         v1);
   size_t tb = 0;
   CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, k1, k2, v1, v2, n, 0, end_bit, s_));
   TRY(temp(tb));

@@ -49,6 +49,8 @@ struct IterArgs {
   uint64_t *trace;         // optional: globaltimer at each barrier, 4 per step + 2
   int64_t *task_ctr;       // per step: next stage-1 task (zero at launch)
   const int32_t *class_kept;  // gated sweeps: vertices the gate kept per class (NULL = all)
+  int64_t nnz;
+  const int64_t *split_row;   // merge-path tile boundaries of the level
 };
 
 // Gated sweeps: how many vertices of each colour class the gate kept.
@@ -83,6 +85,7 @@ constexpr int kPersistThreads = 512;
 constexpr int kPersistTableCap = 4096;  // BIN_BLOCK rows: degree <= 2047
 constexpr int kPersistWarpCap = 256;    // warp-table rows: degree <= 127
 constexpr size_t kPersistSmem = (size_t)kPersistTableCap * (sizeof(double) + sizeof(int32_t));
+static_assert(kPersistSmem >= sizeof(MergeSmem), "merge tiles must fit");
 static_assert(kPersistSmem >= (size_t)(kPersistThreads / 32) * kPersistWarpCap *
                                   (sizeof(double) + sizeof(int32_t)),
               "warp tables must fit in the block-table region");
@@ -105,39 +108,11 @@ __device__ __forceinline__ void apply_deltas_range(const IterArgs &p, int64_t b,
   }
 }
 
-// Modularity partials of one 256-vertex tile (all threads of the block call).
-__device__ __forceinline__ void modularity_tile(const IterArgs &p, int64_t tile, int64_t *s_ptr,
-                                                int32_t *s_cc, double *sh) {
-  const int64_t v0 = tile * kModVB, v1 = min(p.nv, v0 + kModVB);
-  const int nvb = (int)(v1 - v0);
-  double a2 = 0.0, ex = 0.0;
-  if (threadIdx.x < nvb) {
-    const double d = p.cDeg[v0 + threadIdx.x];
-    a2 = __dmul_rn(d, d);
-  }
-  if (p.own_w_mod) {
-    if (threadIdx.x < nvb) ex = p.own_w_mod[v0 + threadIdx.x];
-  } else {
-    for (int k = threadIdx.x; k <= nvb; k += blockDim.x) s_ptr[k] = p.a.ptr[v0 + k];
-    for (int k = threadIdx.x; k < nvb; k += blockDim.x) s_cc[k] = p.C_mod[v0 + k];
-    __syncthreads();
-    const int64_t eb = s_ptr[0], ee = s_ptr[nvb];
-    int hh = 0;
-    for (int64_t e = eb + threadIdx.x; e < ee; e += blockDim.x) {
-      while (s_ptr[hh + 1] <= e) ++hh;
-      if (p.C_mod[p.a.tail[e]] == s_cc[hh]) ex = __dadd_rn(ex, p.a.w[e]);
-    }
-  }
-  ex = block_sum<kPersistThreads>(ex, sh);
-  a2 = block_sum<kPersistThreads>(a2, sh);
-  if (threadIdx.x == 0) { p.part_e[tile] = ex; p.part_a[tile] = a2; }
-  __syncthreads();
-}
-
-__device__ __forceinline__ void modularity_fold(const IterArgs &p, int64_t ntiles, double *sh) {
+// Q from the per-block partials (block 0, all threads).
+__device__ __forceinline__ void modularity_fold(const IterArgs &p, int64_t nparts, double *sh) {
   double e = 0.0, a = 0.0;
-  const int64_t per = (ntiles + blockDim.x - 1) / blockDim.x;
-  const int64_t b = threadIdx.x * per, en = min(ntiles, b + per);
+  const int64_t per = (nparts + blockDim.x - 1) / blockDim.x;
+  const int64_t b = threadIdx.x * per, en = min(nparts, b + per);
   for (int64_t i = b; i < en; ++i) { e = __dadd_rn(e, p.part_e[i]); a = __dadd_rn(a, p.part_a[i]); }
   e = block_sum<kPersistThreads>(e, sh);
   a = block_sum<kPersistThreads>(a, sh);
@@ -154,8 +129,6 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
   extern __shared__ unsigned char smem_raw[];
   __shared__ double s_self[32], s_g[32], sh[32];
   __shared__ int32_t s_c[32];
-  __shared__ int64_t s_ptr[kModVB + 1];
-  __shared__ int32_t s_cc[kModVB];
   const int warp = threadIdx.x >> 5, nwb = blockDim.x >> 5;
   const int64_t gw = (int64_t)blockIdx.x * nwb + warp, ngw = (int64_t)gridDim.x * nwb;
   const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -255,12 +228,22 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
       GLV_TRACE(4 * s + 3);
     }
   }
-  const int64_t ntiles = (p.nv + kModVB - 1) / kModVB;
-  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
-    modularity_tile(p, tile, s_ptr, s_cc, sh);
+  {
+    // merge-path tiles, one partial pair per block
+    double ex = 0.0, a2 = 0.0;
+    const int64_t ntiles = merge_tiles(p.nv, p.nnz);
+    MergeSmem *msm = reinterpret_cast<MergeSmem *>(smem_raw);
+    __syncthreads();  // stage-1 tables in the same shared memory are done
+    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+      modularity_merge_tile<kPersistThreads>(tile, p.nv, p.nnz, p.a.ptr, p.a.tail, p.a.w, p.C_mod,
+                                             p.own_w_mod, p.cDeg, p.split_row, msm, ex, a2);
+    ex = block_sum<kPersistThreads>(ex, sh);
+    a2 = block_sum<kPersistThreads>(a2, sh);
+    if (threadIdx.x == 0) { p.part_e[blockIdx.x] = ex; p.part_a[blockIdx.x] = a2; }
+  }
   grid.sync();
   GLV_TRACE(4 * p.nsteps + 1);
-  if (blockIdx.x == 0) modularity_fold(p, ntiles, sh);
+  if (blockIdx.x == 0) modularity_fold(p, gridDim.x, sh);
   if (p.jacobi && p.nsteps > 0) {
     // Q above used the totals before the moves; now take the moves' deltas.
     apply_deltas_range(p, p.steps[0].apply[0], p.steps[p.nsteps - 1].apply[1], gt, ngt);

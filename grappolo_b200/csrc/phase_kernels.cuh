@@ -138,6 +138,102 @@ __global__ void __launch_bounds__(256) k_modularity_part(int64_t nv, const int64
   if (threadIdx.x == 0) { part_e[blockIdx.x] = ex; part_a[blockIdx.x] = a2; }
 }
 
+// Merge-path tiles.  The items of a level are its rows' entries interleaved
+// with one "row end" per row (row i's entries come before its end), nv + nnz
+// items in all; a tile is kMergeTile consecutive items.  A hub row is cut over
+// many tiles and a run of empty rows costs one item each, so every tile has
+// the same work whatever the degree distribution.
+constexpr int kMergeTile = 4096;
+
+__host__ __device__ inline int64_t merge_tiles(int64_t nv, int64_t nnz) {
+  return (nv + nnz + kMergeTile - 1) / kMergeTile;
+}
+
+// split_row[t] = rows ended before item t * kMergeTile: the largest i in
+// [0, nv] with ptr[i] + i <= d (ptr[i] + i is strictly increasing in i).
+__global__ void k_merge_splits(int64_t nv, int64_t nnz, const int64_t *ptr, int64_t ntiles,
+                               int64_t *split_row) {
+  for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t <= ntiles;
+       t += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t d = min(t * (int64_t)kMergeTile, nv + nnz);
+    int64_t lo = max((int64_t)0, d - nnz), hi = min(d, nv);
+    while (lo < hi) {
+      const int64_t mid = (lo + hi + 1) >> 1;
+      if (ptr[mid] + mid <= d) lo = mid; else hi = mid - 1;
+    }
+    split_row[t] = lo;
+  }
+}
+
+// Shared memory of one merge tile: row starts relative to the tile's first
+// entry (clamped to [0, kMergeTile + 1]) and the rows' communities.
+struct MergeSmem {
+  int32_t off[kMergeTile + 2];
+  int32_t comm[kMergeTile + 1];
+};
+
+// Modularity partials of merge tile `tile` added to (ex, a2): a2 over the rows
+// that end in the tile, ex over its entries whose two ends share a community
+// (colour phases) or the rows' own_w (Jacobi phases).  All NT threads call.
+template <int NT>
+__device__ __forceinline__ void modularity_merge_tile(int64_t tile, int64_t nv, int64_t nnz,
+                                                      const int64_t *ptr, const int32_t *tail,
+                                                      const double *w, const int32_t *C,
+                                                      const double *own_w, const double *cDeg,
+                                                      const int64_t *split_row, MergeSmem *sm,
+                                                      double &ex, double &a2) {
+  const int64_t d0 = tile * (int64_t)kMergeTile;
+  const int64_t d1 = min(d0 + (int64_t)kMergeTile, nv + nnz);
+  const int64_t i0 = split_row[tile], i1 = split_row[tile + 1];
+  const int64_t j0 = d0 - i0, j1 = d1 - i1;
+  for (int64_t i = i0 + threadIdx.x; i < i1; i += NT) {
+    const double dg = cDeg[i];
+    a2 = __dadd_rn(a2, __dmul_rn(dg, dg));
+    if (own_w) ex = __dadd_rn(ex, own_w[i]);
+  }
+  if (own_w || j1 <= j0) return;  // tile-uniform
+  // rows holding entries j0..j1-1: i0 .. ih
+  const int64_t ih = min(i1, nv - 1);
+  const int nr = (int)(ih - i0 + 1);
+  __syncthreads();  // the previous tile's readers are done
+  for (int k = threadIdx.x; k <= nr; k += NT) {
+    const int64_t r = ptr[i0 + k] - j0;
+    sm->off[k] = (int32_t)max((int64_t)0, min(r, (int64_t)kMergeTile + 1));
+  }
+  for (int k = threadIdx.x; k < nr; k += NT) sm->comm[k] = C[i0 + k];
+  __syncthreads();
+  const int ne = (int)(j1 - j0);
+#pragma unroll 4
+  for (int q = threadIdx.x; q < ne; q += NT) {
+    int lo = 0, hi = nr - 1;  // the last row starting at or before q
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (sm->off[mid] <= q) lo = mid; else hi = mid - 1;
+    }
+    const int64_t e = j0 + q;
+    if (C[tail[e]] == sm->comm[lo]) ex = __dadd_rn(ex, w[e]);
+  }
+}
+
+// Graph-of-launches form: each block folds the tiles blockIdx.x + k*gridDim.x
+// and writes one partial pair.
+__global__ void __launch_bounds__(256) k_modularity_merge(int64_t nv, int64_t nnz,
+                                                          const int64_t *ptr, const int32_t *tail,
+                                                          const double *w, const int32_t *C,
+                                                          const double *own_w, const double *cDeg,
+                                                          const int64_t *split_row,
+                                                          double *part_e, double *part_a) {
+  __shared__ MergeSmem sm;
+  __shared__ double sh[8];
+  double ex = 0.0, a2 = 0.0;
+  const int64_t ntiles = merge_tiles(nv, nnz);
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x)
+    modularity_merge_tile<256>(t, nv, nnz, ptr, tail, w, C, own_w, cDeg, split_row, &sm, ex, a2);
+  ex = block_sum<256>(ex, sh);
+  a2 = block_sum<256>(a2, sh);
+  if (threadIdx.x == 0) { part_e[blockIdx.x] = ex; part_a[blockIdx.x] = a2; }
+}
+
 // out[0] = Q, out[1] = e_xx, out[2] = a2_x.  `cst` = {constant, 2m}.
 __global__ void __launch_bounds__(256) k_modularity_final(int nparts, const double *part_e,
                                                           const double *part_a, const double *cst,
@@ -406,31 +502,43 @@ __global__ void k_compose(int64_t n, int32_t *C_orig, const int32_t *C, int firs
 // 0.0) per cluster, then one per CSR entry i->t with a = C[i] >= b = C[t], in
 // (i, j) order; others get the sentinel key.  A stable radix sort by
 // (a << nb) | b groups each pair with its entries still in (i, j) order.
-__global__ void k_coarse_records(int64_t nv, const int64_t *ptr, const int32_t *tail,
-                                 const double *w, const int32_t *C, int64_t ncl, int nb,
-                                 uint64_t sentinel, uint64_t *keys, double *vals) {
+__global__ void __launch_bounds__(256) k_coarse_records(
+    int64_t nv, int64_t nnz, const int64_t *ptr, const int32_t *tail, const double *w,
+    const int32_t *C, int64_t ncl, int nb, uint64_t sentinel, const int64_t *split_row,
+    uint64_t *keys, double *vals) {
   // seeds
   for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < ncl;
        a += (int64_t)gridDim.x * blockDim.x) {
     keys[a] = ((uint64_t)a << nb) | (uint64_t)a;
     vals[a] = 0.0;
   }
-  // entries: block-level edge-parallel walk over 256-vertex tiles
-  __shared__ int64_t s_ptr[kModVB + 1];
-  __shared__ int32_t s_c[kModVB];
-  const int64_t ntiles = (nv + kModVB - 1) / kModVB;
+  // entries: merge-path tiles, so hub rows spread over many blocks
+  __shared__ MergeSmem sm;
+  const int64_t ntiles = merge_tiles(nv, nnz);
   for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int64_t v0 = tile * kModVB, v1 = min(nv, v0 + kModVB);
-    const int nvb = (int)(v1 - v0);
+    const int64_t d0 = tile * (int64_t)kMergeTile;
+    const int64_t d1 = min(d0 + (int64_t)kMergeTile, nv + nnz);
+    const int64_t i0 = split_row[tile], i1 = split_row[tile + 1];
+    const int64_t j0 = d0 - i0, j1 = d1 - i1;
+    if (j1 <= j0) continue;  // tile-uniform
+    const int64_t ih = min(i1, nv - 1);
+    const int nr = (int)(ih - i0 + 1);
     __syncthreads();
-    for (int k = threadIdx.x; k <= nvb; k += blockDim.x) s_ptr[k] = ptr[v0 + k];
-    for (int k = threadIdx.x; k < nvb; k += blockDim.x) s_c[k] = C[v0 + k];
+    for (int k = threadIdx.x; k <= nr; k += blockDim.x) {
+      const int64_t r = ptr[i0 + k] - j0;
+      sm.off[k] = (int32_t)max((int64_t)0, min(r, (int64_t)kMergeTile + 1));
+    }
+    for (int k = threadIdx.x; k < nr; k += blockDim.x) sm.comm[k] = C[i0 + k];
     __syncthreads();
-    const int64_t eb = s_ptr[0], ee = s_ptr[nvb];
-    int h = 0;
-    for (int64_t e = eb + threadIdx.x; e < ee; e += blockDim.x) {
-      while (s_ptr[h + 1] <= e) ++h;
-      const int32_t a = s_c[h];
+    const int ne = (int)(j1 - j0);
+    for (int q = threadIdx.x; q < ne; q += blockDim.x) {
+      int lo = 0, hi = nr - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (sm.off[mid] <= q) lo = mid; else hi = mid - 1;
+      }
+      const int64_t e = j0 + q;
+      const int32_t a = sm.comm[lo];
       const int32_t b = C[tail[e]];
       if (a >= b) {
         keys[ncl + e] = ((uint64_t)a << nb) | (uint64_t)b;
