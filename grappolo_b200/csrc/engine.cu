@@ -1324,62 +1324,38 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
       CK(cudaMemcpy(h_trace.data(), d_trace, h_trace.size() * sizeof(uint64_t),
                     cudaMemcpyDeviceToHost));
       CK(cudaMemsetAsync(d_trace, 0, h_trace.size() * sizeof(uint64_t), s_));
-      // per step: stage-1 time (from the previous barrier), hub stages, apply
+      // Stage times per step (a zero slot = stage not run); steps holding
+      // only hub rows are summed apart.
       const size_t ns = steps.size();
       uint64_t last = h_trace[4 * ns];
-      double st1 = 0, st23 = 0, st4 = 0, worst = 0;
-      size_t worst_k = 0;
+      double acc[2][4] = {{0, 0, 0, 0}, {0, 0, 0, 0}};
+      int cnt[2] = {0, 0};
+      std::vector<double> per(ns, 0.0);
       for (size_t k = 0; k < ns; ++k) {
-        const double a1 = (h_trace[4 * k] - last) * 1e-9;
-        st1 += a1;
-        const uint64_t t1 = h_trace[4 * k];
-        uint64_t t = t1;
-        if (steps[k].hub_segs[1] > steps[k].hub_segs[0] && h_trace[4 * k + 2] > t) { st23 += (h_trace[4 * k + 2] - t) * 1e-9; t = h_trace[4 * k + 2]; }
-        if (steps[k].apply[1] > steps[k].apply[0]) { st4 += (h_trace[4 * k + 3] - t) * 1e-9; t = h_trace[4 * k + 3]; }
-        const double tot = (t - last) * 1e-9;
-        if (tot > worst) { worst = tot; worst_k = k; }
+        const StepDesc &d = steps[k];
+        const int hub_only = (d.seg[BIN_HUB] == d.seg[0] && d.seg[NBINS] > d.seg[0]) ? 1 : 0;
+        if (h_trace[4 * k] == 0) continue;  // skipped step
+        uint64_t t = last;
+        for (int q = 0; q < 4; ++q) {
+          const uint64_t x = h_trace[4 * k + q];
+          if (x == 0 || x < t) continue;
+          acc[hub_only][q] += (x - t) * 1e-9;
+          t = x;
+        }
+        per[k] = (t - last) * 1e-9;
+        ++cnt[hub_only];
         last = t;
       }
-      const double tm = (h_trace[4 * ns + 1] - last) * 1e-9;
-      if (n == 1 || n == 2) {
-        // ten slowest steps with their composition
-        std::vector<std::pair<double, size_t>> per;
-        uint64_t prevt = h_trace[4 * ns];
-        for (size_t k = 0; k < ns; ++k) {
-          uint64_t t = h_trace[4 * k];
-          if (steps[k].hub_segs[1] > steps[k].hub_segs[0] && h_trace[4 * k + 2] > t) t = h_trace[4 * k + 2];
-          if (steps[k].apply[1] > steps[k].apply[0]) t = h_trace[4 * k + 3];
-          per.push_back({(t - prevt) * 1e-9, k});
-          prevt = t;
-        }
-        std::sort(per.begin(), per.end(), [](auto &x, auto &y) { return x.first > y.first; });
-        for (size_t q = 0; q < std::min<size_t>(10, per.size()); ++q) {
-          const StepDesc &d = steps[per[q].second];
-          fprintf(stderr, "   step %zu: %.1f us bins", per[q].second, per[q].first * 1e6);
-          for (int b = 0; b < NBINS; ++b) fprintf(stderr, " %ld", (long)(d.seg[b + 1] - d.seg[b]));
-          fprintf(stderr, " hub_chunks %ld hub_segs %ld\n", (long)(d.hub_chunk[1] - d.hub_chunk[0]),
-                  (long)(d.hub_segs[1] - d.hub_segs[0]));
-        }
-        for (double qf : {0.25, 0.5, 0.75, 0.9}) {
-          const auto &x = per[(size_t)(qf * (per.size() - 1))];
-          const StepDesc &d = steps[x.second];
-          fprintf(stderr, "   q%.2f step %zu: %.1f us bins", qf, x.second, x.first * 1e6);
-          for (int b = 0; b < NBINS; ++b) fprintf(stderr, " %ld", (long)(d.seg[b + 1] - d.seg[b]));
-          fprintf(stderr, " hub_chunks %ld hub_segs %ld\n", (long)(d.hub_chunk[1] - d.hub_chunk[0]),
-                  (long)(d.hub_segs[1] - d.hub_segs[0]));
-        }
-        std::vector<double> t_only;
-        for (auto &x : per) t_only.push_back(x.first);
-        std::sort(t_only.begin(), t_only.end());
-        fprintf(stderr, "   step time median %.1f us p90 %.1f us\n", t_only[t_only.size() / 2] * 1e6,
-                t_only[t_only.size() * 9 / 10] * 1e6);
-      }
+      const double tm = h_trace[4 * ns + 1] > last ? (h_trace[4 * ns + 1] - last) * 1e-9 : 0.0;
+      std::vector<double> sorted = per;
+      std::sort(sorted.begin(), sorted.end());
       fprintf(stderr,
-              "grappolo_b200: iter %d nv=%ld steps=%zu stage1=%.4f hubs=%.4f apply=%.4f "
-              "modularity=%.4f worst step %zu (%.5f s, %ld members, %ld hub chunks)\n",
-              n, (long)L.nv, ns, st1, st23, st4, tm, worst_k, worst,
-              (long)(steps[worst_k].seg[NBINS] - steps[worst_k].seg[0]),
-              (long)(steps[worst_k].hub_chunk[1] - steps[worst_k].hub_chunk[0]));
+              "grappolo_b200: iter %d nv=%ld steps=%zu | mixed %d: stage1 %.4f scan %.4f final "
+              "%.4f apply %.4f | hub-only %d: stage1 %.4f scan %.4f final %.4f apply %.4f | "
+              "modularity %.4f | step median %.1f us p90 %.1f us max %.1f us\n",
+              n, (long)L.nv, ns, cnt[0], acc[0][0], acc[0][1], acc[0][2], acc[0][3], cnt[1],
+              acc[1][0], acc[1][1], acc[1][2], acc[1][3], tm, sorted[ns / 2] * 1e6,
+              sorted[ns * 9 / 10] * 1e6, sorted[ns - 1] * 1e6);
     }
     const double q = h_mod_[0];
     if (debug)
@@ -1754,6 +1730,8 @@ static int device_ready() {
                          kBlockCap * (int)(sizeof(double) + sizeof(int32_t)));
     cudaFuncSetAttribute(k_sweep_iteration, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)kPersistSmem);
+    cudaFuncSetAttribute(k_hub_accum, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         kHubStageCap * (int)(sizeof(double) + sizeof(int32_t)));
     attrs = true;
   }
   return GLV_OK;

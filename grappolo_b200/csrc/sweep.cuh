@@ -206,12 +206,19 @@ __device__ __forceinline__ double warp_accumulate(const SweepArgs &a, int32_t v,
                                                   double *vals, uint32_t mask, bool atomic_add) {
   const int lane = threadIdx.x & 31;
   double self_loop = 0.0;
+  // software pipeline: the next round's entries load while this round's
+  // communities are gathered and folded
+  int32_t t_next = (rb + lane < re) ? a.tail[rb + lane] : -1;
+  double w_next = (rb + lane < re) ? a.w[rb + lane] : 0.0;
   for (int64_t base = rb; base < re; base += stride) {
     const int64_t j = base + lane;
     const bool has = j < re;
-    const int32_t t = has ? a.tail[j] : -1;
-    const double wt = has ? a.w[j] : 0.0;
+    const int32_t t = t_next;
+    const double wt = w_next;
     const int32_t c = has ? a.C[t] : -1;
+    const int64_t jn = j + stride;
+    t_next = (jn < re) ? a.tail[jn] : -1;
+    w_next = (jn < re) ? a.w[jn] : 0.0;
     const uint32_t key = has ? (uint32_t)c : (0x80000000u | lane);
     const unsigned m = __match_any_sync(FULL, key);
     const bool leader = has && (lane == __ffs(m) - 1);
@@ -467,10 +474,47 @@ struct HubWork {
   int32_t *step_big;        // per step: some hub of the step is big (persistent kernel)
 };
 
-constexpr int kHubChunk = 1024;      // CSR entries per accumulation work item
+constexpr int kHubChunk = 2048;      // CSR entries per accumulation work item
 constexpr int kHubSeg = 2048;        // filled slots per scan work item
-constexpr int kHubStageCap = 2048;   // block-local staging table of one chunk
+constexpr int kHubStageCap = 4096;   // block-local staging table of one chunk
 constexpr int kHubInlineCap = 4096;  // filled slots the last chunk's block scans itself
+constexpr int kHubBatch = 4;         // table slots a thread has in flight at once
+static_assert(kHubChunk < kHubStageCap, "a chunk's distinct keys must fit the staging table");
+
+// Best (gain, id) over the filled slots occ[k0..k1) of a hub table; the slots
+// are emptied for the table's next use.  kHubBatch slots per thread are
+// loaded before any is used, so the occ -> key -> cDeg chains overlap.
+__device__ __forceinline__ void hub_scan_slots(const SweepArgs &a, int32_t *keys, double *vals,
+                                               const int32_t *occ, int64_t k0, int64_t k1,
+                                               int32_t own, double eix, double ax, double degree,
+                                               double &g, int32_t &bc) {
+  for (int64_t kb = k0 + threadIdx.x; kb < k1; kb += (int64_t)kHubBatch * blockDim.x) {
+    int32_t s[kHubBatch], c[kHubBatch];
+    double val[kHubBatch], cd[kHubBatch];
+#pragma unroll
+    for (int j = 0; j < kHubBatch; ++j) {
+      const int64_t k = kb + (int64_t)j * blockDim.x;
+      s[j] = (k < k1) ? __ldcg(&occ[k]) : -1;
+    }
+#pragma unroll
+    for (int j = 0; j < kHubBatch; ++j) {
+      c[j] = (s[j] >= 0) ? __ldcg(&keys[s[j]]) : -1;
+      val[j] = (s[j] >= 0) ? __ldcg(&vals[s[j]]) : 0.0;
+    }
+#pragma unroll
+    for (int j = 0; j < kHubBatch; ++j) cd[j] = (c[j] >= 0 && c[j] != own) ? a.cDeg[c[j]] : 0.0;
+#pragma unroll
+    for (int j = 0; j < kHubBatch; ++j) {
+      if (s[j] < 0) continue;
+      if (c[j] != own) {
+        const double gain = louvain_gain(val[j], eix, degree, cd[j], ax, a.constant);
+        if (gain > 0.0 && better(gain, c[j], g, bc)) { g = gain; bc = c[j]; }
+      }
+      keys[s[j]] = -1;
+      vals[s[j]] = 0.0;
+    }
+  }
+}
 
 // All threads of the block call.  The chunk is first folded into a
 // block-local shared table (`skeys`/`svals`, kHubStageCap slots; at most
@@ -498,34 +542,59 @@ __device__ __forceinline__ void hub_accum_chunk(const SweepArgs &a, const HubWor
   double *vals = h.vals + h.tab_off[pos];
   int32_t *occ = h.occ + h.occ_off[pos];
   const int32_t own = a.C[v];
-  for (uint32_t q0 = 0; q0 < kHubStageCap; q0 += blockDim.x) {
-    const uint32_t q = q0 + threadIdx.x;  // blockDim divides kHubStageCap: warp-uniform loop
-    const int32_t c = skeys[q];
-    const double val = svals[q];
-    uint32_t s = 0;
-    bool inserted = false;
-    if (c >= 0) {
-      s = hash_slot(c, mask);
-      while (true) {
-        const int32_t k = keys[s];
-        if (k == c) break;
-        if (k == -1) {
-          const int32_t old = atomicCAS(&keys[s], -1, c);
-          if (old == -1) { inserted = true; break; }
-          if (old == c) break;
-        }
-        s = (s + 1) & mask;
+  // Each thread inserts kHubBatch staged keys at once: the probes of one
+  // round are independent CASes in flight together.
+  for (uint32_t q0 = 0; q0 < kHubStageCap; q0 += kHubBatch * blockDim.x) {
+    // blockDim * kHubBatch divides kHubStageCap: warp-uniform loop
+    int32_t c[kHubBatch];
+    double val[kHubBatch];
+    uint32_t s[kHubBatch];
+    bool pend[kHubBatch], ins[kHubBatch];
+#pragma unroll
+    for (int j = 0; j < kHubBatch; ++j) {
+      const uint32_t q = q0 + j * blockDim.x + threadIdx.x;
+      c[j] = skeys[q];
+      val[j] = svals[q];
+      pend[j] = c[j] >= 0;
+      ins[j] = false;
+      s[j] = pend[j] ? hash_slot(c[j], mask) : 0u;
+    }
+    bool more = pend[0] || pend[1] || pend[2] || pend[3];
+    while (more) {  // per thread; no warp-synchronous work inside
+      int32_t old[kHubBatch];
+#pragma unroll
+      for (int j = 0; j < kHubBatch; ++j) old[j] = pend[j] ? atomicCAS(&keys[s[j]], -1, c[j]) : 0;
+      more = false;
+#pragma unroll
+      for (int j = 0; j < kHubBatch; ++j) {
+        if (!pend[j]) continue;
+        if (old[j] == -1) { ins[j] = true; pend[j] = false; }
+        else if (old[j] == c[j]) pend[j] = false;
+        else { s[j] = (s[j] + 1) & mask; more = true; }
       }
     }
-    // one counter update per warp for the slots it filled
-    const unsigned ins = __ballot_sync(FULL, inserted);
+    // filled-slot list: one counter update per warp
+    int nins = 0;
+#pragma unroll
+    for (int j = 0; j < kHubBatch; ++j) nins += ins[j] ? 1 : 0;
+    int incl = nins;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const int y = __shfl_up_sync(FULL, incl, off);
+      if (lane >= off) incl += y;
+    }
+    const int total = __shfl_sync(FULL, incl, 31);
     int obase = 0;
-    if (lane == __ffs(ins) - 1) obase = atomicAdd(&h.cnt[pos], __popc(ins));
-    obase = __shfl_sync(FULL, obase, ins ? __ffs(ins) - 1 : 0);
-    if (inserted) occ[obase + __popc(ins & ((1u << lane) - 1u))] = (int32_t)s;
-    if (c >= 0) {
-      atomicAdd(&vals[s], val);
-      if (c == own) atomicAdd(&h.own_w[pos], val);
+    if (lane == 31 && total > 0) obase = atomicAdd(&h.cnt[pos], total);
+    obase = __shfl_sync(FULL, obase, 31) + incl - nins;
+#pragma unroll
+    for (int j = 0; j < kHubBatch; ++j)
+      if (ins[j]) occ[obase++] = (int32_t)s[j];
+#pragma unroll
+    for (int j = 0; j < kHubBatch; ++j) {
+      if (c[j] < 0) continue;
+      atomicAdd(&vals[s[j]], val[j]);
+      if (c[j] == own) atomicAdd(&h.own_w[pos], val[j]);
     }
   }
   if (threadIdx.x == 0 && s_self[0] != 0.0) atomicAdd(&h.self_w[pos], s_self[0]);
@@ -567,17 +636,7 @@ __device__ __forceinline__ void hub_accum_chunk(const SweepArgs &a, const HubWor
   const double ax = __dsub_rn(a.cDeg[own], degree);
   double g = 0.0;
   int32_t bc = INT32_MAX;
-  for (int k = threadIdx.x; k < nfill; k += blockDim.x) {
-    const int32_t s = __ldcg(&occ[k]);
-    const int32_t c = __ldcg(&keys[s]);
-    const double val = __ldcg(&vals[s]);
-    if (c != own) {
-      const double gain = louvain_gain(val, eix, degree, a.cDeg[c], ax, a.constant);
-      if (gain > 0.0 && better(gain, c, g, bc)) { g = gain; bc = c; }
-    }
-    keys[s] = -1;
-    vals[s] = 0.0;
-  }
+  hub_scan_slots(a, keys, vals, occ, 0, nfill, own, eix, ax, degree, g, bc);
   warp_argmax(g, bc);
   if (lane == 0) { s_g[warp] = g; s_c[warp] = bc; }
   __syncthreads();
@@ -611,17 +670,7 @@ __device__ __forceinline__ void hub_scan_segment(const SweepArgs &a, const HubWo
   const int64_t oe = min(h.seg_end[si], (int64_t)h.cnt[pos]);
   double g = 0.0;
   int32_t bc = INT32_MAX;
-  for (int64_t k = ob + threadIdx.x; k < oe; k += blockDim.x) {
-    const int32_t s = occ[k];
-    const int32_t c = keys[s];
-    const double val = vals[s];
-    if (c != own) {
-      const double gain = louvain_gain(val, eix, degree, a.cDeg[c], ax, a.constant);
-      if (gain > 0.0 && better(gain, c, g, bc)) { g = gain; bc = c; }
-    }
-    keys[s] = -1;  // leave the table empty for its next use
-    vals[s] = 0.0;
-  }
+  hub_scan_slots(a, keys, vals, occ, ob, oe, own, eix, ax, degree, g, bc);
   warp_argmax(g, bc);
   if (lane == 0) { s_g[warp] = g; s_c[warp] = bc; }
   __syncthreads();

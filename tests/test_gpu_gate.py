@@ -60,13 +60,22 @@ def _trained():
     return p, gate.choose_tau(gate.infer(x, p), y)
 
 
+RUNS = 5  # fast-mode runs differ (atomic order): compare medians
+
+
 def test_learned_gate_gains_over_plain():
-    """Planted power-law graph: the gated run evaluates fewer CSR entries and
-    ends within 1e-3 of the plain run's modularity."""
+    """Planted power-law graph: the gated runs evaluate fewer CSR entries and
+    their median modularity is within 1e-3 of the plain runs' median."""
     p, tau = _trained()
     gate.set_gate(p, tau)
     g = graphs.planted_powerlaw(150000, seed=21)
-    _, plain = louvain.run_multiphase_csr(g, coloring=True, mode=_lib.GLV_MODE_FAST)
-    _, gated = louvain.run_multiphase_csr(g, coloring=True, mode=_lib.GLV_MODE_LEARNED)
-    assert abs(gated['final_modularity'] - plain['final_modularity']) <= 1e-3
-    assert gated['edges_swept'] < 0.9 * plain['edges_swept']
+    plain = [louvain.run_multiphase_csr(g, coloring=True, mode=_lib.GLV_MODE_FAST)[1]
+             for _ in range(RUNS)]
+    gated = [louvain.run_multiphase_csr(g, coloring=True, mode=_lib.GLV_MODE_LEARNED)[1]
+             for _ in range(RUNS)]
+    q_plain = np.median([s['final_modularity'] for s in plain])
+    q_gated = np.median([s['final_modularity'] for s in gated])
+    assert abs(q_gated - q_plain) <= 1e-3
+    e_plain = np.median([s['edges_swept'] for s in plain])
+    e_gated = np.median([s['edges_swept'] for s in gated])
+    assert e_gated < 0.9 * e_plain
