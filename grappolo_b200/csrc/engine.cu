@@ -285,7 +285,7 @@ class Engine {
   int mode_;
   int nsm_ = 148;
   int64_t nv0_ = 0, nnz0_ = 0;
-  BinLimits lim_{127, 2047};
+  BinLimits lim_{127, 4095};
   // schedule buffers
   int32_t *keys_ = nullptr, *keys2_ = nullptr, *members_ = nullptr, *vals_ = nullptr;
   int32_t *move_old_ = nullptr, *move_new_ = nullptr, *hist_ = nullptr;
@@ -380,7 +380,7 @@ int Engine::init(int64_t nv0, int64_t nnz0) {
   CK(cudaMemsetAsync(hub_ownw_, 0, n * sizeof(double), s_));
   if (const char *bm = getenv("GRAPPOLO_B200_BLOCK_MAX")) {
     const int v = atoi(bm);
-    if (v >= lim_.warp_max && v <= 2047) lim_.block_max = v;
+    if (v >= lim_.warp_max && v <= 4095) lim_.block_max = v;
   }
   TRY(alloc(&cst, 4));
   // partials of the modularity pass (one per 256 vertices) and of the

@@ -22,7 +22,7 @@ enum Bin : int {
   BIN_WARP = 4,    // 33..127          : one warp, shared-memory table (<= 256 slots)
   BIN_T128 = 5,    // 128..511         : 128-thread team, shared table (<= 1024 slots)
   BIN_T256 = 6,    // 512..1023        : 256-thread team, shared table (<= 2048 slots)
-  BIN_BLOCK = 7,   // 1024..block_max  : 512-thread block, shared table (<= 4096 slots)
+  BIN_BLOCK = 7,   // 1024..block_max  : 512-thread block, shared table (<= 8192 slots)
   BIN_HUB = 8,     // > block_max      : whole grid per row, global-memory table
   NBINS = 9
 };

@@ -82,7 +82,7 @@ __device__ __forceinline__ uint64_t global_ns() {
   } while (0)
 
 constexpr int kPersistThreads = 512;
-constexpr int kPersistTableCap = 4096;  // BIN_BLOCK rows: degree <= 2047
+constexpr int kPersistTableCap = 8192;  // BIN_BLOCK rows: degree <= 4095
 constexpr int kPersistWarpCap = 256;    // warp-table rows: degree <= 127
 constexpr size_t kPersistSmem = (size_t)kPersistTableCap * (sizeof(double) + sizeof(int32_t));
 static_assert(kPersistSmem >= sizeof(MergeSmem), "merge tiles must fit");
@@ -164,13 +164,13 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
       __syncthreads();
       if (t >= ntask) break;
       if (t < t_hub) {
-        hub_accum_chunk(p.a, p.h, st.hub_chunk[0] + t, reinterpret_cast<int32_t *>(tvals + 4096),
+        hub_accum_chunk(p.a, p.h, st.hub_chunk[0] + t, reinterpret_cast<int32_t *>(tvals + kPersistTableCap),
                         tvals, s_self, s_g, s_c, &s_flag, s);
         continue;
       }
       t -= t_hub;
       if (t < t_blk) {
-        team_vertex<512>(p.a, st.seg[BIN_BLOCK] + t, reinterpret_cast<int32_t *>(tvals + 4096),
+        team_vertex<512>(p.a, st.seg[BIN_BLOCK] + t, reinterpret_cast<int32_t *>(tvals + kPersistTableCap),
                          tvals, 0, s_self, s_g, s_c);
         continue;
       }
@@ -180,7 +180,7 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
         const int team = threadIdx.x / 256;
         const int64_t pos = st.seg[BIN_T256] + 2 * t + team;
         if (pos < st.seg[BIN_T256 + 1])
-          team_vertex<256>(p.a, pos, reinterpret_cast<int32_t *>(tvals + 4096) + team * 2048,
+          team_vertex<256>(p.a, pos, reinterpret_cast<int32_t *>(tvals + kPersistTableCap) + team * 2048,
                            tvals + team * 2048, team, s_self + 8 * team, s_g + 8 * team,
                            s_c + 8 * team);
         continue;
@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
         const int team = threadIdx.x / 128;
         const int64_t pos = st.seg[BIN_T128] + 4 * t + team;
         if (pos < st.seg[BIN_T128 + 1])
-          team_vertex<128>(p.a, pos, reinterpret_cast<int32_t *>(tvals + 4096) + team * 1024,
+          team_vertex<128>(p.a, pos, reinterpret_cast<int32_t *>(tvals + kPersistTableCap) + team * 1024,
                            tvals + team * 1024, team, s_self + 4 * team, s_g + 4 * team,
                            s_c + 4 * team);
         continue;

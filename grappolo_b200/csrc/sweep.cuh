@@ -206,19 +206,27 @@ __device__ __forceinline__ double warp_accumulate(const SweepArgs &a, int32_t v,
                                                   double *vals, uint32_t mask, bool atomic_add) {
   const int lane = threadIdx.x & 31;
   double self_loop = 0.0;
-  // software pipeline: the next round's entries load while this round's
-  // communities are gathered and folded
-  int32_t t_next = (rb + lane < re) ? a.tail[rb + lane] : -1;
-  double w_next = (rb + lane < re) ? a.w[rb + lane] : 0.0;
+  // Software pipeline, two rounds deep: while this round is folded, the next
+  // round's communities are gathered and the round after's entries load.
+  // Neighbours' communities do not change during the sweep of one step.
+  const int64_t j0 = rb + lane, j1 = j0 + stride;
+  int32_t t_cur = (j0 < re) ? a.tail[j0] : -1;
+  double w_cur = (j0 < re) ? a.w[j0] : 0.0;
+  int32_t t_next = (j1 < re) ? a.tail[j1] : -1;
+  double w_next = (j1 < re) ? a.w[j1] : 0.0;
+  int32_t c_cur = (j0 < re) ? a.C[t_cur] : -1;
   for (int64_t base = rb; base < re; base += stride) {
     const int64_t j = base + lane;
     const bool has = j < re;
-    const int32_t t = t_next;
-    const double wt = w_next;
-    const int32_t c = has ? a.C[t] : -1;
-    const int64_t jn = j + stride;
-    t_next = (jn < re) ? a.tail[jn] : -1;
-    w_next = (jn < re) ? a.w[jn] : 0.0;
+    const int32_t t = t_cur;
+    const double wt = w_cur;
+    const int32_t c = c_cur;
+    const int64_t jn = j + stride, jnn = j + 2 * stride;
+    c_cur = (jn < re) ? a.C[t_next] : -1;
+    t_cur = t_next;
+    w_cur = w_next;
+    t_next = (jnn < re) ? a.tail[jnn] : -1;
+    w_next = (jnn < re) ? a.w[jnn] : 0.0;
     const uint32_t key = has ? (uint32_t)c : (0x80000000u | lane);
     const unsigned m = __match_any_sync(FULL, key);
     const bool leader = has && (lane == __ffs(m) - 1);
@@ -255,11 +263,23 @@ __device__ __forceinline__ void scan_table(const SweepArgs &a, const int32_t *ke
                                            const double *vals, uint32_t first, uint32_t cap,
                                            uint32_t stride, int32_t own, double eix, double ax,
                                            double degree, double &g, int32_t &bc) {
-  for (uint32_t s = first; s < cap; s += stride) {
-    const int32_t k = keys[s];
-    if (k >= 0 && k != own) {
-      const double gain = louvain_gain(vals[s], eix, degree, a.cDeg[k], ax, a.constant);
-      if (gain > 0.0 && better(gain, k, g, bc)) { g = gain; bc = k; }
+  // four slots per thread in flight: their cDeg gathers overlap
+  for (uint32_t s0 = first; s0 < cap; s0 += 4 * stride) {
+    int32_t k[4];
+    double cd[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const uint32_t s = s0 + q * stride;
+      k[q] = (s < cap) ? keys[s] : -1;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) cd[q] = (k[q] >= 0 && k[q] != own) ? a.cDeg[k[q]] : 0.0;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      if (k[q] < 0 || k[q] == own) continue;
+      const double gain =
+          louvain_gain(vals[s0 + q * stride], eix, degree, cd[q], ax, a.constant);
+      if (gain > 0.0 && better(gain, k[q], g, bc)) { g = gain; bc = k[q]; }
     }
   }
 }

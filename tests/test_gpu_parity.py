@@ -180,3 +180,51 @@ def test_modularity_matches_oracle(oracle):
         g, z = load(name)
         q = louvain.modularity(g, z['mpc_C'])
         assert q == pytest.approx(oracle.modularity(g, z['mpc_C']), rel=MOD_REL_TOL, abs=1e-15)
+
+
+def _with_hubs(seed=4, num_blocks=200):
+    """Planted partition (blocks of 50) plus three hubs of degree 5000, 4100
+    and 3000, non-integral weights: rows above every shared-memory bin."""
+    base = graphs.planted_partition(num_blocks=num_blocks, block_size=50, seed=seed)
+    rng = np.random.default_rng(seed)
+    nv = base.num_vertices + 3
+    heads = base.heads()
+    keep = heads < base.tail
+    u = [heads[keep]]
+    v = [base.tail[keep]]
+    for k, deg in enumerate((5000, 4100, 3000)):
+        hub = base.num_vertices + k
+        nb = rng.choice(base.num_vertices, deg, replace=False)
+        u.append(np.full(deg, hub))
+        v.append(nb)
+    u = np.concatenate(u)
+    v = np.concatenate(v)
+    w = rng.uniform(0.05, 1.0, u.size)
+    return graphs.csr_from_undirected(nv, u, v, w)
+
+
+@pytest.mark.parametrize('block_max', [None, '128'])
+def test_hub_rows_verify_vs_oracle(block_max, oracle, monkeypatch):
+    """Hub rows (global tables, chunked accumulation, segment scans) give the
+    reference's one-thread results; block_max 128 sends every row above 128
+    entries through the hub path."""
+    if block_max:
+        monkeypatch.setenv('GRAPPOLO_B200_BLOCK_MAX', block_max)
+    g = _with_hubs()
+    C, st = louvain.runMultiPhaseColoring(g, numThreads=1, stats=True)
+    Co, so, recs = oracle.run_multiphase_coloring(g)
+    assert np.array_equal(C, Co)
+    assert st['total_iterations'] == so['total_iterations']
+    g2 = graphs.rmat(14, seed=9)
+    C2 = louvain.runMultiPhaseColoring(g2, numThreads=1)
+    assert np.array_equal(C2, oracle.run_multiphase_coloring(g2)[0])
+
+
+@pytest.mark.parametrize('block_max', [None, '128'])
+def test_hub_rows_fast_mode(block_max, oracle, monkeypatch):
+    if block_max:
+        monkeypatch.setenv('GRAPPOLO_B200_BLOCK_MAX', block_max)
+    g = _with_hubs(seed=5, num_blocks=2000)  # 100k vertices: run-to-run spread well below 1e-3
+    _, st = louvain.runMultiPhaseColoring(g, numThreads=8, stats=True)
+    _, so, _ = oracle.run_multiphase_coloring(g)
+    assert abs(st['final_modularity'] - so['final_mod']) <= FAST_Q_TOL
