@@ -64,6 +64,16 @@ class GlvRunStats(ct.Structure):
         return d
 
 
+class GlvBatchStats(ct.Structure):
+    _fields_ = [('final_modularity', ct.POINTER(ct.c_double)), ('phases', ct.POINTER(ct.c_int)),
+                ('iterations', ct.POINTER(ct.c_int)), ('clusters', ct.POINTER(ct.c_long)),
+                ('done_seconds', ct.POINTER(ct.c_double)), ('rounds', ct.c_int),
+                ('time_total', ct.c_double), ('time_clustering', ct.c_double),
+                ('time_coloring', ct.c_double), ('time_building', ct.c_double),
+                ('time_transfer', ct.c_double), ('edges_swept', ct.c_double),
+                ('kernel_launches', ct.c_long)]
+
+
 class GrappoloError(RuntimeError):
     def __init__(self, code: int, msg: str):
         super().__init__(f'grappolo_b200 error {code} ({ERRORS.get(code, "?")}): {msg}')
@@ -92,7 +102,7 @@ def lib():
                  'glv_renumber_clusters', 'glv_build_next_level', 'glv_modularity',
                  'glv_decide_batch', 'glv_dev_modularity_static', 'glv_gate_set',
                  'glv_gate_infer', 'glv_gate_grad', 'glv_gate_train', 'glv_trace_begin',
-                 'glv_trace_end'):
+                 'glv_trace_end', 'glv_run_batch_csr', 'glv_dev_run_batch'):
         getattr(L, name).restype = ct.c_int
     L.glv_run_multiphase_coloring.argtypes = [P(GlvGraph), P(ct.c_long), ct.c_int, ct.c_int,
                                               ct.c_int, ct.c_long, ct.c_double, ct.c_double,
@@ -127,6 +137,12 @@ def lib():
     L.glv_dev_modularity_static.argtypes = [ct.c_long, ct.c_void_p, ct.c_void_p, ct.c_void_p,
                                             ct.c_void_p, ct.c_void_p, ct.c_double, ct.c_void_p,
                                             ct.c_void_p]
+    L.glv_run_batch_csr.argtypes = [ct.c_int, P(ct.c_long), P(ct.c_long), P(ct.c_long),
+                                    P(ct.c_double), P(ct.c_long), ct.c_int, ct.c_long,
+                                    ct.c_double, ct.c_double, ct.c_int, P(GlvBatchStats)]
+    L.glv_dev_run_batch.argtypes = [ct.c_int, P(ct.c_long), ct.c_void_p, ct.c_void_p,
+                                    ct.c_void_p, ct.c_void_p, ct.c_int, ct.c_long, ct.c_double,
+                                    ct.c_double, ct.c_int, ct.c_void_p, P(GlvBatchStats)]
     fp = P(ct.c_float)
     L.glv_gate_set.argtypes = [fp, ct.c_float]
     L.glv_gate_infer.argtypes = [ct.c_long, ct.c_void_p, ct.c_void_p, ct.c_void_p]

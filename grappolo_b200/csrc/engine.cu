@@ -13,6 +13,7 @@
 
 #include <cub/cub.cuh>
 
+#include "batch_kernels.cuh"
 #include "gate.cuh"
 #include "persist.cuh"
 #include "phase_kernels.cuh"
@@ -176,6 +177,33 @@ struct Probes {
   }
 };
 
+// Per-graph control of a batch level (batch.cuh).  Graph g's vertices at the
+// current level are [voff[g], voff[g+1]) (empty once its run has finished).
+struct Batch {
+  int G = 0;
+  std::vector<int64_t> voff;   // level vertex offsets
+  std::vector<int64_t> gnnz;   // CSR entries per graph at this level
+  int32_t *gid = nullptr;      // device: graph of each level vertex
+  double *gcst = nullptr;      // device: per-graph 1/(2m)
+  double *gsum = nullptr;      // device: per-graph degree sums
+  double *gacc = nullptr;      // device: per-graph {e_xx, a2_x}
+  uint8_t *act = nullptr;      // device: graph still sweeping in this phase
+  std::vector<uint8_t> h_act, in_phase, stale;
+  std::vector<double> h_gcst, h_acc, lower, mod, done_s;
+  std::vector<int> itr;
+  double thresh = 0;
+};
+
+// Per-graph results of a batch run (caller-owned arrays of G entries).
+struct BatchResult {
+  double *final_modularity;
+  int *phases;
+  int *iterations;
+  long *clusters;
+  double *done_s;
+  int rounds;
+};
+
 class Engine {
  public:
   explicit Engine(cudaStream_t s, int mode) : s_(s), mode_(mode) {}
@@ -193,7 +221,13 @@ class Engine {
   int decide(const Level &L, const int32_t *verts, int64_t nverts);
   int run_multiphase(const Level &L0, int32_t *d_C_orig, bool coloring, long min_graph_size,
                      double threshold, double c_threshold, glv_run_stats *st);
+  int run_multiphase_batch(const Level &L0, const std::vector<int64_t> &voff0,
+                           int32_t *d_C_orig, bool coloring, long min_graph_size,
+                           double threshold, double c_threshold, BatchResult *res);
+  int batch_level(Batch &b, const Level &L, const std::vector<int64_t> &voff);
+  int sublevels_batch(const Level &L, const Batch &b, int32_t **d_sub, int *nsub);
   void free_level(Level &L);
+  Batch *bt_ = nullptr;  // set while a batch runs
 
   // state buffers (device)
   double *vDeg = nullptr, *cDeg = nullptr, *dDeg = nullptr, *own_w = nullptr;
@@ -459,6 +493,17 @@ int Engine::phase_init(const Level &L, bool need_past) {
     LAUNCH(k_sum_partials, kConstParts, 256, 0, s_, L.nv, vDeg, part_e_);
     LAUNCH(k_constant_from_partials, 1, 32, 0, s_, kConstParts, part_e_, cst);
   }
+  if (bt_) {
+    // one constant per graph
+    CK(cudaMemsetAsync(bt_->gsum, 0, bt_->G * sizeof(double), s_));
+    LAUNCH(k_graph_degsum, grid_for(L.nv, 256, nsm_ * 8), 256, 0, s_, L.nv, bt_->gid, vDeg,
+           bt_->gsum);
+    LAUNCH(k_graph_cst, grid_for(bt_->G, 256, nsm_ * 4), 256, 0, s_, bt_->G, bt_->gsum,
+           bt_->gcst);
+    CK(cudaMemcpyAsync(bt_->h_gcst.data(), bt_->gcst, bt_->G * sizeof(double),
+                       cudaMemcpyDeviceToHost, s_));
+    CK(cudaStreamSynchronize(s_));
+  }
   return GLV_OK;
 }
 
@@ -469,7 +514,13 @@ int Engine::color(const Level &L, int *ncolors, double *secs) {
     *ncolors = 0;
     return GLV_OK;
   }
-  TRY(mode_ != GLV_MODE_VERIFY ? color_spec(L, ncolors) : color_jp(L, ncolors));
+  // GRAPPOLO_B200_COLORING=jp|spec overrides the mode's colouring (jp: the
+  // deterministic id-priority colouring of verify mode)
+  const char *cm = getenv("GRAPPOLO_B200_COLORING");
+  bool spec = mode_ != GLV_MODE_VERIFY;
+  if (cm && !strcmp(cm, "jp")) spec = false;
+  if (cm && !strcmp(cm, "spec")) spec = true;
+  TRY(spec ? color_spec(L, ncolors) : color_jp(L, ncolors));
   if (secs) *secs = now_s() - t0;
   return GLV_OK;
 }
@@ -937,7 +988,10 @@ int Engine::coloring_phase(const Level &L, int ncolors, bool stale, double lower
   TRY(phase_init(L, false));
   int32_t *d_sub = nullptr;
   int nsub = 1;
-  if (stale) TRY(sublevels(L, ncolors, &d_sub, &nsub));
+  if (stale) {
+    if (bt_) TRY(sublevels_batch(L, *bt_, &d_sub, &nsub));
+    else TRY(sublevels(L, ncolors, &d_sub, &nsub));
+  }
   if (debug) { cudaStreamSynchronize(s_); fprintf(stderr, "grappolo_b200: phase init %.4f s\n", now_s() - td); td = now_s(); }
   std::vector<ClassSched> sched;
   TRY(build_schedule(L, color_, ncolors, d_sub, nsub, &sched));
@@ -1198,13 +1252,19 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
   dfree(step_big_);
   TRY(alloc(&step_big_, steps.size()));
   TRY(upload(s_, d_steps, steps));
-  int64_t *d_cls_b = nullptr, *d_cls_e = nullptr;
+  int64_t *d_cls_b = nullptr;
   int32_t *d_kept = nullptr;
   const int nclass = (int)cls_b.size();
-  if (!jacobi && learned()) {
-    TRY(alloc(&d_cls_b, nclass)); TRY(alloc(&d_cls_e, nclass)); TRY(alloc(&d_kept, nclass));
+  const int64_t nmem = cls_e.empty() ? 0 : cls_e.back();
+  Batch *bt = bt_;
+  if ((!jacobi && learned()) || bt) {
+    TRY(alloc(&d_cls_b, nclass)); TRY(alloc(&d_kept, nclass));
     TRY(upload(s_, d_cls_b, cls_b));
-    TRY(upload(s_, d_cls_e, cls_e));
+  }
+  if (bt) {
+    if (!skip_) TRY(alloc(&skip_, nv0_ + 1));
+    a.gid = bt->gid;
+    a.gcst = bt->gcst;
   }
   IterArgs p{};
   p.a = a;
@@ -1224,6 +1284,10 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
   p.task_ctr = d_ctr;
   p.nnz = L.nnz;
   p.split_row = split_row_;
+  if (bt) {
+    p.gid = bt->gid;
+    p.gacc = bt->gacc;
+  }
   int per_sm = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_iteration, kPersistThreads,
                                                    kPersistSmem));
@@ -1249,8 +1313,19 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
   int n = 0;
   int rc = GLV_OK;
   // learned gate / trace capture (colour phases only)
-  const bool tracing = !jacobi && g_trace.on;
-  const bool gating = !jacobi && learned();
+  const bool tracing = !jacobi && g_trace.on && !bt;
+  const bool gating = !jacobi && learned() && !bt;
+  std::vector<double> bprev;
+  if (bt) {
+    bprev.assign(bt->G, 0.0);
+    for (int g = 0; g < bt->G; ++g) {
+      bt->h_act[g] = bt->in_phase[g];
+      bprev[g] = jacobi ? -1.0 : bt->lower[g];
+      bt->mod[g] = bprev[g];
+      bt->itr[g] = 0;
+    }
+    CK(cudaMemcpyAsync(bt->act, bt->h_act.data(), bt->G, cudaMemcpyHostToDevice, s_));
+  }
   if (gating || tracing) {
     TRY(gate_init());
     CK(cudaMemsetAsync(last_move_, 0, L.nv * sizeof(int32_t), s_));
@@ -1281,11 +1356,26 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
         CK(cudaMemsetAsync(evald_, 0, sizeof(unsigned long long), s_));
         LAUNCH(k_gate_infer, std::max(1, (int)std::min<int64_t>((L.nv + 127) / 128, nsm_ * 8)), 256, 0,
                s_, L.nv, feat_, gate_p_, tau, L.ptr, (float *)nullptr, skip_, evald_);
-        LAUNCH(k_class_kept, std::max(1, std::min(nclass, nsm_ * 4)), 256, 0, s_, nclass, d_cls_b,
-               d_cls_e, members_, skip_, d_kept);
+        CK(cudaMemsetAsync(d_kept, 0, nclass * sizeof(int32_t), s_));
+        LAUNCH(k_class_kept, grid_for(nmem, 256, nsm_ * 8), 256, 0, s_, nclass, d_cls_b, nmem,
+               members_, skip_, d_kept);
         p.a.skip = skip_;
       }
       p.class_kept = gated_now ? d_kept : nullptr;
+    }
+    double batch_edges = 0;
+    if (bt) {
+      // graphs that have converged (or sit out this phase) are skipped whole
+      LAUNCH(k_graph_skip, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, bt->gid, bt->act,
+             skip_);
+      CK(cudaMemsetAsync(d_kept, 0, nclass * sizeof(int32_t), s_));
+      LAUNCH(k_class_kept, grid_for(nmem, 256, nsm_ * 8), 256, 0, s_, nclass, d_cls_b, nmem,
+             members_, skip_, d_kept);
+      CK(cudaMemsetAsync(bt->gacc, 0, 2 * bt->G * sizeof(double), s_));
+      p.a.skip = skip_;
+      p.class_kept = d_kept;
+      for (int g = 0; g < bt->G; ++g)
+        if (bt->h_act[g]) batch_edges += (double)bt->gnnz[g];
     }
     cudaError_t e = cudaMemsetAsync(d_ctr, 0, steps.size() * sizeof(int64_t), s_);
     if (e == cudaSuccess) e = cudaMemsetAsync(step_big_, 0, steps.size() * sizeof(int32_t), s_);
@@ -1300,7 +1390,9 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
     t_sweep += now_s() - t0;
     if (e != cudaSuccess) { g_err = cudaGetErrorString(e); rc = GLV_ERR_CUDA; break; }
     ++launches_;
-    if (gated_now) {
+    if (bt) {
+      edges_swept += batch_edges;
+    } else if (gated_now) {
       unsigned long long ev = 0;
       CK(cudaMemcpy(&ev, evald_, sizeof(ev), cudaMemcpyDeviceToHost));
       edges_swept += (double)ev;
@@ -1357,6 +1449,34 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
               acc[1][0], acc[1][1], acc[1][2], acc[1][3], tm, sorted[ns / 2] * 1e6,
               sorted[ns * 9 / 10] * 1e6, sorted[ns - 1] * 1e6);
     }
+    if (bt) {
+      // per-graph Q = e*c - a*c*c and the phase loop's test, graph by graph
+      CK(cudaMemcpyAsync(bt->h_acc.data(), bt->gacc, 2 * bt->G * sizeof(double),
+                         cudaMemcpyDeviceToHost, s_));
+      CK(cudaStreamSynchronize(s_));
+      bool any = false;
+      for (int g = 0; g < bt->G; ++g) {
+        if (!bt->h_act[g]) continue;
+        const double c = bt->h_gcst[g];
+        const double qg = bt->h_acc[2 * g] * c - bt->h_acc[2 * g + 1] * c * c;
+        bt->itr[g] = n;
+        if (!(qg - bprev[g] >= bt->thresh)) {  // NaN (no edges) ends the graph too
+          bt->h_act[g] = 0;
+          bt->mod[g] = bprev[g];
+          bt->done_s[g] = now_s();
+        } else {
+          bprev[g] = qg;
+          if (jacobi && bprev[g] < bt->lower[g]) bprev[g] = bt->lower[g];
+          any = true;
+        }
+      }
+      if (!any) break;
+      CK(cudaMemcpyAsync(bt->act, bt->h_act.data(), bt->G, cudaMemcpyHostToDevice, s_));
+      if (jacobi)
+        LAUNCH(k_rotate_active, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, bt->gid,
+               bt->act, Cpast, C, Ctgt);
+      continue;
+    }
     const double q = h_mod_[0];
     if (debug)
       fprintf(stderr, "grappolo_b200: iter %d gated %d q %.9f gain %.3e edges %.0f time %.5f\n", n,
@@ -1378,7 +1498,6 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
   dfree(d_trace);
   dfree(d_ctr);
   dfree(d_cls_b);
-  dfree(d_cls_e);
   dfree(d_kept);
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
@@ -1661,6 +1780,8 @@ int Engine::run_multiphase(const Level &L0, int32_t *d_C_orig, bool coloring,
   }
   return GLV_OK;
 }
+
+#include "batch.cuh"
 
 }  // namespace glv
 
@@ -1950,6 +2071,145 @@ int glv_dev_run_multiphase(long nv, const long *d_ptr, const int *d_tail, const 
   TRY(c.eng->upload_check(c.L0));
   TRY(c.eng->run_multiphase(c.L0, d_C_orig, coloring != 0, minGraphSize, threshold, C_threshold,
                             stats));
+  CK(cudaStreamSynchronize(c.s));
+  if (stats) {
+    stats->kernel_launches = c.launches + c.eng->launches_;
+    stats->time_total = now_s() - t0;
+  }
+  return GLV_OK;
+}
+
+// Batches: graph g owns vertices [vertex_offsets[g], vertex_offsets[g+1]) of
+// one CSR whose tails are global vertex ids inside the row's own graph.
+static int check_offsets(int G, const long *voff, long nv) {
+  if (G < 1) return fail(GLV_ERR_ARG, "num_graphs < 1");
+  if (!voff) return fail(GLV_ERR_ARG, "vertex_offsets is NULL");
+  if (voff[0] != 0 || voff[G] != nv) return fail(GLV_ERR_ARG, "vertex_offsets must span [0, nv]");
+  for (int g = 0; g < G; ++g)
+    if (voff[g + 1] <= voff[g]) return fail(GLV_ERR_ARG, "every graph needs a vertex");
+  return GLV_OK;
+}
+
+static int run_batch(Call &c, int G, const long *voff, int32_t *dC, bool coloring,
+                     long min_graph_size, double threshold, double C_threshold,
+                     glv_batch_stats *st) {
+  const int64_t nv = c.L0.nv;
+  std::vector<int64_t> off(voff, voff + G + 1);
+  // every tail inside its row's graph
+  int32_t *gid, *bad;
+  int64_t *d_off;
+  CK(cudaMallocFromPoolAsync((void **)&gid, nv * sizeof(int32_t), engine_pool(), c.s));
+  CK(cudaMallocFromPoolAsync((void **)&bad, sizeof(int32_t), engine_pool(), c.s));
+  CK(cudaMallocFromPoolAsync((void **)&d_off, (G + 1) * sizeof(int64_t), engine_pool(), c.s));
+  CK(cudaMemsetAsync(bad, 0, sizeof(int32_t), c.s));
+  CK(cudaMemcpyAsync(d_off, off.data(), (G + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c.s));
+  k_fill_gid<<<std::max(1, std::min(G, 148 * 16)), 256, 0, c.s>>>(G, d_off, gid);
+  k_check_batch_tails<<<grid_for(nv, 256, 148 * 16), 256, 0, c.s>>>(nv, c.L0.ptr, c.L0.tail, gid,
+                                                                      d_off, bad);
+  c.launches += 2;
+  CK(cudaGetLastError());
+  int32_t hb = 0;
+  CK(cudaMemcpyAsync(&hb, bad, sizeof(int32_t), cudaMemcpyDeviceToHost, c.s));
+  CK(cudaFreeAsync(gid, c.s));
+  CK(cudaFreeAsync(bad, c.s));
+  CK(cudaFreeAsync(d_off, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  if (hb) return fail(GLV_ERR_ARG, "an edge joins two graphs of the batch");
+  std::vector<double> fm(G), ds(G);
+  std::vector<int> ph(G), it(G);
+  std::vector<long> cl(G);
+  BatchResult r{fm.data(), ph.data(), it.data(), cl.data(), ds.data(), 0};
+  TRY(c.eng->run_multiphase_batch(c.L0, off, dC, coloring, min_graph_size, threshold,
+                                  C_threshold, &r));
+  if (st) {
+    for (int g = 0; g < G; ++g) {
+      if (st->final_modularity) st->final_modularity[g] = fm[g];
+      if (st->phases) st->phases[g] = ph[g];
+      if (st->iterations) st->iterations[g] = it[g];
+      if (st->clusters) st->clusters[g] = cl[g];
+      if (st->done_seconds) st->done_seconds[g] = ds[g];
+    }
+    st->rounds = r.rounds;
+    st->time_clustering = c.eng->t_sweep;
+    st->time_coloring = c.eng->t_color;
+    st->time_building = c.eng->t_coarsen;
+    st->edges_swept = c.eng->edges_swept;
+  }
+  return GLV_OK;
+}
+
+static void clear_batch_stats(glv_batch_stats *st) {
+  if (!st) return;
+  st->rounds = 0;
+  st->time_total = st->time_clustering = st->time_coloring = st->time_building = 0;
+  st->time_transfer = st->edges_swept = 0;
+  st->kernel_launches = 0;
+}
+
+int glv_run_batch_csr(int num_graphs, const long *vertex_offsets, const long *ptr,
+                      const long *tail, const double *weight, long *C_out, int coloring,
+                      long minGraphSize, double threshold, double C_threshold, int mode,
+                      glv_batch_stats *stats) {
+  const double t0 = now_s();
+  clear_batch_stats(stats);
+  if (!vertex_offsets || num_graphs < 1) return fail(GLV_ERR_ARG, "no graphs");
+  const long nv = vertex_offsets[num_graphs];
+  TRY(check_offsets(num_graphs, vertex_offsets, nv));
+  if (!C_out) return fail(GLV_ERR_ARG, "C_out is NULL");
+  if (mode < GLV_MODE_VERIFY || mode > GLV_MODE_FAST) return fail(GLV_ERR_ARG, "bad mode");
+  Call c;
+  TRY(open_call(c, mode, nv, ptr, nullptr, tail, weight));
+  int32_t *dC;
+  CK(cudaMallocFromPoolAsync((void **)&dC, nv * sizeof(int32_t), engine_pool(), c.s));
+  TRY(run_batch(c, num_graphs, vertex_offsets, dC, coloring != 0, minGraphSize, threshold,
+                C_threshold, stats));
+  TRY(download_ids(c, dC, nv, C_out));
+  CK(cudaFreeAsync(dC, c.s));
+  if (stats) {
+    stats->time_transfer = c.t_transfer;
+    stats->kernel_launches = c.launches + c.eng->launches_;
+    stats->time_total = now_s() - t0;
+  }
+  return GLV_OK;
+}
+
+int glv_dev_run_batch(int num_graphs, const long *vertex_offsets, const long *d_ptr,
+                      const int *d_tail, const double *d_weight, int *d_C, int coloring,
+                      long minGraphSize, double threshold, double C_threshold, int mode,
+                      void *stream, glv_batch_stats *stats) {
+  const double t0 = now_s();
+  clear_batch_stats(stats);
+  TRY(device_ready());
+  if (!vertex_offsets || num_graphs < 1) return fail(GLV_ERR_ARG, "no graphs");
+  const long nv = vertex_offsets[num_graphs];
+  TRY(check_offsets(num_graphs, vertex_offsets, nv));
+  if (nv >= (1L << 31) - 1) return fail(GLV_ERR_TOO_LARGE, "nv >= 2^31");
+  if (mode < GLV_MODE_VERIFY || mode > GLV_MODE_FAST) return fail(GLV_ERR_ARG, "bad mode");
+  Call c;
+  CK(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
+  if (stream) {
+    cudaEvent_t ev;
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    CK(cudaEventRecord(ev, (cudaStream_t)stream));
+    CK(cudaStreamWaitEvent(c.s, ev, 0));
+    cudaEventDestroy(ev);
+  } else {
+    CK(cudaStreamSynchronize(0));
+  }
+  int64_t nnz = 0;
+  CK(cudaMemcpyAsync(&nnz, d_ptr + nv, sizeof(int64_t), cudaMemcpyDeviceToHost, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  c.eng = new Engine(c.s, mode);
+  TRY(c.eng->init(nv, nnz));
+  c.L0.nv = nv;
+  c.L0.nnz = nnz;
+  c.L0.ptr = (int64_t *)d_ptr;
+  c.L0.tail = (int32_t *)d_tail;
+  c.L0.w = (double *)d_weight;
+  c.L0.owned = false;
+  TRY(c.eng->upload_check(c.L0));
+  TRY(run_batch(c, num_graphs, vertex_offsets, d_C, coloring != 0, minGraphSize, threshold,
+                C_threshold, stats));
   CK(cudaStreamSynchronize(c.s));
   if (stats) {
     stats->kernel_launches = c.launches + c.eng->launches_;

@@ -51,22 +51,25 @@ struct IterArgs {
   const int32_t *class_kept;  // gated sweeps: vertices the gate kept per class (NULL = all)
   int64_t nnz;
   const int64_t *split_row;   // merge-path tile boundaries of the level
+  // batches of graphs: per-graph modularity sums instead of one Q
+  const int32_t *gid;
+  double *gacc;
 };
 
-// Gated sweeps: how many vertices of each colour class the gate kept.
-__global__ void k_class_kept(int nclass, const int64_t *cls_begin, const int64_t *cls_end,
+// Gated or batched sweeps: kept[c] = 1 when some member of colour class c is
+// evaluated (kept must be zero on entry).  Member positions are strided over
+// the grid; a position's class is found by binary search in cls_begin.
+__global__ void k_class_kept(int nclass, const int64_t *cls_begin, int64_t nmem,
                              const int32_t *members, const uint8_t *skip, int32_t *kept) {
-  __shared__ int s_cnt;
-  for (int c = blockIdx.x; c < nclass; c += gridDim.x) {
-    if (threadIdx.x == 0) s_cnt = 0;
-    __syncthreads();
-    int local = 0;
-    for (int64_t pos = cls_begin[c] + threadIdx.x; pos < cls_end[c]; pos += blockDim.x)
-      local += skip[members[pos]] ? 0 : 1;
-    if (local) atomicAdd(&s_cnt, local);
-    __syncthreads();
-    if (threadIdx.x == 0) kept[c] = s_cnt;
-    __syncthreads();
+  for (int64_t pos = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; pos < nmem;
+       pos += (int64_t)gridDim.x * blockDim.x) {
+    if (skip[members[pos]]) continue;
+    int lo = 0, hi = nclass - 1;  // last class starting at or before pos
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (cls_begin[mid] <= pos) lo = mid; else hi = mid - 1;
+    }
+    if (kept[lo] == 0) kept[lo] = 1;
   }
 }
 
@@ -234,16 +237,29 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
     const int64_t ntiles = merge_tiles(p.nv, p.nnz);
     MergeSmem *msm = reinterpret_cast<MergeSmem *>(smem_raw);
     __syncthreads();  // stage-1 tables in the same shared memory are done
-    for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
-      modularity_merge_tile<kPersistThreads>(tile, p.nv, p.nnz, p.a.ptr, p.a.tail, p.a.w, p.C_mod,
-                                             p.own_w_mod, p.cDeg, p.split_row, msm, ex, a2);
+    if (p.gid) {
+      // contiguous tile ranges, so a thread's running pair changes graph rarely
+      GraphAcc acc;
+      const int64_t tb = ntiles * blockIdx.x / gridDim.x;
+      const int64_t te = ntiles * (blockIdx.x + 1) / gridDim.x;
+      for (int64_t tile = tb; tile < te; ++tile)
+        modularity_merge_tile_graphs<kPersistThreads>(tile, p.nv, p.nnz, p.a.ptr, p.a.tail, p.a.w,
+                                                      p.C_mod, p.own_w_mod, p.cDeg, p.split_row,
+                                                      p.gid, p.gacc, msm, acc);
+      graph_acc_flush(acc, p.gacc);
+    } else {
+      for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+        modularity_merge_tile<kPersistThreads>(tile, p.nv, p.nnz, p.a.ptr, p.a.tail, p.a.w,
+                                               p.C_mod, p.own_w_mod, p.cDeg, p.split_row, msm, ex,
+                                               a2);
+    }
     ex = block_sum<kPersistThreads>(ex, sh);
     a2 = block_sum<kPersistThreads>(a2, sh);
     if (threadIdx.x == 0) { p.part_e[blockIdx.x] = ex; p.part_a[blockIdx.x] = a2; }
   }
   grid.sync();
   GLV_TRACE(4 * p.nsteps + 1);
-  if (blockIdx.x == 0) modularity_fold(p, gridDim.x, sh);
+  if (blockIdx.x == 0 && !p.gid) modularity_fold(p, gridDim.x, sh);
   if (p.jacobi && p.nsteps > 0) {
     // Q above used the totals before the moves; now take the moves' deltas.
     apply_deltas_range(p, p.steps[0].apply[0], p.steps[p.nsteps - 1].apply[1], gt, ngt);

@@ -215,6 +215,69 @@ __device__ __forceinline__ void modularity_merge_tile(int64_t tile, int64_t nv, 
   }
 }
 
+// Batches of graphs: per-graph modularity sums {e_xx, a2_x} in gacc[2g],
+// gacc[2g + 1].  A thread keeps one running pair and adds it to its graph's
+// slots when the graph changes, so a contiguous tile range costs a few atomics
+// per thread.
+struct GraphAcc {
+  int32_t g = -1;
+  double e = 0.0, a = 0.0;
+};
+
+__device__ __forceinline__ void graph_acc_flush(GraphAcc &acc, double *gacc) {
+  if (acc.g >= 0) {
+    if (acc.e != 0.0) atomicAdd(&gacc[2 * acc.g], acc.e);
+    if (acc.a != 0.0) atomicAdd(&gacc[2 * acc.g + 1], acc.a);
+  }
+  acc.e = 0.0;
+  acc.a = 0.0;
+}
+
+__device__ __forceinline__ void graph_acc_add(GraphAcc &acc, int32_t g, double e, double a,
+                                              double *gacc) {
+  if (g != acc.g) {
+    graph_acc_flush(acc, gacc);
+    acc.g = g;
+  }
+  acc.e = __dadd_rn(acc.e, e);
+  acc.a = __dadd_rn(acc.a, a);
+}
+
+template <int NT>
+__device__ __forceinline__ void modularity_merge_tile_graphs(
+    int64_t tile, int64_t nv, int64_t nnz, const int64_t *ptr, const int32_t *tail,
+    const double *w, const int32_t *C, const double *own_w, const double *cDeg,
+    const int64_t *split_row, const int32_t *gid, double *gacc, MergeSmem *sm, GraphAcc &acc) {
+  const int64_t d0 = tile * (int64_t)kMergeTile;
+  const int64_t d1 = min(d0 + (int64_t)kMergeTile, nv + nnz);
+  const int64_t i0 = split_row[tile], i1 = split_row[tile + 1];
+  const int64_t j0 = d0 - i0, j1 = d1 - i1;
+  for (int64_t i = i0 + threadIdx.x; i < i1; i += NT) {
+    const double dg = cDeg[i];
+    graph_acc_add(acc, gid[i], own_w ? own_w[i] : 0.0, __dmul_rn(dg, dg), gacc);
+  }
+  if (own_w || j1 <= j0) return;  // tile-uniform
+  const int64_t ih = min(i1, nv - 1);
+  const int nr = (int)(ih - i0 + 1);
+  __syncthreads();
+  for (int k = threadIdx.x; k <= nr; k += NT) {
+    const int64_t r = ptr[i0 + k] - j0;
+    sm->off[k] = (int32_t)max((int64_t)0, min(r, (int64_t)kMergeTile + 1));
+  }
+  for (int k = threadIdx.x; k < nr; k += NT) sm->comm[k] = C[i0 + k];
+  __syncthreads();
+  const int ne = (int)(j1 - j0);
+  for (int q = threadIdx.x; q < ne; q += NT) {
+    int lo = 0, hi = nr - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (sm->off[mid] <= q) lo = mid; else hi = mid - 1;
+    }
+    const int64_t e = j0 + q;
+    if (C[tail[e]] == sm->comm[lo]) graph_acc_add(acc, gid[i0 + lo], w[e], 0.0, gacc);
+  }
+}
+
 // Graph-of-launches form: each block folds the tiles blockIdx.x + k*gridDim.x
 // and writes one partial pair.
 __global__ void __launch_bounds__(256) k_modularity_merge(int64_t nv, int64_t nnz,
@@ -540,7 +603,9 @@ __global__ void __launch_bounds__(256) k_coarse_records(
       const int64_t e = j0 + q;
       const int32_t a = sm.comm[lo];
       const int32_t b = C[tail[e]];
-      if (a >= b) {
+      // b < 0: an endpoint in no community (an isolated vertex, or a graph of a
+      // batch that has finished) contributes no record
+      if (a >= b && b >= 0) {
         keys[ncl + e] = ((uint64_t)a << nb) | (uint64_t)b;
         vals[ncl + e] = w[e];
       } else {

@@ -43,10 +43,18 @@ struct SweepArgs {
   float *rec_gain;         // per vertex: best positive gain of its last evaluation
   int32_t *last_move;      // per vertex: iteration of its last move
   int32_t iter;            // this sweep's iteration number within the phase
+  // batches of graphs (one level holds many graphs; nullptr = one graph)
+  const int32_t *gid;      // per vertex: its graph
+  const double *gcst;      // per graph: 1 / (2m) of that graph
 };
 
 __device__ __forceinline__ bool skipped(const SweepArgs &a, int32_t v) {
   return a.skip && a.skip[v];
+}
+
+// The modularity constant that vertex v's gains use: its own graph's.
+__device__ __forceinline__ double cst_of(const SweepArgs &a, int32_t v) {
+  return a.gid ? a.gcst[a.gid[v]] : a.constant;
 }
 
 // A vertex the gate left out keeps its community and moves nothing.
@@ -144,7 +152,7 @@ __device__ __forceinline__ void small_item(const SweepArgs &a, int64_t base, int
   if (leader && c != own) {
     const double eix = __dsub_rn(own_w, self_loop);
     const double ax = __dsub_rn(a.cDeg[own], degree);
-    const double gain = louvain_gain(sum, eix, degree, a.cDeg[c], ax, a.constant);
+    const double gain = louvain_gain(sum, eix, degree, a.cDeg[c], ax, cst_of(a, v));
     if (gain > 0.0) { g = gain; bc = c; }
   }
 #pragma unroll
@@ -262,7 +270,7 @@ __device__ __forceinline__ double warp_accumulate(const SweepArgs &a, int32_t v,
 __device__ __forceinline__ void scan_table(const SweepArgs &a, const int32_t *keys,
                                            const double *vals, uint32_t first, uint32_t cap,
                                            uint32_t stride, int32_t own, double eix, double ax,
-                                           double degree, double &g, int32_t &bc) {
+                                           double degree, double cst, double &g, int32_t &bc) {
   // four slots per thread in flight: their cDeg gathers overlap
   for (uint32_t s0 = first; s0 < cap; s0 += 4 * stride) {
     int32_t k[4];
@@ -278,7 +286,7 @@ __device__ __forceinline__ void scan_table(const SweepArgs &a, const int32_t *ke
     for (int q = 0; q < 4; ++q) {
       if (k[q] < 0 || k[q] == own) continue;
       const double gain =
-          louvain_gain(vals[s0 + q * stride], eix, degree, cd[q], ax, a.constant);
+          louvain_gain(vals[s0 + q * stride], eix, degree, cd[q], ax, cst);
       if (gain > 0.0 && better(gain, k[q], g, bc)) { g = gain; bc = k[q]; }
     }
   }
@@ -319,7 +327,7 @@ __device__ __forceinline__ void warp_table_vertex(const SweepArgs &a, int64_t po
   const double ax = __dsub_rn(a.cDeg[own], degree);
   double g = 0.0;
   int32_t bc = INT32_MAX;
-  scan_table(a, keys, vals, lane, cap, 32, own, eix, ax, degree, g, bc);
+  scan_table(a, keys, vals, lane, cap, 32, own, eix, ax, degree, cst_of(a, v), g, bc);
   warp_argmax(g, bc);
   if (lane == 0) emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), degree, own_w, g);
   __syncwarp();
@@ -379,7 +387,7 @@ __device__ __forceinline__ void block_vertex(const SweepArgs &a, int64_t pos, in
   const double ax = __dsub_rn(a.cDeg[own], degree);
   double g = 0.0;
   int32_t bc = INT32_MAX;
-  scan_table(a, keys, vals, threadIdx.x, cap, blockDim.x, own, eix, ax, degree, g, bc);
+  scan_table(a, keys, vals, threadIdx.x, cap, blockDim.x, own, eix, ax, degree, cst_of(a, v), g, bc);
   warp_argmax(g, bc);
   if (lane == 0) { s_g[warp] = g; s_c[warp] = bc; }
   __syncthreads();
@@ -431,7 +439,7 @@ __device__ __forceinline__ void team_vertex(const SweepArgs &a, int64_t pos, int
   const double ax = __dsub_rn(a.cDeg[own], degree);
   double g = 0.0;
   int32_t bc = INT32_MAX;
-  scan_table(a, keys, vals, tt, cap, T, own, eix, ax, degree, g, bc);
+  scan_table(a, keys, vals, tt, cap, T, own, eix, ax, degree, cst_of(a, v), g, bc);
   warp_argmax(g, bc);
   if (lane == 0) { s_g[tw] = g; s_c[tw] = bc; }
   team_sync<T>(team);
@@ -507,7 +515,7 @@ static_assert(kHubChunk < kHubStageCap, "a chunk's distinct keys must fit the st
 __device__ __forceinline__ void hub_scan_slots(const SweepArgs &a, int32_t *keys, double *vals,
                                                const int32_t *occ, int64_t k0, int64_t k1,
                                                int32_t own, double eix, double ax, double degree,
-                                               double &g, int32_t &bc) {
+                                               double cst, double &g, int32_t &bc) {
   for (int64_t kb = k0 + threadIdx.x; kb < k1; kb += (int64_t)kHubBatch * blockDim.x) {
     int32_t s[kHubBatch], c[kHubBatch];
     double val[kHubBatch], cd[kHubBatch];
@@ -527,7 +535,7 @@ __device__ __forceinline__ void hub_scan_slots(const SweepArgs &a, int32_t *keys
     for (int j = 0; j < kHubBatch; ++j) {
       if (s[j] < 0) continue;
       if (c[j] != own) {
-        const double gain = louvain_gain(val[j], eix, degree, cd[j], ax, a.constant);
+        const double gain = louvain_gain(val[j], eix, degree, cd[j], ax, cst);
         if (gain > 0.0 && better(gain, c[j], g, bc)) { g = gain; bc = c[j]; }
       }
       keys[s[j]] = -1;
@@ -656,7 +664,7 @@ __device__ __forceinline__ void hub_accum_chunk(const SweepArgs &a, const HubWor
   const double ax = __dsub_rn(a.cDeg[own], degree);
   double g = 0.0;
   int32_t bc = INT32_MAX;
-  hub_scan_slots(a, keys, vals, occ, 0, nfill, own, eix, ax, degree, g, bc);
+  hub_scan_slots(a, keys, vals, occ, 0, nfill, own, eix, ax, degree, cst_of(a, v), g, bc);
   warp_argmax(g, bc);
   if (lane == 0) { s_g[warp] = g; s_c[warp] = bc; }
   __syncthreads();
@@ -690,7 +698,7 @@ __device__ __forceinline__ void hub_scan_segment(const SweepArgs &a, const HubWo
   const int64_t oe = min(h.seg_end[si], (int64_t)h.cnt[pos]);
   double g = 0.0;
   int32_t bc = INT32_MAX;
-  hub_scan_slots(a, keys, vals, occ, ob, oe, own, eix, ax, degree, g, bc);
+  hub_scan_slots(a, keys, vals, occ, ob, oe, own, eix, ax, degree, cst_of(a, v), g, bc);
   warp_argmax(g, bc);
   if (lane == 0) { s_g[warp] = g; s_c[warp] = bc; }
   __syncthreads();

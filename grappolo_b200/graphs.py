@@ -325,3 +325,114 @@ def planted_powerlaw(nv: int, degree_exp: float = 2.5, mean_degree: float = 20.0
     cross = comm[qu] != comm[qv]
     return csr_from_undirected(nv, np.concatenate([pu[same], qu[cross]]),
                                np.concatenate([pv[same], qv[cross]]))
+
+
+def batch_specs(num_graphs: int = 4096, seed: int = 3, nv_range=(500, 200000),
+                block_range=(20, 2000), mu_range=(0.1, 0.6), degree_range=(6.0, 32.0)):
+    """Per-graph parameters of the batched workload: vertex counts and block
+    sizes log-uniform, mixing fraction and mean degree uniform.  Returns an
+    (num_graphs, 4) float64 array of (nv, block_size, mu, mean_degree)."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(nv_range[0]), np.log(nv_range[1])
+    nv = np.floor(np.exp(rng.uniform(lo, hi, num_graphs))).astype(np.int64)
+    blo, bhi = np.log(block_range[0]), np.log(block_range[1])
+    bs = np.floor(np.exp(rng.uniform(blo, bhi, num_graphs))).astype(np.int64)
+    bs = np.minimum(bs, nv)
+    mu = rng.uniform(mu_range[0], mu_range[1], num_graphs)
+    deg = rng.uniform(degree_range[0], degree_range[1], num_graphs)
+    return np.stack([nv, bs, mu, deg], axis=1).astype(np.float64)
+
+
+def planted_batch_device(specs, seed: int = 3, device='cuda', group_pairs: int = 200_000_000):
+    """The graphs of `specs` (rows of :func:`batch_specs`) as one device CSR laid
+    end to end, built with torch on the device: the construction of
+    :func:`planted_partition_mixed` graph by graph (Poisson intra-block pair
+    counts, uniform inter-block pairs, duplicates and self-loops dropped, unit
+    weights), drawn from torch's generator, so a graph differs from the numpy
+    one.  Graphs are built in groups of about `group_pairs` candidate pairs to
+    bound the scratch memory.  Returns (vertex_offsets int64 numpy[G+1],
+    ptr int64[NV+1], tail int32[nnz], weight float64[nnz]) on the device."""
+    import torch
+    specs = np.asarray(specs, dtype=np.float64)
+    G = specs.shape[0]
+    nv = specs[:, 0].astype(np.int64)
+    bs = specs[:, 1].astype(np.int64)
+    mu, deg = specs[:, 2], specs[:, 3]
+    voff = np.zeros(G + 1, dtype=np.int64)
+    np.cumsum(nv, out=voff[1:])
+    rng = np.random.default_rng(seed)
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    expect = (deg * nv / 2.0).astype(np.int64) + 1  # candidate pairs per graph
+    ptr_parts, tail_parts = [], []
+    g0 = 0
+    while g0 < G:
+        g1 = g0 + 1
+        tot = expect[g0]
+        while g1 < G and tot + expect[g1] <= group_pairs:
+            tot += expect[g1]
+            g1 += 1
+        base = voff[g0]
+        n_loc = int(voff[g1] - base)
+        # blocks of the group (host), intra-block pair counts per block
+        bstart, bsize, m_in = [], [], []
+        for g in range(g0, g1):
+            st = np.arange(0, nv[g], bs[g], dtype=np.int64)
+            sz = np.minimum(bs[g], nv[g] - st)
+            bstart.append(st + (voff[g] - base))
+            bsize.append(sz)
+            m_in.append(rng.poisson((1.0 - mu[g]) * deg[g] * sz / 2.0))
+        bstart = torch.from_numpy(np.concatenate(bstart)).to(device)
+        bsize = torch.from_numpy(np.concatenate(bsize)).to(device)
+        m_in = torch.from_numpy(np.concatenate(m_in).astype(np.int64)).to(device)
+        bid = torch.repeat_interleave(torch.arange(bstart.numel(), device=device), m_in)
+        u = bstart[bid] + (torch.rand(bid.numel(), generator=gen, device=device,
+                                      dtype=torch.float64) * bsize[bid]).to(torch.int64)
+        v = bstart[bid] + (torch.rand(bid.numel(), generator=gen, device=device,
+                                      dtype=torch.float64) * bsize[bid]).to(torch.int64)
+        del bid
+        # inter-block pairs per graph
+        m_out = torch.from_numpy(rng.poisson(mu[g0:g1] * deg[g0:g1] * nv[g0:g1] / 2.0)
+                                 .astype(np.int64)).to(device)
+        gst = torch.from_numpy(voff[g0:g1] - base).to(device)
+        gnv = torch.from_numpy(nv[g0:g1]).to(device)
+        gbs = torch.from_numpy(bs[g0:g1]).to(device)
+        gi = torch.repeat_interleave(torch.arange(g1 - g0, device=device), m_out)
+        uo = (torch.rand(gi.numel(), generator=gen, device=device, dtype=torch.float64)
+              * gnv[gi]).to(torch.int64)
+        vo = (torch.rand(gi.numel(), generator=gen, device=device, dtype=torch.float64)
+              * gnv[gi]).to(torch.int64)
+        cross = (uo // gbs[gi]) != (vo // gbs[gi])
+        uo = (uo + gst[gi])[cross]
+        vo = (vo + gst[gi])[cross]
+        del gi, cross
+        u = torch.cat([u, uo])
+        v = torch.cat([v, vo])
+        del uo, vo
+        keep = u != v
+        key = torch.minimum(u, v)[keep] * n_loc + torch.maximum(u, v)[keep]
+        del u, v, keep
+        key = torch.unique(key)
+        lo, hi = key // n_loc, key % n_loc
+        del key
+        src = torch.cat([lo, hi])
+        dst = torch.cat([hi, lo])
+        del lo, hi
+        order = torch.argsort(src * n_loc + dst)
+        src, dst = src[order], dst[order]
+        del order
+        cnt = torch.bincount(src, minlength=n_loc)
+        del src
+        ptr_parts.append(cnt)
+        tail_parts.append((dst + base).to(torch.int32))
+        del dst
+        g0 = g1
+    cnt = torch.cat(ptr_parts)
+    del ptr_parts
+    ptr = torch.zeros(voff[-1] + 1, dtype=torch.int64, device=device)
+    ptr[1:] = torch.cumsum(cnt, 0)
+    del cnt
+    tail = torch.cat(tail_parts)
+    del tail_parts
+    w = torch.ones(tail.numel(), dtype=torch.float64, device=device)
+    return voff, ptr, tail, w

@@ -228,3 +228,73 @@ def run_multiphase_device(nv, d_ptr, d_tail, d_weight, d_C_orig, coloring=True,
                                                  C_threshold, mode, stream or None,
                                                  ct.byref(st)))
     return st.to_dict()
+
+
+def _batch_stats(G):
+    """A glv_batch_stats with its per-graph arrays (kept alive by the dict)."""
+    arrs = {'final_modularity': np.zeros(G), 'phases': np.zeros(G, dtype=np.int32),
+            'iterations': np.zeros(G, dtype=np.int32), 'clusters': np.zeros(G, dtype=np.int64),
+            'done_seconds': np.zeros(G)}
+    st = _lib.GlvBatchStats()
+    st.final_modularity = arrs['final_modularity'].ctypes.data_as(_P(ct.c_double))
+    st.phases = arrs['phases'].ctypes.data_as(_P(ct.c_int))
+    st.iterations = arrs['iterations'].ctypes.data_as(_P(ct.c_int))
+    st.clusters = arrs['clusters'].ctypes.data_as(_P(ct.c_long))
+    st.done_seconds = arrs['done_seconds'].ctypes.data_as(_P(ct.c_double))
+    return st, arrs
+
+
+def _batch_dict(st, arrs):
+    d = {k: getattr(st, k) for k in ('rounds', 'time_total', 'time_clustering', 'time_coloring',
+                                     'time_building', 'time_transfer', 'edges_swept',
+                                     'kernel_launches')}
+    d.update({k: v.copy() for k, v in arrs.items()})
+    return d
+
+
+def union(graphs):
+    """Lay graphs end to end as one CSR (tails shifted to global ids).
+    Returns (vertex_offsets int64[G+1], CSRGraph)."""
+    voff = np.zeros(len(graphs) + 1, dtype=np.int64)
+    np.cumsum([g.num_vertices for g in graphs], out=voff[1:])
+    eoff = np.zeros(len(graphs) + 1, dtype=np.int64)
+    np.cumsum([g.nnz for g in graphs], out=eoff[1:])
+    ptr = np.empty(voff[-1] + 1, dtype=np.int64)
+    tail = np.empty(eoff[-1], dtype=np.int64)
+    w = np.empty(eoff[-1], dtype=np.float64)
+    for k, g in enumerate(graphs):
+        ptr[voff[k]:voff[k + 1]] = g.ptr[:-1] + eoff[k]
+        tail[eoff[k]:eoff[k + 1]] = g.tail + voff[k]
+        w[eoff[k]:eoff[k + 1]] = g.weight
+    ptr[-1] = eoff[-1]
+    return voff, CSRGraph(ptr, tail, w)
+
+
+def run_batch(graphs, coloring: bool = True, minGraphSize=1000, threshold=1e-6,
+              C_threshold=1e-4, mode: int = _lib.GLV_MODE_FAST):
+    """Many independent graphs in one batched run (glv_run_batch_csr).
+
+    Returns (list of per-graph community arrays in graph-local ids, stats dict
+    with per-graph arrays final_modularity/phases/iterations/clusters/done_seconds)."""
+    voff, u = union(graphs)
+    C = np.full(u.num_vertices, -1, dtype=np.int64)
+    st, arrs = _batch_stats(len(graphs))
+    lp = lambda a: a.ctypes.data_as(_P(ct.c_long))  # noqa: E731
+    _lib.check(_lib.lib().glv_run_batch_csr(
+        len(graphs), lp(voff), lp(u.ptr), lp(np.ascontiguousarray(u.tail, dtype=np.int64)),
+        u.weight.ctypes.data_as(_P(ct.c_double)), lp(C), 1 if coloring else 0, minGraphSize,
+        threshold, C_threshold, mode, ct.byref(st)))
+    return [C[voff[k]:voff[k + 1]] for k in range(len(graphs))], _batch_dict(st, arrs)
+
+
+def run_batch_device(vertex_offsets, d_ptr, d_tail, d_weight, d_C, coloring=True,
+                     minGraphSize=1000, threshold=1e-6, C_threshold=1e-4,
+                     mode: int = _lib.GLV_MODE_FAST, stream=0):
+    """Device-resident batch (glv_dev_run_batch); vertex_offsets is a host int64 array."""
+    voff = np.ascontiguousarray(vertex_offsets, dtype=np.int64)
+    st, arrs = _batch_stats(len(voff) - 1)
+    _lib.check(_lib.lib().glv_dev_run_batch(
+        len(voff) - 1, voff.ctypes.data_as(_P(ct.c_long)), d_ptr, d_tail, d_weight, d_C,
+        1 if coloring else 0, minGraphSize, threshold, C_threshold, mode, stream or None,
+        ct.byref(st)))
+    return _batch_dict(st, arrs)

@@ -146,6 +146,43 @@ int glv_dev_run_multiphase(long nv, const long *d_ptr, const int *d_tail, const 
                            int *d_C_orig, int coloring, long minGraphSize, double threshold,
                            double C_threshold, int mode, void *stream, glv_run_stats *stats);
 
+/* ---- batches of independent graphs --------------------------------------
+ * No reference counterpart as one call: a batch runs
+ * runMultiPhaseColoring (Coloring/runMultiPhaseColoring.cpp:51-238) or, with
+ * coloring = 0, runMultiPhaseBasic (BasicCommunitiesDetection/runMultiPhaseBasic.cpp:52-170)
+ * on every graph of the batch, each graph with its own modularity constant,
+ * phase tests and phase count, in one level holding all graphs.  Graph g owns
+ * vertices [vertex_offsets[g], vertex_offsets[g+1]) of one CSR; tails are
+ * global vertex ids and must stay inside their row's graph (GLV_ERR_ARG
+ * otherwise); every graph needs at least one vertex.  C_out receives each
+ * vertex's community as a graph-local id (-1 = isolated).  mode: GLV_MODE_VERIFY
+ * (integral weights only; results equal per-graph runs) or GLV_MODE_FAST. */
+typedef struct {
+  /* per graph: caller-owned arrays of num_graphs entries, each may be NULL */
+  double *final_modularity; /* the phase loop's "Final modularity" (prevMod) */
+  int *phases;
+  int *iterations;
+  long *clusters;
+  double *done_seconds;     /* time from the start of the run until the graph finished */
+  /* whole batch (filled by the call) */
+  int rounds;               /* phase rounds of the batch loop */
+  double time_total, time_clustering, time_coloring, time_building, time_transfer;
+  double edges_swept;
+  long kernel_launches;
+} glv_batch_stats;
+
+int glv_run_batch_csr(int num_graphs, const long *vertex_offsets, const long *ptr,
+                      const long *tail, const double *weight, long *C_out, int coloring,
+                      long minGraphSize, double threshold, double C_threshold, int mode,
+                      glv_batch_stats *stats);
+
+/* Device-resident batch: d_ptr int64[nv+1], d_tail int32[nnz], d_weight f64[nnz],
+ * d_C int32[nv] on the device; vertex_offsets stays a host array. */
+int glv_dev_run_batch(int num_graphs, const long *vertex_offsets, const long *d_ptr,
+                      const int *d_tail, const double *d_weight, int *d_C, int coloring,
+                      long minGraphSize, double threshold, double C_threshold, int mode,
+                      void *stream, glv_batch_stats *stats);
+
 /* ---- single phases and primitives (host buffers) ------------------------ */
 
 /* Replaces algoLouvainWithDistOneColoring (Coloring/parallelLouvainWithColoring.cpp:47-286,

@@ -55,3 +55,45 @@ def test_from_edges_keeps_self_loops_once():
     row1 = g.tail[g.ptr[1]:g.ptr[2]]
     assert list(row1) == [0, 1, 2]
     assert g.num_edges == 3
+
+
+def test_union_lays_graphs_end_to_end():
+    from grappolo_b200 import louvain
+    a = graphs.planted_partition_mixed(50, 10, 0.2, 6, seed=1)
+    b = graphs.planted_partition_mixed(70, 7, 0.3, 5, seed=2)
+    voff, u = louvain.union([a, b])
+    assert list(voff) == [0, 50, 120]
+    assert u.num_vertices == 120 and u.nnz == a.nnz + b.nnz
+    assert np.array_equal(u.ptr[:51], a.ptr)
+    assert np.array_equal(u.tail[:a.nnz], a.tail)
+    assert np.array_equal(u.tail[a.nnz:], b.tail + 50)
+    assert np.array_equal(u.ptr[50:] - a.nnz, b.ptr)
+    heads = u.heads()
+    assert np.all((heads < 50) == (u.tail < 50))
+
+
+def test_batch_specs_ranges():
+    sp = graphs.batch_specs(512, seed=3)
+    assert sp.shape == (512, 4)
+    assert sp[:, 0].min() >= 500 and sp[:, 0].max() < 200000
+    assert np.all(sp[:, 1] >= 20) and np.all(sp[:, 1] <= sp[:, 0])
+    assert np.all((sp[:, 2] >= 0.1) & (sp[:, 2] <= 0.6))
+    assert np.all((sp[:, 3] >= 6) & (sp[:, 3] <= 32))
+
+
+def test_planted_batch_generator_on_cpu():
+    """The device generator (run here with torch on the CPU): tails stay in
+    their graph, rows sorted, no duplicates or self-loops, symmetric."""
+    sp = graphs.batch_specs(6, seed=1, nv_range=(500, 3000))
+    voff, ptr, tail, w = graphs.planted_batch_device(sp, device='cpu', group_pairs=20000)
+    p = ptr.numpy()
+    t = tail.numpy().astype(np.int64)
+    assert p[0] == 0 and p[-1] == t.size and voff[-1] == p.size - 1
+    heads = np.repeat(np.arange(p.size - 1), np.diff(p))
+    g_of = np.searchsorted(voff, heads, side='right') - 1
+    assert np.all((t >= voff[g_of]) & (t < voff[g_of + 1]))
+    n = voff[-1]
+    key = heads * n + t
+    assert np.all(np.diff(key) > 0) and np.all(heads != t)
+    assert np.array_equal(np.sort(t * n + heads), key)
+    assert np.all(w.numpy() == 1.0)
