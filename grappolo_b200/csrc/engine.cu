@@ -514,11 +514,12 @@ int Engine::color(const Level &L, int *ncolors, double *secs) {
     *ncolors = 0;
     return GLV_OK;
   }
-  // GRAPPOLO_B200_COLORING=jp|spec overrides the mode's colouring (jp: the
-  // deterministic id-priority colouring of verify mode)
+  // GRAPPOLO_B200_COLORING overrides the mode's colouring: spec (speculative
+  // largest-degree-first), jp (Jones-Plassmann, hashed priorities in fast
+  // mode), id (Jones-Plassmann in vertex-id order, verify mode's colouring)
   const char *cm = getenv("GRAPPOLO_B200_COLORING");
   bool spec = mode_ != GLV_MODE_VERIFY;
-  if (cm && !strcmp(cm, "jp")) spec = false;
+  if (cm && (!strcmp(cm, "jp") || !strcmp(cm, "id"))) spec = false;
   if (cm && !strcmp(cm, "spec")) spec = true;
   TRY(spec ? color_spec(L, ncolors) : color_jp(L, ncolors));
   if (secs) *secs = now_s() - t0;
@@ -534,7 +535,10 @@ int Engine::color_jp(const Level &L, int *ncolors) {
   CK(cudaMemsetAsync(fcount, 0, 3 * sizeof(int32_t), s_));
   CK(cudaMemsetAsync(status, 0, 2 * sizeof(int32_t), s_));
   CK(cudaMemsetAsync(maxc, 0xff, sizeof(int32_t), s_));
-  const int hashed = (mode_ != GLV_MODE_VERIFY) ? 1 : 0;
+  // fast mode hashes the priorities (independent sets of random order);
+  // GRAPPOLO_B200_COLORING=id keeps the vertex-id order of verify mode
+  const char *cm = getenv("GRAPPOLO_B200_COLORING");
+  const int hashed = (mode_ != GLV_MODE_VERIFY && !(cm && !strcmp(cm, "id"))) ? 1 : 0;
   const uint32_t seed = 0x5bd1e995u;
   LAUNCH(k_color_init, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, L.ptr, L.tail, hashed,
          seed, pending, color_, f0, fcount);
