@@ -414,7 +414,9 @@ def main():
                               'renumber+coarsen': s0['time_building'],
                               'other': s0['time_total'] - s0['time_clustering']
                               - s0['time_coloring'] - s0['time_building']},
-             'step_totals_s': [round(s['time_total'], 4) for s in stats]}
+             'step_totals_s': [round(s['time_total'], 4) for s in stats],
+             'step_splits_s': [[round(s[k], 4) for k in ('time_clustering', 'time_coloring',
+                                                         'time_building')] for s in stats]}
     line = {'metric': METRIC, 'value': value, 'unit': UNIT, 'n_gpus': world, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': 1e3 * t / args.steps,
             'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64',
