@@ -16,6 +16,7 @@
 #include "batch_kernels.cuh"
 #include "gate.cuh"
 #include "persist.cuh"
+#include "recolor.cuh"
 #include "phase_kernels.cuh"
 #include "sweep.cuh"
 
@@ -291,7 +292,7 @@ class Engine {
   int launch_sweep(const Level &L, const Step &st, SweepArgs a, bool ordered, Probes *pr);
   int launch_apply(const ClassSched &cs, bool ordered);
   int launch_modularity(const Level &L, const int32_t *Cm, const double *ownw);
-  int color_jp(const Level &L, int *ncolors);
+  int color_jp(const Level &L, int *ncolors, const int32_t *key = nullptr);
   int run_persistent(const Level &L, const std::vector<ClassSched> &sched, SweepArgs a,
                      bool jacobi, double lower, double thresh, double *mod, int *itr);
   bool persistent() const {
@@ -299,6 +300,7 @@ class Engine {
     return !ordered() && !(e && e[0] == '0');
   }
   int color_spec(const Level &L, int *ncolors);
+  int recolor(const Level &L, int *ncolors, int passes);
   int grow_hub(size_t entries);
   bool ordered() const { return mode_ == GLV_MODE_VERIFY && !integral; }
   void account(Probes &pr, const Level &L) {
@@ -521,14 +523,40 @@ int Engine::color(const Level &L, int *ncolors, double *secs) {
   bool spec = mode_ != GLV_MODE_VERIFY;
   if (cm && (!strcmp(cm, "jp") || !strcmp(cm, "id"))) spec = false;
   if (cm && !strcmp(cm, "spec")) spec = true;
-  TRY(spec ? color_spec(L, ncolors) : color_jp(L, ncolors));
+  if (!spec) {
+    TRY(color_jp(L, ncolors));
+  } else {
+    const bool dbg = getenv("GRAPPOLO_B200_DEBUG") != nullptr;
+    double td = now_s();
+    TRY(color_spec(L, ncolors));
+    if (dbg) {
+      cudaStreamSynchronize(s_);
+      fprintf(stderr, "grappolo_b200: colour spec %.4f s (%d colours)\n", now_s() - td, *ncolors);
+      td = now_s();
+    }
+    // Iterated greedy (Culberson): recolour whole classes, last class first;
+    // such a pass never needs more colours, and on power-law graphs it
+    // removes many.  Every class is a step of every sweep, so fewer classes
+    // mean fewer barriers and shorter latency chains.  Passes stop when one
+    // removes no colour (GRAPPOLO_B200_RECOLOR sets the maximum, 0 = off;
+    // GRAPPOLO_B200_RECOLOR_MIN the colour count below which none is run).
+    // Only colourings with many classes are worth it: a class costs a grid
+    // barrier and its latency chain, a pass costs about one colouring.
+    const char *rp = getenv("GRAPPOLO_B200_RECOLOR");
+    const char *rm = getenv("GRAPPOLO_B200_RECOLOR_MIN");
+    if (*ncolors > (rm ? atoi(rm) : 64)) TRY(recolor(L, ncolors, rp ? atoi(rp) : 2));
+    if (dbg) {
+      cudaStreamSynchronize(s_);
+      fprintf(stderr, "grappolo_b200: recolour %.4f s (%d colours)\n", now_s() - td, *ncolors);
+    }
+  }
   if (secs) *secs = now_s() - t0;
   return GLV_OK;
 }
 
 // Verify mode: Jones-Plassmann in vertex-id priority = the reference's
 // one-thread sequential first-fit.
-int Engine::color_jp(const Level &L, int *ncolors) {
+int Engine::color_jp(const Level &L, int *ncolors, const int32_t *key) {
   int32_t *pending, *f0, *f1, *fcount, *status, *maxc;
   TRY(alloc(&pending, L.nv)); TRY(alloc(&f0, L.nv)); TRY(alloc(&f1, L.nv));
   TRY(alloc(&fcount, 3)); TRY(alloc(&status, 2)); TRY(alloc(&maxc, 1));
@@ -541,7 +569,7 @@ int Engine::color_jp(const Level &L, int *ncolors) {
   const int hashed = (mode_ != GLV_MODE_VERIFY && !(cm && !strcmp(cm, "id"))) ? 1 : 0;
   const uint32_t seed = 0x5bd1e995u;
   LAUNCH(k_color_init, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, L.ptr, L.tail, hashed,
-         seed, pending, color_, f0, fcount);
+         seed, pending, color_, f0, fcount, key);
   int per_sm = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_color_rounds, 256, 0));
   int grid = std::max(1, per_sm) * nsm_;
@@ -550,7 +578,7 @@ int Engine::color_jp(const Level &L, int *ncolors) {
   const int32_t *tail = L.tail;
   int32_t *color = color_;
   void *args[] = {&nv, (void *)&ptr, (void *)&tail, (void *)&hashed, (void *)&seed, &pending,
-                  &color, &f0, &f1, &fcount, &status};
+                  &color, &f0, &f1, &fcount, &status, (void *)&key};
   CK(cudaLaunchCooperativeKernel((void *)k_color_rounds, grid, 256, args, 0, s_));
   ++launches_;
   LAUNCH(k_max_color, grid_for(L.nv, 256, nsm_ * 8), 256, 0, s_, L.nv, color_, maxc);
@@ -868,6 +896,59 @@ int Engine::hub_offsets(const Level &L, std::vector<ClassSched> &sched) {
   CK(cudaStreamSynchronize(s_));
   dfree(d_pos);
   dfree(d_vals);
+  return GLV_OK;
+}
+
+// Iterated greedy passes over the colouring in color_ (recolor.cuh): classes
+// in reverse order, each recoloured first-fit against the classes already
+// done.  Stops after `passes` or when a pass removes no colour.
+int Engine::recolor(const Level &L, int *ncolors, int passes) {
+  if (ordered() || L.nv == 0 || passes <= 0) return GLV_OK;
+  int32_t *key, *newc, *maxc;
+  TRY(alloc(&key, L.nv)); TRY(alloc(&newc, L.nv)); TRY(alloc(&maxc, 1));
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_recolor_pass, kRecolorThreads, 0));
+  if (per_sm < 1) return fail(GLV_ERR_CUDA, "recolouring kernel does not fit on an SM");
+  const int grid = per_sm * nsm_;
+  for (int k = 0; k < passes && *ncolors > 1; ++k) {
+    LAUNCH(k_reverse_class_key, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, color_,
+           (int32_t)*ncolors, key);
+    std::vector<ClassSched> sched;
+    TRY(build_schedule(L, key, *ncolors, nullptr, 1, &sched));
+    std::vector<StepDesc> steps;
+    for (auto &cs : sched)
+      for (auto &st : cs.steps) {
+        StepDesc d{};
+        for (int b = 0; b <= NBINS; ++b) d.seg[b] = st.seg[b];
+        d.hub_chunk[0] = st.hub_chunk[0];
+        d.hub_chunk[1] = st.hub_chunk[1];
+        steps.push_back(d);
+      }
+    StepDesc *d_steps;
+    int64_t *d_ctr;
+    TRY(alloc(&d_steps, steps.size()));
+    TRY(alloc(&d_ctr, steps.size()));
+    TRY(upload(s_, d_steps, steps));
+    CK(cudaMemsetAsync(d_ctr, 0, steps.size() * sizeof(int64_t), s_));
+    CK(cudaMemsetAsync(newc, 0xff, L.nv * sizeof(int32_t), s_));
+    RecolorArgs r{L.ptr, L.tail, members_, newc, d_steps, (int)steps.size(), d_ctr,
+                  chunk_pos_, chunk_beg_, chunk_end_, hub_off_, hub_keys_, hub_left_};
+    void *args[] = {&r};
+    CK(cudaLaunchCooperativeKernel((void *)k_recolor_pass, grid, kRecolorThreads, args, 0, s_));
+    ++launches_;
+    CK(cudaMemsetAsync(maxc, 0xff, sizeof(int32_t), s_));
+    LAUNCH(k_max_color, grid_for(L.nv, 256, nsm_ * 8), 256, 0, s_, L.nv, newc, maxc);
+    int32_t hm = -1;
+    CK(cudaMemcpyAsync(&hm, maxc, sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
+    CK(cudaMemcpyAsync(color_, newc, L.nv * sizeof(int32_t), cudaMemcpyDeviceToDevice, s_));
+    CK(cudaStreamSynchronize(s_));
+    dfree(d_steps);
+    dfree(d_ctr);
+    const bool gained = hm + 1 < *ncolors;
+    *ncolors = hm + 1;
+    if (!gained) break;
+  }
+  dfree(key); dfree(newc); dfree(maxc);
   return GLV_OK;
 }
 
@@ -1641,6 +1722,7 @@ int Engine::coarsen(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
   CK(cudaMemcpyAsync(&o.nnz, o.ptr + ncl, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
   CK(cudaMemcpyAsync(&hne, ne_off, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
   CK(cudaStreamSynchronize(s_));
+  mark("emit counts");
   TRY(alloc(&o.tail, o.nnz)); TRY(alloc(&o.w, o.nnz));
   LAUNCH(k_run_first, gp, 256, 0, s_, np, ukeys, nb, sentinel, lower_first);
   uint64_t *tk1 = k2, *tk2;
@@ -1648,9 +1730,11 @@ int Engine::coarsen(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
   TRY(alloc(&tk2, np)); TRY(alloc(&tv2, np));
   LAUNCH(k_emit_lower, gp, 256, 0, s_, np, ukeys, uvals, nb, o.ptr, lower_first, o.tail, o.w, tk1,
          tv1, sentinel);
+  mark("emit lower");
   CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, tk1, tk2, tv1, tv2, np, 0, end_bit, s_));
   TRY(temp(tb));
   CK(cub::DeviceRadixSort::SortPairs(temp_, tb, tk1, tk2, tv1, tv2, np, 0, end_bit, s_));
+  mark("emit sort");
   LAUNCH(k_run_first, gp, 256, 0, s_, np, tk2, nb, sentinel, upper_first);
   LAUNCH(k_emit_upper, gp, 256, 0, s_, np, tk2, tv2, nb, o.ptr, lower_cnt, upper_first, o.tail,
          o.w, sentinel);
@@ -1832,6 +1916,18 @@ struct Call {
   long launches = 0;
   double t_transfer = 0;
   ~Call() {
+    if (getenv("GRAPPOLO_B200_DEBUG")) {
+      cudaMemPool_t p = engine_pool();
+      uint64_t rc = 0, rh = 0, uc = 0, uh = 0;
+      if (p) {
+        cudaMemPoolGetAttribute(p, cudaMemPoolAttrReservedMemCurrent, &rc);
+        cudaMemPoolGetAttribute(p, cudaMemPoolAttrReservedMemHigh, &rh);
+        cudaMemPoolGetAttribute(p, cudaMemPoolAttrUsedMemCurrent, &uc);
+        cudaMemPoolGetAttribute(p, cudaMemPoolAttrUsedMemHigh, &uh);
+      }
+      fprintf(stderr, "grappolo_b200: pool reserved %.3f GB (high %.3f) used %.3f GB (high %.3f)\n",
+              rc * 1e-9, rh * 1e-9, uc * 1e-9, uh * 1e-9);
+    }
     if (eng) {
       eng->free_level(L0);
       launches += eng->launches_;

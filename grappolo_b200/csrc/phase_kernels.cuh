@@ -322,7 +322,14 @@ __global__ void __launch_bounds__(256) k_modularity_final(int nparts, const doub
 // all coloured.  With priority "lower id first" this is exactly the
 // sequential first-fit pass of Coloring/coloringDistanceOne.cpp:137-150 at one
 // thread; with hashed priorities it is the parallel independent-set form.
-__device__ __forceinline__ bool prio_before(int32_t u, int32_t v, int hashed, uint32_t seed) {
+// With `key` given, priority is (key, id): the iterated-greedy recolouring
+// orders vertices by their previous colour class.
+__device__ __forceinline__ bool prio_before(int32_t u, int32_t v, int hashed, uint32_t seed,
+                                            const int32_t *key = nullptr) {
+  if (key) {
+    const int32_t ku = key[u], kv = key[v];
+    return (ku < kv) || (ku == kv && u < v);
+  }
   if (!hashed) return u < v;
   const uint32_t hu = mix32((uint32_t)u ^ seed), hv = mix32((uint32_t)v ^ seed);
   return (hu < hv) || (hu == hv && u < v);
@@ -330,13 +337,13 @@ __device__ __forceinline__ bool prio_before(int32_t u, int32_t v, int hashed, ui
 
 __global__ void k_color_init(int64_t nv, const int64_t *ptr, const int32_t *tail, int hashed,
                              uint32_t seed, int32_t *pending, int32_t *color, int32_t *frontier,
-                             int32_t *fcount) {
+                             int32_t *fcount, const int32_t *key) {
   for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
        v += (int64_t)gridDim.x * blockDim.x) {
     int32_t cnt = 0;
     for (int64_t j = ptr[v]; j < ptr[v + 1]; ++j) {
       const int32_t u = tail[j];
-      if (u != (int32_t)v && prio_before(u, (int32_t)v, hashed, seed)) ++cnt;
+      if (u != (int32_t)v && prio_before(u, (int32_t)v, hashed, seed, key)) ++cnt;
     }
     pending[v] = cnt;
     color[v] = -1;
@@ -352,7 +359,7 @@ __global__ void __launch_bounds__(256) k_color_rounds(int64_t nv, const int64_t 
                                                       uint32_t seed, int32_t *pending,
                                                       int32_t *color, int32_t *front0,
                                                       int32_t *front1, int32_t *fcount,
-                                                      int32_t *status) {
+                                                      int32_t *status, const int32_t *key) {
   cg::grid_group grid = cg::this_grid();
   __shared__ uint32_t bm[8][kMaxColors / 32];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -374,7 +381,7 @@ __global__ void __launch_bounds__(256) k_color_rounds(int64_t nv, const int64_t 
       __syncwarp();
       for (int64_t j = rb + lane; j < re; j += 32) {
         const int32_t u = tail[j];
-        if (u != v && prio_before(u, v, hashed, seed)) {
+        if (u != v && prio_before(u, v, hashed, seed, key)) {
           const int32_t cu = color[u];
           if (cu >= 0 && cu < words * 32) atomicOr(&mybm[cu >> 5], 1u << (cu & 31));
         }
@@ -395,13 +402,22 @@ __global__ void __launch_bounds__(256) k_color_rounds(int64_t nv, const int64_t 
       __syncwarp();
       for (int64_t j = rb + lane; j < re; j += 32) {
         const int32_t u = tail[j];
-        if (u != v && prio_before(v, u, hashed, seed)) {
+        if (u != v && prio_before(v, u, hashed, seed, key)) {
           if (atomicSub(&pending[u], 1) == 1) nxt[atomicAdd(&fcount[(round + 1) % 3], 1)] = u;
         }
       }
     }
     grid.sync();
   }
+}
+
+// key[v] = ncolors - 1 - color[v]: recolour the last class first (Culberson's
+// reverse-class order; a greedy pass over whole classes never adds colours).
+__global__ void k_reverse_class_key(int64_t nv, const int32_t *color, int32_t ncolors,
+                                    int32_t *key) {
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
+       v += (int64_t)gridDim.x * blockDim.x)
+    key[v] = ncolors - 1 - color[v];
 }
 
 __global__ void k_max_color(int64_t nv, const int32_t *color, int32_t *out) {
