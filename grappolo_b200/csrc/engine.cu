@@ -523,25 +523,22 @@ int Engine::color(const Level &L, int *ncolors, double *secs) {
   bool spec = mode_ != GLV_MODE_VERIFY;
   if (cm && (!strcmp(cm, "jp") || !strcmp(cm, "id"))) spec = false;
   if (cm && !strcmp(cm, "spec")) spec = true;
-  if (!spec) {
-    TRY(color_jp(L, ncolors));
-  } else {
-    const bool dbg = getenv("GRAPPOLO_B200_DEBUG") != nullptr;
-    double td = now_s();
-    TRY(color_spec(L, ncolors));
-    if (dbg) {
-      cudaStreamSynchronize(s_);
-      fprintf(stderr, "grappolo_b200: colour spec %.4f s (%d colours)\n", now_s() - td, *ncolors);
-      td = now_s();
-    }
-    // Iterated greedy (Culberson): recolour whole classes, last class first;
-    // such a pass never needs more colours, and on power-law graphs it
-    // removes many.  Every class is a step of every sweep, so fewer classes
-    // mean fewer barriers and shorter latency chains.  Passes stop when one
-    // removes no colour (GRAPPOLO_B200_RECOLOR sets the maximum, 0 = off;
-    // GRAPPOLO_B200_RECOLOR_MIN the colour count below which none is run).
-    // Only colourings with many classes are worth it: a class costs a grid
-    // barrier and its latency chain, a pass costs about one colouring.
+  const bool dbg = getenv("GRAPPOLO_B200_DEBUG") != nullptr;
+  double td = now_s();
+  TRY(spec ? color_spec(L, ncolors) : color_jp(L, ncolors));
+  if (dbg) {
+    cudaStreamSynchronize(s_);
+    fprintf(stderr, "grappolo_b200: colouring %.4f s (%d colours)\n", now_s() - td, *ncolors);
+    td = now_s();
+  }
+  // Outside verify mode, iterated greedy (Culberson): recolour whole classes,
+  // last class first; such a pass never needs more colours, and on power-law
+  // graphs it removes many.  Every class is a step of every sweep, so fewer
+  // classes mean fewer barriers and shorter latency chains.  Passes stop when
+  // one removes no colour (GRAPPOLO_B200_RECOLOR sets the maximum, 0 = off).
+  // Only colourings with many classes are worth a pass, which costs about one
+  // colouring (GRAPPOLO_B200_RECOLOR_MIN: the class count that triggers it).
+  if (mode_ != GLV_MODE_VERIFY) {
     const char *rp = getenv("GRAPPOLO_B200_RECOLOR");
     const char *rm = getenv("GRAPPOLO_B200_RECOLOR_MIN");
     if (*ncolors > (rm ? atoi(rm) : 64)) TRY(recolor(L, ncolors, rp ? atoi(rp) : 2));

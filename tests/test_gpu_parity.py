@@ -46,6 +46,23 @@ def test_coloring_fast_is_proper(name):
     assert _proper(g, col)
 
 
+@pytest.mark.parametrize('name', CASES + ['rmat14'])
+def test_recolouring_is_proper_and_never_adds_colours(name, monkeypatch):
+    """Iterated greedy passes (forced on every graph here) over the
+    deterministic id-order colouring: still a proper colouring, and never
+    more colours than the colouring they start from."""
+    g = graphs.rmat(14, seed=9) if name == 'rmat14' else load(name)[0]
+    monkeypatch.setenv('GRAPPOLO_B200_COLORING', 'id')
+    monkeypatch.setenv('GRAPPOLO_B200_RECOLOR', '0')
+    _, mc0, _ = louvain.algoDistanceOneVertexColoringOpt(g, nThreads=8)
+    monkeypatch.setenv('GRAPPOLO_B200_RECOLOR', '3')
+    monkeypatch.setenv('GRAPPOLO_B200_RECOLOR_MIN', '0')
+    col, mc, _ = louvain.algoDistanceOneVertexColoringOpt(g, nThreads=8)
+    assert col.min() >= 0 and col.max() == mc
+    assert _proper(g, col)
+    assert mc <= mc0
+
+
 @pytest.mark.parametrize('name', CASES)
 def test_decisions(name):
     g, z = load(name)
