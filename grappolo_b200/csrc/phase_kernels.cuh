@@ -928,4 +928,125 @@ __global__ void k_spec_split(int64_t n, const int32_t *list, const int64_t *ptr,
   }
 }
 
+// ---------------------------------------------------------------------------
+// Chunked coarsening (large levels outside verify mode): every CSR entry
+// i -> t with a = C[i] in [a0, a1) and b = C[t] >= 0 becomes one record
+// ((a - a0) << nb | b, w), plus a seed (a, a, 0.0) per community.  Sorting
+// and summing the records of a chunk gives its coarse rows whole (both
+// directions come from the symmetric input), in (a, b) order, so the chunks'
+// outputs laid end to end are the coarse CSR.  Equal to the two-sort path in
+// exact arithmetic (integral weights); the order of additions differs.
+
+// cnt[a] = 1 (its seed) + the entries of the rows in community a.
+__global__ void k_comm_entry_counts(int64_t nv, const int64_t *ptr, const int32_t *C,
+                                    int64_t *cnt) {
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t a = C[v];
+    const int64_t d = ptr[v + 1] - ptr[v];
+    if (a >= 0 && d > 0) atomicAdd((unsigned long long *)&cnt[a], (unsigned long long)d);
+  }
+}
+
+__global__ void k_fill_i64(int64_t n, int64_t *x, int64_t val) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = val;
+}
+
+// bounds[k] = the first community whose record prefix reaches k * total / K.
+__global__ void k_chunk_bounds(int64_t ncl, const int64_t *prefix, int K, int64_t *bounds) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k > K) return;
+  const int64_t total = prefix[ncl];
+  const int64_t target = (int64_t)((double)total * k / K);
+  int64_t lo = 0, hi = ncl;  // smallest a with prefix[a] >= target
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (prefix[mid] >= target) hi = mid; else lo = mid + 1;
+  }
+  bounds[k] = (k == K) ? ncl : lo;
+}
+
+// Records of the chunk [a0, a1) (merge-path tiles, warp-aggregated slots).
+__global__ void __launch_bounds__(256) k_chunk_records(
+    int64_t nv, int64_t nnz, const int64_t *ptr, const int32_t *tail, const double *w,
+    const int32_t *C, const int64_t *split_row, int32_t a0, int32_t a1, int nb,
+    unsigned long long *counter, uint64_t *keys, double *vals) {
+  __shared__ MergeSmem sm;
+  const int lane = threadIdx.x & 31;
+  // seeds
+  for (int64_t a = a0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < a1;
+       a += (int64_t)gridDim.x * blockDim.x) {
+    const unsigned long long s = atomicAdd(counter, 1ull);
+    keys[s] = ((uint64_t)(a - a0) << nb) | (uint64_t)a;
+    vals[s] = 0.0;
+  }
+  const int64_t ntiles = merge_tiles(nv, nnz);
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t d0 = tile * (int64_t)kMergeTile;
+    const int64_t d1 = min(d0 + (int64_t)kMergeTile, nv + nnz);
+    const int64_t i0 = split_row[tile], i1 = split_row[tile + 1];
+    const int64_t j0 = d0 - i0, j1 = d1 - i1;
+    if (j1 <= j0) continue;  // tile-uniform
+    const int64_t ih = min(i1, nv - 1);
+    const int nr = (int)(ih - i0 + 1);
+    __syncthreads();
+    for (int k = threadIdx.x; k <= nr; k += blockDim.x) {
+      const int64_t r = ptr[i0 + k] - j0;
+      sm.off[k] = (int32_t)max((int64_t)0, min(r, (int64_t)kMergeTile + 1));
+    }
+    for (int k = threadIdx.x; k < nr; k += blockDim.x) sm.comm[k] = C[i0 + k];
+    __syncthreads();
+    const int ne = (int)(j1 - j0);
+    // every lane of a warp runs the same trip count, so the ballot sees them all
+    const int trips = (ne + blockDim.x - 1) / blockDim.x;
+    for (int it = 0; it < trips; ++it) {
+      const int q = it * blockDim.x + threadIdx.x;
+      bool take = false;
+      uint64_t key = 0;
+      double val = 0.0;
+      if (q < ne) {
+        int lo = 0, hi = nr - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (sm.off[mid] <= q) lo = mid; else hi = mid - 1;
+        }
+        const int32_t a = sm.comm[lo];
+        if (a >= a0 && a < a1) {
+          const int64_t e = j0 + q;
+          const int32_t b = C[tail[e]];
+          if (b >= 0) {
+            take = true;
+            key = ((uint64_t)(a - a0) << nb) | (uint64_t)b;
+            val = w[e];
+          }
+        }
+      }
+      const unsigned m = __ballot_sync(FULL, take);
+      if (!m) continue;
+      unsigned long long base = 0;
+      if (lane == __ffs(m) - 1) base = atomicAdd(counter, (unsigned long long)__popc(m));
+      base = __shfl_sync(FULL, base, __ffs(m) - 1);
+      if (take) {
+        const unsigned long long s = base + __popc(m & ((1u << lane) - 1u));
+        keys[s] = key;
+        vals[s] = val;
+      }
+    }
+  }
+}
+
+// Row counts and the chunk's tails of its unique (a, b) pairs.
+__global__ void k_chunk_emit(int64_t np, const uint64_t *ukeys, int nb, int32_t a0,
+                             int64_t *rowc, int32_t *otail) {
+  const uint64_t mask = (1ull << nb) - 1;
+  for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np;
+       p += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t k = ukeys[p];
+    atomicAdd((unsigned long long *)&rowc[a0 + (int64_t)(k >> nb)], 1ull);
+    otail[p] = (int32_t)(k & mask);
+  }
+}
+
 }  // namespace glv

@@ -50,20 +50,19 @@ def test_batch_verify_vs_oracle(oracle):
         assert st['final_modularity'][k] == pytest.approx(so['final_mod'], rel=1e-12)
 
 
-def test_batch_fast_mode_matches_single_runs():
-    """Fast mode's colouring races, and on weakly structured graphs (mu up to
-    0.6) the final Q of two fast runs of one graph differs by up to a few
-    1e-3.  A batched graph must land inside the spread of its own single fast
-    runs (widened by that spread, at least by the fast-mode tolerance)."""
+def test_batch_fast_mode_matches_single_runs(monkeypatch):
+    """Fast mode's speculative colouring races, which spreads the final Q of
+    weakly structured graphs by a few 1e-3 from run to run (the reference's
+    own multi-thread runs spread the same way).  With the deterministic
+    id-order colouring and integral weights every other fast-mode sum is exact,
+    so a batched graph must get exactly the result of its own fast run."""
+    monkeypatch.setenv('GRAPPOLO_B200_COLORING', 'id')
     gs = _mixed_batch(seed=7, sizes=(3000, 30000, 60000, 1200))
     Cs, st = louvain.run_batch(gs, coloring=True, mode=_lib.GLV_MODE_FAST)
     for k, g in enumerate(gs):
-        singles = [louvain.run_multiphase_csr(g, mode=_lib.GLV_MODE_FAST)[1]['final_modularity']
-                   for _ in range(5)]
-        lo, hi = min(singles), max(singles)
-        slack = max(hi - lo, FAST_Q_TOL)
-        assert lo - slack <= st['final_modularity'][k] <= hi + slack, k
-        assert Cs[k].min() >= -1 and Cs[k].max() < g.num_vertices
+        C1, s1 = louvain.run_multiphase_csr(g, mode=_lib.GLV_MODE_FAST)
+        assert np.array_equal(Cs[k], C1), k
+        assert st['final_modularity'][k] == s1['final_modularity'], k
     assert np.all(st['done_seconds'] > 0)
 
 

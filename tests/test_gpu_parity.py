@@ -110,6 +110,33 @@ def test_coarsen(name):
 
 
 @pytest.mark.parametrize('name', CASES)
+def test_coarsen_chunked(name, monkeypatch):
+    """The chunked coarsening (forced, 7-record chunks, so communities are
+    spread over many chunks) builds the same coarse graph: bit for bit on
+    integral weights, to rounding on others (it adds in another order)."""
+    monkeypatch.setenv('GRAPPOLO_B200_COARSEN_CHUNK', '7')
+    g, z = load(name)
+    cg, ne = louvain.buildNextLevelGraphOpt(g, z['renum_C'], int(z['renum_n']), nThreads=8)
+    assert ne == z['coarse_ne']
+    assert np.array_equal(cg.ptr, z['coarse_ptr'])
+    assert np.array_equal(cg.tail, z['coarse_tail'])
+    np.testing.assert_allclose(cg.weight, z['coarse_weight'], rtol=1e-12, atol=1e-300)
+    if np.all(g.weight == np.round(g.weight)):
+        assert np.array_equal(cg.weight, z['coarse_weight'])
+
+
+@pytest.mark.parametrize('name', ['karate', 'pp1000', 'hubs', 'cycle4_ties'])
+def test_multiphase_verify_with_chunked_coarsening(name, monkeypatch):
+    """Integral weights: verify mode with every level coarsened in chunks still
+    gives the reference's one-thread community array."""
+    monkeypatch.setenv('GRAPPOLO_B200_COARSEN_CHUNK', '100')
+    g, z = load(name)
+    assert np.all(g.weight == np.round(g.weight))
+    C = louvain.runMultiPhaseColoring(g, numThreads=1)
+    assert np.array_equal(C, z['mpc_C'])
+
+
+@pytest.mark.parametrize('name', CASES)
 def test_multiphase_coloring_verify(name):
     g, z = load(name)
     C, st = louvain.runMultiPhaseColoring(g, numThreads=1, stats=True)
