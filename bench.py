@@ -44,7 +44,7 @@ def parse_args():
     p.add_argument('--warmup', type=int, default=3)
     p.add_argument('--impl', choices=['ours', 'reference'], default='ours')
     p.add_argument('--scale', type=int, default=24)
-    p.add_argument('--mode', choices=['fast', 'verify'], default='fast')
+    p.add_argument('--mode', choices=['fast', 'verify', 'learned'], default='fast')
     p.add_argument('--no-e2e', action='store_true')
     p.add_argument('--no-cpu-baseline', action='store_true')
     p.add_argument('--profile-level', type=int, default=1,
@@ -59,9 +59,12 @@ def parse_args():
 
 
 def workload_config(args, nv, nnz, extra=None):
-    cfg = {'workload': f'plain multiphase Louvain (coloring=1) on R-MAT scale {args.scale}',
+    kind = 'learned-gated' if args.mode == 'learned' else 'plain'
+    gen = ('bounded-scratch device builder, weights from an edge hash' if args.scale >= 26
+           else 'device builder')
+    cfg = {'workload': f'{kind} multiphase Louvain (coloring=1) on R-MAT scale {args.scale}',
            'graph': f'R-MAT scale {args.scale}, edge factor 16, a=0.57 b=0.19 c=0.19, '
-                    f'symmetrised, dedup, no self-loops, FP64 weights U(0,1], seed 1',
+                    f'symmetrised, dedup, no self-loops, FP64 weights U(0,1], seed 1 ({gen})',
            'num_vertices': nv, 'nnz': nnz, 'threshold': 1e-6, 'C_threshold': 1e-4,
            'minGraphSize': 1000, 'parallelism': f'replicas x{args.gpus}',
            'l2': 'inputs larger than L2 (no flush)'}
@@ -304,9 +307,17 @@ def main():
         dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=600),
                                 device_id=dev)
     L = _lib.lib()
-    mode = _lib.GLV_MODE_FAST if args.mode == 'fast' else _lib.GLV_MODE_VERIFY
+    mode = {'fast': _lib.GLV_MODE_FAST, 'verify': _lib.GLV_MODE_VERIFY,
+            'learned': _lib.GLV_MODE_LEARNED}[args.mode]
+    if args.mode == 'learned':
+        from grappolo_b200 import gate
+        gate.set_gate(*gate.load_default())
 
-    ptr, tail, w = graphs.rmat_device(args.scale, device=dev)
+    if args.scale >= 26:  # edge lists of tens of GB: the bounded-scratch builder
+        ptr, tail, w = graphs.rmat_device_lean(args.scale, device=dev)
+        torch.cuda.empty_cache()  # hand torch's freed scratch back for the engine's pool
+    else:
+        ptr, tail, w = graphs.rmat_device(args.scale, device=dev)
     nv, nnz = ptr.numel() - 1, tail.numel()
     C = torch.empty(nv, dtype=torch.int32, device=dev)
     torch.cuda.synchronize()

@@ -436,3 +436,80 @@ def planted_batch_device(specs, seed: int = 3, device='cuda', group_pairs: int =
     del tail_parts
     w = torch.ones(tail.numel(), dtype=torch.float64, device=device)
     return voff, ptr, tail, w
+
+
+def rmat_device_lean(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19,
+                     c: float = 0.19, seed: int = 1, device='cuda', chunk: int = 1 << 27):
+    """R-MAT in device memory for scales whose edge lists are tens of GB
+    (scale 26 and up): the construction of :func:`rmat_device` with bounded
+    scratch.  Edges are drawn in chunks into one key array, deduplicated by
+    one sort, and the CSR is filled by counting (rows sorted by tail) instead
+    of sorting the symmetric list.  Weights are U(0,1] from a hash of the
+    undirected edge, so both directions carry the same weight.  Returns
+    (ptr int64[NV+1], tail int32[nnz], weight float64[nnz]) on the device."""
+    import torch
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    nv = 1 << scale
+    m = edge_factor * nv
+    keys = torch.empty(m, dtype=torch.int64, device=device)
+    n = 0
+    ab, abc = a + b, a + b + c
+    for s0 in range(0, m, chunk):
+        k = min(chunk, m - s0)
+        u = torch.zeros(k, dtype=torch.int64, device=device)
+        v = torch.zeros(k, dtype=torch.int64, device=device)
+        for _ in range(scale):
+            r = torch.rand(k, generator=gen, device=device)
+            u = (u << 1) | (r >= ab).to(torch.int64)
+            v = (v << 1) | (((r >= a) & (r < ab)) | (r >= abc)).to(torch.int64)
+            del r
+        keep = u != v
+        kk = torch.minimum(u, v)[keep] * nv + torch.maximum(u, v)[keep]
+        keys[n:n + kk.numel()] = kk
+        n += kk.numel()
+        del u, v, keep, kk
+    keys = keys[:n]
+    keys, _ = torch.sort(keys)
+    keys = torch.unique_consecutive(keys)
+    ne = keys.numel()
+    lo = (keys // nv).to(torch.int32)
+    hi = (keys % nv).to(torch.int32)
+    # weight of each undirected edge: top 53 bits of a multiplicative hash
+    h = keys * (-7046029254386353131)  # 0x9E3779B97F4A7C15 as int64, wraps
+    del keys
+    wu = 1.0 - ((h >> 11) & ((1 << 53) - 1)).to(torch.float64) * (2.0 ** -53)
+    del h
+    cnt_lo = torch.bincount(lo, minlength=nv)
+    cnt_hi = torch.bincount(hi, minlength=nv)
+    ptr = torch.zeros(nv + 1, dtype=torch.int64, device=device)
+    ptr[1:] = torch.cumsum(cnt_lo + cnt_hi, 0)
+    nnz = int(ptr[-1])
+    tail = torch.empty(nnz, dtype=torch.int32, device=device)
+    w = torch.empty(nnz, dtype=torch.float64, device=device)
+    # row r = [tails below r (edges (x, r), x ascending)] then [tails above r]
+    first_lo = torch.zeros(nv + 1, dtype=torch.int64, device=device)
+    first_lo[1:] = torch.cumsum(cnt_lo, 0)
+    first_hi = torch.zeros(nv + 1, dtype=torch.int64, device=device)
+    first_hi[1:] = torch.cumsum(cnt_hi, 0)
+    # upper part: the key order is (lo, hi), so each lo's edges are a run
+    for s0 in range(0, ne, chunk):
+        i = torch.arange(s0, min(ne, s0 + chunk), device=device, dtype=torch.int64)
+        r = lo[i].to(torch.int64)
+        at = ptr[r] + cnt_hi[r] + (i - first_lo[r])
+        tail[at] = hi[i]
+        w[at] = wu[i]
+        del i, r, at
+    # lower part: a stable sort by hi keeps each hi's edges in ascending lo
+    hs, perm = torch.sort(hi, stable=True)
+    del hs
+    for s0 in range(0, ne, chunk):
+        kx = torch.arange(s0, min(ne, s0 + chunk), device=device, dtype=torch.int64)
+        p = perm[kx]
+        r = hi[p].to(torch.int64)
+        at = ptr[r] + (kx - first_hi[r])
+        tail[at] = lo[p]
+        w[at] = wu[p]
+        del kx, p, r, at
+    del perm, lo, hi, wu, cnt_lo, cnt_hi, first_lo, first_hi
+    return ptr, tail, w

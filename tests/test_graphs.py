@@ -97,3 +97,21 @@ def test_planted_batch_generator_on_cpu():
     assert np.all(np.diff(key) > 0) and np.all(heads != t)
     assert np.array_equal(np.sort(t * n + heads), key)
     assert np.all(w.numpy() == 1.0)
+
+
+def test_rmat_lean_generator_on_cpu():
+    """The bounded-scratch R-MAT builder (torch on the CPU here): rows sorted
+    by tail, no duplicates or self-loops, symmetric with equal weights, U(0,1]."""
+    ptr, tail, w = graphs.rmat_device_lean(11, device='cpu', chunk=3000)
+    p = ptr.numpy()
+    t = tail.numpy().astype(np.int64)
+    ww = w.numpy()
+    nv = p.size - 1
+    heads = np.repeat(np.arange(nv), np.diff(p))
+    key = heads * nv + t
+    assert np.all(np.diff(key) > 0) and np.all(heads != t)
+    rev = t * nv + heads
+    o = np.argsort(rev)
+    assert np.array_equal(rev[o], key)
+    assert np.array_equal(ww[o], ww)
+    assert ww.min() > 0 and ww.max() <= 1
