@@ -770,6 +770,8 @@ static int upload(cudaStream_t s, T *dst, const std::vector<T> &src) {
 // the parallel path gives every hub of the schedule a private table, cut its
 // row into kHubChunk-entry chunks and its filled-slot list into kHubSeg
 // segments.
+constexpr size_t kHubStepSlots = size_t(1) << 28;  // hub table slots of one step (3 GB)
+
 int Engine::hub_offsets(const Level &L, std::vector<ClassSched> &sched) {
   const bool parallel = !ordered();
   std::vector<int64_t> tab_off, occ_off, seg_b, seg_e;
@@ -796,6 +798,41 @@ int Engine::hub_offsets(const Level &L, std::vector<ClassSched> &sched) {
     CK(cudaStreamSynchronize(s_));
     dfree(d_pos);
     dfree(bounds);
+  }
+  // A step whose hubs' tables would pass kHubStepSlots is cut into several
+  // steps of the same class (its other bins stay in the first): members of a
+  // class are independent and its deltas are applied after its last step, so
+  // the decisions do not change.
+  if (!hpos.empty()) {
+    size_t hc = 0;
+    for (auto &cs : sched) {
+      std::vector<Step> out;
+      for (auto &st : cs.steps) {
+        const int64_t b = st.seg[BIN_HUB], e = st.seg[BIN_HUB + 1];
+        size_t acc = 0;
+        int64_t cut = b;
+        Step cur = st;
+        for (int64_t k = b; k < e; ++k) {
+          const int64_t deg = hb_all[2 * (hc + (k - b)) + 1] - hb_all[2 * (hc + (k - b))];
+          const size_t cap = table_cap(deg);
+          if (acc > 0 && acc + cap > kHubStepSlots) {
+            cur.seg[BIN_HUB] = cut;
+            for (int q = BIN_HUB + 1; q <= NBINS; ++q) cur.seg[q] = k;
+            out.push_back(cur);
+            Step nx;
+            for (int q = 0; q <= BIN_HUB; ++q) nx.seg[q] = k;
+            for (int q = BIN_HUB + 1; q <= NBINS; ++q) nx.seg[q] = e;
+            cur = nx;
+            cut = k;
+            acc = 0;
+          }
+          acc += cap;
+        }
+        hc += (size_t)(e - b);
+        out.push_back(cur);
+      }
+      cs.steps = out;
+    }
   }
   size_t hcur = 0;
   size_t need_occ = 0;
@@ -1748,7 +1785,9 @@ int Engine::coarsen(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
   const int g = grid_for(n, 256, nsm_ * 16);
   if (n > crec_cap_) {
     dfree(ck1_); dfree(ck2_); dfree(cv1_); dfree(cv2_);
-    crec_cap_ = std::max<int64_t>(n, nnz0_ + nv0_);
+    // sized for level 0 when that is modest, so every level reuses them
+    const int64_t lvl0 = nnz0_ + nv0_;
+    crec_cap_ = lvl0 <= (int64_t(1) << 30) ? std::max<int64_t>(n, lvl0) : n;
     TRY(alloc(&ck1_, crec_cap_)); TRY(alloc(&ck2_, crec_cap_));
     TRY(alloc(&cv1_, crec_cap_)); TRY(alloc(&cv2_, crec_cap_));
   }
