@@ -1688,42 +1688,104 @@ int Engine::coarsen_chunked(const Level &in, const int32_t *Cm, int64_t ncl, Lev
   CK(cudaStreamSynchronize(s_));
   int64_t maxrec = 1;
   for (int k = 0; k < K; ++k) maxrec = std::max(maxrec, hp[k + 1] - hp[k]);
-  uint64_t *k1, *k2, *uk;
-  double *v1, *v2, *uv;
+  // record buffers of at most 2 x budget entries; a chunk with more records
+  // (one community with a huge row sum) is read in tile slices whose partial
+  // sums are gathered in the accumulation buffer and reduced once more
+  const int64_t cap = std::min<int64_t>(maxrec, 2 * budget);
+  uint64_t *k1, *k2, *uk, *ak;
+  double *v1, *v2, *uv, *av;
   unsigned long long *counter;
   int64_t *d_np;
-  TRY(alloc(&k1, maxrec)); TRY(alloc(&k2, maxrec)); TRY(alloc(&uk, maxrec));
-  TRY(alloc(&v1, maxrec)); TRY(alloc(&v2, maxrec)); TRY(alloc(&uv, maxrec));
+  TRY(alloc(&k1, cap)); TRY(alloc(&k2, cap)); TRY(alloc(&uk, cap));
+  TRY(alloc(&v1, cap)); TRY(alloc(&v2, cap)); TRY(alloc(&uv, cap));
   TRY(alloc(&counter, 1)); TRY(alloc(&d_np, 1));
+  const bool sliced = maxrec > cap;
+  ak = nullptr;
+  av = nullptr;
+  if (sliced) { TRY(alloc(&ak, cap)); TRY(alloc(&av, cap)); }
   CK(cudaMemsetAsync(rowc, 0, (ncl + 1) * sizeof(int64_t), s_));
   TRY(merge_splits(in));
   struct Part { int32_t *t; double *w; int64_t n; };
   std::vector<Part> parts;
-  const int grid = std::max(1, (int)std::min<int64_t>(merge_tiles(in.nv, in.nnz), nsm_ * 8));
-  for (int k = 0; k < K; ++k) {
-    const int64_t a0 = hb[k], a1 = hb[k + 1];
-    if (a1 <= a0) continue;
-    CK(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s_));
-    LAUNCH(k_chunk_records, grid, 256, 0, s_, in.nv, in.nnz, in.ptr, in.tail, in.w, Cm,
-           split_row_, (int32_t)a0, (int32_t)a1, nb, counter, k1, v1);
-    unsigned long long hn = 0;
-    CK(cudaMemcpyAsync(&hn, counter, sizeof(hn), cudaMemcpyDeviceToHost, s_));
-    CK(cudaStreamSynchronize(s_));
-    const int64_t n = (int64_t)hn;
-    const int end_bit = nb + bits_for(std::max<int64_t>(a1 - a0 - 1, 1));
-    cub::DoubleBuffer<uint64_t> dk(k1, k2);
-    cub::DoubleBuffer<double> dv(v1, v2);
+  const int64_t ntiles = merge_tiles(in.nv, in.nnz);
+  const int grid = std::max(1, (int)std::min<int64_t>(ntiles, nsm_ * 8));
+  // sort + reduce n records of (kin, vin) into (kout, vout); returns the pairs
+  auto sort_reduce = [&](uint64_t *ka, uint64_t *kb, double *va, double *vb, int64_t n,
+                         int end_bit, uint64_t *kout, double *vout, int64_t *np) -> int {
+    cub::DoubleBuffer<uint64_t> dk(ka, kb);
+    cub::DoubleBuffer<double> dv(va, vb);
     CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, dk, dv, n, 0, end_bit, s_));
     TRY(temp(tb));
     CK(cub::DeviceRadixSort::SortPairs(temp_, tb, dk, dv, n, 0, end_bit, s_));
-    CK(cub::DeviceReduce::ReduceByKey(nullptr, tb, dk.Current(), uk, dv.Current(), uv, d_np,
+    CK(cub::DeviceReduce::ReduceByKey(nullptr, tb, dk.Current(), kout, dv.Current(), vout, d_np,
                                       cuda::std::plus<>{}, n, s_));
     TRY(temp(tb));
-    CK(cub::DeviceReduce::ReduceByKey(temp_, tb, dk.Current(), uk, dv.Current(), uv, d_np,
+    CK(cub::DeviceReduce::ReduceByKey(temp_, tb, dk.Current(), kout, dv.Current(), vout, d_np,
                                       cuda::std::plus<>{}, n, s_));
-    int64_t np = 0;
-    CK(cudaMemcpyAsync(&np, d_np, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
+    CK(cudaMemcpyAsync(np, d_np, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
     CK(cudaStreamSynchronize(s_));
+    return GLV_OK;
+  };
+  // records of tiles [t0, t1) into (k1, v1); returns their count (may pass cap)
+  auto records = [&](int64_t a0, int64_t a1, int64_t t0, int64_t t1, int seeds,
+                     int64_t *n) -> int {
+    CK(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s_));
+    LAUNCH(k_chunk_records, grid, 256, 0, s_, in.nv, in.nnz, in.ptr, in.tail, in.w, Cm,
+           split_row_, (int32_t)a0, (int32_t)a1, nb, t0, t1, seeds, (unsigned long long)cap,
+           counter, k1, v1);
+    unsigned long long hn = 0;
+    CK(cudaMemcpyAsync(&hn, counter, sizeof(hn), cudaMemcpyDeviceToHost, s_));
+    CK(cudaStreamSynchronize(s_));
+    *n = (int64_t)hn;
+    return GLV_OK;
+  };
+  for (int k = 0; k < K; ++k) {
+    const int64_t a0 = hb[k], a1 = hb[k + 1];
+    if (a1 <= a0) continue;
+    const int end_bit = nb + bits_for(std::max<int64_t>(a1 - a0 - 1, 1));
+    int64_t np = 0;
+    if (hp[k + 1] - hp[k] <= cap) {
+      int64_t n = 0;
+      TRY(records(a0, a1, 0, ntiles, 1, &n));
+      TRY(sort_reduce(k1, k2, v1, v2, n, end_bit, uk, uv, &np));
+    } else {
+      // slices of tiles; a slice whose records overflow is cut in two
+      int64_t acc = 0;
+      std::vector<std::pair<int64_t, int64_t>> todo;
+      const int64_t nsl = 2 * ((hp[k + 1] - hp[k] + cap - 1) / cap);
+      for (int64_t q = nsl - 1; q >= 0; --q)
+        todo.push_back({ntiles * q / nsl, ntiles * (q + 1) / nsl});
+      bool first = true;
+      while (!todo.empty()) {
+        const auto sl = todo.back();
+        todo.pop_back();
+        int64_t n = 0;
+        TRY(records(a0, a1, sl.first, sl.second, first ? 1 : 0, &n));
+        if (n > cap) {
+          if (sl.second - sl.first <= 1)
+            return fail(GLV_ERR_OOM, "a coarsening tile exceeds the record buffer");
+          const int64_t mid = (sl.first + sl.second) / 2;
+          todo.push_back({mid, sl.second});
+          todo.push_back({sl.first, mid});
+          continue;
+        }
+        first = false;
+        int64_t pn = 0;
+        TRY(sort_reduce(k1, k2, v1, v2, n, end_bit, uk, uv, &pn));
+        if (acc + pn > cap) {  // fold what has been gathered so far
+          int64_t an = 0;
+          TRY(sort_reduce(ak, k1, av, v1, acc, end_bit, k2, v2, &an));
+          CK(cudaMemcpyAsync(ak, k2, an * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s_));
+          CK(cudaMemcpyAsync(av, v2, an * sizeof(double), cudaMemcpyDeviceToDevice, s_));
+          acc = an;
+          if (acc + pn > cap) return fail(GLV_ERR_OOM, "coarsening partial sums exceed the buffer");
+        }
+        CK(cudaMemcpyAsync(ak + acc, uk, pn * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s_));
+        CK(cudaMemcpyAsync(av + acc, uv, pn * sizeof(double), cudaMemcpyDeviceToDevice, s_));
+        acc += pn;
+      }
+      TRY(sort_reduce(ak, k1, av, v1, acc, end_bit, uk, uv, &np));
+    }
     Part pt{nullptr, nullptr, np};
     TRY(alloc(&pt.t, np)); TRY(alloc(&pt.w, np));
     LAUNCH(k_chunk_emit, grid_for(np, 256, nsm_ * 16), 256, 0, s_, np, uk, nb, (int32_t)a0, rowc,
@@ -1731,6 +1793,7 @@ int Engine::coarsen_chunked(const Level &in, const int32_t *Cm, int64_t ncl, Lev
     CK(cudaMemcpyAsync(pt.w, uv, np * sizeof(double), cudaMemcpyDeviceToDevice, s_));
     parts.push_back(pt);
   }
+  dfree(ak); dfree(av);
   dfree(k1); dfree(k2); dfree(uk); dfree(v1); dfree(v2); dfree(uv);
   dfree(counter); dfree(d_np); dfree(bounds); dfree(pb); dfree(cnt); dfree(prefix);
   Level o;
@@ -1765,7 +1828,7 @@ int Engine::coarsen(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
   // GRAPPOLO_B200_COARSEN_CHUNK=<records> forces it with that chunk size.
   {
     const char *cc = getenv("GRAPPOLO_B200_COARSEN_CHUNK");
-    const int64_t budget = cc ? std::max<int64_t>(atoll(cc), 1) : (int64_t(1) << 28);
+    const int64_t budget = cc ? std::max<int64_t>(atoll(cc), 1) : (int64_t(1) << 27);
     if (!ordered() && ncl > 0 && (cc || ncl + in.nnz > (int64_t(1) << 30)))
       return coarsen_chunked(in, Cm, ncl, out, num_edges, budget);
   }

@@ -969,21 +969,27 @@ __global__ void k_chunk_bounds(int64_t ncl, const int64_t *prefix, int K, int64_
 }
 
 // Records of the chunk [a0, a1) (merge-path tiles, warp-aggregated slots).
+// Only tiles [t0, t1) are read (a chunk too large for the buffer is done in
+// slices); seeds come with the slice that has `seeds` set; records past `cap`
+// are counted but not written (the caller then cuts the slice finer).
 __global__ void __launch_bounds__(256) k_chunk_records(
     int64_t nv, int64_t nnz, const int64_t *ptr, const int32_t *tail, const double *w,
-    const int32_t *C, const int64_t *split_row, int32_t a0, int32_t a1, int nb,
-    unsigned long long *counter, uint64_t *keys, double *vals) {
+    const int32_t *C, const int64_t *split_row, int32_t a0, int32_t a1, int nb, int64_t t0,
+    int64_t t1, int seeds, unsigned long long cap, unsigned long long *counter, uint64_t *keys,
+    double *vals) {
   __shared__ MergeSmem sm;
   const int lane = threadIdx.x & 31;
-  // seeds
-  for (int64_t a = a0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < a1;
-       a += (int64_t)gridDim.x * blockDim.x) {
-    const unsigned long long s = atomicAdd(counter, 1ull);
-    keys[s] = ((uint64_t)(a - a0) << nb) | (uint64_t)a;
-    vals[s] = 0.0;
+  if (seeds) {
+    for (int64_t a = a0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < a1;
+         a += (int64_t)gridDim.x * blockDim.x) {
+      const unsigned long long s = atomicAdd(counter, 1ull);
+      if (s < cap) {
+        keys[s] = ((uint64_t)(a - a0) << nb) | (uint64_t)a;
+        vals[s] = 0.0;
+      }
+    }
   }
-  const int64_t ntiles = merge_tiles(nv, nnz);
-  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+  for (int64_t tile = t0 + blockIdx.x; tile < t1; tile += gridDim.x) {
     const int64_t d0 = tile * (int64_t)kMergeTile;
     const int64_t d1 = min(d0 + (int64_t)kMergeTile, nv + nnz);
     const int64_t i0 = split_row[tile], i1 = split_row[tile + 1];
@@ -1030,8 +1036,10 @@ __global__ void __launch_bounds__(256) k_chunk_records(
       base = __shfl_sync(FULL, base, __ffs(m) - 1);
       if (take) {
         const unsigned long long s = base + __popc(m & ((1u << lane) - 1u));
-        keys[s] = key;
-        vals[s] = val;
+        if (s < cap) {
+          keys[s] = key;
+          vals[s] = val;
+        }
       }
     }
   }
