@@ -1691,7 +1691,12 @@ int Engine::coarsen_chunked(const Level &in, const int32_t *Cm, int64_t ncl, Lev
   // record buffers of at most 2 x budget entries; a chunk with more records
   // (one community with a huge row sum) is read in tile slices whose partial
   // sums are gathered in the accumulation buffer and reduced once more
-  const int64_t cap = std::min<int64_t>(maxrec, 2 * budget);
+  // (never below one tile's records plus a chunk's seeds: a slice is at
+  // least one merge-path tile)
+  int64_t maxseeds = 1;
+  for (int k = 0; k < K; ++k) maxseeds = std::max(maxseeds, hb[k + 1] - hb[k]);
+  const int64_t cap =
+      std::min<int64_t>(maxrec, std::max<int64_t>(2 * budget, 2 * kMergeTile + maxseeds));
   uint64_t *k1, *k2, *uk, *ak;
   double *v1, *v2, *uv, *av;
   unsigned long long *counter;
