@@ -269,6 +269,12 @@ class Engine {
   int alloc(T **p, size_t n) {
     if (!pool_) pool_ = engine_pool();
     if (!pool_) return fail(GLV_ERR_CUDA, "could not create the device memory pool");
+    if (n * sizeof(T) >= (size_t(1) << 30) && getenv("GRAPPOLO_B200_DEBUG")) {
+      uint64_t used = 0;
+      cudaMemPoolGetAttribute(pool_, cudaMemPoolAttrUsedMemCurrent, &used);
+      fprintf(stderr, "grappolo_b200: alloc %.2f GB (pool used %.2f GB)\n",
+              n * sizeof(T) * 1e-9, used * 1e-9);
+    }
     CK(cudaMallocFromPoolAsync((void **)p, size_class(std::max<size_t>(n, 1) * sizeof(T)), pool_,
                                s_));
     return GLV_OK;
@@ -1710,8 +1716,14 @@ int Engine::coarsen_chunked(const Level &in, const int32_t *Cm, int64_t ncl, Lev
   if (sliced) { TRY(alloc(&ak, cap)); TRY(alloc(&av, cap)); }
   CK(cudaMemsetAsync(rowc, 0, (ncl + 1) * sizeof(int64_t), s_));
   TRY(merge_splits(in));
-  struct Part { int32_t *t; double *w; int64_t n; };
-  std::vector<Part> parts;
+  // the coarse rows go straight to their place: `total` (records of all
+  // chunks) bounds the coarse entries, and a copy of the chunks' outputs
+  // would double the peak on levels of billions of entries
+  Level o;
+  o.nv = ncl;
+  o.owned = true;
+  TRY(alloc(&o.tail, std::max<int64_t>(total, 1))); TRY(alloc(&o.w, std::max<int64_t>(total, 1)));
+  int64_t at = 0;
   const int64_t ntiles = merge_tiles(in.nv, in.nnz);
   const int grid = std::max(1, (int)std::min<int64_t>(ntiles, nsm_ * 8));
   // sort + reduce n records of (kin, vin) into (kout, vout); returns the pairs
@@ -1791,34 +1803,19 @@ int Engine::coarsen_chunked(const Level &in, const int32_t *Cm, int64_t ncl, Lev
       }
       TRY(sort_reduce(ak, k1, av, v1, acc, end_bit, uk, uv, &np));
     }
-    Part pt{nullptr, nullptr, np};
-    TRY(alloc(&pt.t, np)); TRY(alloc(&pt.w, np));
     LAUNCH(k_chunk_emit, grid_for(np, 256, nsm_ * 16), 256, 0, s_, np, uk, nb, (int32_t)a0, rowc,
-           pt.t);
-    CK(cudaMemcpyAsync(pt.w, uv, np * sizeof(double), cudaMemcpyDeviceToDevice, s_));
-    parts.push_back(pt);
+           o.tail + at);
+    CK(cudaMemcpyAsync(o.w + at, uv, np * sizeof(double), cudaMemcpyDeviceToDevice, s_));
+    at += np;
   }
   dfree(ak); dfree(av);
   dfree(k1); dfree(k2); dfree(uk); dfree(v1); dfree(v2); dfree(uv);
   dfree(counter); dfree(d_np); dfree(bounds); dfree(pb); dfree(cnt); dfree(prefix);
-  Level o;
-  o.nv = ncl;
-  o.owned = true;
   TRY(alloc(&o.ptr, ncl + 1));
   CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, rowc, o.ptr, ncl + 1, s_));
   TRY(temp(tb));
   CK(cub::DeviceScan::ExclusiveSum(temp_, tb, rowc, o.ptr, ncl + 1, s_));
-  o.nnz = 0;
-  for (auto &pt : parts) o.nnz += pt.n;
-  TRY(alloc(&o.tail, o.nnz)); TRY(alloc(&o.w, o.nnz));
-  int64_t at = 0;
-  for (auto &pt : parts) {
-    CK(cudaMemcpyAsync(o.tail + at, pt.t, pt.n * sizeof(int32_t), cudaMemcpyDeviceToDevice, s_));
-    CK(cudaMemcpyAsync(o.w + at, pt.w, pt.n * sizeof(double), cudaMemcpyDeviceToDevice, s_));
-    at += pt.n;
-    dfree(pt.t);
-    dfree(pt.w);
-  }
+  o.nnz = at;
   dfree(rowc);
   CK(cudaStreamSynchronize(s_));
   *out = o;
