@@ -275,8 +275,16 @@ class Engine {
       fprintf(stderr, "grappolo_b200: alloc %.2f GB (pool used %.2f GB)\n",
               n * sizeof(T) * 1e-9, used * 1e-9);
     }
-    CK(cudaMallocFromPoolAsync((void **)p, size_class(std::max<size_t>(n, 1) * sizeof(T)), pool_,
-                               s_));
+    const size_t bytes = size_class(std::max<size_t>(n, 1) * sizeof(T));
+    cudaError_t e = cudaMallocFromPoolAsync((void **)p, bytes, pool_, s_);
+    if (e == cudaErrorMemoryAllocation) {
+      // the pool keeps freed blocks; hand the unused ones back and retry once
+      cudaGetLastError();
+      cudaStreamSynchronize(s_);
+      cudaMemPoolTrimTo(pool_, 0);
+      e = cudaMallocFromPoolAsync((void **)p, bytes, pool_, s_);
+    }
+    CK(e);
     return GLV_OK;
   }
   template <class T>
@@ -1722,7 +1730,6 @@ int Engine::coarsen_chunked(const Level &in, const int32_t *Cm, int64_t ncl, Lev
   Level o;
   o.nv = ncl;
   o.owned = true;
-  TRY(alloc(&o.tail, std::max<int64_t>(total, 1))); TRY(alloc(&o.w, std::max<int64_t>(total, 1)));
   int64_t at = 0;
   const int64_t ntiles = merge_tiles(in.nv, in.nnz);
   const int grid = std::max(1, (int)std::min<int64_t>(ntiles, nsm_ * 8));
@@ -1756,57 +1763,73 @@ int Engine::coarsen_chunked(const Level &in, const int32_t *Cm, int64_t ncl, Lev
     *n = (int64_t)hn;
     return GLV_OK;
   };
-  for (int k = 0; k < K; ++k) {
-    const int64_t a0 = hb[k], a1 = hb[k + 1];
-    if (a1 <= a0) continue;
-    const int end_bit = nb + bits_for(std::max<int64_t>(a1 - a0 - 1, 1));
-    int64_t np = 0;
-    if (hp[k + 1] - hp[k] <= cap) {
-      int64_t n = 0;
-      TRY(records(a0, a1, 0, ntiles, 1, &n));
-      TRY(sort_reduce(k1, k2, v1, v2, n, end_bit, uk, uv, &np));
-    } else {
-      // slices of tiles; a slice whose records overflow is cut in two
-      int64_t acc = 0;
-      std::vector<std::pair<int64_t, int64_t>> todo;
-      const int64_t nsl = 2 * ((hp[k + 1] - hp[k] + cap - 1) / cap);
-      for (int64_t q = nsl - 1; q >= 0; --q)
-        todo.push_back({ntiles * q / nsl, ntiles * (q + 1) / nsl});
-      bool first = true;
-      while (!todo.empty()) {
-        const auto sl = todo.back();
-        todo.pop_back();
-        int64_t n = 0;
-        TRY(records(a0, a1, sl.first, sl.second, first ? 1 : 0, &n));
-        if (n > cap) {
-          if (sl.second - sl.first <= 1)
-            return fail(GLV_ERR_OOM, "a coarsening tile exceeds the record buffer");
-          const int64_t mid = (sl.first + sl.second) / 2;
-          todo.push_back({mid, sl.second});
-          todo.push_back({sl.first, mid});
-          continue;
-        }
-        first = false;
-        int64_t pn = 0;
-        TRY(sort_reduce(k1, k2, v1, v2, n, end_bit, uk, uv, &pn));
-        if (acc + pn > cap) {  // fold what has been gathered so far
-          int64_t an = 0;
-          TRY(sort_reduce(ak, k1, av, v1, acc, end_bit, k2, v2, &an));
-          CK(cudaMemcpyAsync(ak, k2, an * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s_));
-          CK(cudaMemcpyAsync(av, v2, an * sizeof(double), cudaMemcpyDeviceToDevice, s_));
-          acc = an;
-          if (acc + pn > cap) return fail(GLV_ERR_OOM, "coarsening partial sums exceed the buffer");
-        }
-        CK(cudaMemcpyAsync(ak + acc, uk, pn * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s_));
-        CK(cudaMemcpyAsync(av + acc, uv, pn * sizeof(double), cudaMemcpyDeviceToDevice, s_));
-        acc += pn;
-      }
-      TRY(sort_reduce(ak, k1, av, v1, acc, end_bit, uk, uv, &np));
+  // The coarse rows go straight to their place.  `total` (records of all
+  // chunks) bounds the coarse entries; when that bound is large the chunks
+  // are run twice, first only to count, so the level gets its exact size.
+  const bool two_pass = total * (int64_t)(sizeof(int32_t) + sizeof(double)) > (int64_t(16) << 30) ||
+                        getenv("GRAPPOLO_B200_COARSEN_EXACT") != nullptr;
+  for (int pass = two_pass ? 0 : 1; pass < 2; ++pass) {
+    const bool counting = pass == 0;
+    if (!counting) {
+      const int64_t n_out = two_pass ? at : total;
+      TRY(alloc(&o.tail, std::max<int64_t>(n_out, 1)));
+      TRY(alloc(&o.w, std::max<int64_t>(n_out, 1)));
+      at = 0;
     }
-    LAUNCH(k_chunk_emit, grid_for(np, 256, nsm_ * 16), 256, 0, s_, np, uk, nb, (int32_t)a0, rowc,
-           o.tail + at);
-    CK(cudaMemcpyAsync(o.w + at, uv, np * sizeof(double), cudaMemcpyDeviceToDevice, s_));
-    at += np;
+    for (int k = 0; k < K; ++k) {
+      const int64_t a0 = hb[k], a1 = hb[k + 1];
+      if (a1 <= a0) continue;
+      const int end_bit = nb + bits_for(std::max<int64_t>(a1 - a0 - 1, 1));
+      int64_t np = 0;
+      if (hp[k + 1] - hp[k] <= cap) {
+        int64_t n = 0;
+        TRY(records(a0, a1, 0, ntiles, 1, &n));
+        TRY(sort_reduce(k1, k2, v1, v2, n, end_bit, uk, uv, &np));
+      } else {
+        // slices of tiles; a slice whose records overflow is cut in two
+        int64_t acc = 0;
+        std::vector<std::pair<int64_t, int64_t>> todo;
+        const int64_t nsl = 2 * ((hp[k + 1] - hp[k] + cap - 1) / cap);
+        for (int64_t q = nsl - 1; q >= 0; --q)
+          todo.push_back({ntiles * q / nsl, ntiles * (q + 1) / nsl});
+        bool first = true;
+        while (!todo.empty()) {
+          const auto sl = todo.back();
+          todo.pop_back();
+          int64_t n = 0;
+          TRY(records(a0, a1, sl.first, sl.second, first ? 1 : 0, &n));
+          if (n > cap) {
+            if (sl.second - sl.first <= 1)
+              return fail(GLV_ERR_OOM, "a coarsening tile exceeds the record buffer");
+            const int64_t mid = (sl.first + sl.second) / 2;
+            todo.push_back({mid, sl.second});
+            todo.push_back({sl.first, mid});
+            continue;
+          }
+          first = false;
+          int64_t pn = 0;
+          TRY(sort_reduce(k1, k2, v1, v2, n, end_bit, uk, uv, &pn));
+          if (acc + pn > cap) {  // fold what has been gathered so far
+            int64_t an = 0;
+            TRY(sort_reduce(ak, k1, av, v1, acc, end_bit, k2, v2, &an));
+            CK(cudaMemcpyAsync(ak, k2, an * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s_));
+            CK(cudaMemcpyAsync(av, v2, an * sizeof(double), cudaMemcpyDeviceToDevice, s_));
+            acc = an;
+            if (acc + pn > cap) return fail(GLV_ERR_OOM, "coarsening partial sums exceed the buffer");
+          }
+          CK(cudaMemcpyAsync(ak + acc, uk, pn * sizeof(uint64_t), cudaMemcpyDeviceToDevice, s_));
+          CK(cudaMemcpyAsync(av + acc, uv, pn * sizeof(double), cudaMemcpyDeviceToDevice, s_));
+          acc += pn;
+        }
+        TRY(sort_reduce(ak, k1, av, v1, acc, end_bit, uk, uv, &np));
+      }
+      if (!counting) {
+        LAUNCH(k_chunk_emit, grid_for(np, 256, nsm_ * 16), 256, 0, s_, np, uk, nb, (int32_t)a0,
+               rowc, o.tail + at);
+        CK(cudaMemcpyAsync(o.w + at, uv, np * sizeof(double), cudaMemcpyDeviceToDevice, s_));
+      }
+      at += np;
+    }
   }
   dfree(ak); dfree(av);
   dfree(k1); dfree(k2); dfree(uk); dfree(v1); dfree(v2); dfree(uv);
