@@ -102,7 +102,8 @@ def lib():
                  'glv_renumber_clusters', 'glv_build_next_level', 'glv_modularity',
                  'glv_decide_batch', 'glv_dev_modularity_static', 'glv_gate_set',
                  'glv_gate_infer', 'glv_gate_grad', 'glv_gate_train', 'glv_trace_begin',
-                 'glv_trace_end', 'glv_run_batch_csr', 'glv_dev_run_batch'):
+                 'glv_trace_end', 'glv_run_batch_csr', 'glv_dev_run_batch',
+                 'glv_vertex_following', 'glv_build_new_graph_vf'):
         getattr(L, name).restype = ct.c_int
     L.glv_run_multiphase_coloring.argtypes = [P(GlvGraph), P(ct.c_long), ct.c_int, ct.c_int,
                                               ct.c_int, ct.c_long, ct.c_double, ct.c_double,
@@ -131,6 +132,9 @@ def lib():
     L.glv_build_next_level.argtypes = [P(GlvGraph), P(GlvGraph), P(ct.c_long), ct.c_long,
                                        ct.c_int, P(ct.c_double)]
     L.glv_modularity.argtypes = [P(GlvGraph), P(ct.c_long), P(ct.c_double)]
+    L.glv_vertex_following.argtypes = [P(GlvGraph), P(ct.c_long), P(ct.c_long)]
+    L.glv_build_new_graph_vf.argtypes = [P(GlvGraph), P(GlvGraph), P(ct.c_long), ct.c_long,
+                                         P(ct.c_double)]
     L.glv_decide_batch.argtypes = [ct.c_long, P(ct.c_long), P(ct.c_long), P(ct.c_double),
                                    P(ct.c_long), P(ct.c_double), P(ct.c_double), P(ct.c_long),
                                    ct.c_double, ct.c_long, P(ct.c_long), P(ct.c_long)]

@@ -108,6 +108,21 @@ long renumberClustersContiguously(long *C, long size) {
   return n;
 }
 
+long vertexFollowing(graph *G, long *C) {
+  long n = 0;
+  int rc = glv_vertex_following((const glv_graph *)G, C, &n);
+  if (rc != GLV_OK) die("vertexFollowing", rc);
+  return n;
+}
+
+double buildNewGraphVF(graph *Gin, graph *Gout, long *C, long numUniqueClusters) {
+  double t = 0;
+  int rc = glv_build_new_graph_vf((const glv_graph *)Gin, (glv_graph *)Gout, C, numUniqueClusters,
+                                  &t);
+  if (rc != GLV_OK) die("buildNewGraphVF", rc);
+  return t;
+}
+
 double buildNextLevelGraphOpt(graph *Gin, graph *Gout, long *C, long numUniqueClusters,
                               int nThreads) {
   double t = 0;

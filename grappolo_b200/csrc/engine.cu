@@ -219,7 +219,7 @@ class Engine {
   int renumber(int32_t *C, int64_t n, int64_t *ncl);
   int coarsen(const Level &in, const int32_t *C, int64_t ncl, Level *out, int64_t *num_edges);
   int coarsen_chunked(const Level &in, const int32_t *C, int64_t ncl, Level *out,
-                      int64_t *num_edges, int64_t budget);
+                      int64_t *num_edges, int64_t budget, bool vf = false);
   int modularity_of(const Level &L, const int32_t *C, double *q);
   int decide(const Level &L, const int32_t *verts, int64_t nverts);
   int run_multiphase(const Level &L0, int32_t *d_C_orig, bool coloring, long min_graph_size,
@@ -1675,12 +1675,14 @@ __global__ void k_add_counts(int64_t n, const int64_t *a, const int64_t *b, int6
 // Chunked coarsening (phase_kernels.cuh): records for one range of row
 // communities at a time, at most about `budget` records per chunk, so a level
 // of billions of entries needs a fraction of the two-sort path's buffers.
+// vf: the vertex-following graph (Utility/vertexFollowing.cpp:91-255) — no
+// zero self-loop seeds, every weight cast to long before it is summed.
 int Engine::coarsen_chunked(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
-                            int64_t *num_edges, int64_t budget) {
+                            int64_t *num_edges, int64_t budget, bool vf) {
   const int nb = bits_for(std::max<int64_t>(ncl - 1, 1));
   int64_t *cnt, *prefix, *rowc;
   TRY(alloc(&cnt, ncl + 1)); TRY(alloc(&prefix, ncl + 1)); TRY(alloc(&rowc, ncl + 1));
-  LAUNCH(k_fill_i64, grid_for(ncl, 256, nsm_ * 16), 256, 0, s_, ncl, cnt, (int64_t)1);
+  LAUNCH(k_fill_i64, grid_for(ncl, 256, nsm_ * 16), 256, 0, s_, ncl, cnt, (int64_t)(vf ? 0 : 1));
   CK(cudaMemsetAsync(cnt + ncl, 0, sizeof(int64_t), s_));
   LAUNCH(k_comm_entry_counts, grid_for(in.nv, 256, nsm_ * 16), 256, 0, s_, in.nv, in.ptr, Cm,
          cnt);
@@ -1713,11 +1715,12 @@ int Engine::coarsen_chunked(const Level &in, const int32_t *Cm, int64_t ncl, Lev
       std::min<int64_t>(maxrec, std::max<int64_t>(2 * budget, 2 * kMergeTile + maxseeds));
   uint64_t *k1, *k2, *uk, *ak;
   double *v1, *v2, *uv, *av;
-  unsigned long long *counter;
+  unsigned long long *counter, *ndiag;
   int64_t *d_np;
   TRY(alloc(&k1, cap)); TRY(alloc(&k2, cap)); TRY(alloc(&uk, cap));
   TRY(alloc(&v1, cap)); TRY(alloc(&v2, cap)); TRY(alloc(&uv, cap));
-  TRY(alloc(&counter, 1)); TRY(alloc(&d_np, 1));
+  TRY(alloc(&counter, 1)); TRY(alloc(&d_np, 1)); TRY(alloc(&ndiag, 1));
+  CK(cudaMemsetAsync(ndiag, 0, sizeof(unsigned long long), s_));
   const bool sliced = maxrec > cap;
   ak = nullptr;
   av = nullptr;
@@ -1755,8 +1758,8 @@ int Engine::coarsen_chunked(const Level &in, const int32_t *Cm, int64_t ncl, Lev
                      int64_t *n) -> int {
     CK(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s_));
     LAUNCH(k_chunk_records, grid, 256, 0, s_, in.nv, in.nnz, in.ptr, in.tail, in.w, Cm,
-           split_row_, (int32_t)a0, (int32_t)a1, nb, t0, t1, seeds, (unsigned long long)cap,
-           counter, k1, v1);
+           split_row_, (int32_t)a0, (int32_t)a1, nb, t0, t1, vf ? 0 : seeds, vf ? 1 : 0,
+           (unsigned long long)cap, counter, k1, v1);
     unsigned long long hn = 0;
     CK(cudaMemcpyAsync(&hn, counter, sizeof(hn), cudaMemcpyDeviceToHost, s_));
     CK(cudaStreamSynchronize(s_));
@@ -1825,7 +1828,7 @@ int Engine::coarsen_chunked(const Level &in, const int32_t *Cm, int64_t ncl, Lev
       }
       if (!counting) {
         LAUNCH(k_chunk_emit, grid_for(np, 256, nsm_ * 16), 256, 0, s_, np, uk, nb, (int32_t)a0,
-               rowc, o.tail + at);
+               rowc, o.tail + at, ndiag);
         CK(cudaMemcpyAsync(o.w + at, uv, np * sizeof(double), cudaMemcpyDeviceToDevice, s_));
       }
       at += np;
@@ -1833,7 +1836,9 @@ int Engine::coarsen_chunked(const Level &in, const int32_t *Cm, int64_t ncl, Lev
   }
   dfree(ak); dfree(av);
   dfree(k1); dfree(k2); dfree(uk); dfree(v1); dfree(v2); dfree(uv);
-  dfree(counter); dfree(d_np); dfree(bounds); dfree(pb); dfree(cnt); dfree(prefix);
+  unsigned long long hdiag = 0;
+  CK(cudaMemcpyAsync(&hdiag, ndiag, sizeof(hdiag), cudaMemcpyDeviceToHost, s_));
+  dfree(counter); dfree(d_np); dfree(ndiag); dfree(bounds); dfree(pb); dfree(cnt); dfree(prefix);
   TRY(alloc(&o.ptr, ncl + 1));
   CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, rowc, o.ptr, ncl + 1, s_));
   TRY(temp(tb));
@@ -1842,7 +1847,9 @@ int Engine::coarsen_chunked(const Level &in, const int32_t *Cm, int64_t ncl, Lev
   dfree(rowc);
   CK(cudaStreamSynchronize(s_));
   *out = o;
-  *num_edges = (o.nnz - ncl) / 2 + ncl;
+  // off-diagonal pairs once, plus the diagonal ones (every cluster has its
+  // seed unless vf)
+  *num_edges = (o.nnz - (int64_t)hdiag) / 2 + (int64_t)hdiag;
   return GLV_OK;
 }
 
@@ -2645,6 +2652,71 @@ int glv_build_next_level(const glv_graph *Gin, glv_graph *Gout, const long *C,
   }
   glv_edge *daos;
   CK(cudaMallocFromPoolAsync((void **)&daos, std::max<int64_t>(out.nnz, 1) * sizeof(glv_edge), engine_pool(), c.s));
+  k_fill_aos<<<grid_for(out.nv, 256, 148 * 8), 256, 0, c.s>>>(out.nv, out.ptr, out.tail, out.w,
+                                                              daos);
+  ++c.launches;
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(hp, out.ptr, (numUniqueClusters + 1) * sizeof(long), cudaMemcpyDeviceToHost,
+                     c.s));
+  CK(cudaMemcpyAsync(he, daos, out.nnz * sizeof(glv_edge), cudaMemcpyDeviceToHost, c.s));
+  CK(cudaFreeAsync(daos, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  c.eng->free_level(out);
+  Gout->numVertices = numUniqueClusters;
+  Gout->sVertices = numUniqueClusters;
+  Gout->numEdges = ne;
+  Gout->edgeListPtrs = hp;
+  Gout->edgeList = he;
+  if (totTime) *totTime = now_s() - t0;
+  return GLV_OK;
+}
+
+int glv_vertex_following(const glv_graph *G, long *C, long *numVtxToFix) {
+  if (!G || (!C && G->numVertices > 0)) return fail(GLV_ERR_ARG, "NULL argument");
+  Call c;
+  TRY(open_call(c, GLV_MODE_VERIFY, G->numVertices, G->edgeListPtrs, G->edgeList, nullptr,
+                nullptr));
+  unsigned long long *num;
+  CK(cudaMallocFromPoolAsync((void **)&num, sizeof(*num), engine_pool(), c.s));
+  CK(cudaMemsetAsync(num, 0, sizeof(*num), c.s));
+  if (c.L0.nv > 0) {
+    k_vertex_following<<<grid_for(c.L0.nv, 256, 148 * 16), 256, 0, c.s>>>(
+        c.L0.nv, c.L0.ptr, c.L0.tail, c.eng->C, num);
+    ++c.launches;
+    CK(cudaGetLastError());
+  }
+  unsigned long long h = 0;
+  CK(cudaMemcpyAsync(&h, num, sizeof(h), cudaMemcpyDeviceToHost, c.s));
+  CK(cudaFreeAsync(num, c.s));
+  TRY(download_ids(c, c.eng->C, c.L0.nv, C));
+  if (numVtxToFix) *numVtxToFix = (long)h;
+  return GLV_OK;
+}
+
+int glv_build_new_graph_vf(const glv_graph *Gin, glv_graph *Gout, const long *C,
+                           long numUniqueClusters, double *totTime) {
+  const double t0 = now_s();
+  if (!Gin || !Gout || (!C && Gin->numVertices > 0)) return fail(GLV_ERR_ARG, "NULL argument");
+  if (numUniqueClusters < 1 || numUniqueClusters > Gin->numVertices)
+    return fail(GLV_ERR_ARG, "numUniqueClusters out of range");
+  Call c;
+  TRY(open_call(c, GLV_MODE_VERIFY, Gin->numVertices, Gin->edgeListPtrs, Gin->edgeList, nullptr,
+                nullptr));
+  TRY(upload_ids(c, C, Gin->numVertices, c.eng->C, numUniqueClusters));
+  Level out;
+  int64_t ne = 0;
+  TRY(c.eng->coarsen_chunked(c.L0, c.eng->C, numUniqueClusters, &out, &ne, int64_t(1) << 27,
+                             true));
+  long *hp = (long *)malloc((numUniqueClusters + 1) * sizeof(long));
+  glv_edge *he = (glv_edge *)malloc(std::max<int64_t>(out.nnz, 1) * sizeof(glv_edge));
+  if (!hp || !he) {
+    free(hp); free(he);
+    c.eng->free_level(out);
+    return fail(GLV_ERR_OOM, "host allocation failed");
+  }
+  glv_edge *daos;
+  CK(cudaMallocFromPoolAsync((void **)&daos, std::max<int64_t>(out.nnz, 1) * sizeof(glv_edge),
+                             engine_pool(), c.s));
   k_fill_aos<<<grid_for(out.nv, 256, 148 * 8), 256, 0, c.s>>>(out.nv, out.ptr, out.tail, out.w,
                                                               daos);
   ++c.launches;

@@ -975,8 +975,8 @@ __global__ void k_chunk_bounds(int64_t ncl, const int64_t *prefix, int K, int64_
 __global__ void __launch_bounds__(256) k_chunk_records(
     int64_t nv, int64_t nnz, const int64_t *ptr, const int32_t *tail, const double *w,
     const int32_t *C, const int64_t *split_row, int32_t a0, int32_t a1, int nb, int64_t t0,
-    int64_t t1, int seeds, unsigned long long cap, unsigned long long *counter, uint64_t *keys,
-    double *vals) {
+    int64_t t1, int seeds, int trunc, unsigned long long cap, unsigned long long *counter,
+    uint64_t *keys, double *vals) {
   __shared__ MergeSmem sm;
   const int lane = threadIdx.x & 31;
   if (seeds) {
@@ -1025,7 +1025,7 @@ __global__ void __launch_bounds__(256) k_chunk_records(
           if (b >= 0) {
             take = true;
             key = ((uint64_t)(a - a0) << nb) | (uint64_t)b;
-            val = w[e];
+            val = trunc ? (double)(long long)w[e] : w[e];
           }
         }
       }
@@ -1046,14 +1046,39 @@ __global__ void __launch_bounds__(256) k_chunk_records(
 }
 
 // Row counts and the chunk's tails of its unique (a, b) pairs.
+// (ndiag counts the diagonal pairs)
 __global__ void k_chunk_emit(int64_t np, const uint64_t *ukeys, int nb, int32_t a0,
-                             int64_t *rowc, int32_t *otail) {
+                             int64_t *rowc, int32_t *otail, unsigned long long *ndiag) {
   const uint64_t mask = (1ull << nb) - 1;
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np;
        p += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t k = ukeys[p];
-    atomicAdd((unsigned long long *)&rowc[a0 + (int64_t)(k >> nb)], 1ull);
-    otail[p] = (int32_t)(k & mask);
+    const int64_t a = a0 + (int64_t)(k >> nb), b = (int64_t)(k & mask);
+    atomicAdd((unsigned long long *)&rowc[a], 1ull);
+    otail[p] = (int32_t)b;
+    if (a == b) atomicAdd(ndiag, 1ull);
+  }
+}
+
+// Utility/vertexFollowing.cpp:46-88: C[i] = i, -1 when isolated, its only
+// neighbour t when i has degree one and t has degree > 1 or i > t.
+__global__ void k_vertex_following(int64_t nv, const int64_t *ptr, const int32_t *tail,
+                                   int32_t *C, unsigned long long *num) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nv;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t d = ptr[i + 1] - ptr[i];
+    int32_t c = (int32_t)i;
+    if (d == 0) {
+      c = -1;
+      atomicAdd(num, 1ull);
+    } else if (d == 1) {
+      const int32_t t = tail[ptr[i]];
+      if (ptr[t + 1] - ptr[t] > 1 || i > t) {
+        c = t;
+        atomicAdd(num, 1ull);
+      }
+    }
+    C[i] = c;
   }
 }
 

@@ -142,6 +142,35 @@ def buildNextLevelGraphOpt(G, C, numUniqueClusters, nThreads=1):
     _lib.check(L.glv_build_next_level(ct.byref(G.struct), ct.byref(out),
                                       C.ctypes.data_as(_P(ct.c_long)), numUniqueClusters,
                                       _mode(nThreads), ct.byref(tt)))
+    return _take_graph(out)
+
+
+def vertexFollowing(G):
+    """Utility/vertexFollowing.cpp:46 — returns (C int64[NV], numVtxToFix)."""
+    G = _as_graph(G)
+    C = np.empty(G.numVertices, dtype=np.int64)
+    n = ct.c_long(0)
+    _lib.check(_lib.lib().glv_vertex_following(ct.byref(G.struct),
+                                               C.ctypes.data_as(_P(ct.c_long)), ct.byref(n)))
+    return C, n.value
+
+
+def buildNewGraphVF(G, C, numUniqueClusters):
+    """Utility/vertexFollowing.cpp:91 — returns (CSRGraph, numEdges) of the
+    vertex-following graph (no zero self-loops, weights cast to integers)."""
+    G = _as_graph(G)
+    C = np.ascontiguousarray(C, dtype=np.int64)
+    out = _lib.GlvGraph()
+    tt = ct.c_double(0)
+    _lib.check(_lib.lib().glv_build_new_graph_vf(ct.byref(G.struct), ct.byref(out),
+                                                 C.ctypes.data_as(_P(ct.c_long)),
+                                                 numUniqueClusters, ct.byref(tt)))
+    return _take_graph(out)
+
+
+def _take_graph(out):
+    """CSRGraph + numEdges from a glv_graph whose arrays the library malloc'd
+    (released here)."""
     nv = out.numVertices
     ptr = np.ctypeslib.as_array(out.edgeListPtrs, (nv + 1,)).copy()
     nnz = int(ptr[-1])

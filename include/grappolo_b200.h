@@ -146,6 +146,20 @@ int glv_dev_run_multiphase(long nv, const long *d_ptr, const int *d_tail, const 
                            int *d_C_orig, int coloring, long minGraphSize, double threshold,
                            double C_threshold, int mode, void *stream, glv_run_stats *stats);
 
+/* Replaces vertexFollowing (Utility/vertexFollowing.cpp:46-88, basic_util.h:14):
+ * C[i] = i, -1 for an isolated vertex, its neighbour for a degree-one vertex
+ * whose neighbour has degree > 1 (or a lower id).  *numVtxToFix = isolated +
+ * following vertices. */
+int glv_vertex_following(const glv_graph *G, long *C, long *numVtxToFix);
+
+/* Replaces buildNewGraphVF (Utility/vertexFollowing.cpp:91-255, basic_util.h:15):
+ * the graph of the (renumbered) clusters C, without the zero self-loops of
+ * buildNextLevelGraphOpt and with every weight cast to long before it is
+ * summed, as the reference does.  Gout's arrays are malloc'd (free() them).
+ * Rows are sorted by tail (the reference's one-thread order). */
+int glv_build_new_graph_vf(const glv_graph *Gin, glv_graph *Gout, const long *C,
+                           long numUniqueClusters, double *totTime);
+
 /* ---- batches of independent graphs --------------------------------------
  * No reference counterpart as one call: a batch runs
  * runMultiPhaseColoring (Coloring/runMultiPhaseColoring.cpp:51-238) or, with

@@ -51,5 +51,8 @@ int algoDistanceOneVertexColoringOpt(graph *G, int *vtxColor, int nThreads, doub
 long renumberClustersContiguously(long *C, long size);
 double buildNextLevelGraphOpt(graph *Gin, graph *Gout, long *C, long numUniqueClusters,
                               int nThreads);
+/* DefineStructure/basic_util.h:14-15 (Utility/vertexFollowing.cpp) */
+long vertexFollowing(graph *G, long *C);
+double buildNewGraphVF(graph *Gin, graph *Gout, long *C, long numUniqueClusters);
 
 #endif /* GRAPPOLO_COMPAT_H */

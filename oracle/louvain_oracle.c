@@ -455,6 +455,100 @@ long lvo_build_next_level(long nv, const long *ptr, const long *tail, const doub
     return onnz;
 }
 
+/* Utility/vertexFollowing.cpp:46-88 vertexFollowing.  C[i] = i; an isolated
+ * vertex gets -1; a degree-one vertex i with neighbour t follows it (C[i] = t)
+ * when t has degree > 1 or i > t (so of two degree-one partners the higher id
+ * follows).  Returns the number of isolated plus following vertices.       */
+long lvo_vertex_following(long nv, const long *ptr, const long *tail, long *C) {
+    long num = 0;
+    for (long i = 0; i < nv; i++) C[i] = i;
+    for (long i = 0; i < nv; i++) {
+        long d = ptr[i + 1] - ptr[i];
+        if (d == 0) { num++; C[i] = -1; continue; }
+        if (d == 1) {
+            long t = tail[ptr[i]];
+            if ((ptr[t + 1] - ptr[t]) > 1 || i > t) { num++; C[i] = t; }
+        }
+    }
+    return num;
+}
+
+/* Utility/vertexFollowing.cpp:91-255 buildNewGraphVF at one thread.  Like
+ * lvo_build_next_level but with no zero self-loop seeds and with each entry's
+ * weight cast to long before it is added (:150-152: `(long)weight`), the sums
+ * kept in long (:113 map<long,long>).  Rows come out sorted by tail: cluster
+ * i's map (keys b <= i, ascending) fills row i, and each mirror goes to row b
+ * after b's own entries (:190-210).  *numEdges_out = NE_out + NE_self.      */
+long lvo_build_new_graph_vf(long nv, const long *ptr, const long *tail, const double *w,
+                            const long *C, long ncl, long **optr, long **otail, double **ow,
+                            long *numEdges_out) {
+    long nnz = ptr[nv];
+    long cap = 16;
+    while (cap < 2 * (nnz + 1)) cap <<= 1;
+    long *keys = (long *)malloc(sizeof(long) * cap);
+    long *slot = (long *)malloc(sizeof(long) * cap);
+    for (long k = 0; k < cap; k++) keys[k] = -1;
+    long *pa = (long *)malloc(sizeof(long) * (nnz + 1));
+    long *pb = (long *)malloc(sizeof(long) * (nnz + 1));
+    long *pw = (long *)malloc(sizeof(long) * (nnz + 1));
+    long np = 0;
+    for (long i = 0; i < nv; i++) {
+        if (C[i] < 0 || C[i] > ncl) continue;
+        for (long j = ptr[i]; j < ptr[i + 1]; j++) {
+            long a = C[i], b = C[tail[j]];
+            if (a < b) continue;
+            long key = a * ncl + b;
+            uint64_t h = ((uint64_t)key * 0x9E3779B97F4A7C15ull) & (uint64_t)(cap - 1);
+            while (1) {
+                if (keys[h] == key) { pw[slot[h]] += (long)w[j]; break; }
+                if (keys[h] == -1) {
+                    keys[h] = key; slot[h] = np;
+                    pa[np] = a; pb[np] = b; pw[np] = (long)w[j]; np++;
+                    break;
+                }
+                h = (h + 1) & (uint64_t)(cap - 1);
+            }
+        }
+    }
+    long *rp = (long *)calloc(ncl + 1, sizeof(long));
+    long ne_out = 0, ne_self = 0;
+    for (long p = 0; p < np; p++) {
+        rp[pa[p] + 1]++;
+        if (pa[p] > pb[p]) { rp[pb[p] + 1]++; ne_out++; } else ne_self++;
+    }
+    for (long a = 0; a < ncl; a++) rp[a + 1] += rp[a];
+    long onnz = rp[ncl];
+    long *ot = (long *)malloc(sizeof(long) * (onnz ? onnz : 1));
+    double *owt = (double *)malloc(sizeof(double) * (onnz ? onnz : 1));
+    /* pairs sorted by (a, b) (counting sorts), then emitted cluster by cluster */
+    long *ord = (long *)malloc(sizeof(long) * (np ? np : 1));
+    long *tmp = (long *)malloc(sizeof(long) * (np ? np : 1));
+    long *cnt = (long *)calloc(ncl + 1, sizeof(long));
+    for (long p = 0; p < np; p++) cnt[pb[p] + 1]++;
+    for (long k = 0; k < ncl; k++) cnt[k + 1] += cnt[k];
+    for (long p = 0; p < np; p++) tmp[cnt[pb[p]]++] = p;
+    memset(cnt, 0, sizeof(long) * (ncl + 1));
+    for (long p = 0; p < np; p++) cnt[pa[p] + 1]++;
+    for (long k = 0; k < ncl; k++) cnt[k + 1] += cnt[k];
+    for (long q = 0; q < np; q++) { long p = tmp[q]; ord[cnt[pa[p]]++] = p; }
+    long *fill = (long *)calloc(ncl + 1, sizeof(long));
+    for (long q = 0; q < np; q++) {
+        long p = ord[q];
+        long a = pa[p], b = pb[p];
+        long where = rp[a] + fill[a]++;
+        ot[where] = b; owt[where] = (double)pw[p];
+        if (a != b) {
+            where = rp[b] + fill[b]++;
+            ot[where] = a; owt[where] = (double)pw[p];
+        }
+    }
+    free(fill); free(cnt); free(tmp); free(ord);
+    free(keys); free(slot); free(pa); free(pb); free(pw);
+    *optr = rp; *otail = ot; *ow = owt;
+    *numEdges_out = ne_out + ne_self;
+    return onnz;
+}
+
 void lvo_free(void *p) { free(p); }
 
 /* Q of a final assignment over the original graph.  The reference's

@@ -79,6 +79,8 @@ class COracle:
         L.lvo_basic_phase.restype = ct.c_double
         L.lvo_renumber.restype = ct.c_long
         L.lvo_build_next_level.restype = ct.c_long
+        L.lvo_vertex_following.restype = ct.c_long
+        L.lvo_build_new_graph_vf.restype = ct.c_long
         L.lvo_modularity.restype = ct.c_double
         L.lvo_run_multiphase_coloring.restype = ct.c_int
         L.lvo_run_multiphase_basic.restype = ct.c_int
@@ -131,6 +133,30 @@ class COracle:
         onnz = self.L.lvo_build_next_level(ct.c_long(g.num_vertices), _lp(p), _lp(t), _dp(w),
                                            _lp(C), ct.c_long(ncl), ct.byref(op), ct.byref(ot),
                                            ct.byref(ow), ct.byref(ne))
+        out = CSRGraph(np.ctypeslib.as_array(op, (ncl + 1,)).copy(),
+                       np.ctypeslib.as_array(ot, (max(onnz, 1),))[:onnz].copy(),
+                       np.ctypeslib.as_array(ow, (max(onnz, 1),))[:onnz].copy())
+        for a in (op, ot, ow):
+            self.L.lvo_free(a)
+        return out, ne.value
+
+    def vertex_following(self, g):
+        """(C, numVtxToFix) of Utility/vertexFollowing.cpp:46 (restated)."""
+        p, t, _ = _csr(g)
+        C = np.empty(g.num_vertices, dtype=np.int64)
+        n = self.L.lvo_vertex_following(ct.c_long(g.num_vertices), _lp(p), _lp(t), _lp(C))
+        return C, n
+
+    def build_new_graph_vf(self, g, C, ncl):
+        """(CSRGraph, numEdges) of Utility/vertexFollowing.cpp:91 (restated)."""
+        from grappolo_b200.graphs import CSRGraph
+        p, t, w = _csr(g)
+        C = np.ascontiguousarray(C, dtype=np.int64)
+        op, ot, ow = _c_long_p(), _c_long_p(), _c_double_p()
+        ne = ct.c_long(0)
+        onnz = self.L.lvo_build_new_graph_vf(ct.c_long(g.num_vertices), _lp(p), _lp(t), _dp(w),
+                                             _lp(C), ct.c_long(ncl), ct.byref(op), ct.byref(ot),
+                                             ct.byref(ow), ct.byref(ne))
         out = CSRGraph(np.ctypeslib.as_array(op, (ncl + 1,)).copy(),
                        np.ctypeslib.as_array(ot, (max(onnz, 1),))[:onnz].copy(),
                        np.ctypeslib.as_array(ow, (max(onnz, 1),))[:onnz].copy())
@@ -226,6 +252,8 @@ class Reference:
         L.ref_basic_phase.restype = ct.c_double
         L.ref_renumber.restype = ct.c_long
         L.ref_build_next_level.restype = ct.c_long
+        L.ref_vertex_following.restype = ct.c_long
+        L.ref_build_new_graph_vf.restype = ct.c_long
         L.ref_vertex_degrees.restype = ct.c_double
         L.ref_run_multiphase_coloring.restype = ct.c_long
         L.ref_run_multiphase_basic.restype = ct.c_long
@@ -284,6 +312,34 @@ class Reference:
                                            ct.byref(op), ct.byref(ot), ct.byref(ow), ct.byref(ne))
         if onnz < 0:
             raise RuntimeError('reference coarse graph has a head/row mismatch')
+        out = CSRGraph(np.ctypeslib.as_array(op, (ncl + 1,)).copy(),
+                       np.ctypeslib.as_array(ot, (max(onnz, 1),))[:onnz].copy(),
+                       np.ctypeslib.as_array(ow, (max(onnz, 1),))[:onnz].copy())
+        for a in (op, ot, ow):
+            self.L.ref_free(a)
+        return out, ne.value
+
+    def vertex_following(self, g, nthreads=1):
+        """(C, numVtxToFix) of the reference's vertexFollowing."""
+        p, t, w = _csr(g)
+        C = np.empty(g.num_vertices, dtype=np.int64)
+        n = self.L.ref_vertex_following(ct.c_long(g.num_vertices), _lp(p), _lp(t), _dp(w), _lp(C),
+                                        ct.c_int(nthreads))
+        return C, n
+
+    def build_new_graph_vf(self, g, C, ncl, nthreads=1):
+        """(CSRGraph, numEdges) of the reference's buildNewGraphVF."""
+        from grappolo_b200.graphs import CSRGraph
+        p, t, w = _csr(g)
+        C = np.array(C, dtype=np.int64, copy=True)
+        op, ot, ow = _c_long_p(), _c_long_p(), _c_double_p()
+        ne = ct.c_long(0)
+        onnz = self.L.ref_build_new_graph_vf(ct.c_long(g.num_vertices), _lp(p), _lp(t), _dp(w),
+                                             _lp(C), ct.c_long(ncl), ct.c_int(nthreads),
+                                             ct.byref(op), ct.byref(ot), ct.byref(ow),
+                                             ct.byref(ne))
+        if onnz < 0:
+            raise RuntimeError('reference VF graph has a head/row mismatch')
         out = CSRGraph(np.ctypeslib.as_array(op, (ncl + 1,)).copy(),
                        np.ctypeslib.as_array(ot, (max(onnz, 1),))[:onnz].copy(),
                        np.ctypeslib.as_array(ow, (max(onnz, 1),))[:onnz].copy())

@@ -9,6 +9,7 @@
 // back.  It is what pins the C restatement in louvain_oracle.c, generates the
 // golden fixtures, and is the CPU baseline that bench.py times.
 #include <cstdio>
+#include <omp.h>
 #include <cstdlib>
 #include <cstring>
 #include <map>
@@ -131,6 +132,48 @@ long ref_build_next_level(long nv, const long *ptr, const long *tail, const doub
     graph *Gout = (graph *)malloc(sizeof(graph));
     quiet_begin();
     buildNextLevelGraphOpt(G, Gout, C, ncl, nthreads);
+    quiet_end();
+    long onv = Gout->numVertices;
+    long onnz = Gout->edgeListPtrs[onv];
+    long *p = (long *)malloc(sizeof(long) * (onv + 1));
+    long *t = (long *)malloc(sizeof(long) * (onnz ? onnz : 1));
+    double *ww = (double *)malloc(sizeof(double) * (onnz ? onnz : 1));
+    memcpy(p, Gout->edgeListPtrs, sizeof(long) * (onv + 1));
+    long bad = 0;
+    for (long i = 0; i < onv; i++)
+        for (long j = p[i]; j < p[i + 1]; j++) {
+            t[j] = Gout->edgeList[j].tail;
+            ww[j] = Gout->edgeList[j].weight;
+            if (Gout->edgeList[j].head != i) bad++;
+        }
+    *numEdges = Gout->numEdges;
+    free_graph(Gout);
+    free_graph(G);
+    *optr = p; *otail = t; *ow = ww;
+    return bad ? -1 : onnz;
+}
+
+// Utility/vertexFollowing.cpp:46 vertexFollowing: C and the count to fix.
+long ref_vertex_following(long nv, const long *ptr, const long *tail, const double *w, long *C,
+                          int nthreads) {
+    graph *G = make_graph(nv, ptr, tail, w);
+    omp_set_num_threads(nthreads);
+    quiet_begin();
+    long r = vertexFollowing(G, C);
+    quiet_end();
+    free_graph(G);
+    return r;
+}
+
+// Utility/vertexFollowing.cpp:91 buildNewGraphVF, output as ref_build_next_level.
+long ref_build_new_graph_vf(long nv, const long *ptr, const long *tail, const double *w,
+                            long *C, long ncl, int nthreads, long **optr, long **otail,
+                            double **ow, long *numEdges) {
+    graph *G = make_graph(nv, ptr, tail, w);
+    graph *Gout = (graph *)malloc(sizeof(graph));
+    omp_set_num_threads(nthreads);
+    quiet_begin();
+    buildNewGraphVF(G, Gout, C, ncl);
     quiet_end();
     long onv = Gout->numVertices;
     long onnz = Gout->edgeListPtrs[onv];

@@ -3,6 +3,7 @@
 Run from the repository root after ``make -C oracle``:
 
     python tests/golden/make_golden.py [/path/to/grappolo]
+    python tests/golden/make_golden.py --vf     # only vf.npz (vertex following)
 
 Each fixture ``<case>.npz`` holds an input CSR and what the reference's
 functions return for it at OMP_NUM_THREADS=1: the distance-1 colouring, one
@@ -101,9 +102,44 @@ def make_case(R, g, rng):
     return out
 
 
+def with_leaves(seed=0):
+    """A random core with degree-one leaves, isolated pairs and isolated
+    vertices; weights in (0.2, 3.7), so the integer cast of buildNewGraphVF
+    matters."""
+    rng = np.random.default_rng(seed)
+    nv = 300
+    e = [tuple(x) for x in rng.integers(0, 200, size=(400, 2))]
+    e += [(200 + k, int(rng.integers(0, 200))) for k in range(60)]
+    e += [(260 + 2 * k, 261 + 2 * k) for k in range(15)]
+    w = rng.uniform(0.2, 3.7, len(e))
+    return graphs.from_edges(nv, e, w)
+
+
+def make_vf(R, ref_root):
+    """vf.npz: vertexFollowing, renumbering and buildNewGraphVF at one thread."""
+    cases = {k: v for k, v in all_cases(ref_root).items()
+             if k in ('karate', 'pp1000_w', 'loops_isolated', 'hubs_w')}
+    cases['leaves'] = with_leaves(0)
+    out = {}
+    for name, g in cases.items():
+        C, num = R.vertex_following(g)
+        Cr, ncl = R.renumber(C)
+        cg, ne = R.build_new_graph_vf(g, Cr, ncl)
+        out.update({f'{name}_ptr': g.ptr, f'{name}_tail': g.tail, f'{name}_weight': g.weight,
+                    f'{name}_C': C, f'{name}_num': num, f'{name}_renum': Cr, f'{name}_ncl': ncl,
+                    f'{name}_cptr': cg.ptr, f'{name}_ctail': cg.tail, f'{name}_cweight': cg.weight,
+                    f'{name}_ne': ne})
+    np.savez_compressed(os.path.join(HERE, 'vf.npz'), names=np.array(list(cases)), **out)
+    print('wrote vf', list(cases))
+
+
 def main():
-    ref_root = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+    ref_root = sys.argv[1] if len(sys.argv) > 1 and not sys.argv[1].startswith('--') \
+        else '/root/reference'
     R = Reference()
+    if '--vf' in sys.argv:
+        make_vf(R, ref_root)
+        return
     rng = np.random.default_rng(2024)
     for name, g in all_cases(ref_root).items():
         np.savez_compressed(os.path.join(HERE, f'{name}.npz'), **make_case(R, g, rng))

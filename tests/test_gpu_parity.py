@@ -276,3 +276,27 @@ def test_hub_rows_fast_mode(block_max, oracle, monkeypatch):
     _, st = louvain.runMultiPhaseColoring(g, numThreads=8, stats=True)
     _, so, _ = oracle.run_multiphase_coloring(g)
     assert abs(st['final_modularity'] - so['final_mod']) <= FAST_Q_TOL
+
+
+def _vf_cases():
+    import os
+    z = np.load(os.path.join(os.path.dirname(__file__), 'golden', 'vf.npz'))
+    for name in z['names']:
+        name = str(name)
+        g = graphs.CSRGraph(z[f'{name}_ptr'], z[f'{name}_tail'], z[f'{name}_weight'])
+        yield name, g, {k[len(name) + 1:]: z[k] for k in z.files if k.startswith(name + '_')}
+
+
+@pytest.mark.parametrize('name,g,ref', list(_vf_cases()),
+                         ids=lambda x: x if isinstance(x, str) else '')
+def test_vertex_following(name, g, ref):
+    """glv_vertex_following / glv_build_new_graph_vf equal the reference's
+    vertexFollowing and buildNewGraphVF at one thread, bit for bit."""
+    C, n = louvain.vertexFollowing(g)
+    assert n == int(ref['num']) and np.array_equal(C, ref['C'])
+    Cr, ncl = louvain.renumberClustersContiguously(C)
+    assert ncl == int(ref['ncl']) and np.array_equal(Cr, ref['renum'])
+    cg, ne = louvain.buildNewGraphVF(g, Cr, ncl)
+    assert ne == int(ref['ne'])
+    assert np.array_equal(cg.ptr, ref['cptr']) and np.array_equal(cg.tail, ref['ctail'])
+    assert np.array_equal(cg.weight, ref['cweight'])

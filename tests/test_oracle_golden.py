@@ -1,5 +1,6 @@
 """The C oracle against the golden fixtures generated by the reference itself."""
 import hashlib
+import os
 
 import numpy as np
 import pytest
@@ -84,3 +85,23 @@ def test_pinned_100k(oracle, name):
     assert abs(s['final_mod'] - pin['final_mod']) <= 5e-7
     assert [r.num_colors for r in recs if r.colored] == pin['colors']
     assert [r.clusters for r in recs] == pin['clusters']
+
+
+def _vf_cases():
+    z = np.load(os.path.join(os.path.dirname(__file__), 'golden', 'vf.npz'))
+    for name in z['names']:
+        name = str(name)
+        g = graphs.CSRGraph(z[f'{name}_ptr'], z[f'{name}_tail'], z[f'{name}_weight'])
+        yield name, g, {k[len(name) + 1:]: z[k] for k in z.files if k.startswith(name + '_')}
+
+
+@pytest.mark.parametrize('name,g,ref', list(_vf_cases()), ids=lambda x: x if isinstance(x, str) else '')
+def test_vertex_following_golden(oracle, name, g, ref):
+    """Utility/vertexFollowing.cpp at one thread: follow map, count, and the
+    vertex-following graph (integer-cast weights, no zero self-loops)."""
+    C, n = oracle.vertex_following(g)
+    assert n == int(ref['num']) and np.array_equal(C, ref['C'])
+    cg, ne = oracle.build_new_graph_vf(g, ref['renum'], int(ref['ncl']))
+    assert ne == int(ref['ne'])
+    assert np.array_equal(cg.ptr, ref['cptr']) and np.array_equal(cg.tail, ref['ctail'])
+    assert np.array_equal(cg.weight, ref['cweight'])

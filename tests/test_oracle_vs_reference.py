@@ -58,3 +58,29 @@ def test_decisions_with_ties_and_singletons(oracle, reference):
     t_o = oracle.decide_batch(g, C, vdeg, vdeg, np.ones(8, dtype=np.int64), const, verts)
     t_r = reference.decide_batch(g, C, vdeg, vdeg, np.ones(8, dtype=np.int64), const, verts)
     assert np.array_equal(t_o, t_r)
+
+
+def _with_leaves(seed):
+    """Random core, degree-one leaves, isolated pairs and vertices, weights in
+    (0.2, 3.7) so the reference's integer cast of weights matters."""
+    rng = np.random.default_rng(seed)
+    nv = 300
+    e = [tuple(x) for x in rng.integers(0, 200, size=(400, 2))]
+    e += [(200 + k, int(rng.integers(0, 200))) for k in range(60)]
+    e += [(260 + 2 * k, 261 + 2 * k) for k in range(15)]
+    w = rng.uniform(0.2, 3.7, len(e))
+    return graphs.from_edges(nv, e, w)
+
+
+@pytest.mark.parametrize('seed', [0, 1, 2])
+def test_vertex_following_matches_reference(seed, oracle, reference):
+    g = _with_leaves(seed)
+    C1, n1 = oracle.vertex_following(g)
+    C2, n2 = reference.vertex_following(g)
+    assert n1 == n2 and np.array_equal(C1, C2)
+    Cr, ncl = reference.renumber(C2)
+    a, ne1 = oracle.build_new_graph_vf(g, Cr, ncl)
+    b, ne2 = reference.build_new_graph_vf(g, Cr, ncl)
+    assert ne1 == ne2
+    assert np.array_equal(a.ptr, b.ptr) and np.array_equal(a.tail, b.tail)
+    assert np.array_equal(a.weight, b.weight)
