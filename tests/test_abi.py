@@ -45,6 +45,8 @@ REFERENCE_SYMBOLS = [
     '_Z32algoDistanceOneVertexColoringOptP5graphPiiPd',
     '_Z28renumberClustersContiguouslyPll',
     '_Z22buildNextLevelGraphOptP5graphS0_Plli',
+    '_Z15vertexFollowingP5graphPl',
+    '_Z15buildNewGraphVFP5graphS0_Pll',
 ]
 
 
@@ -66,7 +68,9 @@ def test_compat_header_matches_reference_mangling(tmp_path):
                    '  parallelLouvianMethod(g, c, 1, -1, 1e-6, t, it);\n'
                    '  algoDistanceOneVertexColoringOpt(g, col, 1, t);\n'
                    '  renumberClustersContiguously(c, 4);\n'
-                   '  buildNextLevelGraphOpt(g, o, c, 2, 1);\n}\n')
+                   '  buildNextLevelGraphOpt(g, o, c, 2, 1);\n'
+                   '  vertexFollowing(g, c);\n'
+                   '  buildNewGraphVF(g, o, c, 2);\n}\n')
     obj = tmp_path / 'use.o'
     subprocess.run(['g++', '-c', '-I', os.path.join(ROOT, 'include'), str(src), '-o', str(obj)],
                    check=True)
