@@ -98,7 +98,7 @@ def lib():
     for name in ('glv_run_multiphase_coloring', 'glv_run_multiphase_basic',
                  'glv_run_multiphase_coloring_csr', 'glv_run_multiphase_basic_csr',
                  'glv_dev_run_multiphase', 'glv_louvain_coloring_phase',
-                 'glv_louvain_basic_phase', 'glv_distance_one_coloring',
+                 'glv_louvain_basic_phase', 'glv_distance_one_coloring', 'glv_color_multihash',
                  'glv_renumber_clusters', 'glv_build_next_level', 'glv_modularity',
                  'glv_decide_batch', 'glv_dev_modularity_static', 'glv_gate_set',
                  'glv_gate_infer', 'glv_gate_grad', 'glv_gate_train', 'glv_trace_begin',
@@ -128,6 +128,8 @@ def lib():
                                           P(ct.c_double)]
     L.glv_distance_one_coloring.argtypes = [P(GlvGraph), P(ct.c_int), ct.c_int, P(ct.c_int),
                                             P(ct.c_double)]
+    L.glv_color_multihash.argtypes = [P(GlvGraph), P(ct.c_int), ct.c_int, ct.c_int, P(ct.c_int),
+                                      P(ct.c_double)]
     L.glv_renumber_clusters.argtypes = [P(ct.c_long), ct.c_long, P(ct.c_long)]
     L.glv_build_next_level.argtypes = [P(GlvGraph), P(GlvGraph), P(ct.c_long), ct.c_long,
                                        ct.c_int, P(ct.c_double)]

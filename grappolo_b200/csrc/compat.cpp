@@ -56,7 +56,7 @@ void runMultiPhaseColoring(graph *G, long *C_orig, int coloring, int numColors, 
                                        replaceMap, minGraphSize, threshold, C_threshold,
                                        mode_for(numThreads), s);
   if (rc != GLV_OK) die("runMultiPhaseColoring", rc);
-  print_summary(*s, coloring == 1, numThreads);
+  print_summary(*s, coloring != 0, numThreads);
   free(s);
   free_graph(G);  // the reference consumes G (runMultiPhaseColoring.cpp:226-232)
 }
@@ -98,6 +98,15 @@ int algoDistanceOneVertexColoringOpt(graph *G, int *vtxColor, int nThreads, doub
   int rc = glv_distance_one_coloring((const glv_graph *)G, vtxColor, mode_for(nThreads), &mc,
                                      totTime);
   if (rc != GLV_OK) die("algoDistanceOneVertexColoringOpt", rc);
+  return mc;
+}
+
+int algoColoringMultiHashMaxMin(graph *G, int *vtxColor, int nThreads, double *totTime, int nHash,
+                                int nItrs) {
+  (void)nThreads;
+  int mc = -1;
+  int rc = glv_color_multihash((const glv_graph *)G, vtxColor, nHash, nItrs, &mc, totTime);
+  if (rc != GLV_OK) die("algoColoringMultiHashMaxMin", rc);
   return mc;
 }
 

@@ -231,6 +231,12 @@ class Engine {
   int sublevels_batch(const Level &L, const Batch &b, int32_t **d_sub, int *nsub);
   void free_level(Level &L);
   Batch *bt_ = nullptr;  // set while a batch runs
+  // colouring of colour phases: 1 = distance-1 (the default), 3 = the
+  // incomplete multi-hash max/min colouring with mhash_nhash_ hashes and
+  // mhash_itrs_ iterations
+  int color_algo_ = 1;
+  int mhash_nhash_ = 2, mhash_itrs_ = 4;
+  int color_mhash(const Level &L, int *ncolors);
 
   // state buffers (device)
   double *vDeg = nullptr, *cDeg = nullptr, *dDeg = nullptr, *own_w = nullptr;
@@ -528,7 +534,7 @@ int Engine::phase_init(const Level &L, bool need_past) {
 // ----------------------------------------------------------------- colouring
 int Engine::color(const Level &L, int *ncolors, double *secs) {
   const double t0 = now_s();
-  if (L.nv == 0) {
+  if (L.nv == 0 && color_algo_ != 3) {
     *ncolors = 0;
     return GLV_OK;
   }
@@ -541,6 +547,11 @@ int Engine::color(const Level &L, int *ncolors, double *secs) {
   if (cm && !strcmp(cm, "spec")) spec = true;
   const bool dbg = getenv("GRAPPOLO_B200_DEBUG") != nullptr;
   double td = now_s();
+  if (color_algo_ == 3) {
+    TRY(color_mhash(L, ncolors));
+    if (secs) *secs = now_s() - t0;
+    return GLV_OK;
+  }
   TRY(spec ? color_spec(L, ncolors) : color_jp(L, ncolors));
   if (dbg) {
     cudaStreamSynchronize(s_);
@@ -653,6 +664,60 @@ int Engine::color_spec(const Level &L, int *ncolors) {
   dfree(wl); dfree(bl); dfree(nx); dfree(cnt); dfree(status); dfree(maxc);
   if (hs) return fail(GLV_ERR_COLORS, "colouring needs more than 4096 colours");
   *ncolors = hm + 1;
+  return GLV_OK;
+}
+
+template <class T>
+static int upload(cudaStream_t s, T *dst, const std::vector<T> &src);
+
+// Coloring/coloringMultiHashMaxMin.cpp:59-228.  The random values are the
+// reference's: rand() of the C library, hash by hash, vertex by vertex
+// (:45-57, :95-101), so a process that seeds it the same way gets the same
+// colouring.  Vertices left uncoloured keep colour maxColor (an improper
+// class); *ncolors = maxColor + 1, as runMultiPhaseColoring counts them.
+int Engine::color_mhash(const Level &L, int *ncolors) {
+  const int nHash = mhash_nhash_, nItrs = mhash_itrs_;
+  const int64_t nv = L.nv;
+  if (nv == 0) {  // the first iteration colours nothing and all are coloured (:160-168)
+    *ncolors = 2 * (0 - 1) * nHash + 2 * nHash + 1 + 1;
+    return GLV_OK;
+  }
+  std::vector<double> h((size_t)nHash * nv);
+  for (int k = 0; k < nHash; ++k)
+    for (int64_t v = 0; v < nv; ++v) h[(size_t)k * nv + v] = (double)rand();
+  double *rnd;
+  unsigned long long *count;
+  TRY(alloc(&rnd, h.size()));
+  TRY(alloc(&count, 1));
+  TRY(upload(s_, rnd, h));
+  int maxColor = 2 * nHash * nItrs;
+  LAUNCH(k_fill_i32, grid_for(nv, 256, nsm_ * 16), 256, 0, s_, nv, color_, maxColor);
+  long totalColored = 0;
+  unsigned long long iterFreq = 0;
+  for (int itr = 0; itr < nItrs; ++itr) {
+    CK(cudaMemsetAsync(count, 0, sizeof(*count), s_));
+    for (int ih = 0; ih < nHash; ++ih) {
+      const int cur = 2 * itr * nHash + 2 * ih;
+      LAUNCH(k_mhash_pass, grid_for(nv * 32, 256, nsm_ * 16), 256, 0, s_, nv, L.ptr, L.tail,
+             rnd + (size_t)ih * nv, color_, (int32_t)(2 * nHash * nItrs), (int32_t)cur, count);
+    }
+    unsigned long long c = 0;
+    CK(cudaMemcpyAsync(&c, count, sizeof(c), cudaMemcpyDeviceToHost, s_));
+    CK(cudaStreamSynchronize(s_));
+    iterFreq += c;
+    totalColored += (long)iterFreq;
+    if (iterFreq == 0) {
+      if (totalColored == nv) {
+        maxColor = 2 * (itr - 1) * nHash + 2 * nHash + 1;
+        break;
+      }
+    } else {
+      iterFreq = 0;
+    }
+  }
+  dfree(rnd);
+  dfree(count);
+  *ncolors = maxColor + 1;
   return GLV_OK;
 }
 
@@ -2047,7 +2112,9 @@ int Engine::run_multiphase(const Level &L0, int32_t *d_C_orig, bool coloring,
     const double ts0 = t_sweep, es0 = edges_swept;
     phase_index_ = (int)phase - 1;
     if (!non_color) {
-      TRY(coloring_phase(L, ncolors, !recolored, curr, c_threshold, &curr, &itr));
+      // a multi-hash colouring leaves an improper class: sublevels as for stale ones
+      TRY(coloring_phase(L, ncolors, !recolored || color_algo_ == 3, curr, c_threshold, &curr,
+                         &itr));
     } else {
       TRY(basic_phase(L, curr, threshold, &curr, &itr));
     }
@@ -2309,12 +2376,17 @@ static int upload_ids(Call &c, const long *host, int64_t n, int32_t *d, int64_t 
 
 static int run_host(int mode, long nv, const long *ptr, const glv_edge *edges, const long *tail64,
                     const double *w, long *C_orig, bool coloring, long min_graph_size,
-                    double threshold, double c_threshold, glv_run_stats *st) {
+                    double threshold, double c_threshold, glv_run_stats *st,
+                    int color_algo = 1, int num_colors = 16) {
   const double t0 = now_s();
   if (!C_orig && nv > 0) return fail(GLV_ERR_ARG, "C_orig is NULL");
   if (st) memset(st, 0, sizeof(*st));
   Call c;
   TRY(open_call(c, mode, nv, ptr, edges, tail64, w));
+  c.eng->color_algo_ = color_algo;
+  // runMultiPhaseColoring's parameters (Coloring/runMultiPhaseColoring.cpp:77-86)
+  c.eng->mhash_nhash_ = 2;
+  c.eng->mhash_itrs_ = std::max(1, num_colors / 4);
   int32_t *dC;
   CK(cudaMallocFromPoolAsync((void **)&dC, std::max<long>(nv, 1) * sizeof(int32_t), engine_pool(), c.s));
   TRY(c.eng->run_multiphase(c.L0, dC, coloring, min_graph_size, threshold, c_threshold, st));
@@ -2347,12 +2419,14 @@ void glv_set_profiling(int on) { g_profile = on < 0 ? 0 : (on > 2 ? 2 : on); }
 int glv_run_multiphase_coloring(const glv_graph *G, long *C_orig, int coloring, int numColors,
                                 int replaceMap, long minGraphSize, double threshold,
                                 double C_threshold, int mode, glv_run_stats *stats) {
-  (void)numColors;  // only the incomplete colouring (coloring = 3) reads it
   if (!G) return fail(GLV_ERR_ARG, "G is NULL");
-  if (coloring != 1) return fail(GLV_ERR_UNSUPPORTED, "only coloring = 1 is implemented");
+  if (coloring != 1 && coloring != 3)
+    return fail(GLV_ERR_UNSUPPORTED, "only coloring = 1 and 3 are implemented");
+  if (coloring == 3 && 4L * std::max(1, numColors / 4) + 1 >= kMaxColors)
+    return fail(GLV_ERR_COLORS, "numColors reaches the colour cap");
   if (replaceMap != 0) return fail(GLV_ERR_UNSUPPORTED, "replaceMap = 1 is not implemented");
   return run_host(mode, G->numVertices, G->edgeListPtrs, G->edgeList, nullptr, nullptr, C_orig,
-                  true, minGraphSize, threshold, C_threshold, stats);
+                  true, minGraphSize, threshold, C_threshold, stats, coloring, numColors);
 }
 
 int glv_run_multiphase_basic(const glv_graph *G, long *C_orig, int basicOpt, long minGraphSize,
@@ -2607,6 +2681,29 @@ int glv_distance_one_coloring(const glv_graph *G, int *vtxColor, int mode, int *
   int nc = 0;
   double secs = 0;
   if (G->numVertices > 0) TRY(c.eng->color(c.L0, &nc, &secs));
+  CK(cudaMemcpyAsync(vtxColor, c.eng->color_, G->numVertices * sizeof(int32_t),
+                     cudaMemcpyDeviceToHost, c.s));
+  CK(cudaStreamSynchronize(c.s));
+  if (maxColor) *maxColor = nc - 1;
+  if (totTime) *totTime = secs;
+  return GLV_OK;
+}
+
+int glv_color_multihash(const glv_graph *G, int *vtxColor, int nHash, int nItrs,
+                        int *maxColor, double *totTime) {
+  if (!G || (!vtxColor && G->numVertices > 0)) return fail(GLV_ERR_ARG, "NULL argument");
+  if (nHash < 1 || nItrs < 1) return fail(GLV_ERR_ARG, "nHash and nItrs must be positive");
+  if ((long)2 * nHash * nItrs + 1 >= kMaxColors)
+    return fail(GLV_ERR_COLORS, "2 * nHash * nItrs reaches the colour cap");
+  Call c;
+  TRY(open_call(c, GLV_MODE_VERIFY, G->numVertices, G->edgeListPtrs, G->edgeList, nullptr,
+                nullptr));
+  c.eng->color_algo_ = 3;
+  c.eng->mhash_nhash_ = nHash;
+  c.eng->mhash_itrs_ = nItrs;
+  int nc = 0;
+  double secs = 0;
+  TRY(c.eng->color(c.L0, &nc, &secs));
   CK(cudaMemcpyAsync(vtxColor, c.eng->color_, G->numVertices * sizeof(int32_t),
                      cudaMemcpyDeviceToHost, c.s));
   CK(cudaStreamSynchronize(c.s));

@@ -411,6 +411,39 @@ __global__ void __launch_bounds__(256) k_color_rounds(int64_t nv, const int64_t 
   }
 }
 
+// Coloring/coloringMultiHashMaxMin.cpp:124-160: one (iteration, hash) pass of
+// the incomplete max/min colouring.  An uncoloured vertex (colour maxColor)
+// takes `cur` when its random value beats every neighbour not coloured in an
+// earlier pass, `cur` + 1 when it is below all of them.  A neighbour coloured
+// in this pass still compares (its colour is >= cur), so the outcome does not
+// depend on the order of the vertices.  One warp per vertex.
+__global__ void k_mhash_pass(int64_t nv, const int64_t *ptr, const int32_t *tail,
+                             const double *rnd, int32_t *col, int32_t maxColor, int32_t cur,
+                             unsigned long long *count) {
+  const int lane = threadIdx.x & 31;
+  const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t v = wid; v < nv; v += nw) {
+    if (col[v] != maxColor) continue;  // warp-uniform
+    const double rv = rnd[v];
+    bool isMax = true, isMin = true;
+    for (int64_t j = ptr[v] + lane; j < ptr[v + 1]; j += 32) {
+      const int32_t u = tail[j];
+      if (u == (int32_t)v) continue;
+      if (col[u] < cur) continue;
+      const double ru = rnd[u];
+      if (rv <= ru) isMax = false;
+      if (rv >= ru) isMin = false;
+    }
+    isMax = __all_sync(FULL, isMax);
+    isMin = __all_sync(FULL, isMin);
+    if (lane == 0 && (isMax || isMin)) {
+      col[v] = isMax ? cur : cur + 1;
+      atomicAdd(count, 1ull);
+    }
+  }
+}
+
 // key[v] = ncolors - 1 - color[v]: recolour the last class first (Culberson's
 // reverse-class order; a greedy pass over whole classes never adds colours).
 __global__ void k_reverse_class_key(int64_t nv, const int32_t *color, int32_t ncolors,

@@ -123,6 +123,18 @@ def algoDistanceOneVertexColoringOpt(G, nThreads=1):
     return col, mc.value, tt.value
 
 
+def algoColoringMultiHashMaxMin(G, nThreads=1, nHash=2, nItrs=4):
+    """Coloring/coloringMultiHashMaxMin.cpp:59 — returns (vtxColor int32[NV],
+    maxColor, totTime).  Random values come from the C library's rand()."""
+    G = _as_graph(G)
+    col = np.full(G.numVertices, -1, dtype=np.int32)
+    mc, tt = ct.c_int(0), ct.c_double(0)
+    _lib.check(_lib.lib().glv_color_multihash(
+        ct.byref(G.struct), col.ctypes.data_as(_P(ct.c_int)), nHash, nItrs, ct.byref(mc),
+        ct.byref(tt)))
+    return col, mc.value, tt.value
+
+
 def renumberClustersContiguously(C):
     """Utility/buildNextPhase.cpp:48 — returns (renumbered C, numUniqueClusters)."""
     C = np.array(C, dtype=np.int64, copy=True)

@@ -40,7 +40,7 @@ enum {
   GLV_ERR_OOM = 3,        /* device or host allocation failed */
   GLV_ERR_COLORS = 4,     /* a colouring needed >= 4096 colours (coloringUtils.cpp:57-60) */
   GLV_ERR_TOO_LARGE = 5,  /* numVertices >= 2^31 (ids are int32 on the device) */
-  GLV_ERR_UNSUPPORTED = 6,/* option outside this engine's scope (e.g. coloring 2/3, replaceMap) */
+  GLV_ERR_UNSUPPORTED = 6,/* option outside this engine's scope (e.g. coloring 2, replaceMap) */
   GLV_ERR_NO_DEVICE = 7,  /* no CUDA device */
   GLV_ERR_LIMIT = 8       /* a size exceeds a fixed limit of the entry point */
 };
@@ -114,9 +114,14 @@ typedef struct glv_run_stats {
 /* ---- multiphase drivers ------------------------------------------------- */
 
 /* Replaces runMultiPhaseColoring (Coloring/runMultiPhaseColoring.cpp:51-238,
- * declared DefineStructure/color_comm.h:7-8).  coloring must be 1 (distance-1
- * colouring); replaceMap must be 0.  C_orig[numVertices] receives the final
- * community of every input vertex (-1 for isolated vertices).  Unlike the
+ * declared DefineStructure/color_comm.h:7-8).  coloring = 1 is the distance-1
+ * colouring; coloring = 3 the incomplete multi-hash max/min colouring
+ * (Coloring/coloringMultiHashMaxMin.cpp:59-228) with two hashes and
+ * max(1, numColors / 4) iterations, its random values drawn from the C
+ * library's rand() exactly as the reference draws them (seed with srand() to
+ * reproduce a reference run).  coloring = 2 (vBase balancing) is
+ * GLV_ERR_UNSUPPORTED; replaceMap must be 0.  C_orig[numVertices] receives the
+ * final community of every input vertex (-1 for isolated vertices).  Unlike the
  * reference, G is not freed.  `stats` may be NULL. */
 int glv_run_multiphase_coloring(const glv_graph *G, long *C_orig, int coloring, int numColors,
                                 int replaceMap, long minGraphSize, double threshold,
@@ -216,6 +221,15 @@ int glv_louvain_basic_phase(const glv_graph *G, long *C, double Lower, double th
  * return value). */
 int glv_distance_one_coloring(const glv_graph *G, int *vtxColor, int mode, int *maxColor,
                               double *totTime);
+
+/* Replaces algoColoringMultiHashMaxMin (Coloring/coloringMultiHashMaxMin.cpp:59-228,
+ * coloring.h:12): the incomplete colouring with nHash hashes and nItrs
+ * iterations.  Random values come from the C library's rand(), drawn as the
+ * reference draws them; vertices left uncoloured hold *maxColor (the
+ * reference's return value).  GLV_ERR_COLORS when 2 * nHash * nItrs + 1
+ * reaches 4096. */
+int glv_color_multihash(const glv_graph *G, int *vtxColor, int nHash, int nItrs,
+                        int *maxColor, double *totTime);
 
 /* Replaces renumberClustersContiguously (Utility/buildNextPhase.cpp:48-79,
  * basic_util.h:5). */

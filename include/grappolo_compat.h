@@ -47,6 +47,9 @@ double parallelLouvianMethod(graph *G, long *C, int nThreads, double Lower, doub
                              double *totTime, int *numItr);
 /* DefineStructure/coloring.h:8 */
 int algoDistanceOneVertexColoringOpt(graph *G, int *vtxColor, int nThreads, double *totTime);
+/* DefineStructure/coloring.h:12 (Coloring/coloringMultiHashMaxMin.cpp) */
+int algoColoringMultiHashMaxMin(graph *G, int *vtxColor, int nThreads, double *totTime, int nHash,
+                                int nItrs);
 /* DefineStructure/basic_util.h:5-6 */
 long renumberClustersContiguously(long *C, long size);
 double buildNextLevelGraphOpt(graph *Gin, graph *Gout, long *C, long numUniqueClusters,

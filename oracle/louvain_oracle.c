@@ -205,6 +205,54 @@ int lvo_color_greedy(long nv, const long *ptr, const long *tail, int *color) {
     return maxc;
 }
 
+/* Coloring/coloringMultiHashMaxMin.cpp:59-228 (incomplete colouring) at one
+ * thread.  Draws nHash x nv values from the C library's rand(), hash after
+ * hash (:45-57, :95-101); every vertex starts at maxColor = 2*nHash*nItrs
+ * (:106-110).  In pass (itr, ihash) an uncoloured vertex takes colour
+ * cur = 2*itr*nHash + 2*ihash when its value is above that of every
+ * neighbour still at a colour >= cur, cur + 1 when below all of them
+ * (:117-155).  An iteration that colours nothing after all vertices are
+ * coloured lowers maxColor to 2*(itr-1)*nHash + 2*nHash + 1 (:160-168).
+ * Returns maxColor; uncoloured vertices keep it.                           */
+int lvo_color_mhash(long nv, const long *ptr, const long *tail, int nHash, int nItrs,
+                    int *color) {
+    double *rnd = (double *)malloc(sizeof(double) * (size_t)nHash * (nv ? nv : 1));
+    for (int h = 0; h < nHash; h++)
+        for (long v = 0; v < nv; v++) rnd[(size_t)h * nv + v] = (double)rand();
+    int maxColor = 2 * nHash * nItrs;
+    for (long v = 0; v < nv; v++) color[v] = maxColor;
+    long totalColored = 0, iterFreq = 0;
+    for (int itr = 0; itr < nItrs; itr++) {
+        for (int h = 0; h < nHash; h++) {
+            const int cur = 2 * itr * nHash + 2 * h;
+            const double *r = rnd + (size_t)h * nv;
+            for (long v = 0; v < nv; v++) {
+                if (color[v] != maxColor) continue;
+                int isMax = 1, isMin = 1;
+                for (long k = ptr[v]; k < ptr[v + 1]; k++) {
+                    long u = tail[k];
+                    if (u == v || color[u] < cur) continue;
+                    if (r[v] <= r[u]) isMax = 0;
+                    if (r[v] >= r[u]) isMin = 0;
+                }
+                if (isMax) { color[v] = cur; iterFreq++; }
+                else if (isMin) { color[v] = cur + 1; iterFreq++; }
+            }
+        }
+        totalColored += iterFreq;
+        if (iterFreq == 0) {
+            if (totalColored == nv) {
+                maxColor = 2 * (itr - 1) * nHash + 2 * nHash + 1;
+                break;
+            }
+        } else {
+            iterFreq = 0;
+        }
+    }
+    free(rnd);
+    return maxColor;
+}
+
 /* Modularity pieces shared by both sweeps: Q = e_xx*c - a2_x*c*c
  * (parallelLouvainWithColoring.cpp:222-249, parallelLouvainMethod.cpp:244-255). */
 static double modularity_from(long nv, const double *cWI, const double *cDeg, double c) {
@@ -602,23 +650,35 @@ static void free_graph(long *ptr, long *tail, double *w, int owned) {
     if (owned) { free(ptr); free(tail); free(w); }
 }
 
-/* Coloring/runMultiPhaseColoring.cpp:51-238 at one thread, coloring = 1.
+/* Coloring/runMultiPhaseColoring.cpp:51-238 at one thread, coloring = 1 or 3
+ * (3: lvo_color_mhash with two hashes and max(1, numColors / 4) iterations,
+ * :76-86, :187-196).
  * Later phases recolour only when NV > minGraphSize and still colouring
  * (:173); otherwise the first NV entries of the previous colouring are reused
  * with the previous colour count (:61-66,113-115).  The first colour phase
  * that fails to gain switches to Jacobi phases on the same graph (:199-206).
  * C_orig is composed after every phase, before the gain test (:128-144).     */
+static int color_for(int coloring, int numColors, long nv, const long *ptr, const long *tail,
+                     int *colors) {
+    if (coloring == 3) {
+        int nItrs = numColors / 4;
+        if (nItrs <= 0) nItrs = 1;
+        return lvo_color_mhash(nv, ptr, tail, 2, nItrs, colors);
+    }
+    for (long i = 0; i < nv; i++) colors[i] = -1;
+    return lvo_color_greedy(nv, ptr, tail, colors);
+}
+
 int lvo_run_multiphase_coloring(long nv, const long *ptr0, const long *tail0,
-                                const double *w0, long *C_orig, long minGraphSize,
-                                double threshold, double C_threshold,
+                                const double *w0, long *C_orig, int coloring, int numColors,
+                                long minGraphSize, double threshold, double C_threshold,
                                 lvo_summary *sum, lvo_phase *rec, int rec_cap) {
     long *ptr = (long *)ptr0, *tail = (long *)tail0;
     double *w = (double *)w0;
     int owned = 0;
     long NV = nv, gnv = nv;
     int *colors = (int *)malloc(sizeof(int) * (nv ? nv : 1));
-    for (long i = 0; i < nv; i++) colors[i] = -1;
-    int nColors = lvo_color_greedy(gnv, ptr, tail, colors);
+    int nColors = color_for(coloring, numColors, gnv, ptr, tail, colors);
     if (nColors == -2) { free(colors); return -1; }
     nColors += 1;
     int recolored = 1;
@@ -667,8 +727,7 @@ int lvo_run_multiphase_coloring(long nv, const long *ptr0, const long *tail0,
             phase++;
             recolored = 0;
             if ((gnv > minGraphSize) && !nonColor) {
-                for (long i = 0; i < gnv; i++) colors[i] = -1;
-                int mc = lvo_color_greedy(gnv, ptr, tail, colors);
+                int mc = color_for(coloring, numColors, gnv, ptr, tail, colors);
                 if (mc == -2) { free(colors); free(C); free_graph(ptr, tail, w, owned); return -1; }
                 nColors = mc + 1;
                 recolored = 1;

@@ -75,6 +75,7 @@ class COracle:
         self.L = L
         L.lvo_vertex_degrees.restype = ct.c_double
         L.lvo_color_greedy.restype = ct.c_int
+        L.lvo_color_mhash.restype = ct.c_int
         L.lvo_coloring_phase.restype = ct.c_double
         L.lvo_basic_phase.restype = ct.c_double
         L.lvo_renumber.restype = ct.c_long
@@ -186,13 +187,23 @@ class COracle:
         return [PhaseRecord(r.nv, r.nnz, bool(r.colored), bool(r.recolored), r.num_colors,
                             r.iterations, r.mod, r.clusters) for r in recs[:n]]
 
-    def run_multiphase_coloring(self, g, min_graph_size=1000, threshold=1e-6, c_threshold=1e-4):
+    def color_mhash(self, g, num_colors=16):
+        """Multi-hash max/min colouring; draws from the C library's rand()."""
+        p, t, _ = _csr(g)
+        col = np.empty(g.num_vertices, dtype=np.int32)
+        mc = self.L.lvo_color_mhash(ct.c_long(g.num_vertices), _lp(p), _lp(t), ct.c_int(2),
+                                    ct.c_int(max(1, num_colors // 4)), _ip(col))
+        return col, mc
+
+    def run_multiphase_coloring(self, g, min_graph_size=1000, threshold=1e-6, c_threshold=1e-4,
+                                coloring=1, num_colors=16):
         p, t, w = _csr(g)
         C = np.full(g.num_vertices, -1, dtype=np.int64)
         s = _SummaryC()
         recs = (_PhaseC * 256)()
         rc = self.L.lvo_run_multiphase_coloring(ct.c_long(g.num_vertices), _lp(p), _lp(t), _dp(w),
-                                                _lp(C), ct.c_long(min_graph_size),
+                                                _lp(C), ct.c_int(coloring), ct.c_int(num_colors),
+                                                ct.c_long(min_graph_size),
                                                 ct.c_double(threshold), ct.c_double(c_threshold),
                                                 ct.byref(s), recs, ct.c_int(256))
         if rc != 0:
@@ -248,6 +259,7 @@ class Reference:
         L = ct.CDLL(path)
         self.L = L
         L.ref_color.restype = ct.c_int
+        L.ref_color_mhash.restype = ct.c_int
         L.ref_coloring_phase.restype = ct.c_double
         L.ref_basic_phase.restype = ct.c_double
         L.ref_renumber.restype = ct.c_long
@@ -275,6 +287,15 @@ class Reference:
         mc = self.L.ref_color(ct.c_long(g.num_vertices), _lp(p), _lp(t), _dp(w), _ip(col),
                               ct.c_int(nthreads), ct.byref(tt))
         return col, mc, tt.value
+
+    def color_mhash(self, g, num_colors=16, nthreads=1):
+        """The reference's multi-hash max/min colouring (rand() values)."""
+        p, t, w = _csr(g)
+        col = np.empty(g.num_vertices, dtype=np.int32)
+        mc = self.L.ref_color_mhash(ct.c_long(g.num_vertices), _lp(p), _lp(t), _dp(w),
+                                    ct.c_int(2), ct.c_int(max(1, num_colors // 4)), _ip(col),
+                                    ct.c_int(nthreads))
+        return col, mc
 
     def coloring_phase(self, g, colors, num_colors, lower=-1.0, thresh=1e-4, nthreads=1):
         p, t, w = _csr(g)

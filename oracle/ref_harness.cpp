@@ -89,6 +89,19 @@ int ref_color(long nv, const long *ptr, const long *tail, const double *w, int *
     return mc;
 }
 
+// Coloring/coloringMultiHashMaxMin.cpp:59 algoColoringMultiHashMaxMin; its
+// random values come from the C library's rand().
+int ref_color_mhash(long nv, const long *ptr, const long *tail, const double *w, int nHash,
+                    int nItrs, int *color, int nthreads) {
+    graph *G = make_graph(nv, ptr, tail, w);
+    double t = 0;
+    quiet_begin();
+    int mc = algoColoringMultiHashMaxMin(G, color, nthreads, &t, nHash, nItrs);
+    quiet_end();
+    free_graph(G);
+    return mc;
+}
+
 // Coloring/parallelLouvainWithColoring.cpp:47 algoLouvainWithDistOneColoring
 double ref_coloring_phase(long nv, const long *ptr, const long *tail, const double *w,
                           long *C, int *color, int numColor, double Lower, double thresh,

@@ -20,3 +20,30 @@ def load(name):
 def pins():
     with open(os.path.join(GOLDEN, 'pins.json')) as f:
         return json.load(f)
+
+
+def mhash_cases():
+    """(name, graph, numColors, expected) for every case of mhash.npz: the
+    incomplete colouring (coloring = 3) of the reference at one thread, its
+    rand() seeded by srand(seed) before each call."""
+    z = np.load(os.path.join(GOLDEN, 'mhash.npz'))
+    seed = int(z['seed'])
+    out = []
+    for name in map(str, z['names']):
+        if f'{name}_ptr' in z.files:
+            g = CSRGraph(z[f'{name}_ptr'], z[f'{name}_tail'].astype(np.int64),
+                         np.ones(len(z[f'{name}_tail'])))
+        else:
+            g, _ = load(name)
+        for nc in map(int, z['colors']):
+            p = f'{name}_{nc}_'
+            exp = {k[len(p):]: z[k] for k in z.files if k.startswith(p)}
+            exp['seed'] = seed
+            out.append((f'{name}-{nc}', g, nc, exp))
+    return out
+
+
+def srand(seed):
+    """Seed the C library's rand(), which the multi-hash colouring draws from."""
+    import ctypes as ct
+    ct.CDLL(None).srand(seed)

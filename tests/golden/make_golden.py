@@ -4,6 +4,7 @@ Run from the repository root after ``make -C oracle``:
 
     python tests/golden/make_golden.py [/path/to/grappolo]
     python tests/golden/make_golden.py --vf     # only vf.npz (vertex following)
+    python tests/golden/make_golden.py --mhash  # only mhash.npz (coloring = 3)
 
 Each fixture ``<case>.npz`` holds an input CSR and what the reference's
 functions return for it at OMP_NUM_THREADS=1: the distance-1 colouring, one
@@ -133,12 +134,49 @@ def make_vf(R, ref_root):
     print('wrote vf', list(cases))
 
 
+MHASH_SEED = 1  # srand() seed drawn before each multi-hash call
+MHASH_COLORS = (4, 16)
+
+
+def make_mhash(R, ref_root):
+    """mhash.npz: the incomplete multi-hash max/min colouring (coloring = 3)
+    alone and inside runMultiPhaseColoring, at one thread, with the C
+    library's rand() seeded by srand(MHASH_SEED) before each call.  Inputs are
+    those of the <case>.npz fixtures, plus an unweighted 6000-vertex planted
+    partition stored here."""
+    import ctypes as ct
+    libc = ct.CDLL(None)
+    cases = {k: v for k, v in all_cases(ref_root).items()
+             if k in ('karate', 'pp1000', 'pp1000_w', 'rmat10', 'loops_isolated', 'hubs')}
+    cases['pp6k'] = graphs.planted_partition_mixed(6000, 40, 0.3, 8.0, seed=3)
+    out = {}
+    for name, g in cases.items():
+        if name == 'pp6k':  # the others are the inputs of <name>.npz
+            out.update({f'{name}_ptr': g.ptr, f'{name}_tail': g.tail.astype(np.int32)})
+        for nc in MHASH_COLORS:
+            libc.srand(MHASH_SEED)
+            col, mc = R.color_mhash(g, nc)
+            libc.srand(MHASH_SEED)
+            Co, s, _ = R.run_multiphase_coloring(g, 1000, 1e-6, 1e-4, coloring=3, num_colors=nc)
+            out.update({f'{name}_{nc}_color': col.astype(np.int16), f'{name}_{nc}_max_color': mc,
+                        f'{name}_{nc}_C': Co.astype(np.int32), f'{name}_{nc}_phases': s['phases'],
+                        f'{name}_{nc}_itr': s['total_iterations'],
+                        f'{name}_{nc}_clusters': s['final_clusters'],
+                        f'{name}_{nc}_mod': s['final_mod']})
+    np.savez_compressed(os.path.join(HERE, 'mhash.npz'), names=np.array(list(cases)),
+                        colors=np.array(MHASH_COLORS), seed=MHASH_SEED, **out)
+    print('wrote mhash', list(cases))
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 and not sys.argv[1].startswith('--') \
         else '/root/reference'
     R = Reference()
     if '--vf' in sys.argv:
         make_vf(R, ref_root)
+        return
+    if '--mhash' in sys.argv:
+        make_mhash(R, ref_root)
         return
     rng = np.random.default_rng(2024)
     for name, g in all_cases(ref_root).items():

@@ -47,6 +47,7 @@ REFERENCE_SYMBOLS = [
     '_Z22buildNextLevelGraphOptP5graphS0_Plli',
     '_Z15vertexFollowingP5graphPl',
     '_Z15buildNewGraphVFP5graphS0_Pll',
+    '_Z27algoColoringMultiHashMaxMinP5graphPiiPdii',
 ]
 
 
@@ -70,7 +71,8 @@ def test_compat_header_matches_reference_mangling(tmp_path):
                    '  renumberClustersContiguously(c, 4);\n'
                    '  buildNextLevelGraphOpt(g, o, c, 2, 1);\n'
                    '  vertexFollowing(g, c);\n'
-                   '  buildNewGraphVF(g, o, c, 2);\n}\n')
+                   '  buildNewGraphVF(g, o, c, 2);\n'
+                   '  algoColoringMultiHashMaxMin(g, col, 1, t, 2, 4);\n}\n')
     obj = tmp_path / 'use.o'
     subprocess.run(['g++', '-c', '-I', os.path.join(ROOT, 'include'), str(src), '-o', str(obj)],
                    check=True)

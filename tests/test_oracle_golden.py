@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from grappolo_b200 import graphs
-from _golden import CASES, load, pins
+from _golden import CASES, load, mhash_cases, pins, srand
 
 
 @pytest.mark.parametrize('name', CASES)
@@ -105,3 +105,26 @@ def test_vertex_following_golden(oracle, name, g, ref):
     assert ne == int(ref['ne'])
     assert np.array_equal(cg.ptr, ref['cptr']) and np.array_equal(cg.tail, ref['ctail'])
     assert np.array_equal(cg.weight, ref['cweight'])
+
+
+@pytest.mark.parametrize('case', mhash_cases(), ids=lambda c: c[0])
+def test_multihash_coloring_golden(oracle, case):
+    """Coloring/coloringMultiHashMaxMin.cpp at one thread: colours, maxColor."""
+    _, g, nc, exp = case
+    srand(exp['seed'])
+    col, mc = oracle.color_mhash(g, nc)
+    assert mc == int(exp['max_color'])
+    assert np.array_equal(col, exp['color'])
+
+
+@pytest.mark.parametrize('case', mhash_cases(), ids=lambda c: c[0])
+def test_multiphase_multihash_golden(oracle, case):
+    """runMultiPhaseColoring with coloring = 3: C_orig and the summary."""
+    _, g, nc, exp = case
+    srand(exp['seed'])
+    C, s, _ = oracle.run_multiphase_coloring(g, coloring=3, num_colors=nc)
+    assert np.array_equal(C, exp['C'])
+    assert s['phases'] == int(exp['phases'])
+    assert s['total_iterations'] == int(exp['itr'])
+    assert s['final_clusters'] == int(exp['clusters'])
+    assert abs(s['final_mod'] - float(exp['mod'])) <= 5e-7  # the reference prints %lf

@@ -84,3 +84,23 @@ def test_vertex_following_matches_reference(seed, oracle, reference):
     assert ne1 == ne2
     assert np.array_equal(a.ptr, b.ptr) and np.array_equal(a.tail, b.tail)
     assert np.array_equal(a.weight, b.weight)
+
+
+@pytest.mark.parametrize('name,g', list(_graphs()))
+@pytest.mark.parametrize('num_colors', [4, 12, 40])
+def test_multihash_matches_reference(oracle, reference, name, g, num_colors):
+    """Coloring/coloringMultiHashMaxMin.cpp and runMultiPhaseColoring with
+    coloring = 3, the C library's rand() seeded alike before each side."""
+    from _golden import srand
+    srand(5)
+    col_o, mc_o = oracle.color_mhash(g, num_colors)
+    srand(5)
+    col_r, mc_r = reference.color_mhash(g, num_colors)
+    assert mc_o == mc_r and np.array_equal(col_o, col_r)
+    srand(9)
+    Co, so, _ = oracle.run_multiphase_coloring(g, coloring=3, num_colors=num_colors)
+    srand(9)
+    Cr, sr, _ = reference.run_multiphase_coloring(g, coloring=3, num_colors=num_colors)
+    assert np.array_equal(Co, Cr)
+    assert so['phases'] == sr['phases'] and so['total_iterations'] == sr['total_iterations']
+    assert abs(so['final_mod'] - sr['final_mod']) <= 5e-7
