@@ -13,6 +13,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, 'libgrappolo_b200.so')
 
 GLV_OK = 0
+GLV_CSR_REMOVE_EDGES = 1
+GLV_CSR_SORT_ROWS = 2
 GLV_MODE_VERIFY = 0
 GLV_MODE_FAST = 1
 GLV_MODE_LEARNED = 2
@@ -103,7 +105,10 @@ def lib():
                  'glv_decide_batch', 'glv_dev_modularity_static', 'glv_gate_set',
                  'glv_gate_infer', 'glv_gate_grad', 'glv_gate_train', 'glv_trace_begin',
                  'glv_trace_end', 'glv_run_batch_csr', 'glv_dev_run_batch',
-                 'glv_vertex_following', 'glv_build_new_graph_vf'):
+                 'glv_vertex_following', 'glv_build_new_graph_vf', 'glv_remove_edges',
+                 'glv_sort_edges_undirected', 'glv_sort_node_edges_by_index', 'glv_build_csr',
+                 'glv_dev_build_csr', 'glv_binary_header', 'glv_load_binary', 'glv_write_binary',
+                 'glv_dev_load_binary'):
         getattr(L, name).restype = ct.c_int
     L.glv_run_multiphase_coloring.argtypes = [P(GlvGraph), P(ct.c_long), ct.c_int, ct.c_int,
                                               ct.c_int, ct.c_long, ct.c_double, ct.c_double,
@@ -130,6 +135,19 @@ def lib():
                                             P(ct.c_double)]
     L.glv_color_multihash.argtypes = [P(GlvGraph), P(ct.c_int), ct.c_int, ct.c_int, P(ct.c_int),
                                       P(ct.c_double)]
+    L.glv_remove_edges.argtypes = [ct.c_long, ct.c_long, P(GlvEdge), P(ct.c_long)]
+    L.glv_sort_edges_undirected.argtypes = [ct.c_long, ct.c_long, P(GlvEdge), P(GlvEdge),
+                                            P(ct.c_long)]
+    L.glv_sort_node_edges_by_index.argtypes = [ct.c_long, P(GlvEdge), P(GlvEdge), P(ct.c_long)]
+    L.glv_build_csr.argtypes = [ct.c_long, ct.c_long, P(GlvEdge), ct.c_int, P(GlvGraph)]
+    L.glv_dev_build_csr.argtypes = [ct.c_long, ct.c_long, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                    ct.c_int, ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                    P(ct.c_long), ct.c_void_p]
+    L.glv_binary_header.argtypes = [ct.c_char_p, P(ct.c_long), P(ct.c_long), P(ct.c_long)]
+    L.glv_load_binary.argtypes = [ct.c_char_p, P(GlvGraph)]
+    L.glv_write_binary.argtypes = [P(GlvGraph), ct.c_char_p, ct.c_long]
+    L.glv_dev_load_binary.argtypes = [ct.c_char_p, ct.c_long, ct.c_long, ct.c_void_p, ct.c_void_p,
+                                      ct.c_void_p, ct.c_void_p]
     L.glv_renumber_clusters.argtypes = [P(ct.c_long), ct.c_long, P(ct.c_long)]
     L.glv_build_next_level.argtypes = [P(GlvGraph), P(GlvGraph), P(ct.c_long), ct.c_long,
                                        ct.c_int, P(ct.c_double)]

@@ -110,6 +110,35 @@ int algoColoringMultiHashMaxMin(graph *G, int *vtxColor, int nThreads, double *t
   return mc;
 }
 
+long removeEdges(long NV, long NE, edge *edgeList) {
+  long n = 0;
+  int rc = glv_remove_edges(NV, NE, (glv_edge *)edgeList, &n);
+  if (rc != GLV_OK) die("removeEdges", rc);
+  return n;
+}
+
+void SortEdgesUndirected(long NV, long NE, edge *list1, edge *list2, long *ptrs) {
+  int rc = glv_sort_edges_undirected(NV, NE, (const glv_edge *)list1, (glv_edge *)list2, ptrs);
+  if (rc != GLV_OK) die("SortEdgesUndirected", rc);
+}
+
+void SortNodeEdgesByIndex(long NV, edge *list1, edge *list2, long *ptrs) {
+  int rc = glv_sort_node_edges_by_index(NV, (glv_edge *)list1, (glv_edge *)list2, ptrs);
+  if (rc != GLV_OK) die("SortNodeEdgesByIndex", rc);
+}
+
+void parse_EdgeListBinaryNew(graph *G, char *fileName) {
+  printf("Parsing a file in binary format...\n");
+  int rc = glv_load_binary(fileName, (glv_graph *)G);
+  if (rc != GLV_OK) die("parse_EdgeListBinaryNew", rc);
+}
+
+void writeGraphBinaryFormatNew(graph *G, char *filename, long weighted) {
+  int rc = glv_write_binary((const glv_graph *)G, filename, weighted);
+  if (rc != GLV_OK) die("writeGraphBinaryFormatNew", rc);
+  printf("Graph has been stored in file: %s\n", filename);
+}
+
 long renumberClustersContiguously(long *C, long size) {
   long n = 0;
   int rc = glv_renumber_clusters(C, size, &n);

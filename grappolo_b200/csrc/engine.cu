@@ -2876,6 +2876,11 @@ int glv_decide_batch(long nv, const long *ptr, const long *tail, const double *w
 }  // extern "C"
 
 // =========================================================================
+// Edge lists to CSR, binary graph files
+// =========================================================================
+#include "csr_build.cuh"
+
+// =========================================================================
 // Modularity without allocation (glv_dev_modularity_static)
 // =========================================================================
 #include <mutex>

@@ -180,6 +180,118 @@ def buildNewGraphVF(G, C, numUniqueClusters):
     return _take_graph(out)
 
 
+def _edges(head, tail, weight=None):
+    """A contiguous glv_edge array (Graph.EDGE records) from three arrays."""
+    head = np.asarray(head, dtype=np.int64)
+    e = np.empty(head.shape[0], dtype=Graph.EDGE)
+    e['head'] = head
+    e['tail'] = np.asarray(tail, dtype=np.int64)
+    e['weight'] = 1.0 if weight is None else np.asarray(weight, dtype=np.float64)
+    return e
+
+
+def _ep(e):
+    return e.ctypes.data_as(_P(_lib.GlvEdge))
+
+
+def removeEdges(NV, edgeList):
+    """Utility/utilityFunctions.cpp:416 — on a copy of ``edgeList`` (Graph.EDGE
+    records): returns (edges, NGE); the first NGE records are the kept edges in
+    the reference's order, the rest as they were."""
+    e = np.array(edgeList, dtype=Graph.EDGE, copy=True)
+    n = ct.c_long(0)
+    _lib.check(_lib.lib().glv_remove_edges(NV, e.shape[0], _ep(e), ct.byref(n)))
+    return e, n.value
+
+
+def SortEdgesUndirected(NV, list1):
+    """Utility/utilityFunctions.cpp:463 — returns (ptrs int64[NV+2], list2 of
+    2*NE records: every edge in the rows of both ends, in list order)."""
+    e = np.ascontiguousarray(list1, dtype=Graph.EDGE)
+    out = np.empty(2 * e.shape[0], dtype=Graph.EDGE)
+    ptrs = np.zeros(NV + 2, dtype=np.int64)
+    _lib.check(_lib.lib().glv_sort_edges_undirected(NV, e.shape[0], _ep(e), _ep(out),
+                                                    ptrs.ctypes.data_as(_P(ct.c_long))))
+    return ptrs, out
+
+
+def SortNodeEdgesByIndex(NV, list1, ptrs):
+    """Utility/utilityFunctions.cpp:501 — returns a copy of ``list1`` with each
+    row sorted by tail (equal tails: later entry first, as the reference)."""
+    e = np.array(list1, dtype=Graph.EDGE, copy=True)
+    p = np.ascontiguousarray(ptrs, dtype=np.int64)
+    _lib.check(_lib.lib().glv_sort_node_edges_by_index(NV, _ep(e), None,
+                                                       p.ctypes.data_as(_P(ct.c_long))))
+    return e
+
+
+def build_csr(NV, head, tail, weight=None, remove_edges=True, sort_rows=False):
+    """Edge list to CSR on the GPU as the reference's loaders build it
+    (glv_build_csr): optional removeEdges, both directions of every edge in list
+    order, optional per-row sort.  Returns (CSRGraph, numEdges)."""
+    e = _edges(head, tail, weight)
+    flags = (_lib.GLV_CSR_REMOVE_EDGES if remove_edges else 0) | \
+        (_lib.GLV_CSR_SORT_ROWS if sort_rows else 0)
+    out = _lib.GlvGraph()
+    _lib.check(_lib.lib().glv_build_csr(NV, e.shape[0], _ep(e), flags, ct.byref(out)))
+    return _take_graph(out)
+
+
+def build_csr_device(NV, d_head, d_tail, d_weight=None, remove_edges=True, sort_rows=False,
+                     device='cuda'):
+    """Device form (glv_dev_build_csr) on torch tensors: int64 heads / tails,
+    float64 weights or None.  Returns (ptr int64[NV+1], tail int32, weight
+    float64) tensors holding exactly the built entries."""
+    import torch
+    ne = int(d_head.shape[0])
+    ptr = torch.empty(NV + 1, dtype=torch.int64, device=device)
+    tail = torch.empty(max(2 * ne, 1), dtype=torch.int32, device=device)
+    w = torch.empty(max(2 * ne, 1), dtype=torch.float64, device=device)
+    flags = (_lib.GLV_CSR_REMOVE_EDGES if remove_edges else 0) | \
+        (_lib.GLV_CSR_SORT_ROWS if sort_rows else 0)
+    nnz = ct.c_long(0)
+    stream = torch.cuda.current_stream(device).cuda_stream
+    _lib.check(_lib.lib().glv_dev_build_csr(
+        NV, ne, d_head.data_ptr(), d_tail.data_ptr(),
+        d_weight.data_ptr() if d_weight is not None else None, flags, ptr.data_ptr(),
+        tail.data_ptr(), w.data_ptr(), ct.byref(nnz), stream or None))
+    return ptr, tail[:nnz.value], w[:nnz.value]
+
+
+def parse_EdgeListBinaryNew(fileName):
+    """InputsOutput/loadBinary.cpp:6 — returns (CSRGraph, numEdges)."""
+    out = _lib.GlvGraph()
+    _lib.check(_lib.lib().glv_load_binary(os.fsencode(fileName), ct.byref(out)))
+    return _take_graph(out)
+
+
+def writeGraphBinaryFormatNew(G, filename, weighted=1):
+    """InputsOutput/writeBinary.cpp:2 — writes ``G`` (numEdges = nnz / 2 records
+    pairs, as the reference stores 2*numEdges entries)."""
+    G = _as_graph(G)
+    st = _lib.GlvGraph(G.struct.numVertices, G.struct.sVertices, G.csr.nnz // 2,
+                       G.struct.edgeListPtrs, G.struct.edgeList)
+    _lib.check(_lib.lib().glv_write_binary(ct.byref(st), os.fsencode(filename), weighted))
+
+
+def load_binary_device(fileName, device='cuda'):
+    """Streams a binary graph file into device memory (glv_dev_load_binary).
+    Returns (ptr int64[NV+1], tail int32[2*NE], weight float64[2*NE]) tensors."""
+    import torch
+    nv, ne, wt = ct.c_long(0), ct.c_long(0), ct.c_long(0)
+    path = os.fsencode(fileName)
+    L = _lib.lib()
+    _lib.check(L.glv_binary_header(path, ct.byref(nv), ct.byref(ne), ct.byref(wt)))
+    nnz = 2 * ne.value
+    ptr = torch.empty(nv.value + 1, dtype=torch.int64, device=device)
+    tail = torch.empty(max(nnz, 1), dtype=torch.int32, device=device)
+    w = torch.empty(max(nnz, 1), dtype=torch.float64, device=device)
+    stream = torch.cuda.current_stream(device).cuda_stream
+    _lib.check(L.glv_dev_load_binary(path, nv.value, nnz, ptr.data_ptr(), tail.data_ptr(),
+                                     w.data_ptr(), stream or None))
+    return ptr, tail[:nnz], w[:nnz]
+
+
 def _take_graph(out):
     """CSRGraph + numEdges from a glv_graph whose arrays the library malloc'd
     (released here)."""

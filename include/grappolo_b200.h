@@ -42,7 +42,8 @@ enum {
   GLV_ERR_TOO_LARGE = 5,  /* numVertices >= 2^31 (ids are int32 on the device) */
   GLV_ERR_UNSUPPORTED = 6,/* option outside this engine's scope (e.g. coloring 2, replaceMap) */
   GLV_ERR_NO_DEVICE = 7,  /* no CUDA device */
-  GLV_ERR_LIMIT = 8       /* a size exceeds a fixed limit of the entry point */
+  GLV_ERR_LIMIT = 8,      /* a size exceeds a fixed limit of the entry point */
+  GLV_ERR_IO = 9          /* a graph file could not be opened, read or written */
 };
 
 /* Execution modes.
@@ -110,6 +111,63 @@ typedef struct glv_run_stats {
   int nphase;               /* entries filled in phase[] */
   glv_phase_stats phase[GLV_MAX_PHASES];
 } glv_run_stats;
+
+/* ---- graph construction and files ---------------------------------------- */
+
+/* Replaces removeEdges (Utility/utilityFunctions.cpp:416-460, input_output.h:5):
+ * drops self-loops and every repeat of a (head, tail) pair (the first stays),
+ * compacting in place as the reference does: the first *numGoodEdges entries
+ * are the kept edges in the reference's order; entries past them are left as
+ * they were.  Runs on the GPU. */
+int glv_remove_edges(long NV, long NE, glv_edge *edgeList, long *numGoodEdges);
+
+/* Replaces SortEdgesUndirected (utilityFunctions.cpp:463-498, input_output.h:6):
+ * list2[2*NE] receives every edge in the rows of both its ends, in list order;
+ * ptrs[NV+2] the row offsets (ptrs[NV+1] = 2*NE, as the reference leaves it). */
+int glv_sort_edges_undirected(long NV, long NE, const glv_edge *list1, glv_edge *list2,
+                              long *ptrs);
+
+/* Replaces SortNodeEdgesByIndex (utilityFunctions.cpp:501-531,
+ * utilityClusteringFunctions.h:83): each row of list1 sorted by tail, equal
+ * tails in the order the reference's merge sort leaves them (later entry
+ * first).  list2 is not written (the reference uses it as scratch). */
+int glv_sort_node_edges_by_index(long NV, glv_edge *list1, glv_edge *list2, const long *ptrs);
+
+/* Edge list to CSR in one call, as the reference's loaders do it
+ * (e.g. InputsOutput/loadPajekFormat.cpp:94-150): GLV_CSR_REMOVE_EDGES first
+ * applies removeEdges; every edge is then stored in the rows of both ends in
+ * list order; GLV_CSR_SORT_ROWS then applies SortNodeEdgesByIndex.  Gout's
+ * arrays are malloc'd (free with free()); Gout->numEdges = kept edges. */
+#define GLV_CSR_REMOVE_EDGES 1
+#define GLV_CSR_SORT_ROWS 2
+int glv_build_csr(long NV, long NE, const glv_edge *edges, int flags, glv_graph *Gout);
+
+/* Device-resident form of glv_build_csr: int64 heads / tails and double
+ * weights (NULL: all 1.0) on the device; d_ptr[NV+1] int64, d_tail_out and
+ * d_weight_out must hold 2*NE entries (int32 / double); *nnz receives the
+ * entries written.  Ordered on `stream` (a cudaStream_t, NULL = legacy
+ * default stream); returns after it has finished. */
+int glv_dev_build_csr(long NV, long NE, const long *d_head, const long *d_tail,
+                      const double *d_weight, int flags, long *d_ptr, int *d_tail_out,
+                      double *d_weight_out, long *nnz, void *stream);
+
+/* Grappolo's binary graph file (InputsOutput/loadBinary.cpp:6-48,
+ * writeBinary.cpp:2-29, input_output.h:15,25): NV, NE, weighted as three
+ * longs, edgeListPtrs[NV+1], then 2*NE glv_edge records.  glv_load_binary
+ * replaces parse_EdgeListBinaryNew (arrays malloc'd); glv_write_binary
+ * replaces writeGraphBinaryFormatNew (G->edgeList must hold 2*numEdges
+ * entries). */
+int glv_binary_header(const char *path, long *numVertices, long *numEdges, long *weighted);
+int glv_load_binary(const char *path, glv_graph *G);
+int glv_write_binary(const glv_graph *G, const char *path, long weighted);
+
+/* Streams a binary graph file straight into device memory: d_ptr[NV+1]
+ * int64, d_tail[2*NE] int32, d_weight[2*NE] double (sizes from
+ * glv_binary_header; nnz = 2*NE).  The file is read in chunks through two
+ * pinned buffers while earlier chunks are copied and split on `stream`;
+ * tails are checked against NV.  Returns after the stream has finished. */
+int glv_dev_load_binary(const char *path, long numVertices, long nnz, long *d_ptr, int *d_tail,
+                        double *d_weight, void *stream);
 
 /* ---- multiphase drivers ------------------------------------------------- */
 

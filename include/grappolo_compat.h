@@ -58,4 +58,13 @@ double buildNextLevelGraphOpt(graph *Gin, graph *Gout, long *C, long numUniqueCl
 long vertexFollowing(graph *G, long *C);
 double buildNewGraphVF(graph *Gin, graph *Gout, long *C, long numUniqueClusters);
 
+/* DefineStructure/input_output.h:5-6, utilityClusteringFunctions.h:83
+ * (Utility/utilityFunctions.cpp:416-531), computed on the GPU */
+long removeEdges(long NV, long NE, edge *edgeList);
+void SortEdgesUndirected(long NV, long NE, edge *list1, edge *list2, long *ptrs);
+void SortNodeEdgesByIndex(long NV, edge *list1, edge *list2, long *ptrs);
+/* DefineStructure/input_output.h:15,25 (InputsOutput/loadBinary.cpp, writeBinary.cpp) */
+void parse_EdgeListBinaryNew(graph *G, char *fileName);
+void writeGraphBinaryFormatNew(graph *G, char *filename, long weighted);
+
 #endif /* GRAPPOLO_COMPAT_H */

@@ -597,6 +597,95 @@ long lvo_build_new_graph_vf(long nv, const long *ptr, const long *tail, const do
     return onnz;
 }
 
+/* ---- edge-list preprocessing (Utility/utilityFunctions.cpp:416-531) ---- */
+
+static const long *g_key_head, *g_key_tail;
+static int cmp_pair_then_index(const void *a, const void *b) {
+    long i = *(const long *)a, j = *(const long *)b;
+    if (g_key_head[i] != g_key_head[j]) return g_key_head[i] < g_key_head[j] ? -1 : 1;
+    if (g_key_tail[i] != g_key_tail[j]) return g_key_tail[i] < g_key_tail[j] ? -1 : 1;
+    return i < j ? -1 : (i > j);
+}
+
+/* removeEdges (utilityFunctions.cpp:416-460) on SoA arrays, in place.  An
+ * edge is kept when it is not a self-loop and no earlier edge has the same
+ * (head, tail) (:428-446).  The compaction (:448-455) fills the dropped slots
+ * below NGE, in ascending order, with the kept edges at positions >= NGE
+ * taken from the top down; positions >= NGE are left as they were.
+ * Returns NGE.                                                              */
+long lvo_remove_edges(long nv, long ne, long *head, long *tail, double *w) {
+    (void)nv;
+    long *idx = (long *)malloc(sizeof(long) * (ne ? ne : 1));
+    unsigned char *good = (unsigned char *)calloc(ne ? ne : 1, 1);
+    for (long i = 0; i < ne; i++) idx[i] = i;
+    g_key_head = head; g_key_tail = tail;
+    qsort(idx, ne, sizeof(long), cmp_pair_then_index);
+    long nge = 0;
+    for (long s = 0; s < ne; s++) {
+        long i = idx[s];
+        int first = s == 0 || head[idx[s - 1]] != head[i] || tail[idx[s - 1]] != tail[i];
+        if (first && head[i] != tail[i]) { good[i] = 1; nge++; }
+    }
+    long top = ne - 1;
+    for (long k = 0; k < nge; k++) {
+        if (good[k]) continue;
+        while (!good[top]) top--;
+        head[k] = head[top]; tail[k] = tail[top]; w[k] = w[top];
+        top--;
+    }
+    free(idx); free(good);
+    return nge;
+}
+
+/* SortEdgesUndirected (utilityFunctions.cpp:463-498): every edge i, in list
+ * order, is appended to its head's row as head->tail and then to its tail's
+ * row as tail->head.  ptrs[0..NV] is the CSR offset array and ptrs[NV+1]
+ * = 2*NE, as the reference's shifted histogram leaves it.                 */
+void lvo_sort_edges_undirected(long nv, long ne, const long *head, const long *tail,
+                               const double *w, long *ptrs, long *ohead, long *otail,
+                               double *ow) {
+    long *fill = (long *)calloc(nv + 1, sizeof(long));
+    for (long i = 0; i <= nv + 1; i++) ptrs[i] = 0;
+    for (long i = 0; i < ne; i++) { ptrs[head[i] + 1]++; ptrs[tail[i] + 1]++; }
+    for (long v = 0; v < nv; v++) ptrs[v + 1] += ptrs[v];
+    ptrs[nv + 1] = 2 * ne;
+    for (long v = 0; v < nv; v++) fill[v] = ptrs[v];
+    for (long i = 0; i < ne; i++) {
+        long a = fill[head[i]]++;
+        ohead[a] = head[i]; otail[a] = tail[i]; ow[a] = w[i];
+        long b = fill[tail[i]]++;
+        ohead[b] = tail[i]; otail[b] = head[i]; ow[b] = w[i];
+    }
+    free(fill);
+}
+
+static const long *g_row_tail;
+static int cmp_tail_then_later(const void *a, const void *b) {
+    long i = *(const long *)a, j = *(const long *)b;
+    if (g_row_tail[i] != g_row_tail[j]) return g_row_tail[i] < g_row_tail[j] ? -1 : 1;
+    return i > j ? -1 : (i < j);
+}
+
+/* SortNodeEdgesByIndex (utilityFunctions.cpp:501-531): each row sorted by
+ * tail.  Its bottom-up merge takes the right run's element on equal tails
+ * (:517-518), and two entries of one row first meet when the higher-placed
+ * one is in the right run, so equal tails end in descending position.     */
+void lvo_sort_node_edges(long nv, const long *ptrs, long *head, long *tail, double *w) {
+    long nnz = ptrs[nv];
+    long *idx = (long *)malloc(sizeof(long) * (nnz ? nnz : 1));
+    long *th = (long *)malloc(sizeof(long) * (nnz ? nnz : 1));
+    long *tt = (long *)malloc(sizeof(long) * (nnz ? nnz : 1));
+    double *tw = (double *)malloc(sizeof(double) * (nnz ? nnz : 1));
+    memcpy(th, head, sizeof(long) * nnz); memcpy(tt, tail, sizeof(long) * nnz);
+    memcpy(tw, w, sizeof(double) * nnz);
+    for (long j = 0; j < nnz; j++) idx[j] = j;
+    g_row_tail = tt;
+    for (long v = 0; v < nv; v++)
+        qsort(idx + ptrs[v], ptrs[v + 1] - ptrs[v], sizeof(long), cmp_tail_then_later);
+    for (long j = 0; j < nnz; j++) { head[j] = th[idx[j]]; tail[j] = tt[idx[j]]; w[j] = tw[idx[j]]; }
+    free(idx); free(th); free(tt); free(tw);
+}
+
 void lvo_free(void *p) { free(p); }
 
 /* Q of a final assignment over the original graph.  The reference's

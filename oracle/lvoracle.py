@@ -76,6 +76,7 @@ class COracle:
         L.lvo_vertex_degrees.restype = ct.c_double
         L.lvo_color_greedy.restype = ct.c_int
         L.lvo_color_mhash.restype = ct.c_int
+        L.lvo_remove_edges.restype = ct.c_long
         L.lvo_coloring_phase.restype = ct.c_double
         L.lvo_basic_phase.restype = ct.c_double
         L.lvo_renumber.restype = ct.c_long
@@ -164,6 +165,33 @@ class COracle:
         for a in (op, ot, ow):
             self.L.lvo_free(a)
         return out, ne.value
+
+    def remove_edges(self, nv, head, tail, w):
+        """removeEdges on copies of the SoA arrays: (head, tail, w, NGE)."""
+        h, t = np.array(head, dtype=np.int64), np.array(tail, dtype=np.int64)
+        ww = np.array(w, dtype=np.float64)
+        n = self.L.lvo_remove_edges(ct.c_long(nv), ct.c_long(len(h)), _lp(h), _lp(t), _dp(ww))
+        return h, t, ww, n
+
+    def sort_edges_undirected(self, nv, head, tail, w):
+        """SortEdgesUndirected: (ptrs[NV+2], head, tail, w) of the 2*NE entries."""
+        h, t = np.ascontiguousarray(head, dtype=np.int64), np.ascontiguousarray(tail, dtype=np.int64)
+        ww = np.ascontiguousarray(w, dtype=np.float64)
+        ne = len(h)
+        ptrs = np.zeros(nv + 2, dtype=np.int64)
+        oh, ot = np.zeros(2 * ne, dtype=np.int64), np.zeros(2 * ne, dtype=np.int64)
+        ow = np.zeros(2 * ne)
+        self.L.lvo_sort_edges_undirected(ct.c_long(nv), ct.c_long(ne), _lp(h), _lp(t), _dp(ww),
+                                             _lp(ptrs), _lp(oh), _lp(ot), _dp(ow))
+        return ptrs, oh, ot, ow
+
+    def sort_node_edges(self, nv, ptrs, head, tail, w):
+        """SortNodeEdgesByIndex on copies: (head, tail, w)."""
+        p = np.ascontiguousarray(ptrs, dtype=np.int64)
+        h, t = np.array(head, dtype=np.int64), np.array(tail, dtype=np.int64)
+        ww = np.array(w, dtype=np.float64)
+        self.L.lvo_sort_node_edges(ct.c_long(nv), _lp(p), _lp(h), _lp(t), _dp(ww))
+        return h, t, ww
 
     def decide_batch(self, g, C, vdeg, cdeg, csize, constant, verts):
         p, t, w = _csr(g)
@@ -260,6 +288,8 @@ class Reference:
         self.L = L
         L.ref_color.restype = ct.c_int
         L.ref_color_mhash.restype = ct.c_int
+        L.ref_remove_edges.restype = ct.c_long
+        L.ref_load_binary.restype = ct.c_long
         L.ref_coloring_phase.restype = ct.c_double
         L.ref_basic_phase.restype = ct.c_double
         L.ref_renumber.restype = ct.c_long
@@ -367,6 +397,53 @@ class Reference:
         for a in (op, ot, ow):
             self.L.ref_free(a)
         return out, ne.value
+
+    def remove_edges(self, nv, head, tail, w):
+        """removeEdges on copies of the SoA arrays: (head, tail, w, NGE)."""
+        h, t = np.array(head, dtype=np.int64), np.array(tail, dtype=np.int64)
+        ww = np.array(w, dtype=np.float64)
+        n = self.L.ref_remove_edges(ct.c_long(nv), ct.c_long(len(h)), _lp(h), _lp(t), _dp(ww))
+        return h, t, ww, n
+
+    def sort_edges_undirected(self, nv, head, tail, w):
+        """SortEdgesUndirected: (ptrs[NV+2], head, tail, w) of the 2*NE entries."""
+        h, t = np.ascontiguousarray(head, dtype=np.int64), np.ascontiguousarray(tail, dtype=np.int64)
+        ww = np.ascontiguousarray(w, dtype=np.float64)
+        ne = len(h)
+        ptrs = np.zeros(nv + 2, dtype=np.int64)
+        oh, ot = np.zeros(2 * ne, dtype=np.int64), np.zeros(2 * ne, dtype=np.int64)
+        ow = np.zeros(2 * ne)
+        self.L.ref_sort_edges_undirected(ct.c_long(nv), ct.c_long(ne), _lp(h), _lp(t), _dp(ww),
+                                             _lp(ptrs), _lp(oh), _lp(ot), _dp(ow))
+        return ptrs, oh, ot, ow
+
+    def sort_node_edges(self, nv, ptrs, head, tail, w):
+        """SortNodeEdgesByIndex on copies: (head, tail, w)."""
+        p = np.ascontiguousarray(ptrs, dtype=np.int64)
+        h, t = np.array(head, dtype=np.int64), np.array(tail, dtype=np.int64)
+        ww = np.array(w, dtype=np.float64)
+        self.L.ref_sort_node_edges(ct.c_long(nv), _lp(p), _lp(h), _lp(t), _dp(ww))
+        return h, t, ww
+
+    def write_binary(self, g, path, num_edges=None, weighted=1):
+        """writeGraphBinaryFormatNew of a CSR graph."""
+        p, t, w = _csr(g)
+        ne = g.nnz // 2 if num_edges is None else num_edges
+        self.L.ref_write_binary(ct.c_long(g.num_vertices), _lp(p), _lp(t), _dp(w), ct.c_long(ne),
+                                ct.c_long(weighted), str(path).encode())
+
+    def load_binary(self, path):
+        """parse_EdgeListBinaryNew: (ptr, head, tail, w, numEdges)."""
+        op, oh, ot, ow = _c_long_p(), _c_long_p(), _c_long_p(), _c_double_p()
+        ne = ct.c_long(0)
+        nv = self.L.ref_load_binary(str(path).encode(), ct.byref(op), ct.byref(oh), ct.byref(ot),
+                                    ct.byref(ow), ct.byref(ne))
+        nnz = 2 * ne.value
+        ptr = np.ctypeslib.as_array(op, (nv + 1,)).copy()
+        arr = [np.ctypeslib.as_array(a, (max(nnz, 1),))[:nnz].copy() for a in (oh, ot, ow)]
+        for a in (op, oh, ot, ow):
+            self.L.ref_free(a)
+        return ptr, arr[0], arr[1], arr[2], ne.value
 
     def decide_batch(self, g, C, vdeg, cdeg, csize, constant, verts):
         p, t, w = _csr(g)

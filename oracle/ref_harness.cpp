@@ -346,6 +346,78 @@ long ref_run_multiphase_basic(long nv, const long *ptr, const long *tail, const 
     return run_captured(log, cap, call_basic, &a);
 }
 
+static edge *make_edges(long n, const long *h, const long *t, const double *w) {
+    edge *e = (edge *)malloc(sizeof(edge) * (n ? n : 1));
+    for (long i = 0; i < n; i++) { e[i].head = h[i]; e[i].tail = t[i]; e[i].weight = w[i]; }
+    return e;
+}
+
+static void take_edges(long n, const edge *e, long *h, long *t, double *w) {
+    for (long i = 0; i < n; i++) { h[i] = e[i].head; t[i] = e[i].tail; w[i] = e[i].weight; }
+}
+
+// Utility/utilityFunctions.cpp:416 removeEdges; all NE entries written back.
+long ref_remove_edges(long nv, long ne, long *h, long *t, double *w) {
+    edge *e = make_edges(ne, h, t, w);
+    quiet_begin();
+    long nge = removeEdges(nv, ne, e);
+    quiet_end();
+    take_edges(ne, e, h, t, w);
+    free(e);
+    return nge;
+}
+
+// Utility/utilityFunctions.cpp:463 SortEdgesUndirected; ptrs holds NV+2 entries.
+void ref_sort_edges_undirected(long nv, long ne, const long *h, const long *t, const double *w,
+                               long *ptrs, long *oh, long *ot, double *ow) {
+    edge *e1 = make_edges(ne, h, t, w);
+    edge *e2 = (edge *)malloc(sizeof(edge) * (2 * ne ? 2 * ne : 1));
+    SortEdgesUndirected(nv, ne, e1, e2, ptrs);
+    take_edges(2 * ne, e2, oh, ot, ow);
+    free(e1); free(e2);
+}
+
+// Utility/utilityFunctions.cpp:501 SortNodeEdgesByIndex, rows in place.
+void ref_sort_node_edges(long nv, const long *ptrs, long *h, long *t, double *w) {
+    long nnz = ptrs[nv];
+    edge *e1 = make_edges(nnz, h, t, w);
+    edge *e2 = (edge *)malloc(sizeof(edge) * (nnz ? nnz : 1));
+    SortNodeEdgesByIndex(nv, e1, e2, (long *)ptrs);
+    take_edges(nnz, e1, h, t, w);
+    free(e1); free(e2);
+}
+
+// InputsOutput/writeBinary.cpp:2 writeGraphBinaryFormatNew.
+void ref_write_binary(long nv, const long *ptr, const long *tail, const double *w, long numEdges,
+                      long weighted, const char *path) {
+    graph *G = make_graph(nv, ptr, tail, w);
+    G->numEdges = numEdges;
+    quiet_begin();
+    writeGraphBinaryFormatNew(G, (char *)path, weighted);
+    quiet_end();
+    free_graph(G);
+}
+
+// InputsOutput/loadBinary.cpp:6 parse_EdgeListBinaryNew -> SoA CSR (malloc'd).
+long ref_load_binary(const char *path, long **optr, long **ohead, long **otail, double **ow,
+                     long *numEdges) {
+    graph G;
+    quiet_begin();
+    parse_EdgeListBinaryNew(&G, (char *)path);
+    quiet_end();
+    long nv = G.numVertices, nnz = 2 * G.numEdges;
+    long *p = (long *)malloc(sizeof(long) * (nv + 1));
+    long *hh = (long *)malloc(sizeof(long) * (nnz ? nnz : 1));
+    long *t = (long *)malloc(sizeof(long) * (nnz ? nnz : 1));
+    double *ww = (double *)malloc(sizeof(double) * (nnz ? nnz : 1));
+    memcpy(p, G.edgeListPtrs, sizeof(long) * (nv + 1));
+    take_edges(nnz, G.edgeList, hh, t, ww);
+    free(G.edgeListPtrs);
+    free(G.edgeList);
+    *optr = p; *ohead = hh; *otail = t; *ow = ww; *numEdges = G.numEdges;
+    return nv;
+}
+
 // InputsOutput/loadMetis.cpp:19 loadMetisFileFormat -> SoA CSR (malloc'd).
 long ref_load_metis(const char *path, long **optr, long **otail, double **ow) {
     graph G;

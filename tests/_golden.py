@@ -47,3 +47,20 @@ def srand(seed):
     """Seed the C library's rand(), which the multi-hash colouring draws from."""
     import ctypes as ct
     ct.CDLL(None).srand(seed)
+
+
+def csr_cases():
+    """(name, expected) for every edge list of csr_build.npz: the reference's
+    removeEdges, SortEdgesUndirected and SortNodeEdgesByIndex outputs."""
+    z = np.load(os.path.join(GOLDEN, 'csr_build.npz'))
+    out = []
+    for name in map(str, z['names']):
+        p = f'{name}_'
+        exp = {k[len(p):]: z[k] for k in z.files if k.startswith(p)}
+        for k in list(exp):
+            if exp[k].dtype == np.int32:
+                exp[k] = exp[k].astype(np.float64 if k.endswith('weight') else np.int64)
+        exp['nv'] = int(exp['nv'])
+        exp['nge'] = int(exp['nge'])
+        out.append((name, exp))
+    return out

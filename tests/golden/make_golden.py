@@ -5,6 +5,7 @@ Run from the repository root after ``make -C oracle``:
     python tests/golden/make_golden.py [/path/to/grappolo]
     python tests/golden/make_golden.py --vf     # only vf.npz (vertex following)
     python tests/golden/make_golden.py --mhash  # only mhash.npz (coloring = 3)
+    python tests/golden/make_golden.py --csr    # only csr_build.npz and karate.bin
 
 Each fixture ``<case>.npz`` holds an input CSR and what the reference's
 functions return for it at OMP_NUM_THREADS=1: the distance-1 colouring, one
@@ -168,6 +169,54 @@ def make_mhash(R, ref_root):
     print('wrote mhash', list(cases))
 
 
+def edge_list_cases(seed=17):
+    """Edge lists with repeated pairs, pairs listed both ways round and
+    self-loops, as raw inputs of removeEdges and the loaders' CSR build.
+    Weights are integral (stored as int32)."""
+    rng = np.random.default_rng(seed)
+    out = {}
+    for name, nv, ne, dup, wkind in [('tiny', 10, 60, 0.3, 'id'),
+                                     ('mid', 200, 1500, 0.2, 'int'),
+                                     ('wide', 1000, 2500, 0.1, 'id')]:
+        h = rng.integers(0, nv, ne)
+        t = rng.integers(0, nv, ne)
+        k = int(ne * dup)
+        src, dst = rng.integers(0, ne, k), rng.integers(0, ne, k)
+        h[dst], t[dst] = h[src], t[src]
+        flip = rng.random(ne) < 0.25
+        h, t = np.where(flip, t, h), np.where(flip, h, t)
+        # 'id': weight i + 1 names edge i, so every output weight shows which
+        # input edge it came from
+        w = np.arange(1.0, ne + 1) if wkind == 'id' else rng.integers(1, 6, ne) * 1.0
+        out[name] = (nv, h.astype(np.int64), t.astype(np.int64), w)
+    return out
+
+
+def make_csr(R, ref_root):
+    """csr_build.npz: removeEdges, SortEdgesUndirected and SortNodeEdgesByIndex
+    of the reference on raw edge lists; karate.bin: karate written by the
+    reference's writeGraphBinaryFormatNew."""
+    out = {}
+    cases = edge_list_cases()
+    for name, (nv, h, t, w) in cases.items():
+        rh, rt, rw, nge = R.remove_edges(nv, h, t, w)
+        ptrs, sh, st, sw = R.sort_edges_undirected(nv, rh[:nge], rt[:nge], rw[:nge])
+        oh, ot, ow = R.sort_node_edges(nv, ptrs, sh, st, sw)
+        rptrs, _, rawt, raww = R.sort_edges_undirected(nv, h, t, w)
+        i32 = lambda a: np.asarray(a).astype(np.int32)  # noqa: E731
+        out.update({f'{name}_nv': nv, f'{name}_head': i32(h), f'{name}_tail': i32(t),
+                    f'{name}_weight': i32(w), f'{name}_rm_head': i32(rh),
+                    f'{name}_rm_tail': i32(rt), f'{name}_rm_weight': i32(rw), f'{name}_nge': nge,
+                    f'{name}_ptrs': ptrs, f'{name}_rows_tail': i32(st),
+                    f'{name}_rows_weight': i32(sw), f'{name}_sorted_tail': i32(ot),
+                    f'{name}_sorted_weight': i32(ow), f'{name}_raw_ptrs': rptrs,
+                    f'{name}_raw_tail': i32(rawt), f'{name}_raw_weight': i32(raww)})
+    np.savez_compressed(os.path.join(HERE, 'csr_build.npz'), names=np.array(list(cases)), **out)
+    g = all_cases(ref_root)['karate']
+    R.write_binary(g, os.path.join(HERE, 'karate.bin'))
+    print('wrote csr_build', list(cases), 'and karate.bin')
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 and not sys.argv[1].startswith('--') \
         else '/root/reference'
@@ -177,6 +226,9 @@ def main():
         return
     if '--mhash' in sys.argv:
         make_mhash(R, ref_root)
+        return
+    if '--csr' in sys.argv:
+        make_csr(R, ref_root)
         return
     rng = np.random.default_rng(2024)
     for name, g in all_cases(ref_root).items():

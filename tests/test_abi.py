@@ -48,6 +48,11 @@ REFERENCE_SYMBOLS = [
     '_Z15vertexFollowingP5graphPl',
     '_Z15buildNewGraphVFP5graphS0_Pll',
     '_Z27algoColoringMultiHashMaxMinP5graphPiiPdii',
+    '_Z11removeEdgesllP4edge',
+    '_Z19SortEdgesUndirectedllP4edgeS0_Pl',
+    '_Z20SortNodeEdgesByIndexlP4edgeS0_Pl',
+    '_Z23parse_EdgeListBinaryNewP5graphPc',
+    '_Z25writeGraphBinaryFormatNewP5graphPcl',
 ]
 
 
@@ -72,7 +77,12 @@ def test_compat_header_matches_reference_mangling(tmp_path):
                    '  buildNextLevelGraphOpt(g, o, c, 2, 1);\n'
                    '  vertexFollowing(g, c);\n'
                    '  buildNewGraphVF(g, o, c, 2);\n'
-                   '  algoColoringMultiHashMaxMin(g, col, 1, t, 2, 4);\n}\n')
+                   '  algoColoringMultiHashMaxMin(g, col, 1, t, 2, 4);\n'
+                   '  removeEdges(4, 2, g->edgeList);\n'
+                   '  SortEdgesUndirected(4, 2, g->edgeList, o->edgeList, c);\n'
+                   '  SortNodeEdgesByIndex(4, g->edgeList, o->edgeList, c);\n'
+                   '  parse_EdgeListBinaryNew(g, (char *)"f");\n'
+                   '  writeGraphBinaryFormatNew(g, (char *)"f", 1);\n}\n')
     obj = tmp_path / 'use.o'
     subprocess.run(['g++', '-c', '-I', os.path.join(ROOT, 'include'), str(src), '-o', str(obj)],
                    check=True)
@@ -90,3 +100,26 @@ def test_no_gpu_fails_loudly():
     with pytest.raises(_lib.GrappoloError) as e:
         louvain.runMultiPhaseColoring(graphs.from_edges(2, [(0, 1)]))
     assert e.value.code == 7
+
+
+def test_binary_files_through_the_library(tmp_path):
+    """glv_load_binary / glv_write_binary (host file I/O, no GPU needed) read
+    the reference-written karate.bin and write the same bytes back."""
+    import numpy as np
+    from grappolo_b200 import louvain
+    path = os.path.join(ROOT, 'tests', 'golden', 'karate.bin')
+    g, ne = louvain.parse_EdgeListBinaryNew(path)
+    z = np.load(os.path.join(ROOT, 'tests', 'golden', 'karate.npz'))
+    assert ne == 78
+    assert np.array_equal(g.ptr, z['ptr']) and np.array_equal(g.tail, z['tail'])
+    assert np.array_equal(g.weight, z['weight'])
+    out = tmp_path / 'k.bin'
+    louvain.writeGraphBinaryFormatNew(g, str(out))
+    assert out.read_bytes() == open(path, 'rb').read()
+    with pytest.raises(_lib.GrappoloError) as e:
+        louvain.parse_EdgeListBinaryNew(str(tmp_path / 'missing.bin'))
+    assert e.value.code == 9  # GLV_ERR_IO
+    (tmp_path / 'short.bin').write_bytes(open(path, 'rb').read()[:100])
+    with pytest.raises(_lib.GrappoloError) as e:
+        louvain.parse_EdgeListBinaryNew(str(tmp_path / 'short.bin'))
+    assert e.value.code == 9

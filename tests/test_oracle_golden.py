@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 from grappolo_b200 import graphs
-from _golden import CASES, load, mhash_cases, pins, srand
+from _golden import CASES, csr_cases, load, mhash_cases, pins, srand
 
 
 @pytest.mark.parametrize('name', CASES)
@@ -128,3 +128,36 @@ def test_multiphase_multihash_golden(oracle, case):
     assert s['total_iterations'] == int(exp['itr'])
     assert s['final_clusters'] == int(exp['clusters'])
     assert abs(s['final_mod'] - float(exp['mod'])) <= 5e-7  # the reference prints %lf
+
+
+@pytest.mark.parametrize('case', csr_cases(), ids=lambda c: c[0])
+def test_edge_list_preprocessing_golden(oracle, case):
+    """removeEdges, SortEdgesUndirected and SortNodeEdgesByIndex
+    (Utility/utilityFunctions.cpp:416-531) on raw edge lists."""
+    _, e = case
+    nv = e['nv']
+    h, t, w, nge = oracle.remove_edges(nv, e['head'], e['tail'], e['weight'])
+    assert nge == e['nge']
+    assert np.array_equal(h, e['rm_head']) and np.array_equal(t, e['rm_tail'])
+    assert np.array_equal(w, e['rm_weight'])
+    ptrs, sh, st, sw = oracle.sort_edges_undirected(nv, h[:nge], t[:nge], w[:nge])
+    assert np.array_equal(ptrs, e['ptrs'])
+    assert np.array_equal(st, e['rows_tail']) and np.array_equal(sw, e['rows_weight'])
+    _, ot, ow = oracle.sort_node_edges(nv, ptrs, sh, st, sw)
+    assert np.array_equal(ot, e['sorted_tail']) and np.array_equal(ow, e['sorted_weight'])
+    rp, _, rt, rw = oracle.sort_edges_undirected(nv, e['head'], e['tail'], e['weight'])
+    assert np.array_equal(rp, e['raw_ptrs'])
+    assert np.array_equal(rt, e['raw_tail']) and np.array_equal(rw, e['raw_weight'])
+
+
+def test_binary_file_golden(tmp_path):
+    """karate.bin was written by the reference's writeGraphBinaryFormatNew:
+    the Python reader gets karate back and the writer gives the same bytes."""
+    path = os.path.join(os.path.dirname(__file__), 'golden', 'karate.bin')
+    g, z = load('karate')
+    r = graphs.read_binary(path)
+    assert np.array_equal(r.ptr, z['ptr']) and np.array_equal(r.tail, z['tail'])
+    assert np.array_equal(r.weight, z['weight'])
+    out = tmp_path / 'k.bin'
+    graphs.write_binary(g, str(out))
+    assert out.read_bytes() == open(path, 'rb').read()

@@ -104,3 +104,28 @@ def test_multihash_matches_reference(oracle, reference, name, g, num_colors):
     assert np.array_equal(Co, Cr)
     assert so['phases'] == sr['phases'] and so['total_iterations'] == sr['total_iterations']
     assert abs(so['final_mod'] - sr['final_mod']) <= 5e-7
+
+
+@pytest.mark.parametrize('seed', [1, 2, 3])
+def test_edge_list_preprocessing_matches_reference(oracle, reference, seed):
+    """removeEdges / SortEdgesUndirected / SortNodeEdgesByIndex, raw and
+    cleaned lists, random sizes with many repeats and self-loops."""
+    rng = np.random.default_rng(seed)
+    nv = int(rng.integers(5, 3000))
+    ne = int(rng.integers(0, 20000))
+    h, t = rng.integers(0, nv, ne), rng.integers(0, nv, ne)
+    k = ne // 3
+    src, dst = rng.integers(0, max(ne, 1), k), rng.integers(0, max(ne, 1), k)
+    h[dst], t[dst] = h[src], t[src]
+    flip = rng.random(ne) < 0.3
+    h, t = np.where(flip, t, h), np.where(flip, h, t)
+    w = rng.uniform(0.1, 3.0, ne)
+    a, b = oracle.remove_edges(nv, h, t, w), reference.remove_edges(nv, h, t, w)
+    assert a[3] == b[3] and all(np.array_equal(x, y) for x, y in zip(a[:3], b[:3]))
+    for hh, tt, ww in [(h, t, w), (a[0][:a[3]], a[1][:a[3]], a[2][:a[3]])]:
+        so = oracle.sort_edges_undirected(nv, hh, tt, ww)
+        sr = reference.sort_edges_undirected(nv, hh, tt, ww)
+        assert all(np.array_equal(x, y) for x, y in zip(so, sr))
+        no = oracle.sort_node_edges(nv, *so)
+        nr = reference.sort_node_edges(nv, *sr)
+        assert all(np.array_equal(x, y) for x, y in zip(no, nr))
