@@ -49,9 +49,12 @@ def parse_args():
     p.add_argument('--no-cpu-baseline', action='store_true')
     p.add_argument('--profile-level', type=int, default=1,
                    help='1: time each class sweep (roofline); 2: time every launch by kind')
-    p.add_argument('--workload', choices=['rmat', 'batch'], default='rmat',
+    p.add_argument('--workload', choices=['rmat', 'batch', 'csr'], default='rmat',
                    help='rmat: one R-MAT graph (default); batch: 4,096 planted-partition '
-                        'graphs run as batches')
+                        'graphs run as batches; csr: edge list to CSR (removeEdges, both '
+                        'directions, rows sorted) of a raw R-MAT edge list')
+    p.add_argument('--csr-sample-scale', type=int, default=16,
+                   help='csr workload: R-MAT scale of the reference\'s CPU sample')
     p.add_argument('--batch-graphs', type=int, default=4096)
     p.add_argument('--wave-pairs', type=float, default=3.5e8,
                    help='batch workload: expected undirected pairs per batched run')
@@ -150,6 +153,8 @@ def aggregate(seconds, edges, dist=None, device=None):
 def run_reference(args, rank):
     if rank != 0:
         return 0
+    if args.workload == 'csr':
+        return run_csr_reference(args)
     import numpy as np
     import torch
     from grappolo_b200 import graphs
@@ -189,7 +194,177 @@ def run_reference(args, rank):
     return 0
 
 
+CSR_METRIC = 'CSR build input edges/s'
+CSR_UNIT = 'edges/s'
+
+
+def csr_config(args, nv, ne, nnz=None, extra=None):
+    cfg = {'workload': f'edge list to CSR (removeEdges, every edge in both rows, rows sorted by '
+                       f'tail) of a raw R-MAT scale {args.scale} edge list',
+           'graph': f'R-MAT scale {args.scale}, edge factor 16, a=0.57 b=0.19 c=0.19, raw '
+                    f'(repeats and self-loops kept), FP64 weights U(0,1], seed 1',
+           'num_vertices': nv, 'num_input_edges': ne, 'nnz': nnz,
+           'parallelism': f'replicas x{args.gpus}', 'l2': 'inputs larger than L2 (no flush)'}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def csr_cpu_sample(scale):
+    """The reference's removeEdges + SortEdgesUndirected + SortNodeEdgesByIndex
+    (Utility/utilityFunctions.cpp:416-531; sequential code, one core) on a raw
+    R-MAT edge list of the given scale.  Returns (edges/s, seconds, edges)."""
+    from grappolo_b200 import graphs
+    from oracle import Reference
+    R = Reference(fast=True)
+    h, t, w = graphs.rmat_edges(scale, seed=1)
+    nv = 1 << scale
+    t0 = time.perf_counter()
+    rh, rt, rw, n = R.remove_edges(nv, h, t, w)
+    ptrs, sh, st, sw = R.sort_edges_undirected(nv, rh[:n], rt[:n], rw[:n])
+    R.sort_node_edges(nv, ptrs, sh, st, sw)
+    dt = time.perf_counter() - t0
+    return len(h) / dt, dt, len(h)
+
+
+def csr_sample_text(scale, dt, ne):
+    return (f'reference removeEdges + SortEdgesUndirected + SortNodeEdgesByIndex (sequential, '
+            f'-Ofast build) on a raw R-MAT scale {scale} edge list ({ne} edges, {dt:.1f} s); '
+            f'removeEdges walks a per-head list, so its time grows with the square of the '
+            f'largest degree and larger samples do not finish in minutes')
+
+
+def run_csr_reference(args):
+    vals = []
+    for k in range(args.warmup + args.steps):
+        v, dt, ne = csr_cpu_sample(args.csr_sample_scale)
+        if k >= args.warmup:
+            vals.append(v)
+    value = statistics.median(vals)
+    nv = 1 << args.scale
+    line = {'metric': CSR_METRIC, 'value': value, 'unit': CSR_UNIT, 'impl': 'reference',
+            'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': 1e3 * (16 << args.scale) / value, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'int64', 'data': 'synthetic',
+            'config': csr_config(args, nv, 16 << args.scale),
+            'cpu_baseline': {'value': value, 'unit': CSR_UNIT, 'cores': 1, 'kind': 'reference',
+                             'sample': csr_sample_text(args.csr_sample_scale, dt, ne)},
+            'e2e': {'value': value, 'unit': CSR_UNIT, 'h2d_bytes_per_step': 0,
+                    'd2h_bytes_per_step': 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 # --------------------------------------------------------------------------- our arm
+def run_csr_workload(args, world, rank, local):
+    """A step builds the CSR of a raw R-MAT edge list resident in HBM with
+    glv_dev_build_csr (removeEdges, both directions of every kept edge in list
+    order, rows sorted by tail: the reference loaders' result).  e2e: the same
+    build through glv_build_csr from a pinned host edge list to a host CSR."""
+    import ctypes as ct
+    import torch
+    from grappolo_b200 import graphs, _lib
+    torch.cuda.set_device(local)
+    dev = torch.device('cuda', local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=600),
+                                device_id=dev)
+    L = _lib.lib()
+    u, v, w = graphs.rmat_edges_device(args.scale, seed=1, device=dev)
+    nv, ne = 1 << args.scale, u.numel()
+    ptr = torch.empty(nv + 1, dtype=torch.int64, device=dev)
+    tail = torch.empty(2 * ne, dtype=torch.int32, device=dev)
+    wout = torch.empty(2 * ne, dtype=torch.float64, device=dev)
+    flags = _lib.GLV_CSR_REMOVE_EDGES | _lib.GLV_CSR_SORT_ROWS
+    stream = torch.cuda.current_stream().cuda_stream
+    nnz = ct.c_long(0)
+
+    def step():
+        _lib.check(L.glv_dev_build_csr(nv, ne, u.data_ptr(), v.data_ptr(), w.data_ptr(), flags,
+                                       ptr.data_ptr(), tail.data_ptr(), wout.data_ptr(),
+                                       ct.byref(nnz), stream))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    l0 = L.glv_kernel_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        step()
+    ev1.record()
+    torch.cuda.synchronize()
+    launches = L.glv_kernel_launch_count() - l0
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    t = ev0.elapsed_time(ev1) * 1e-3
+    t_max, e_all = aggregate(t, float(ne * args.steps), dist, dev)
+    value = e_all / t_max
+    out_nnz = nnz.value
+    # algorithmic bytes: read every input edge (24 B), write the CSR (12 B per
+    # entry + the row offsets)
+    alg = 24 * ne + 12 * out_nnz + 8 * (nv + 1)
+    peak, peak_kind = measured_peak()
+    achieved = alg / (t / args.steps) / 1e9
+    roofline = {'bound': 'hbm', 'kernel': 'the whole build (our kernels and the CUB radix sorts '
+                                          'and scans between them), per step',
+                'achieved': achieved, 'peak': peak, 'unit': 'GB/s', 'frac': achieved / peak,
+                'peak_kind': peak_kind, 'traffic': None,
+                'algorithmic_bytes_per_launch': alg, 'avg_launch_s': t / args.steps}
+    e2e = None
+    if not args.no_e2e:
+        aos = torch.empty((ne, 3), dtype=torch.int64, pin_memory=True)
+        aos.copy_(torch.stack([u, v, w.view(torch.int64)], dim=1))
+        libc = ct.CDLL(None)
+
+        def e2e_step():
+            out = _lib.GlvGraph()
+            _lib.check(L.glv_build_csr(nv, ne, ct.cast(aos.data_ptr(), ct.POINTER(_lib.GlvEdge)),
+                                       flags, ct.byref(out)))
+            libc.free(ct.cast(out.edgeListPtrs, ct.c_void_p))
+            libc.free(ct.cast(out.edgeList, ct.c_void_p))
+            return out.numEdges
+
+        e2e_step()
+        if dist:
+            dist.barrier()
+        e0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        et = time.perf_counter() - e0
+        et, ee = aggregate(et, float(ne * args.steps), dist, dev)
+        e2e = {'value': ee / et, 'unit': CSR_UNIT, 'h2d_bytes_per_step': 24 * ne,
+               'd2h_bytes_per_step': 24 * out_nnz + 8 * (nv + 1),
+               'seconds_per_step': et / args.steps}
+        del aos
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cv, cdt, cne = csr_cpu_sample(args.csr_sample_scale)
+        cpu = {'value': cv, 'unit': CSR_UNIT, 'cores': 1, 'kind': 'reference',
+               'sample': csr_sample_text(args.csr_sample_scale, cdt, cne)}
+    line = {'metric': CSR_METRIC, 'value': value, 'unit': CSR_UNIT, 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 * t / args.steps,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'int64',
+            'data': 'synthetic (seeded raw R-MAT edge list generated on the device)',
+            'config': csr_config(args, nv, ne, out_nnz,
+                                 {'kept_edges': out_nnz // 2,
+                                  'flags': 'GLV_CSR_REMOVE_EDGES | GLV_CSR_SORT_ROWS'}),
+            'roofline': roofline, 'cpu_baseline': cpu, 'e2e': e2e, 'gpu_launches': launches,
+            'clocks': clk}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
 def run_batch_workload(args, world, rank, local):
     """Many planted-partition graphs (vertex counts log-U[500, 200k], block sizes
     log-U[20, 2000], mu U[0.1, 0.6], mean degree U[6, 32], unit weights),
@@ -295,6 +470,8 @@ def main():
         return run_reference(args, rank)
     if args.workload == 'batch':
         return run_batch_workload(args, world, rank, local)
+    if args.workload == 'csr':
+        return run_csr_workload(args, world, rank, local)
     import numpy as np
     import torch
     from grappolo_b200 import graphs, louvain, _lib

@@ -26,6 +26,14 @@ namespace glv {
 constexpr int kIdBits = 31;
 constexpr uint64_t kIdMask = (1ull << kIdBits) - 1;
 
+// Bits that hold every id below nv: sort keys (row, col) take 2 * id_bits(nv)
+// bits, so the radix sorts make only the passes the graph needs.
+static int id_bits(int64_t nv) {
+  int b = 1;
+  while (b < kIdBits && (int64_t(1) << b) < nv) ++b;
+  return b;
+}
+
 // Edge arrays as the kernels read them: AoS glv_edge (stride 3 words) or
 // separate int64 heads / tails and double weights (stride 1).  A null weight
 // array reads as 1.0.
@@ -44,7 +52,7 @@ static EdgeView aos_view(const glv_edge *e) {
   return EdgeView{base, base + 1, reinterpret_cast<const double *>(base + 2), 3};
 }
 
-__global__ void k_edge_pair_keys(int64_t ne, EdgeView ev, int64_t nv, uint64_t *keys,
+__global__ void k_edge_pair_keys(int64_t ne, EdgeView ev, int64_t nv, int bits, uint64_t *keys,
                                  int64_t *idx, int32_t *bad) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < ne;
        i += (int64_t)gridDim.x * blockDim.x) {
@@ -53,21 +61,21 @@ __global__ void k_edge_pair_keys(int64_t ne, EdgeView ev, int64_t nv, uint64_t *
       atomicOr(bad, 1);
       h = t = 0;
     }
-    keys[i] = ((uint64_t)h << kIdBits) | (uint64_t)t;
+    keys[i] = ((uint64_t)h << bits) | (uint64_t)t;
     idx[i] = i;
   }
 }
 
 // After the stable sort: the first edge of each (head, tail) run is kept
 // unless it is a self-loop.
-__global__ void k_mark_kept(int64_t ne, const uint64_t *skeys, const int64_t *sidx, uint8_t *kept,
-                            unsigned long long *count) {
+__global__ void k_mark_kept(int64_t ne, int bits, const uint64_t *skeys, const int64_t *sidx,
+                            uint8_t *kept, unsigned long long *count) {
   unsigned int mine = 0;
   for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < ne;
        s += (int64_t)gridDim.x * blockDim.x) {
     const uint64_t k = skeys[s];
     const bool first = s == 0 || skeys[s - 1] != k;
-    const bool loop = (k >> kIdBits) == (k & kIdMask);
+    const bool loop = (k >> bits) == (k & ((1ull << bits) - 1));
     const bool g = first && !loop;
     kept[sidx[s]] = g ? 1 : 0;
     mine += g ? 1u : 0u;
@@ -118,14 +126,14 @@ __device__ __forceinline__ void entry_of(int64_t e, const int64_t *order, const 
 // Keys of the 2 * nk directed entries.  sorted_rows lists them in reverse and
 // keys them by (row, col); otherwise in order, keyed by row.  Row degrees are
 // counted on the way.
-__global__ void k_entry_keys(int64_t m, bool sorted_rows, const int64_t *order, EdgeView ev,
-                             uint64_t *keys, int64_t *vals, unsigned long long *deg) {
+__global__ void k_entry_keys(int64_t m, bool sorted_rows, int bits, const int64_t *order,
+                             EdgeView ev, uint64_t *keys, int64_t *vals, unsigned long long *deg) {
   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < m;
        q += (int64_t)gridDim.x * blockDim.x) {
     const int64_t e = sorted_rows ? m - 1 - q : q;
     int64_t src, row, col;
     entry_of(e, order, ev, &src, &row, &col);
-    keys[q] = sorted_rows ? (((uint64_t)row << kIdBits) | (uint64_t)col) : (uint64_t)row;
+    keys[q] = sorted_rows ? (((uint64_t)row << bits) | (uint64_t)col) : (uint64_t)row;
     vals[q] = e;
     atomicAdd(&deg[row], 1ull);
   }
@@ -161,6 +169,8 @@ __global__ void k_row_ids(int64_t nv, const int64_t *ptr, int64_t *rowid) {
 // SortNodeEdgesByIndex keys: positions listed in reverse, keyed (row, tail).
 __global__ void k_row_sort_keys(int64_t nnz, const int64_t *rowid, const glv_edge *e,
                                 uint64_t *keys, int64_t *vals, int32_t *bad) {
+  // the row above the tail's 31 bits: tails of a given CSR are not bounded by
+  // its row count
   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < nnz;
        q += (int64_t)gridDim.x * blockDim.x) {
     const int64_t p = nnz - 1 - q;
@@ -234,15 +244,16 @@ static int kept_order(cudaStream_t s, int64_t nv, int64_t ne, EdgeView ev, DevSc
   TRY(d.get(&cnt, 1));
   CK(cudaMemsetAsync(bad, 0, sizeof(int32_t), s));
   CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), s));
-  k_edge_pair_keys<<<csr_grid(ne), 256, 0, s>>>(ne, ev, nv, k1, v1, bad);
+  const int bits = id_bits(nv);
+  k_edge_pair_keys<<<csr_grid(ne), 256, 0, s>>>(ne, ev, nv, bits, k1, v1, bad);
   ++*launches;
   CK(cudaGetLastError());
   size_t tb = 0;
-  CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, k1, k2, v1, v2, ne, 0, 2 * kIdBits, s));
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, k1, k2, v1, v2, ne, 0, 2 * bits, s));
   void *temp;
   TRY(d.get((char **)&temp, (int64_t)tb));
-  CK(cub::DeviceRadixSort::SortPairs(temp, tb, k1, k2, v1, v2, ne, 0, 2 * kIdBits, s));
-  k_mark_kept<<<csr_grid(ne), 256, 0, s>>>(ne, k2, v2, kept, cnt);
+  CK(cub::DeviceRadixSort::SortPairs(temp, tb, k1, k2, v1, v2, ne, 0, 2 * bits, s));
+  k_mark_kept<<<csr_grid(ne), 256, 0, s>>>(ne, bits, k2, v2, kept, cnt);
   ++*launches;
   CK(cudaGetLastError());
   int32_t hbad = 0;
@@ -299,10 +310,11 @@ static int row_entries(cudaStream_t s, int64_t nv, int64_t nk, const int64_t *or
   TRY(d.get(&deg, nv));
   CK(cudaMemsetAsync(deg, 0, std::max<int64_t>(nv, 1) * sizeof(*deg), s));
   if (m > 0) {
-    k_entry_keys<<<csr_grid(m), 256, 0, s>>>(m, sorted_rows, order, ev, k1, v1, deg);
+    const int ib = id_bits(nv);
+    k_entry_keys<<<csr_grid(m), 256, 0, s>>>(m, sorted_rows, ib, order, ev, k1, v1, deg);
     ++*launches;
     CK(cudaGetLastError());
-    const int bits = sorted_rows ? 2 * kIdBits : kIdBits;
+    const int bits = sorted_rows ? 2 * ib : ib;
     size_t tb = 0;
     CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, k1, k2, v1, *svals, m, 0, bits, s));
     void *temp;
@@ -399,7 +411,8 @@ int glv_sort_edges_undirected(long NV, long NE, const glv_edge *list1, glv_edge 
     TRY(d.get(&k, NE));
     TRY(d.get(&v, NE));
     if (NE > 0) {
-      k_edge_pair_keys<<<csr_grid(NE), 256, 0, c.s>>>(NE, aos_view(din), NV, k, v, bad);
+      k_edge_pair_keys<<<csr_grid(NE), 256, 0, c.s>>>(NE, aos_view(din), NV, id_bits(NV), k, v,
+                                                     bad);
       ++c.launches;
       CK(cudaGetLastError());
     }
@@ -453,10 +466,11 @@ int glv_sort_node_edges_by_index(long NV, glv_edge *list1, glv_edge *list2, cons
     c.launches += 2;
     CK(cudaGetLastError());
     size_t tb = 0;
-    CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, k1, k2, v1, v2, nnz, 0, 2 * kIdBits, c.s));
+    const int bits = kIdBits + id_bits(NV);
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, k1, k2, v1, v2, nnz, 0, bits, c.s));
     void *temp;
     TRY(d.get((char **)&temp, (int64_t)tb));
-    CK(cub::DeviceRadixSort::SortPairs(temp, tb, k1, k2, v1, v2, nnz, 0, 2 * kIdBits, c.s));
+    CK(cub::DeviceRadixSort::SortPairs(temp, tb, k1, k2, v1, v2, nnz, 0, bits, c.s));
     k_gather_edges<<<csr_grid(nnz), 256, 0, c.s>>>(nnz, v2, din, dout);
     ++c.launches;
     CK(cudaGetLastError());
@@ -492,7 +506,8 @@ int glv_build_csr(long NV, long NE, const glv_edge *edges, int flags, glv_graph 
     TRY(d.get(&k, NE));
     TRY(d.get(&v, NE));
     CK(cudaMemsetAsync(bad, 0, sizeof(int32_t), c.s));
-    k_edge_pair_keys<<<csr_grid(NE), 256, 0, c.s>>>(NE, aos_view(din), NV, k, v, bad);
+    k_edge_pair_keys<<<csr_grid(NE), 256, 0, c.s>>>(NE, aos_view(din), NV, id_bits(NV), k, v,
+                                                     bad);
     ++c.launches;
     CK(cudaGetLastError());
     int32_t hb = 0;
@@ -560,7 +575,7 @@ int glv_dev_build_csr(long NV, long NE, const long *d_head, const long *d_tail,
       TRY(d.get(&k, NE));
       TRY(d.get(&v, NE));
       CK(cudaMemsetAsync(bad, 0, sizeof(int32_t), s));
-      k_edge_pair_keys<<<csr_grid(NE), 256, 0, s>>>(NE, ev, NV, k, v, bad);
+      k_edge_pair_keys<<<csr_grid(NE), 256, 0, s>>>(NE, ev, NV, id_bits(NV), k, v, bad);
       ++launches;
       CK(cudaGetLastError());
       int32_t hb = 0;

@@ -195,6 +195,44 @@ def read_binary(path: str) -> CSRGraph:
     return CSRGraph(ptr, rec['tail'].astype(np.int64), rec['weight'].astype(np.float64))
 
 
+def rmat_edges_device(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19,
+                      c: float = 0.19, seed: int = 1, device='cuda'):
+    """The raw R-MAT edge list, as an edge-list file would hold it: 2^scale
+    vertices, edge_factor * 2^scale edges with their repeats and self-loops,
+    weights uniform in (0, 1].  Returns device tensors (head int64, tail
+    int64, weight float64), drawn from torch's device generator."""
+    import torch
+    gen = torch.Generator(device=device)
+    gen.manual_seed(seed)
+    m = edge_factor << scale
+    u = torch.zeros(m, dtype=torch.int64, device=device)
+    v = torch.zeros(m, dtype=torch.int64, device=device)
+    ab, abc = a + b, a + b + c
+    for _ in range(scale):
+        r = torch.rand(m, generator=gen, device=device)
+        u = (u << 1) | (r >= ab).to(torch.int64)
+        v = (v << 1) | (((r >= a) & (r < ab)) | (r >= abc)).to(torch.int64)
+        del r
+    w = 1.0 - torch.rand(m, generator=gen, device=device, dtype=torch.float64)
+    return u, v, w
+
+
+def rmat_edges(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19,
+               c: float = 0.19, seed: int = 1):
+    """Host (numpy) counterpart of :func:`rmat_edges_device` (a different
+    stream of random numbers): raw (head, tail, weight) arrays."""
+    rng = np.random.default_rng(seed)
+    m = edge_factor << scale
+    u = np.zeros(m, dtype=np.int64)
+    v = np.zeros(m, dtype=np.int64)
+    ab, abc = a + b, a + b + c
+    for _ in range(scale):
+        r = rng.random(m)
+        u = (u << 1) | (r >= ab)
+        v = (v << 1) | (((r >= a) & (r < ab)) | (r >= abc))
+    return u, v, 1.0 - rng.random(m)
+
+
 def rmat_device(scale: int, edge_factor: int = 16, a: float = 0.57, b: float = 0.19,
                 c: float = 0.19, seed: int = 1, device='cuda', weighted: bool = True):
     """R-MAT graph built directly in device memory with torch (large inputs).
