@@ -123,32 +123,59 @@ __device__ __forceinline__ void entry_of(int64_t e, const int64_t *order, const 
   *col = (e & 1) ? h : t;
 }
 
-// Keys of the 2 * nk directed entries.  sorted_rows lists them in reverse and
-// keys them by (row, col); otherwise in order, keyed by row.  Row degrees are
-// counted on the way.
-__global__ void k_entry_keys(int64_t m, bool sorted_rows, int bits, const int64_t *order,
-                             EdgeView ev, uint64_t *keys, int64_t *vals, unsigned long long *deg) {
+// Sort records of the 2 * nk directed entries, one per entry e = 2k + d.
+// sorted_rows: listed in reverse, key (row, col), sorted on all 2 * bits;
+// otherwise in order, key (col above row), sorted on the row bits only, so
+// the column rides along in the key's upper bits.  The weight is the sort
+// value: the sorted records are the CSR, with nothing left to gather.
+__global__ void k_entry_keys(int64_t m, bool sorted_rows, int bits, int64_t nv,
+                             const int64_t *order, EdgeView ev, uint64_t *keys, double *vals,
+                             int32_t *bad) {
   for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < m;
        q += (int64_t)gridDim.x * blockDim.x) {
     const int64_t e = sorted_rows ? m - 1 - q : q;
     int64_t src, row, col;
     entry_of(e, order, ev, &src, &row, &col);
-    keys[q] = sorted_rows ? (((uint64_t)row << bits) | (uint64_t)col) : (uint64_t)row;
-    vals[q] = e;
-    atomicAdd(&deg[row], 1ull);
+    if (row < 0 || row >= nv || col < 0 || col >= nv) {
+      atomicOr(bad, 1);
+      row = col = 0;
+    }
+    keys[q] = sorted_rows ? (((uint64_t)row << bits) | (uint64_t)col)
+                          : (((uint64_t)col << bits) | (uint64_t)row);
+    vals[q] = ev.wt(src);
   }
 }
 
-__global__ void k_emit_entries(int64_t m, const int64_t *svals, const int64_t *order, EdgeView ev,
-                               int32_t *otail, double *ow, glv_edge *oaos) {
+__device__ __forceinline__ int64_t key_row(uint64_t k, bool sorted_rows, int bits) {
+  return sorted_rows ? (int64_t)(k >> bits) : (int64_t)(k & ((1ull << bits) - 1));
+}
+
+__device__ __forceinline__ int64_t key_col(uint64_t k, bool sorted_rows, int bits) {
+  return sorted_rows ? (int64_t)(k & ((1ull << bits) - 1)) : (int64_t)(k >> bits);
+}
+
+// Row offsets from the sorted records: position s opens every row after the
+// previous record's row up to its own (s = m closes the rest).
+__global__ void k_row_bounds(int64_t m, int64_t nv, bool sorted_rows, int bits,
+                             const uint64_t *skeys, int64_t *ptr) {
+  for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s <= m;
+       s += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t here = s < m ? key_row(skeys[s], sorted_rows, bits) : nv;
+    const int64_t prev = s > 0 ? key_row(skeys[s - 1], sorted_rows, bits) : -1;
+    for (int64_t r = prev + 1; r <= here; ++r) ptr[r] = s;
+  }
+}
+
+__global__ void k_emit_entries(int64_t m, bool sorted_rows, int bits, const uint64_t *skeys,
+                               const double *svals, int32_t *otail, double *ow, glv_edge *oaos) {
   for (int64_t s = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; s < m;
        s += (int64_t)gridDim.x * blockDim.x) {
-    int64_t src, row, col;
-    entry_of(svals[s], order, ev, &src, &row, &col);
-    const double w = ev.wt(src);
+    const uint64_t k = skeys[s];
+    const int64_t col = key_col(k, sorted_rows, bits);
+    const double w = svals[s];
     if (otail) otail[s] = (int32_t)col;
     if (ow) ow[s] = w;
-    if (oaos) oaos[s] = glv_edge{(long)row, (long)col, w};
+    if (oaos) oaos[s] = glv_edge{(long)key_row(k, sorted_rows, bits), (long)col, w};
   }
 }
 
@@ -294,50 +321,170 @@ static int kept_order(cudaStream_t s, int64_t nv, int64_t ne, EdgeView ev, DevSc
 }
 
 // The 2 * nk directed entries of the kept edges in row order (sorted_rows:
-// rows sorted by tail, equal tails latest first); d_ptr[nv + 1] receives the
-// row offsets and *svals the entry of every CSR position.
+// rows sorted by tail, equal tails latest first), written as a CSR: d_ptr[nv
+// + 1] and any of otail / ow (SoA) and oaos (glv_edge records).  Ids outside
+// [0, nv) are GLV_ERR_ARG.
 static int row_entries(cudaStream_t s, int64_t nv, int64_t nk, const int64_t *order, EdgeView ev,
-                       bool sorted_rows, DevScratch &d, int64_t *d_ptr, int64_t **svals,
-                       long *launches) {
+                       bool sorted_rows, DevScratch &d, int64_t *d_ptr, int32_t *otail, double *ow,
+                       glv_edge *oaos, long *launches) {
   const int64_t m = 2 * nk;
+  const int ib = id_bits(nv);
   uint64_t *k1, *k2;
-  int64_t *v1;
-  unsigned long long *deg;
+  double *v1, *v2;
+  int32_t *bad;
   TRY(d.get(&k1, m));
   TRY(d.get(&k2, m));
   TRY(d.get(&v1, m));
-  TRY(d.get(svals, m));
-  TRY(d.get(&deg, nv));
-  CK(cudaMemsetAsync(deg, 0, std::max<int64_t>(nv, 1) * sizeof(*deg), s));
+  TRY(d.get(&v2, m));
+  TRY(d.get(&bad, 1));
+  CK(cudaMemsetAsync(bad, 0, sizeof(int32_t), s));
   if (m > 0) {
-    const int ib = id_bits(nv);
-    k_entry_keys<<<csr_grid(m), 256, 0, s>>>(m, sorted_rows, ib, order, ev, k1, v1, deg);
+    k_entry_keys<<<csr_grid(m), 256, 0, s>>>(m, sorted_rows, ib, nv, order, ev, k1, v1, bad);
     ++*launches;
     CK(cudaGetLastError());
     const int bits = sorted_rows ? 2 * ib : ib;
     size_t tb = 0;
-    CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, k1, k2, v1, *svals, m, 0, bits, s));
+    CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, k1, k2, v1, v2, m, 0, bits, s));
     void *temp;
     TRY(d.get((char **)&temp, (int64_t)tb));
-    CK(cub::DeviceRadixSort::SortPairs(temp, tb, k1, k2, v1, *svals, m, 0, bits, s));
+    CK(cub::DeviceRadixSort::SortPairs(temp, tb, k1, k2, v1, v2, m, 0, bits, s));
   }
-  CK(cudaMemsetAsync(d_ptr, 0, sizeof(int64_t), s));
-  if (nv > 0) {
-    size_t tb = 0;
-    const int64_t *din = reinterpret_cast<const int64_t *>(deg);
-    CK(cub::DeviceScan::InclusiveSum(nullptr, tb, din, d_ptr + 1, nv, s));
-    void *temp;
-    TRY(d.get((char **)&temp, (int64_t)tb));
-    CK(cub::DeviceScan::InclusiveSum(temp, tb, din, d_ptr + 1, nv, s));
+  k_row_bounds<<<csr_grid(m + 1), 256, 0, s>>>(m, nv, sorted_rows, ib, k2, d_ptr);
+  ++*launches;
+  CK(cudaGetLastError());
+  if (m > 0) {
+    k_emit_entries<<<csr_grid(m), 256, 0, s>>>(m, sorted_rows, ib, k2, v2, otail, ow, oaos);
+    ++*launches;
+    CK(cudaGetLastError());
   }
+  int32_t hb = 0;
+  CK(cudaMemcpyAsync(&hb, bad, sizeof(hb), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (hb) return fail(GLV_ERR_ARG, "an edge end is outside [0, NV)");
   return GLV_OK;
+}
+
+// Device-to-host copy of a large result into ordinary (pageable, possibly
+// never touched) host memory, such as the malloc'd arrays the reference's API
+// returns.  A plain cudaMemcpy into such memory runs at the speed of one
+// thread faulting pages in; here the data moves by DMA into two pinned
+// staging buffers while a team of host threads copies the previous chunk out
+// (and takes the page faults in parallel).
+static bool page_locked(const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+static void parallel_memcpy(char *dst, const char *src, int64_t n) {
+  const int nthreads = (int)std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  std::vector<std::thread> team;
+  const int64_t part = (n + nthreads - 1) / nthreads;
+  for (int t = 0; t < nthreads; ++t) {
+    const int64_t a = t * part, b = std::min(n, a + part);
+    if (a >= b) break;
+    team.emplace_back([=] { memcpy(dst + a, src + a, b - a); });
+  }
+  for (auto &th : team) th.join();
+}
+
+static int d2h_large(cudaStream_t s, void *host, const void *dev, int64_t bytes) {
+  if (bytes <= 0) return GLV_OK;
+  if (bytes < (int64_t(64) << 20) || page_locked(host)) {
+    CK(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return GLV_OK;
+  }
+  const int64_t chunk = int64_t(128) << 20;
+  char *stage[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  struct Guard {
+    char **st;
+    cudaEvent_t *ev;
+    ~Guard() {
+      for (int k = 0; k < 2; ++k) {
+        if (ev[k]) {
+          cudaEventSynchronize(ev[k]);
+          cudaEventDestroy(ev[k]);
+        }
+        if (st[k]) cudaFreeHost(st[k]);
+      }
+    }
+  } guard{stage, ev};
+  for (int k = 0; k < 2; ++k) {
+    CK(cudaHostAlloc((void **)&stage[k], chunk, cudaHostAllocDefault));
+    CK(cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming));
+  }
+  auto copy_out = [](const char *src, char *dst, int64_t n) { parallel_memcpy(dst, src, n); };
+  const char *d = static_cast<const char *>(dev);
+  char *h = static_cast<char *>(host);
+  int64_t prev_off = -1, prev_n = 0;
+  int k = 0;
+  for (int64_t off = 0; off < bytes; off += chunk, k ^= 1) {
+    const int64_t n = std::min(chunk, bytes - off);
+    CK(cudaMemcpyAsync(stage[k], d + off, n, cudaMemcpyDeviceToHost, s));
+    CK(cudaEventRecord(ev[k], s));
+    if (prev_off >= 0) {  // the previous chunk's DMA is done: copy it out meanwhile
+      CK(cudaEventSynchronize(ev[k ^ 1]));
+      copy_out(stage[k ^ 1], h + prev_off, prev_n);
+    }
+    prev_off = off;
+    prev_n = n;
+    // stage[k ^ 1] is free again for the next chunk's DMA
+  }
+  CK(cudaEventSynchronize(ev[k ^ 1]));
+  copy_out(stage[k ^ 1], h + prev_off, prev_n);
+  return GLV_OK;
+}
+
+// Host-to-device counterpart of d2h_large for pageable sources: host threads
+// copy chunk i + 1 into a pinned staging buffer while chunk i moves by DMA.
+static int h2d_large(cudaStream_t s, void *dev, const void *host, int64_t bytes) {
+  if (bytes <= 0) return GLV_OK;
+  if (bytes < (int64_t(64) << 20) || page_locked(host)) {
+    CK(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, s));
+    return GLV_OK;
+  }
+  const int64_t chunk = int64_t(128) << 20;
+  char *stage[2] = {nullptr, nullptr};
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  struct Guard {
+    char **st;
+    cudaEvent_t *ev;
+    ~Guard() {
+      for (int k = 0; k < 2; ++k) {
+        if (ev[k]) {
+          cudaEventSynchronize(ev[k]);
+          cudaEventDestroy(ev[k]);
+        }
+        if (st[k]) cudaFreeHost(st[k]);
+      }
+    }
+  } guard{stage, ev};
+  for (int k = 0; k < 2; ++k) {
+    CK(cudaHostAlloc((void **)&stage[k], chunk, cudaHostAllocDefault));
+    CK(cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming));
+  }
+  const char *h = static_cast<const char *>(host);
+  char *d = static_cast<char *>(dev);
+  int k = 0;
+  for (int64_t off = 0; off < bytes; off += chunk, k ^= 1) {
+    const int64_t n = std::min(chunk, bytes - off);
+    CK(cudaEventSynchronize(ev[k]));  // this buffer's previous DMA has finished
+    parallel_memcpy(stage[k], h + off, n);
+    CK(cudaMemcpyAsync(d + off, stage[k], n, cudaMemcpyHostToDevice, s));
+    CK(cudaEventRecord(ev[k], s));
+  }
+  return GLV_OK;  // the guard waits for both buffers' last DMA
 }
 
 static int upload_edges(cudaStream_t s, const glv_edge *host, int64_t n, DevScratch &d,
                         glv_edge **dev) {
   TRY(d.get(dev, n));
-  if (n > 0) CK(cudaMemcpyAsync(*dev, host, n * sizeof(glv_edge), cudaMemcpyHostToDevice, s));
-  return GLV_OK;
+  return h2d_large(s, *dev, host, n * (int64_t)sizeof(glv_edge));
 }
 
 static int open_stream(Call &c) {
@@ -381,7 +528,7 @@ int glv_remove_edges(long NV, long NE, glv_edge *edgeList, long *numGoodEdges) {
     k_gather_edges<<<csr_grid(nge), 256, 0, c.s>>>(nge, order, din, dout);
     ++c.launches;
     CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(edgeList, dout, nge * sizeof(glv_edge), cudaMemcpyDeviceToHost, c.s));
+    TRY(d2h_large(c.s, edgeList, dout, nge * (int64_t)sizeof(glv_edge)));
   }
   CK(cudaStreamSynchronize(c.s));
   g_launches += c.launches;
@@ -398,38 +545,13 @@ int glv_sort_edges_undirected(long NV, long NE, const glv_edge *list1, glv_edge 
   TRY(open_stream(c));
   DevScratch d(c.s);
   glv_edge *din, *dout;
-  int64_t *dptr, *svals;
-  int32_t *bad;
+  int64_t *dptr;
   TRY(upload_edges(c.s, list1, NE, d, &din));
   TRY(d.get(&dptr, NV + 1));
-  TRY(d.get(&bad, 1));
-  CK(cudaMemsetAsync(bad, 0, sizeof(int32_t), c.s));
-  {
-    // ids are checked with the pair-key kernel's test (keys discarded)
-    uint64_t *k;
-    int64_t *v;
-    TRY(d.get(&k, NE));
-    TRY(d.get(&v, NE));
-    if (NE > 0) {
-      k_edge_pair_keys<<<csr_grid(NE), 256, 0, c.s>>>(NE, aos_view(din), NV, id_bits(NV), k, v,
-                                                     bad);
-      ++c.launches;
-      CK(cudaGetLastError());
-    }
-    int32_t hb = 0;
-    CK(cudaMemcpyAsync(&hb, bad, sizeof(hb), cudaMemcpyDeviceToHost, c.s));
-    CK(cudaStreamSynchronize(c.s));
-    if (hb) return fail(GLV_ERR_ARG, "an edge end is outside [0, NV)");
-  }
-  TRY(row_entries(c.s, NV, NE, nullptr, aos_view(din), false, d, dptr, &svals, &c.launches));
   TRY(d.get(&dout, 2 * NE));
-  if (NE > 0) {
-    k_emit_entries<<<csr_grid(2 * NE), 256, 0, c.s>>>(2 * NE, svals, nullptr, aos_view(din),
-                                                       nullptr, nullptr, dout);
-    ++c.launches;
-    CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(list2, dout, 2 * NE * sizeof(glv_edge), cudaMemcpyDeviceToHost, c.s));
-  }
+  TRY(row_entries(c.s, NV, NE, nullptr, aos_view(din), false, d, dptr, nullptr, nullptr, dout,
+                  &c.launches));
+  TRY(d2h_large(c.s, list2, dout, 2 * NE * (int64_t)sizeof(glv_edge)));
   CK(cudaMemcpyAsync(ptrs, dptr, (NV + 1) * sizeof(long), cudaMemcpyDeviceToHost, c.s));
   CK(cudaStreamSynchronize(c.s));
   ptrs[NV + 1] = 2 * NE;  // the reference's shifted histogram leaves 2*NE here
@@ -478,7 +600,7 @@ int glv_sort_node_edges_by_index(long NV, glv_edge *list1, glv_edge *list2, cons
     CK(cudaMemcpyAsync(&hb, bad, sizeof(hb), cudaMemcpyDeviceToHost, c.s));
     CK(cudaStreamSynchronize(c.s));
     if (hb) return fail(GLV_ERR_ARG, "a tail is outside [0, 2^31)");
-    CK(cudaMemcpyAsync(list1, dout, nnz * sizeof(glv_edge), cudaMemcpyDeviceToHost, c.s));
+    TRY(d2h_large(c.s, list1, dout, nnz * (int64_t)sizeof(glv_edge)));
   }
   CK(cudaStreamSynchronize(c.s));
   g_launches += c.launches;
@@ -493,38 +615,15 @@ int glv_build_csr(long NV, long NE, const glv_edge *edges, int flags, glv_graph 
   TRY(open_stream(c));
   DevScratch d(c.s);
   glv_edge *din, *dout;
-  int64_t *dptr, *svals, *order = nullptr, nk = NE;
+  int64_t *dptr, *order = nullptr, nk = NE;
   TRY(upload_edges(c.s, edges, NE, d, &din));
   TRY(d.get(&dptr, NV + 1));
-  if (NE > 0 && (flags & GLV_CSR_REMOVE_EDGES)) {
+  if (NE > 0 && (flags & GLV_CSR_REMOVE_EDGES))
     TRY(kept_order(c.s, NV, NE, aos_view(din), d, &order, &nk, &c.launches));
-  } else if (NE > 0) {
-    int32_t *bad;
-    uint64_t *k;
-    int64_t *v;
-    TRY(d.get(&bad, 1));
-    TRY(d.get(&k, NE));
-    TRY(d.get(&v, NE));
-    CK(cudaMemsetAsync(bad, 0, sizeof(int32_t), c.s));
-    k_edge_pair_keys<<<csr_grid(NE), 256, 0, c.s>>>(NE, aos_view(din), NV, id_bits(NV), k, v,
-                                                     bad);
-    ++c.launches;
-    CK(cudaGetLastError());
-    int32_t hb = 0;
-    CK(cudaMemcpyAsync(&hb, bad, sizeof(hb), cudaMemcpyDeviceToHost, c.s));
-    CK(cudaStreamSynchronize(c.s));
-    if (hb) return fail(GLV_ERR_ARG, "an edge end is outside [0, NV)");
-  }
-  TRY(row_entries(c.s, NV, nk, order, aos_view(din), (flags & GLV_CSR_SORT_ROWS) != 0, d, dptr,
-                  &svals, &c.launches));
   const int64_t m = 2 * nk;
   TRY(d.get(&dout, m));
-  if (m > 0) {
-    k_emit_entries<<<csr_grid(m), 256, 0, c.s>>>(m, svals, order, aos_view(din), nullptr, nullptr,
-                                                 dout);
-    ++c.launches;
-    CK(cudaGetLastError());
-  }
+  TRY(row_entries(c.s, NV, nk, order, aos_view(din), (flags & GLV_CSR_SORT_ROWS) != 0, d, dptr,
+                  nullptr, nullptr, dout, &c.launches));
   long *hp = (long *)malloc((NV + 1) * sizeof(long));
   glv_edge *he = (glv_edge *)malloc(std::max<int64_t>(m, 1) * sizeof(glv_edge));
   if (!hp || !he) {
@@ -532,13 +631,12 @@ int glv_build_csr(long NV, long NE, const glv_edge *edges, int flags, glv_graph 
     free(he);
     return fail(GLV_ERR_OOM, "host allocation failed");
   }
-  cudaMemcpyAsync(hp, dptr, (NV + 1) * sizeof(long), cudaMemcpyDeviceToHost, c.s);
-  if (m > 0) cudaMemcpyAsync(he, dout, m * sizeof(glv_edge), cudaMemcpyDeviceToHost, c.s);
-  const cudaError_t e = cudaStreamSynchronize(c.s);
-  if (e != cudaSuccess) {
+  int rc = d2h_large(c.s, hp, dptr, (NV + 1) * sizeof(long));
+  if (rc == GLV_OK) rc = d2h_large(c.s, he, dout, m * (int64_t)sizeof(glv_edge));
+  if (rc != GLV_OK) {
     free(hp);
     free(he);
-    return fail(GLV_ERR_CUDA, cudaGetErrorString(e));
+    return rc;
   }
   g_launches += c.launches;
   Gout->numVertices = NV;
@@ -560,37 +658,16 @@ int glv_dev_build_csr(long NV, long NE, const long *d_head, const long *d_tail,
   if (!engine_pool()) return fail(GLV_ERR_CUDA, "could not create the device memory pool");
   cudaStream_t s = (cudaStream_t)stream;
   long launches = 0;
-  int64_t *svals = nullptr, *order = nullptr, nk = NE;
+  int64_t *order = nullptr, nk = NE;
   const EdgeView ev{reinterpret_cast<const int64_t *>(d_head),
                     reinterpret_cast<const int64_t *>(d_tail), d_weight, 1};
   {
     DevScratch d(s);
-    if (NE > 0 && (flags & GLV_CSR_REMOVE_EDGES)) {
+    if (NE > 0 && (flags & GLV_CSR_REMOVE_EDGES))
       TRY(kept_order(s, NV, NE, ev, d, &order, &nk, &launches));
-    } else if (NE > 0) {
-      int32_t *bad;
-      uint64_t *k;
-      int64_t *v;
-      TRY(d.get(&bad, 1));
-      TRY(d.get(&k, NE));
-      TRY(d.get(&v, NE));
-      CK(cudaMemsetAsync(bad, 0, sizeof(int32_t), s));
-      k_edge_pair_keys<<<csr_grid(NE), 256, 0, s>>>(NE, ev, NV, id_bits(NV), k, v, bad);
-      ++launches;
-      CK(cudaGetLastError());
-      int32_t hb = 0;
-      CK(cudaMemcpyAsync(&hb, bad, sizeof(hb), cudaMemcpyDeviceToHost, s));
-      CK(cudaStreamSynchronize(s));
-      if (hb) return fail(GLV_ERR_ARG, "an edge end is outside [0, NV)");
-    }
     TRY(row_entries(s, NV, nk, order, ev, (flags & GLV_CSR_SORT_ROWS) != 0, d,
-                    reinterpret_cast<int64_t *>(d_ptr), &svals, &launches));
-    if (nk > 0) {
-      k_emit_entries<<<csr_grid(2 * nk), 256, 0, s>>>(2 * nk, svals, order, ev, d_tail_out,
-                                                       d_weight_out, nullptr);
-      ++launches;
-      CK(cudaGetLastError());
-    }
+                    reinterpret_cast<int64_t *>(d_ptr), d_tail_out, d_weight_out, nullptr,
+                    &launches));
   }
   CK(cudaStreamSynchronize(s));
   g_launches += launches;

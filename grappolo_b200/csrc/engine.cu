@@ -10,6 +10,7 @@
 #include <vector>
 
 #include <mutex>
+#include <thread>
 
 #include <cub/cub.cuh>
 
