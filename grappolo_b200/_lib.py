@@ -39,6 +39,17 @@ class GlvGraph(ct.Structure):
                 ('edgeListPtrs', ct.POINTER(ct.c_long)), ('edgeList', ct.POINTER(GlvEdge))]
 
 
+class GlvComparison(ct.Structure):
+    _fields_ = [('n1', ct.c_long), ('n2', ct.c_long), ('num_communities1', ct.c_long),
+                ('num_communities2', ct.c_long), ('same_same', ct.c_long),
+                ('same_diff', ct.c_long), ('diff_same', ct.c_long), ('precision', ct.c_double),
+                ('recall', ct.c_double), ('f_score', ct.c_double), ('gini1', ct.c_double),
+                ('gini2', ct.c_double)]
+
+    def to_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
 class GlvPhaseStats(ct.Structure):
     _fields_ = [('num_vertices', ct.c_long), ('nnz', ct.c_long), ('colored', ct.c_int),
                 ('recolored', ct.c_int), ('num_colors', ct.c_int), ('iterations', ct.c_int),
@@ -108,7 +119,8 @@ def lib():
                  'glv_vertex_following', 'glv_build_new_graph_vf', 'glv_remove_edges',
                  'glv_sort_edges_undirected', 'glv_sort_node_edges_by_index', 'glv_build_csr',
                  'glv_dev_build_csr', 'glv_binary_header', 'glv_load_binary', 'glv_write_binary',
-                 'glv_dev_load_binary'):
+                 'glv_dev_load_binary', 'glv_compare_communities',
+                 'glv_dev_compare_communities', 'glv_gini_coefficient'):
         getattr(L, name).restype = ct.c_int
     L.glv_run_multiphase_coloring.argtypes = [P(GlvGraph), P(ct.c_long), ct.c_int, ct.c_int,
                                               ct.c_int, ct.c_long, ct.c_double, ct.c_double,
@@ -148,6 +160,11 @@ def lib():
     L.glv_write_binary.argtypes = [P(GlvGraph), ct.c_char_p, ct.c_long]
     L.glv_dev_load_binary.argtypes = [ct.c_char_p, ct.c_long, ct.c_long, ct.c_void_p, ct.c_void_p,
                                       ct.c_void_p, ct.c_void_p]
+    L.glv_compare_communities.argtypes = [P(ct.c_long), ct.c_long, P(ct.c_long), ct.c_long,
+                                          P(GlvComparison)]
+    L.glv_dev_compare_communities.argtypes = [ct.c_long, ct.c_void_p, ct.c_void_p,
+                                              P(GlvComparison), ct.c_void_p]
+    L.glv_gini_coefficient.argtypes = [P(ct.c_long), ct.c_int, P(ct.c_double)]
     L.glv_renumber_clusters.argtypes = [P(ct.c_long), ct.c_long, P(ct.c_long)]
     L.glv_build_next_level.argtypes = [P(GlvGraph), P(GlvGraph), P(ct.c_long), ct.c_long,
                                        ct.c_int, P(ct.c_double)]

@@ -1,5 +1,6 @@
 // Grappolo's C++ entry points (include/grappolo_compat.h) over the C ABI.
 #include <cstdio>
+#include <vector>
 #include <cstdlib>
 #include <cstring>
 
@@ -137,6 +138,38 @@ void writeGraphBinaryFormatNew(graph *G, char *filename, long weighted) {
   int rc = glv_write_binary((const glv_graph *)G, filename, weighted);
   if (rc != GLV_OK) die("writeGraphBinaryFormatNew", rc);
   printf("Graph has been stored in file: %s\n", filename);
+}
+
+void computeCommunityComparisons(std::vector<long> &C1, long N1, std::vector<long> &C2, long N2) {
+  glv_comparison r;
+  int rc = glv_compare_communities(C1.data(), N1, C2.data(), N2, &r);
+  if (rc != GLV_OK) die("computeCommunityComparisons", rc);
+  printf("*******************************************\n");
+  printf("Cluster comparison statistics: \n");
+  printf("*******************************************\n");
+  printf("|C1| (truth)          : %ld\n", r.n1);
+  printf("Num communities in C1 : %ld\n", r.num_communities1);
+  printf("|C2| (output)         : %ld\n", r.n2);
+  printf("Num communities in C2 : %ld\n", r.num_communities2);
+  printf("-------------------------------------------\n");
+  printf("Same-Same (True positive)  : %ld\n", r.same_same);
+  printf("Same-Diff (False negative) : %ld\n", r.same_diff);
+  printf("Diff-Same (False positive) : %ld\n", r.diff_same);
+  printf("-------------------------------------------\n");
+  printf("Precision             :  %lf (%3.2lf%%)\n", r.precision, r.precision * 100);
+  printf("Recall                :  %lf (%3.2lf%%)\n", r.recall, r.recall * 100);
+  printf("F-score               :  %lf\n", r.f_score);
+  printf("-------------------------------------------\n");
+  printf("Gini coefficient, C1  :  %lf \n", r.gini1);
+  printf("Gini coefficient, C2  :  %lf \n", r.gini2);
+  printf("*******************************************\n");
+}
+
+double computeGiniCoefficient(long *colorSize, int numColors) {
+  double g = 0;
+  int rc = glv_gini_coefficient(colorSize, numColors, &g);
+  if (rc != GLV_OK) die("computeGiniCoefficient", rc);
+  return g;
 }
 
 long renumberClustersContiguously(long *C, long size) {

@@ -2,6 +2,7 @@
 // degree-bin schedule, CUDA-graph-captured sweep iterations, the multiphase
 // drivers and the C ABI declared in include/grappolo_b200.h.
 #include <algorithm>
+#include <climits>
 #include <atomic>
 #include <chrono>
 #include <cstdlib>
@@ -2880,6 +2881,7 @@ int glv_decide_batch(long nv, const long *ptr, const long *tail, const double *w
 // Edge lists to CSR, binary graph files
 // =========================================================================
 #include "csr_build.cuh"
+#include "compare.cuh"
 
 // =========================================================================
 // Modularity without allocation (glv_dev_modularity_static)

@@ -292,6 +292,39 @@ def load_binary_device(fileName, device='cuda'):
     return ptr, tail[:nnz], w[:nnz]
 
 
+def computeCommunityComparisons(C1, C2):
+    """Utility/utilityClusterComparisonMetrics.cpp:50 — C1 is the truth.
+    Returns (statistics dict, C1', C2'): the pair counts (same_same,
+    same_diff, diff_same), precision, recall, f_score, the Gini coefficients
+    and the label arrays relabelled as the reference leaves them."""
+    a = np.array(C1, dtype=np.int64, copy=True)
+    b = np.array(C2, dtype=np.int64, copy=True)
+    r = _lib.GlvComparison()
+    lp = lambda x: x.ctypes.data_as(_P(ct.c_long))  # noqa: E731
+    _lib.check(_lib.lib().glv_compare_communities(lp(a), a.shape[0], lp(b), b.shape[0],
+                                                  ct.byref(r)))
+    return r.to_dict(), a, b
+
+
+def compare_communities_device(d_C1, d_C2, stream=0):
+    """glv_dev_compare_communities on int64 torch tensors (relabelled in place)."""
+    r = _lib.GlvComparison()
+    _lib.check(_lib.lib().glv_dev_compare_communities(d_C1.numel(), d_C1.data_ptr(),
+                                                      d_C2.data_ptr(), ct.byref(r),
+                                                      stream or None))
+    return r.to_dict()
+
+
+def computeGiniCoefficient(colorSize):
+    """utilityClusterComparisonMetrics.cpp:310 — returns (Gini coefficient,
+    sizes sorted ascending)."""
+    s = np.array(colorSize, dtype=np.int64, copy=True)
+    g = ct.c_double(0)
+    _lib.check(_lib.lib().glv_gini_coefficient(s.ctypes.data_as(_P(ct.c_long)), s.shape[0],
+                                               ct.byref(g)))
+    return g.value, s
+
+
 def _take_graph(out):
     """CSRGraph + numEdges from a glv_graph whose arrays the library malloc'd
     (released here)."""

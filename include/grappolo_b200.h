@@ -169,6 +169,38 @@ int glv_write_binary(const glv_graph *G, const char *path, long weighted);
 int glv_dev_load_binary(const char *path, long numVertices, long nnz, long *d_ptr, int *d_tail,
                         double *d_weight, void *stream);
 
+/* ---- comparing community assignments -------------------------------------- */
+
+typedef struct {
+  long n1, n2;                /* vertices labelled by C1 (truth) and C2 (output) */
+  long num_communities1;      /* nC1 and nC2 as the reference counts them */
+  long num_communities2;
+  long same_same;             /* pairs together in both (true positives) */
+  long same_diff;             /* together in C1, apart in C2 (false negatives) */
+  long diff_same;             /* apart in C1, together in C2 (false positives) */
+  double precision, recall, f_score;
+  double gini1, gini2;        /* Gini coefficient of each side's community sizes */
+} glv_comparison;
+
+/* Replaces computeCommunityComparisons
+ * (Utility/utilityClusterComparisonMetrics.cpp:50-307,
+ * utilityClusteringFunctions.h:71): C1 is the truth.  Ids may be 0- or
+ * 1-based; -1 entries are relabelled in place as the reference does (C1: a
+ * new community; C2: N2 + 1).  The pair counts come from the contingency
+ * table of the two labellings on the GPU, equal to the reference's pair
+ * enumeration.  N1 must equal N2. */
+int glv_compare_communities(long *C1, long N1, long *C2, long N2, glv_comparison *out);
+
+/* Device form: int64 label arrays in device memory (relabelled in place). */
+int glv_dev_compare_communities(long n, long *d_C1, long *d_C2, glv_comparison *out,
+                                void *stream);
+
+/* Replaces computeGiniCoefficient (utilityClusterComparisonMetrics.cpp:310-330,
+ * basic_util.h:18): sorts colorSize[numColors] ascending in place and returns
+ * the coefficient through *gini.  Sums are exact 64-bit integers (the
+ * reference's FP64 sums agree while they stay below 2^53). */
+int glv_gini_coefficient(long *colorSize, int numColors, double *gini);
+
 /* ---- multiphase drivers ------------------------------------------------- */
 
 /* Replaces runMultiPhaseColoring (Coloring/runMultiPhaseColoring.cpp:51-238,

@@ -67,4 +67,10 @@ void SortNodeEdgesByIndex(long NV, edge *list1, edge *list2, long *ptrs);
 void parse_EdgeListBinaryNew(graph *G, char *fileName);
 void writeGraphBinaryFormatNew(graph *G, char *filename, long weighted);
 
+/* DefineStructure/utilityClusteringFunctions.h:71,73
+ * (Utility/utilityClusterComparisonMetrics.cpp), computed on the GPU */
+#include <vector>
+void computeCommunityComparisons(std::vector<long> &C1, long N1, std::vector<long> &C2, long N2);
+double computeGiniCoefficient(long *colorSize, int numColors);
+
 #endif /* GRAPPOLO_COMPAT_H */

@@ -686,6 +686,91 @@ void lvo_sort_node_edges(long nv, const long *ptrs, long *head, long *tail, doub
     free(idx); free(th); free(tt); free(tw);
 }
 
+/* ---- comparing community assignments (utilityClusterComparisonMetrics.cpp) */
+
+static int cmp_long(const void *a, const void *b) {
+    long x = *(const long *)a, y = *(const long *)b;
+    return x < y ? -1 : (x > y);
+}
+
+/* computeGiniCoefficient (:310-330): sizes sorted ascending in place. */
+double lvo_gini(long *size, int n) {
+    qsort(size, n, sizeof(long), cmp_long);
+    double num = 0.0, den = 0.0;
+    for (long i = 0; i < n; i++) {
+        num = num + ((i + 1) * size[i]);
+        den = den + size[i];
+    }
+    return ((2 * num) / (n * den)) - ((double)(n + 1) / (double)n);
+}
+
+/* Members of each community (0-based index ids[i] in [0, nc)), in vertex order. */
+static void group(long n, const long *ids, long nc, long **ptr_out, long **idx_out) {
+    long *ptr = (long *)calloc(nc + 1, sizeof(long));
+    long *idx = (long *)malloc(sizeof(long) * (n ? n : 1));
+    long *fill = (long *)calloc(nc, sizeof(long));
+    for (long i = 0; i < n; i++) ptr[ids[i] + 1]++;
+    for (long c = 0; c < nc; c++) ptr[c + 1] += ptr[c];
+    for (long i = 0; i < n; i++) idx[ptr[ids[i]] + fill[ids[i]]++] = i;
+    free(fill);
+    *ptr_out = ptr; *idx_out = idx;
+}
+
+/* computeCommunityComparisons (:50-307) at one thread.  C1, C2 are
+ * relabelled in place as the reference does: C1's -1 entries become the
+ * community count, which then grows by one (:63-87); C2's become N + 1
+ * (:89-113).  Ids are 0-based when 0 occurs, else 1-based.  Pairs are
+ * enumerated inside each community of C1 (:203-225) and of C2 (:228-251).
+ * res: SameSame, SameDiff, DiffSame, nC1, nC2; dres: precision, recall,
+ * F-score, Gini C1, Gini C2.  Returns -1 when an id is below -1.            */
+int lvo_compare_communities(long *C1, long *C2, long n, long *res, double *dres) {
+    long nC1 = -1, nC2 = -1;
+    int z1 = 0, z2 = 0, m1 = 0;
+    for (long i = 0; i < n; i++) {
+        if (C1[i] < -1 || C2[i] < -1) return -1;
+        if (C1[i] == 0) z1 = 1;
+        if (C1[i] == -1) m1 = 1;
+        if (C1[i] > nC1) nC1 = C1[i];
+        if (C2[i] == -1) C2[i] = n + 1;
+        if (C2[i] == 0) z2 = 1;
+        if (C2[i] > nC2) nC2 = C2[i];
+    }
+    if (z1) nC1++;
+    if (m1) {
+        for (long i = 0; i < n; i++) if (C1[i] == -1) C1[i] = nC1;
+        nC1++;
+    }
+    if (z2) nC2++;
+    long *t1 = (long *)malloc(sizeof(long) * n), *t2 = (long *)malloc(sizeof(long) * n);
+    for (long i = 0; i < n; i++) { t1[i] = C1[i] - (z1 ? 0 : 1); t2[i] = C2[i] - (z2 ? 0 : 1); }
+    long *p1, *i1, *p2, *i2;
+    group(n, t1, nC1, &p1, &i1);
+    group(n, t2, nC2, &p2, &i2);
+    long ss = 0, sd = 0, ds = 0, agree = 0;
+    for (long c = 0; c < nC1; c++)
+        for (long a = p1[c]; a < p1[c + 1]; a++)
+            for (long b = a + 1; b < p1[c + 1]; b++) {
+                if (C2[i1[a]] == C2[i1[b]]) ss++; else sd++;
+            }
+    for (long c = 0; c < nC2; c++)
+        for (long a = p2[c]; a < p2[c + 1]; a++)
+            for (long b = a + 1; b < p2[c + 1]; b++) {
+                if (C1[i2[a]] == C1[i2[b]]) agree++; else ds++;
+            }
+    double precision = (double)ss / (double)(ss + ds);
+    double recall = (double)ss / (double)(ss + sd);
+    long *s1 = (long *)malloc(sizeof(long) * nC1), *s2 = (long *)malloc(sizeof(long) * nC2);
+    for (long c = 0; c < nC1; c++) s1[c] = p1[c + 1] - p1[c];
+    for (long c = 0; c < nC2; c++) s2[c] = p2[c + 1] - p2[c];
+    res[0] = ss; res[1] = sd; res[2] = ds; res[3] = nC1; res[4] = nC2;
+    dres[0] = precision; dres[1] = recall;
+    dres[2] = 2 * ((precision * recall) / (precision + recall));
+    dres[3] = lvo_gini(s1, (int)nC1);
+    dres[4] = lvo_gini(s2, (int)nC2);
+    free(t1); free(t2); free(p1); free(i1); free(p2); free(i2); free(s1); free(s2);
+    return 0;
+}
+
 void lvo_free(void *p) { free(p); }
 
 /* Q of a final assignment over the original graph.  The reference's

@@ -76,6 +76,8 @@ class COracle:
         L.lvo_vertex_degrees.restype = ct.c_double
         L.lvo_color_greedy.restype = ct.c_int
         L.lvo_color_mhash.restype = ct.c_int
+        L.lvo_gini.restype = ct.c_double
+        L.lvo_compare_communities.restype = ct.c_int
         L.lvo_remove_edges.restype = ct.c_long
         L.lvo_coloring_phase.restype = ct.c_double
         L.lvo_basic_phase.restype = ct.c_double
@@ -193,6 +195,23 @@ class COracle:
         self.L.lvo_sort_node_edges(ct.c_long(nv), _lp(p), _lp(h), _lp(t), _dp(ww))
         return h, t, ww
 
+    def compare(self, C1, C2):
+        """computeCommunityComparisons on copies: (stats dict, C1', C2')."""
+        a, b = np.array(C1, dtype=np.int64), np.array(C2, dtype=np.int64)
+        res, dres = np.zeros(5, dtype=np.int64), np.zeros(5)
+        rc = self.L.lvo_compare_communities(_lp(a), _lp(b), ct.c_long(len(a)), _lp(res),
+                                            _dp(dres))
+        if rc != 0:
+            raise ValueError('a community id below -1')
+        return dict(same_same=int(res[0]), same_diff=int(res[1]), diff_same=int(res[2]),
+                    num_communities1=int(res[3]), num_communities2=int(res[4]),
+                    precision=dres[0], recall=dres[1], f_score=dres[2], gini1=dres[3],
+                    gini2=dres[4]), a, b
+
+    def gini(self, sizes):
+        s = np.array(sizes, dtype=np.int64)
+        return self.L.lvo_gini(_lp(s), ct.c_int(len(s))), s
+
     def decide_batch(self, g, C, vdeg, cdeg, csize, constant, verts):
         p, t, w = _csr(g)
         C = np.ascontiguousarray(C, dtype=np.int64)
@@ -276,6 +295,26 @@ def parse_reference_log(text: str) -> dict:
     return out
 
 
+def parse_comparison_log(text: str) -> dict:
+    """The statistics block computeCommunityComparisons prints."""
+    pats = {'num_communities1': r'Num communities in C1\s*:\s*(\d+)',
+            'num_communities2': r'Num communities in C2\s*:\s*(\d+)',
+            'same_same': r'Same-Same \(True positive\)\s*:\s*(\d+)',
+            'same_diff': r'Same-Diff \(False negative\)\s*:\s*(\d+)',
+            'diff_same': r'Diff-Same \(False positive\)\s*:\s*(\d+)',
+            'precision': r'Precision\s*:\s*([-\d.naif]+)',
+            'recall': r'Recall\s*:\s*([-\d.naif]+)',
+            'f_score': r'F-score\s*:\s*([-\d.naif]+)',
+            'gini1': r'Gini coefficient, C1\s*:\s*([-\d.naif]+)',
+            'gini2': r'Gini coefficient, C2\s*:\s*([-\d.naif]+)'}
+    out = {}
+    for k, p in pats.items():
+        m = re.search(p, text)
+        if m:
+            out[k] = int(m.group(1)) if p.endswith(r'(\d+)') else float(m.group(1))
+    return out
+
+
 class Reference:
     """Grappolo's own functions, compiled from its sources (oracle/_ref)."""
 
@@ -288,6 +327,8 @@ class Reference:
         self.L = L
         L.ref_color.restype = ct.c_int
         L.ref_color_mhash.restype = ct.c_int
+        L.ref_gini.restype = ct.c_double
+        L.ref_compare.restype = ct.c_long
         L.ref_remove_edges.restype = ct.c_long
         L.ref_load_binary.restype = ct.c_long
         L.ref_coloring_phase.restype = ct.c_double
@@ -444,6 +485,18 @@ class Reference:
         for a in (op, oh, ot, ow):
             self.L.ref_free(a)
         return ptr, arr[0], arr[1], arr[2], ne.value
+
+    def compare(self, C1, C2, nthreads=1):
+        """computeCommunityComparisons: (parsed statistics, C1', C2')."""
+        a, b = np.array(C1, dtype=np.int64), np.array(C2, dtype=np.int64)
+        buf = ct.create_string_buffer(1 << 16)
+        self.L.ref_compare(_lp(a), _lp(b), ct.c_long(len(a)), ct.c_int(nthreads), buf,
+                           ct.c_long(1 << 16))
+        return parse_comparison_log(buf.value.decode(errors='replace')), a, b
+
+    def gini(self, sizes):
+        s = np.array(sizes, dtype=np.int64)
+        return self.L.ref_gini(_lp(s), ct.c_int(len(s))), s
 
     def decide_batch(self, g, C, vdeg, cdeg, csize, constant, verts):
         p, t, w = _csr(g)

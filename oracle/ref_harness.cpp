@@ -418,6 +418,28 @@ long ref_load_binary(const char *path, long **optr, long **ohead, long **otail, 
     return nv;
 }
 
+// Utility/utilityClusterComparisonMetrics.cpp:50 computeCommunityComparisons;
+// the relabelled arrays are written back, the printed statistics go to log.
+long ref_compare(long *C1, long *C2, long n, int nthreads, char *log, long cap) {
+    struct Args { long *C1, *C2, n; int nthreads; } a{C1, C2, n, nthreads};
+    return run_captured(log, cap, [](void *p) {
+        Args *a = (Args *)p;
+        omp_set_num_threads(a->nthreads);
+        std::vector<long> v1(a->C1, a->C1 + a->n), v2(a->C2, a->C2 + a->n);
+        computeCommunityComparisons(v1, a->n, v2, a->n);
+        memcpy(a->C1, v1.data(), sizeof(long) * a->n);
+        memcpy(a->C2, v2.data(), sizeof(long) * a->n);
+    }, &a);
+}
+
+// utilityClusterComparisonMetrics.cpp:310 computeGiniCoefficient (sorts sizes).
+double ref_gini(long *size, int n) {
+    quiet_begin();
+    double g = computeGiniCoefficient(size, n);
+    quiet_end();
+    return g;
+}
+
 // InputsOutput/loadMetis.cpp:19 loadMetisFileFormat -> SoA CSR (malloc'd).
 long ref_load_metis(const char *path, long **optr, long **otail, double **ow) {
     graph G;

@@ -64,3 +64,25 @@ def csr_cases():
         exp['nge'] = int(exp['nge'])
         out.append((name, exp))
     return out
+
+
+def compare_cases():
+    """(name, C1, C2, expected) of compare.npz (computeCommunityComparisons
+    as the reference printed it, and the arrays it left relabelled)."""
+    z = np.load(os.path.join(GOLDEN, 'compare.npz'))
+    out = []
+    for name in map(str, z['names']):
+        p = f'{name}_'
+        exp = {k[len(p):]: z[k] for k in z.files if k.startswith(p)}
+        out.append((name, exp.pop('C1').astype(np.int64), exp.pop('C2').astype(np.int64), exp))
+    return out
+
+
+def gini_cases():
+    z = np.load(os.path.join(GOLDEN, 'compare.npz'))
+    return [(z[f'gini{k}_sizes'], float(z[f'gini{k}_value']), z[f'gini{k}_sorted'])
+            for k in range(int(z['ngini']))]
+
+
+COMPARE_INTS = ('same_same', 'same_diff', 'diff_same', 'num_communities1', 'num_communities2')
+COMPARE_FLOATS = ('precision', 'recall', 'f_score', 'gini1', 'gini2')

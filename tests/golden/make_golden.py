@@ -6,6 +6,7 @@ Run from the repository root after ``make -C oracle``:
     python tests/golden/make_golden.py --vf     # only vf.npz (vertex following)
     python tests/golden/make_golden.py --mhash  # only mhash.npz (coloring = 3)
     python tests/golden/make_golden.py --csr    # only csr_build.npz and karate.bin
+    python tests/golden/make_golden.py --compare  # only compare.npz
 
 Each fixture ``<case>.npz`` holds an input CSR and what the reference's
 functions return for it at OMP_NUM_THREADS=1: the distance-1 colouring, one
@@ -217,6 +218,45 @@ def make_csr(R, ref_root):
     print('wrote csr_build', list(cases), 'and karate.bin')
 
 
+def comparison_cases(ref_root):
+    """(truth, output) label pairs: planted blocks against the reference's
+    own Louvain result, and random labellings with -1 entries, 0- and
+    1-based ids."""
+    z = np.load(os.path.join(HERE, 'pp1000.npz'))
+    out = {'pp1000': (np.arange(1000) // 50, z['mpc_C'])}
+    rng = np.random.default_rng(23)
+    for name, n, k1, k2, b1, b2, m1, m2 in [('rand0', 3000, 40, 25, 0, 0, 0, 0),
+                                             ('rand_neg', 4000, 60, 30, 1, 0, 40, 25),
+                                             ('rand_one', 2500, 7, 300, 1, 1, 5, 50)]:
+        C1 = rng.integers(0, k1, n) + b1
+        C2 = rng.integers(0, k2, n) + b2
+        C1[rng.integers(0, n, m1)] = -1
+        C2[rng.integers(0, n, m2)] = -1
+        out[name] = (C1, C2)
+    return out
+
+
+def make_compare(R, ref_root):
+    """compare.npz: computeCommunityComparisons (printed statistics and the
+    relabelled arrays) and computeGiniCoefficient of the reference."""
+    out = {}
+    cases = comparison_cases(ref_root)
+    for name, (C1, C2) in cases.items():
+        st, a, b = R.compare(C1, C2)
+        out.update({f'{name}_C1': C1.astype(np.int32), f'{name}_C2': C2.astype(np.int32),
+                    f'{name}_C1_after': a.astype(np.int32), f'{name}_C2_after': b.astype(np.int32)})
+        out.update({f'{name}_{k}': v for k, v in st.items()})
+    rng = np.random.default_rng(29)
+    sizes = [rng.integers(0, 1000, 77), np.array([5]), rng.integers(0, 3, 500),
+             np.arange(1, 4097)]
+    for k, sz in enumerate(sizes):
+        g, srt = R.gini(sz)
+        out.update({f'gini{k}_sizes': sz, f'gini{k}_value': g, f'gini{k}_sorted': srt})
+    np.savez_compressed(os.path.join(HERE, 'compare.npz'), names=np.array(list(cases)),
+                        ngini=len(sizes), **out)
+    print('wrote compare', list(cases))
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 and not sys.argv[1].startswith('--') \
         else '/root/reference'
@@ -229,6 +269,9 @@ def main():
         return
     if '--csr' in sys.argv:
         make_csr(R, ref_root)
+        return
+    if '--compare' in sys.argv:
+        make_compare(R, ref_root)
         return
     rng = np.random.default_rng(2024)
     for name, g in all_cases(ref_root).items():

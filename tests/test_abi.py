@@ -53,6 +53,8 @@ REFERENCE_SYMBOLS = [
     '_Z20SortNodeEdgesByIndexlP4edgeS0_Pl',
     '_Z23parse_EdgeListBinaryNewP5graphPc',
     '_Z25writeGraphBinaryFormatNewP5graphPcl',
+    '_Z27computeCommunityComparisonsRSt6vectorIlSaIlEElS2_l',
+    '_Z22computeGiniCoefficientPli',
 ]
 
 
@@ -82,7 +84,10 @@ def test_compat_header_matches_reference_mangling(tmp_path):
                    '  SortEdgesUndirected(4, 2, g->edgeList, o->edgeList, c);\n'
                    '  SortNodeEdgesByIndex(4, g->edgeList, o->edgeList, c);\n'
                    '  parse_EdgeListBinaryNew(g, (char *)"f");\n'
-                   '  writeGraphBinaryFormatNew(g, (char *)"f", 1);\n}\n')
+                   '  writeGraphBinaryFormatNew(g, (char *)"f", 1);\n'
+                   '  std::vector<long> v1, v2;\n'
+                   '  computeCommunityComparisons(v1, 0, v2, 0);\n'
+                   '  computeGiniCoefficient(c, 4);\n}\n')
     obj = tmp_path / 'use.o'
     subprocess.run(['g++', '-c', '-I', os.path.join(ROOT, 'include'), str(src), '-o', str(obj)],
                    check=True)

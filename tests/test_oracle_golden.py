@@ -6,7 +6,8 @@ import numpy as np
 import pytest
 
 from grappolo_b200 import graphs
-from _golden import CASES, csr_cases, load, mhash_cases, pins, srand
+from _golden import (CASES, COMPARE_FLOATS, COMPARE_INTS, compare_cases, csr_cases, gini_cases,
+                     load, mhash_cases, pins, srand)
 
 
 @pytest.mark.parametrize('name', CASES)
@@ -161,3 +162,23 @@ def test_binary_file_golden(tmp_path):
     out = tmp_path / 'k.bin'
     graphs.write_binary(g, str(out))
     assert out.read_bytes() == open(path, 'rb').read()
+
+
+@pytest.mark.parametrize('case', compare_cases(), ids=lambda c: c[0])
+def test_community_comparison_golden(oracle, case):
+    """computeCommunityComparisons: pair counts exact, rates to the printed
+    six decimals, the relabelled arrays as the reference leaves them."""
+    _, C1, C2, exp = case
+    st, a, b = oracle.compare(C1, C2)
+    for k in COMPARE_INTS:
+        assert st[k] == int(exp[k]), k
+    for k in COMPARE_FLOATS:
+        assert abs(st[k] - float(exp[k])) <= 5e-7, k
+    assert np.array_equal(a, exp['C1_after']) and np.array_equal(b, exp['C2_after'])
+
+
+@pytest.mark.parametrize('k', range(4))
+def test_gini_golden(oracle, k):
+    sizes, value, srt = gini_cases()[k]
+    g, s = oracle.gini(sizes)
+    assert g == value and np.array_equal(s, srt)

@@ -129,3 +129,22 @@ def test_edge_list_preprocessing_matches_reference(oracle, reference, seed):
         no = oracle.sort_node_edges(nv, *so)
         nr = reference.sort_node_edges(nv, *sr)
         assert all(np.array_equal(x, y) for x, y in zip(no, nr))
+
+
+@pytest.mark.parametrize('seed', [4, 5, 6])
+def test_community_comparison_matches_reference(oracle, reference, seed):
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(50, 5000))
+    C1 = rng.integers(0, int(rng.integers(2, 80)), n) + int(rng.integers(0, 2))
+    C2 = rng.integers(0, int(rng.integers(2, 300)), n) + int(rng.integers(0, 2))
+    C1[rng.integers(0, n, int(rng.integers(0, 30)))] = -1
+    C2[rng.integers(0, n, int(rng.integers(0, 30)))] = -1
+    o, a1, a2 = oracle.compare(C1, C2)
+    r, b1, b2 = reference.compare(C1, C2)
+    for k in ('same_same', 'same_diff', 'diff_same', 'num_communities1', 'num_communities2'):
+        assert o[k] == r[k], k
+    for k in ('precision', 'recall', 'f_score', 'gini1', 'gini2'):
+        assert abs(o[k] - r[k]) <= 5e-7, k
+    assert np.array_equal(a1, b1) and np.array_equal(a2, b2)
+    sz = rng.integers(0, 10000, int(rng.integers(1, 3000)))
+    assert oracle.gini(sz)[0] == reference.gini(sz)[0]
