@@ -49,10 +49,11 @@ def parse_args():
     p.add_argument('--no-cpu-baseline', action='store_true')
     p.add_argument('--profile-level', type=int, default=1,
                    help='1: time each class sweep (roofline); 2: time every launch by kind')
-    p.add_argument('--workload', choices=['rmat', 'batch', 'csr'], default='rmat',
+    p.add_argument('--workload', choices=['rmat', 'batch', 'csr', 'compare'], default='rmat',
                    help='rmat: one R-MAT graph (default); batch: 4,096 planted-partition '
                         'graphs run as batches; csr: edge list to CSR (removeEdges, both '
-                        'directions, rows sorted) of a raw R-MAT edge list')
+                        'directions, rows sorted) of a raw R-MAT edge list; compare: '
+                        'community-comparison metrics of two labellings of 2^scale vertices')
     p.add_argument('--csr-sample-scale', type=int, default=16,
                    help='csr workload: R-MAT scale of the reference\'s CPU sample')
     p.add_argument('--batch-graphs', type=int, default=4096)
@@ -155,6 +156,8 @@ def run_reference(args, rank):
         return 0
     if args.workload == 'csr':
         return run_csr_reference(args)
+    if args.workload == 'compare':
+        return run_compare_reference(args)
     import numpy as np
     import torch
     from grappolo_b200 import graphs
@@ -252,6 +255,174 @@ def run_csr_reference(args):
             'e2e': {'value': value, 'unit': CSR_UNIT, 'h2d_bytes_per_step': 0,
                     'd2h_bytes_per_step': 0}}
     print(json.dumps(line), flush=True)
+    return 0
+
+
+CMP_METRIC = 'labelled vertices compared/s'
+CMP_UNIT = 'vertices/s'
+CMP_BLOCK = 1000
+
+
+def compare_labels(n, seed=7):
+    """Truth: consecutive blocks of CMP_BLOCK vertices; output: the truth with
+    20% of the vertices moved to random labels and 0.05% of either side -1."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    C1 = np.arange(n, dtype=np.int64) // CMP_BLOCK
+    C2 = C1.copy()
+    flip = rng.random(n) < 0.2
+    C2[flip] = rng.integers(0, 2 * max(1, n // CMP_BLOCK), int(flip.sum()))
+    C1[rng.integers(0, n, n // 2000)] = -1
+    C2[rng.integers(0, n, n // 2000)] = -1
+    return C1, C2
+
+
+def compare_config(args, n):
+    return {'workload': f'computeCommunityComparisons (pair counts, precision, recall, F-score, '
+                        f'Gini) of two labellings of 2^{args.scale} vertices',
+            'labels': f'truth: blocks of {CMP_BLOCK}; output: 20% of vertices relabelled at '
+                      f'random, 0.05% of each side -1; seed 7',
+            'num_vertices': n, 'parallelism': f'replicas x{args.gpus}',
+            'l2': 'inputs larger than L2 (no flush)' if n >= (1 << 24) else 'inputs in L2'}
+
+
+def compare_cpu_sample(scale):
+    """The reference's computeCommunityComparisons on one sample of 2^scale
+    vertices, at one thread: its pair loops sit in an `omp parallel for`
+    nested inside an `omp parallel` region, so with T threads every thread
+    runs every pair (T times the work, and counts T times too large).
+    Returns (vertices/s, seconds, n, threads)."""
+    from oracle import Reference
+    n = 1 << scale
+    C1, C2 = compare_labels(n)
+    cores = 1
+    R = Reference(fast=True)
+    t0 = time.perf_counter()
+    R.compare(C1, C2, nthreads=cores)
+    dt = time.perf_counter() - t0
+    return n / dt, dt, n, cores
+
+
+def run_compare_reference(args):
+    vals = []
+    for k in range(args.warmup + args.steps):
+        v, dt, n, cores = compare_cpu_sample(min(args.scale, 20))
+        if k >= args.warmup:
+            vals.append(v)
+    value = statistics.median(vals)
+    line = {'metric': CMP_METRIC, 'value': value, 'unit': CMP_UNIT, 'impl': 'reference',
+            'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
+            'ms_per_step': 1e3 * (1 << args.scale) / value, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'int64', 'data': 'synthetic',
+            'config': compare_config(args, 1 << args.scale),
+            'cpu_baseline': {'value': value, 'unit': CMP_UNIT, 'cores': cores,
+                             'kind': 'reference',
+                             'sample': f'reference computeCommunityComparisons, one thread (its '
+                                       f'nested OpenMP regions repeat all work per thread), '
+                                       f'-Ofast build, on {n} vertices ({dt:.2f} s)'},
+            'e2e': {'value': value, 'unit': CMP_UNIT, 'h2d_bytes_per_step': 0,
+                    'd2h_bytes_per_step': 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_compare_workload(args, world, rank, local):
+    """A step compares two device-resident labellings (glv_dev_compare_communities);
+    e2e: glv_compare_communities from host arrays, relabelled arrays copied back."""
+    import torch
+    from grappolo_b200 import louvain, _lib
+    torch.cuda.set_device(local)
+    dev = torch.device('cuda', local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=600),
+                                device_id=dev)
+    L = _lib.lib()
+    n = 1 << args.scale
+    C1, C2 = compare_labels(n)
+    d1, d2 = torch.tensor(C1, device=dev), torch.tensor(C2, device=dev)
+    w1, w2 = d1.clone(), d2.clone()
+    stream = torch.cuda.current_stream().cuda_stream
+
+    def step():
+        w1.copy_(d1)  # the call relabels in place; every step starts from the inputs
+        w2.copy_(d2)
+        return louvain.compare_communities_device(w1, w2, stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    l0 = L.glv_kernel_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(args.steps):
+        st = step()
+    ev1.record()
+    torch.cuda.synchronize()
+    launches = L.glv_kernel_launch_count() - l0
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    t = ev0.elapsed_time(ev1) * 1e-3
+    t_max, n_all = aggregate(t, float(n * args.steps), dist, dev)
+    # algorithmic bytes: both labellings read once (8 B each per vertex)
+    alg = 16 * n
+    peak, peak_kind = measured_peak()
+    achieved = alg / (t / args.steps) / 1e9
+    roofline = {'bound': 'hbm', 'kernel': 'the whole comparison (our kernels, the CUB radix sort '
+                                          'and run-length encode), per step',
+                'achieved': achieved, 'peak': peak, 'unit': 'GB/s', 'frac': achieved / peak,
+                'peak_kind': peak_kind, 'traffic': None, 'algorithmic_bytes_per_launch': alg,
+                'avg_launch_s': t / args.steps}
+    e2e = None
+    if not args.no_e2e:
+        h1 = torch.from_numpy(C1).pin_memory()
+        h2 = torch.from_numpy(C2).pin_memory()
+        import numpy as np
+        a, b = h1.numpy(), h2.numpy()
+
+        def e2e_step():
+            a[:] = C1
+            b[:] = C2
+            r = _lib.GlvComparison()
+            import ctypes as ct
+            lp = lambda x: ct.cast(x.data_ptr(), ct.POINTER(ct.c_long))  # noqa: E731
+            _lib.check(L.glv_compare_communities(lp(h1), n, lp(h2), n, ct.byref(r)))
+            return r
+
+        e2e_step()
+        e0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        et = time.perf_counter() - e0
+        et, ee = aggregate(et, float(n * args.steps), dist, dev)
+        e2e = {'value': ee / et, 'unit': CMP_UNIT, 'h2d_bytes_per_step': 16 * n,
+               'd2h_bytes_per_step': 16 * n, 'seconds_per_step': et / args.steps,
+               'note': 'timed on the host clock; includes resetting the pinned inputs'}
+        del np
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cv, cdt, cn, cores = compare_cpu_sample(min(args.scale, 20))
+        cpu = {'value': cv, 'unit': CMP_UNIT, 'cores': cores, 'kind': 'reference',
+               'sample': f'reference computeCommunityComparisons, one thread (its nested '
+                         f'OpenMP regions repeat all work per thread), -Ofast build, on {cn} '
+                         f'vertices ({cdt:.2f} s)'}
+    extra = {'f_score': st['f_score'], 'same_same': st['same_same']}
+    line = {'metric': CMP_METRIC, 'value': n_all / t_max, 'unit': CMP_UNIT, 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 * t / args.steps,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'int64',
+            'data': 'synthetic (seeded labellings)',
+            'config': dict(compare_config(args, n), **extra), 'roofline': roofline,
+            'cpu_baseline': cpu, 'e2e': e2e, 'gpu_launches': launches, 'clocks': clk}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
     return 0
 
 
@@ -472,6 +643,8 @@ def main():
         return run_batch_workload(args, world, rank, local)
     if args.workload == 'csr':
         return run_csr_workload(args, world, rank, local)
+    if args.workload == 'compare':
+        return run_compare_workload(args, world, rank, local)
     import numpy as np
     import torch
     from grappolo_b200 import graphs, louvain, _lib
