@@ -111,18 +111,19 @@ static double gini_from(unsigned long long num, unsigned long long den, int numC
 }
 
 // Sizes sorted ascending (into *sorted) and the Gini sums of them
-// (sums[0] numerator, sums[1] total).
-static int gini_sums(cudaStream_t s, const unsigned long long *sizes, int64_t m, DevScratch &d,
-                     unsigned long long **sorted, unsigned long long sums[2], long *launches) {
+// (sums[0] numerator, sums[1] total); sizes take at most `bits` bits.
+static int gini_sums(cudaStream_t s, const unsigned long long *sizes, int64_t m, int bits,
+                     DevScratch &d, unsigned long long **sorted, unsigned long long sums[2],
+                     long *launches) {
   unsigned long long *acc;
   TRY(d.get(sorted, m));
   TRY(d.get(&acc, 2));
   CK(cudaMemsetAsync(acc, 0, 2 * sizeof(*acc), s));
   size_t tb = 0;
-  CK(cub::DeviceRadixSort::SortKeys(nullptr, tb, sizes, *sorted, m, 0, 64, s));
+  CK(cub::DeviceRadixSort::SortKeys(nullptr, tb, sizes, *sorted, m, 0, bits, s));
   void *temp;
   TRY(d.get((char **)&temp, (int64_t)tb));
-  CK(cub::DeviceRadixSort::SortKeys(temp, tb, sizes, *sorted, m, 0, 64, s));
+  CK(cub::DeviceRadixSort::SortKeys(temp, tb, sizes, *sorted, m, 0, bits, s));
   k_gini_sums<<<csr_grid(m), 256, 0, s>>>(m, *sorted, acc);
   ++*launches;
   CK(cudaGetLastError());
@@ -201,8 +202,10 @@ static int compare_device(cudaStream_t s, int64_t n, int64_t *dC1, int64_t *dC2,
   CK(cudaMemcpyAsync(pairs, acc, sizeof(pairs), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));
   unsigned long long g1[2], g2[2], *srt;
-  TRY(gini_sums(s, h1, nC1, d, &srt, g1, launches));
-  TRY(gini_sums(s, h2, nC2, d, &srt, g2, launches));
+  // community sizes are at most n: sort only the bits that can be set
+  const int size_bits = id_bits(n + 1);
+  TRY(gini_sums(s, h1, nC1, size_bits, d, &srt, g1, launches));
+  TRY(gini_sums(s, h2, nC2, size_bits, d, &srt, g2, launches));
   const long SameSame = (long)pairs[0];
   const long SameDiff = (long)(pairs[1] - pairs[0]);
   const long DiffSame = (long)(pairs[2] - pairs[0]);
@@ -288,7 +291,7 @@ int glv_gini_coefficient(long *colorSize, int numColors, double *gini) {
   CK(cudaMemcpyAsync(&hf, fl, sizeof(hf), cudaMemcpyDeviceToHost, c.s));
   CK(cudaStreamSynchronize(c.s));
   if (hf & 6) return fail(GLV_ERR_ARG, "a negative size");
-  TRY(gini_sums(c.s, dh, numColors, d, &sorted, sums, &c.launches));
+  TRY(gini_sums(c.s, dh, numColors, 64, d, &sorted, sums, &c.launches));
   // the reference sorts colorSize in place
   CK(cudaMemcpyAsync(colorSize, sorted, numColors * sizeof(long), cudaMemcpyDeviceToHost, c.s));
   CK(cudaStreamSynchronize(c.s));
