@@ -120,7 +120,8 @@ def lib():
                  'glv_sort_edges_undirected', 'glv_sort_node_edges_by_index', 'glv_build_csr',
                  'glv_dev_build_csr', 'glv_binary_header', 'glv_load_binary', 'glv_write_binary',
                  'glv_dev_load_binary', 'glv_compare_communities',
-                 'glv_dev_compare_communities', 'glv_gini_coefficient'):
+                 'glv_dev_compare_communities', 'glv_gini_coefficient',
+                 'glv_vbase_redistribution'):
         getattr(L, name).restype = ct.c_int
     L.glv_run_multiphase_coloring.argtypes = [P(GlvGraph), P(ct.c_long), ct.c_int, ct.c_int,
                                               ct.c_int, ct.c_long, ct.c_double, ct.c_double,
@@ -165,6 +166,8 @@ def lib():
     L.glv_dev_compare_communities.argtypes = [ct.c_long, ct.c_void_p, ct.c_void_p,
                                               P(GlvComparison), ct.c_void_p]
     L.glv_gini_coefficient.argtypes = [P(ct.c_long), ct.c_int, P(ct.c_double)]
+    L.glv_vbase_redistribution.argtypes = [P(GlvGraph), P(ct.c_int), ct.c_int, ct.c_int,
+                                           P(ct.c_long)]
     L.glv_renumber_clusters.argtypes = [P(ct.c_long), ct.c_long, P(ct.c_long)]
     L.glv_build_next_level.argtypes = [P(GlvGraph), P(GlvGraph), P(ct.c_long), ct.c_long,
                                        ct.c_int, P(ct.c_double)]

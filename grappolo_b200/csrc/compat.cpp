@@ -172,6 +172,13 @@ double computeGiniCoefficient(long *colorSize, int numColors) {
   return g;
 }
 
+int vBaseRedistribution(graph *G, int *vtxColor, int ncolors, int type) {
+  long moves = 0;
+  int rc = glv_vbase_redistribution((const glv_graph *)G, vtxColor, ncolors, type, &moves);
+  if (rc != GLV_OK) die("vBaseRedistribution", rc);
+  return (int)moves;
+}
+
 long renumberClustersContiguously(long *C, long size) {
   long n = 0;
   int rc = glv_renumber_clusters(C, size, &n);

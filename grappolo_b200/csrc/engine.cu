@@ -2,6 +2,7 @@
 // degree-bin schedule, CUDA-graph-captured sweep iterations, the multiphase
 // drivers and the C ABI declared in include/grappolo_b200.h.
 #include <algorithm>
+#include <cmath>
 #include <climits>
 #include <atomic>
 #include <chrono>
@@ -14,11 +15,13 @@
 #include <thread>
 
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 
 #include "batch_kernels.cuh"
 #include "gate.cuh"
 #include "persist.cuh"
 #include "recolor.cuh"
+#include "vbase.cuh"
 #include "phase_kernels.cuh"
 #include "sweep.cuh"
 
@@ -233,12 +236,15 @@ class Engine {
   int sublevels_batch(const Level &L, const Batch &b, int32_t **d_sub, int *nsub);
   void free_level(Level &L);
   Batch *bt_ = nullptr;  // set while a batch runs
-  // colouring of colour phases: 1 = distance-1 (the default), 3 = the
-  // incomplete multi-hash max/min colouring with mhash_nhash_ hashes and
-  // mhash_itrs_ iterations
+  // colouring of colour phases: 1 = distance-1 (the default), 2 = distance-1
+  // then balanced (vBaseRedistribution, first fit), 3 = the incomplete
+  // multi-hash max/min colouring with mhash_nhash_ hashes and mhash_itrs_
+  // iterations
   int color_algo_ = 1;
   int mhash_nhash_ = 2, mhash_itrs_ = 4;
   int color_mhash(const Level &L, int *ncolors);
+  // Balanced recolouring of a proper colouring (coloring = 2); *moves may be NULL
+  int vbase(const Level &L, int ncolors, int type, long *moves);
 
   // state buffers (device)
   double *vDeg = nullptr, *cDeg = nullptr, *dDeg = nullptr, *own_w = nullptr;
@@ -576,7 +582,50 @@ int Engine::color(const Level &L, int *ncolors, double *secs) {
       fprintf(stderr, "grappolo_b200: recolour %.4f s (%d colours)\n", now_s() - td, *ncolors);
     }
   }
+  // coloring = 2: runMultiPhaseColoring.cpp:67-74, 180-186
+  if (color_algo_ == 2) TRY(vbase(L, *ncolors, 0, nullptr));
   if (secs) *secs = now_s() - t0;
+  return GLV_OK;
+}
+
+int Engine::vbase(const Level &L, int ncolors, int type, long *moves) {
+  if (L.nv == 0 || ncolors <= 0) {
+    if (moves) *moves = 0;
+    return GLV_OK;
+  }
+  if (ncolors > kMaxColors) return fail(GLV_ERR_COLORS, "more colours than the 4096 cap");
+  const int64_t nv = L.nv;
+  const int64_t avg = (int64_t)ceil((double)nv / (double)ncolors);  // vBase.cpp:80
+  int32_t *freq, *flag, *cand;
+  int64_t *ncand;
+  unsigned long long *dmoves;
+  TRY(alloc(&freq, ncolors));
+  TRY(alloc(&flag, nv));
+  TRY(alloc(&cand, nv));
+  TRY(alloc(&ncand, 1));
+  TRY(alloc(&dmoves, 1));
+  CK(cudaMemsetAsync(freq, 0, ncolors * sizeof(int32_t), s_));
+  LAUNCH(k_color_hist, grid_for(nv, 256, nsm_ * 16), 256, 0, s_, nv, color_, freq);
+  LAUNCH(k_vbase_flags, grid_for(nv, 256, nsm_ * 16), 256, 0, s_, nv, color_, freq, avg, flag);
+  size_t tb = 0;
+  CK(cub::DeviceSelect::Flagged(nullptr, tb, thrust::counting_iterator<int32_t>(0), flag, cand,
+                                ncand, nv, s_));
+  char *temp;
+  TRY(alloc(&temp, (int64_t)tb));
+  CK(cub::DeviceSelect::Flagged(temp, tb, thrust::counting_iterator<int32_t>(0), flag, cand,
+                                ncand, nv, s_));
+  LAUNCH(k_vbase, 1, kVbaseThreads, 0, s_, L.ptr, L.tail, color_, cand, ncand, freq, ncolors,
+         avg, type, dmoves);
+  unsigned long long hm = 0;
+  CK(cudaMemcpyAsync(&hm, dmoves, sizeof(hm), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  dfree(temp);
+  dfree(freq);
+  dfree(flag);
+  dfree(cand);
+  dfree(ncand);
+  dfree(dmoves);
+  if (moves) *moves = (long)hm;
   return GLV_OK;
 }
 
@@ -2422,8 +2471,7 @@ int glv_run_multiphase_coloring(const glv_graph *G, long *C_orig, int coloring, 
                                 int replaceMap, long minGraphSize, double threshold,
                                 double C_threshold, int mode, glv_run_stats *stats) {
   if (!G) return fail(GLV_ERR_ARG, "G is NULL");
-  if (coloring != 1 && coloring != 3)
-    return fail(GLV_ERR_UNSUPPORTED, "only coloring = 1 and 3 are implemented");
+  if (coloring < 1 || coloring > 3) return fail(GLV_ERR_ARG, "coloring must be 1, 2 or 3");
   if (coloring == 3 && 4L * std::max(1, numColors / 4) + 1 >= kMaxColors)
     return fail(GLV_ERR_COLORS, "numColors reaches the colour cap");
   if (replaceMap != 0) return fail(GLV_ERR_UNSUPPORTED, "replaceMap = 1 is not implemented");
@@ -2711,6 +2759,32 @@ int glv_color_multihash(const glv_graph *G, int *vtxColor, int nHash, int nItrs,
   CK(cudaStreamSynchronize(c.s));
   if (maxColor) *maxColor = nc - 1;
   if (totTime) *totTime = secs;
+  return GLV_OK;
+}
+
+int glv_vbase_redistribution(const glv_graph *G, int *vtxColor, int ncolors, int type,
+                             long *moves) {
+  if (!G || (!vtxColor && G->numVertices > 0)) return fail(GLV_ERR_ARG, "NULL argument");
+  if (type != 0 && type != 1) return fail(GLV_ERR_ARG, "type must be 0 or 1");
+  if (ncolors <= 0 && G->numVertices > 0) return fail(GLV_ERR_ARG, "ncolors must be positive");
+  if (ncolors > kMaxColors) return fail(GLV_ERR_COLORS, "more colours than the 4096 cap");
+  for (long v = 0; v < G->numVertices; ++v)
+    if (vtxColor[v] < 0 || vtxColor[v] >= ncolors)
+      return fail(GLV_ERR_ARG, "a colour outside [0, ncolors)");
+  Call c;
+  TRY(open_call(c, GLV_MODE_VERIFY, G->numVertices, G->edgeListPtrs, G->edgeList, nullptr,
+                nullptr));
+  const long nv = G->numVertices;
+  if (nv > 0) {
+    CK(cudaMemcpyAsync(c.eng->color_, vtxColor, nv * sizeof(int32_t), cudaMemcpyHostToDevice,
+                       c.s));
+    TRY(c.eng->vbase(c.L0, ncolors, type, moves));
+    CK(cudaMemcpyAsync(vtxColor, c.eng->color_, nv * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                       c.s));
+    CK(cudaStreamSynchronize(c.s));
+  } else if (moves) {
+    *moves = 0;
+  }
   return GLV_OK;
 }
 

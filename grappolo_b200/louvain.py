@@ -123,6 +123,16 @@ def algoDistanceOneVertexColoringOpt(G, nThreads=1):
     return col, mc.value, tt.value
 
 
+def vBaseRedistribution(G, vtxColor, ncolors, type=0):
+    """Coloring/vBase.cpp:6 — returns (rebalanced colours int32[NV], vertices moved)."""
+    G = _as_graph(G)
+    col = np.array(vtxColor, dtype=np.int32, copy=True)
+    n = ct.c_long(0)
+    _lib.check(_lib.lib().glv_vbase_redistribution(
+        ct.byref(G.struct), col.ctypes.data_as(_P(ct.c_int)), ncolors, type, ct.byref(n)))
+    return col, n.value
+
+
 def algoColoringMultiHashMaxMin(G, nThreads=1, nHash=2, nItrs=4):
     """Coloring/coloringMultiHashMaxMin.cpp:59 — returns (vtxColor int32[NV],
     maxColor, totTime).  Random values come from the C library's rand()."""

@@ -40,7 +40,7 @@ enum {
   GLV_ERR_OOM = 3,        /* device or host allocation failed */
   GLV_ERR_COLORS = 4,     /* a colouring needed >= 4096 colours (coloringUtils.cpp:57-60) */
   GLV_ERR_TOO_LARGE = 5,  /* numVertices >= 2^31 (ids are int32 on the device) */
-  GLV_ERR_UNSUPPORTED = 6,/* option outside this engine's scope (e.g. coloring 2, replaceMap) */
+  GLV_ERR_UNSUPPORTED = 6,/* option outside this engine's scope (e.g. replaceMap = 1) */
   GLV_ERR_NO_DEVICE = 7,  /* no CUDA device */
   GLV_ERR_LIMIT = 8,      /* a size exceeds a fixed limit of the entry point */
   GLV_ERR_IO = 9          /* a graph file could not be opened, read or written */
@@ -209,8 +209,9 @@ int glv_gini_coefficient(long *colorSize, int numColors, double *gini);
  * (Coloring/coloringMultiHashMaxMin.cpp:59-228) with two hashes and
  * max(1, numColors / 4) iterations, its random values drawn from the C
  * library's rand() exactly as the reference draws them (seed with srand() to
- * reproduce a reference run).  coloring = 2 (vBase balancing) is
- * GLV_ERR_UNSUPPORTED; replaceMap must be 0.  C_orig[numVertices] receives the
+ * reproduce a reference run).  coloring = 2 applies glv_vbase_redistribution
+ * (type 0) after each distance-1 colouring; other values are GLV_ERR_ARG.
+ * replaceMap must be 0.  C_orig[numVertices] receives the
  * final community of every input vertex (-1 for isolated vertices).  Unlike the
  * reference, G is not freed.  `stats` may be NULL. */
 int glv_run_multiphase_coloring(const glv_graph *G, long *C_orig, int coloring, int numColors,
@@ -311,6 +312,17 @@ int glv_louvain_basic_phase(const glv_graph *G, long *C, double Lower, double th
  * return value). */
 int glv_distance_one_coloring(const glv_graph *G, int *vtxColor, int mode, int *maxColor,
                               double *totTime);
+
+/* Replaces vBaseRedistribution (Coloring/vBase.cpp:6-168, coloring.h:15):
+ * rebalances a proper colouring with ncolors colours in place.  Classes above
+ * avg = ceil(NV / ncolors) give vertices, in vertex order, to colours below
+ * avg that were not above it and that no neighbour has: the first such
+ * colour (type 0) or the least used (type 1).  The result stays proper.
+ * Where no colour qualifies the vertex keeps its colour (the reference's
+ * type 0 reads past its frequency array there).  *moves (may be NULL)
+ * receives the number of vertices recoloured (the reference returns nothing). */
+int glv_vbase_redistribution(const glv_graph *G, int *vtxColor, int ncolors, int type,
+                             long *moves);
 
 /* Replaces algoColoringMultiHashMaxMin (Coloring/coloringMultiHashMaxMin.cpp:59-228,
  * coloring.h:12): the incomplete colouring with nHash hashes and nItrs

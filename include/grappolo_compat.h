@@ -47,6 +47,8 @@ double parallelLouvianMethod(graph *G, long *C, int nThreads, double Lower, doub
                              double *totTime, int *numItr);
 /* DefineStructure/coloring.h:8 */
 int algoDistanceOneVertexColoringOpt(graph *G, int *vtxColor, int nThreads, double *totTime);
+/* DefineStructure/coloring.h:15 (Coloring/vBase.cpp); returns the vertices moved */
+int vBaseRedistribution(graph *G, int *vtxColor, int ncolors, int type);
 /* DefineStructure/coloring.h:12 (Coloring/coloringMultiHashMaxMin.cpp) */
 int algoColoringMultiHashMaxMin(graph *G, int *vtxColor, int nThreads, double *totTime, int nHash,
                                 int nItrs);

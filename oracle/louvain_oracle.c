@@ -18,6 +18,7 @@
  * reference's evaluation order and the file is compiled with
  * -ffp-contract=off so no FMA contraction changes a rounding.
  */
+#include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
@@ -251,6 +252,58 @@ int lvo_color_mhash(long nv, const long *ptr, const long *tail, int nHash, int n
     }
     free(rnd);
     return maxColor;
+}
+
+/* vBaseRedistribution (Coloring/vBase.cpp:6-168) at one thread; type 0 takes
+ * the first qualifying colour, type 1 the least used (lowest on ties).  avg = ceil(NV / ncolors); a class is oversized when it holds more
+ * than avg vertices (:78-90).  In vertex order, a vertex of an oversized class
+ * whose class still holds more than avg moves to the smallest colour that no
+ * neighbour has, that holds fewer than avg and that was not oversized
+ * (:94-134).  When no colour below ncolors qualifies, type 0 in the reference
+ * reads one entry past its frequency arrays (:113-116); here the vertex stays
+ * (what type 1 does, and what the reference's checks of myColor != ncolors
+ * at :128-130 expect), and
+ * *stuck (may be NULL) counts those vertices.  Moves are sequential, so the
+ * colouring stays proper and the conflict pass (:137-141) finds nothing.
+ * Returns the number of moves.                                              */
+long lvo_vbase(long nv, const long *ptr, const long *tail, int *color, int ncolors, int type,
+               long *stuck) {
+    long *freq = (long *)calloc(ncolors + 1, sizeof(long));
+    unsigned char *over = (unsigned char *)calloc(ncolors + 1, 1);
+    unsigned char *mark = (unsigned char *)calloc(ncolors + 1, 1);
+    long *base = (long *)malloc(sizeof(long) * (nv ? nv : 1));
+    for (long v = 0; v < nv; v++) { base[v] = color[v]; freq[color[v]]++; }
+    long avg = (long)ceil((double)nv / (double)ncolors);
+    for (int c = 0; c < ncolors; c++) over[c] = freq[c] > avg;
+    long moves = 0;
+    for (long v = 0; v < nv; v++) {
+        if (!over[base[v]]) continue;
+        if (color[v] != -1 && freq[color[v]] <= avg) continue;
+        for (long k = ptr[v]; k < ptr[v + 1]; k++) {
+            long u = tail[k];
+            if (u != v && color[u] >= 0 && color[u] < ncolors) mark[color[u]] = 1;
+        }
+        int my = -1;
+        for (int c = 0; c < ncolors; c++) {
+            if (mark[c] || freq[c] >= avg || over[c]) continue;
+            if (type == 0) { my = c; break; }                /* first fit (:112-117) */
+            if (my == -1 || freq[my] > freq[c]) my = c;       /* least used (:118-126) */
+        }
+        for (long k = ptr[v]; k < ptr[v + 1]; k++) {
+            long u = tail[k];
+            if (u != v && color[u] >= 0 && color[u] < ncolors) mark[color[u]] = 0;
+        }
+        if (my >= 0) {
+            freq[my]++;
+            freq[color[v]]--;
+            color[v] = my;
+            moves++;
+        } else if (stuck) {
+            (*stuck)++;
+        }
+    }
+    free(freq); free(over); free(mark); free(base);
+    return moves;
 }
 
 /* Modularity pieces shared by both sweeps: Q = e_xx*c - a2_x*c*c
@@ -824,8 +877,9 @@ static void free_graph(long *ptr, long *tail, double *w, int owned) {
     if (owned) { free(ptr); free(tail); free(w); }
 }
 
-/* Coloring/runMultiPhaseColoring.cpp:51-238 at one thread, coloring = 1 or 3
- * (3: lvo_color_mhash with two hashes and max(1, numColors / 4) iterations,
+/* Coloring/runMultiPhaseColoring.cpp:51-238 at one thread, coloring = 1, 2
+ * or 3 (2: lvo_vbase after the distance-1 colouring, :67-73, :180-186;
+ * 3: lvo_color_mhash with two hashes and max(1, numColors / 4) iterations,
  * :76-86, :187-196).
  * Later phases recolour only when NV > minGraphSize and still colouring
  * (:173); otherwise the first NV entries of the previous colouring are reused
@@ -840,7 +894,10 @@ static int color_for(int coloring, int numColors, long nv, const long *ptr, cons
         return lvo_color_mhash(nv, ptr, tail, 2, nItrs, colors);
     }
     for (long i = 0; i < nv; i++) colors[i] = -1;
-    return lvo_color_greedy(nv, ptr, tail, colors);
+    int mc = lvo_color_greedy(nv, ptr, tail, colors);
+    /* coloring = 2 balances the colouring (runMultiPhaseColoring.cpp:67-73) */
+    if (coloring == 2 && mc >= 0) lvo_vbase(nv, ptr, tail, colors, mc + 1, 0, NULL);
+    return mc;
 }
 
 int lvo_run_multiphase_coloring(long nv, const long *ptr0, const long *tail0,

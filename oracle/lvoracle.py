@@ -76,6 +76,7 @@ class COracle:
         L.lvo_vertex_degrees.restype = ct.c_double
         L.lvo_color_greedy.restype = ct.c_int
         L.lvo_color_mhash.restype = ct.c_int
+        L.lvo_vbase.restype = ct.c_long
         L.lvo_gini.restype = ct.c_double
         L.lvo_compare_communities.restype = ct.c_int
         L.lvo_remove_edges.restype = ct.c_long
@@ -211,6 +212,16 @@ class COracle:
     def gini(self, sizes):
         s = np.array(sizes, dtype=np.int64)
         return self.L.lvo_gini(_lp(s), ct.c_int(len(s))), s
+
+    def vbase(self, g, color, ncolors, vtype=0):
+        """vBaseRedistribution on a copy: (colours, moves, vertices for which
+        no colour qualified -- where type 0 of the reference is undefined)."""
+        p, t, _ = _csr(g)
+        col = np.array(color, dtype=np.int32)
+        stuck = ct.c_long(0)
+        n = self.L.lvo_vbase(ct.c_long(g.num_vertices), _lp(p), _lp(t), _ip(col),
+                             ct.c_int(ncolors), ct.c_int(vtype), ct.byref(stuck))
+        return col, n, stuck.value
 
     def decide_batch(self, g, C, vdeg, cdeg, csize, constant, verts):
         p, t, w = _csr(g)

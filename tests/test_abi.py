@@ -55,6 +55,7 @@ REFERENCE_SYMBOLS = [
     '_Z25writeGraphBinaryFormatNewP5graphPcl',
     '_Z27computeCommunityComparisonsRSt6vectorIlSaIlEElS2_l',
     '_Z22computeGiniCoefficientPli',
+    '_Z19vBaseRedistributionP5graphPiii',
 ]
 
 
@@ -87,7 +88,8 @@ def test_compat_header_matches_reference_mangling(tmp_path):
                    '  writeGraphBinaryFormatNew(g, (char *)"f", 1);\n'
                    '  std::vector<long> v1, v2;\n'
                    '  computeCommunityComparisons(v1, 0, v2, 0);\n'
-                   '  computeGiniCoefficient(c, 4);\n}\n')
+                   '  computeGiniCoefficient(c, 4);\n'
+                   '  vBaseRedistribution(g, col, 4, 0);\n}\n')
     obj = tmp_path / 'use.o'
     subprocess.run(['g++', '-c', '-I', os.path.join(ROOT, 'include'), str(src), '-o', str(obj)],
                    check=True)

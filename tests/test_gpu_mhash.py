@@ -76,5 +76,5 @@ def test_multihash_rejects_bad_arguments():
         louvain.algoColoringMultiHashMaxMin(g, nHash=2, nItrs=1024)
     assert e.value.code == 4  # GLV_ERR_COLORS
     with pytest.raises(_lib.GrappoloError) as e:
-        louvain.runMultiPhaseColoring(g, coloring=2)
-    assert e.value.code == 6  # GLV_ERR_UNSUPPORTED
+        louvain.runMultiPhaseColoring(g, coloring=4)
+    assert e.value.code == 1  # GLV_ERR_ARG

@@ -1,0 +1,61 @@
+"""The oracle's balanced recolouring (vBaseRedistribution, Coloring/vBase.cpp)
+against a second, pure-Python restatement of the same rule, and its
+invariants.  The reference's own function cannot serve as the checker here:
+it is declared int but returns nothing (the call traps when built by g++),
+and its first-fit scan reads past its frequency array when no colour
+qualifies, after which it need not terminate."""
+import math
+
+import numpy as np
+import pytest
+
+from grappolo_b200 import graphs
+
+
+def vbase_py(g, color, ncolors, vtype):
+    col = [int(c) for c in color]
+    freq = [0] * ncolors
+    for c in col:
+        freq[c] += 1
+    avg = math.ceil(g.num_vertices / ncolors)
+    over = [f > avg for f in freq]
+    base = list(col)
+    for v in range(g.num_vertices):
+        if not over[base[v]] or freq[col[v]] <= avg:
+            continue
+        used = {col[u] for u in g.tail[g.ptr[v]:g.ptr[v + 1]] if u != v}
+        ok = [c for c in range(ncolors) if c not in used and freq[c] < avg and not over[c]]
+        if not ok:
+            continue
+        my = ok[0] if vtype == 0 else min(ok, key=lambda c: (freq[c], c))
+        freq[my] += 1
+        freq[col[v]] -= 1
+        col[v] = my
+    return np.array(col, dtype=np.int32)
+
+
+def _graphs():
+    yield 'pp1000', graphs.planted_partition(num_blocks=20, block_size=50, intra_degree=10,
+                                             inter_degree=3, seed=2)
+    yield 'rmat10', graphs.rmat(10, seed=4)
+    yield 'mixed', graphs.planted_partition_mixed(3000, 30, 0.4, 6.0, seed=9)
+    yield 'star', graphs.from_edges(60, [(0, i) for i in range(1, 60)] + [(1, 2), (3, 4)])
+
+
+@pytest.mark.parametrize('name,g', list(_graphs()))
+@pytest.mark.parametrize('vtype', [0, 1])
+def test_vbase_oracle(oracle, name, g, vtype):
+    col, mc = oracle.color_greedy(g)
+    nc = mc + 1
+    out, moves, stuck = oracle.vbase(g, col, nc, vtype)
+    assert np.array_equal(out, vbase_py(g, col, nc, vtype))
+    heads = g.heads()
+    off = heads != g.tail
+    assert not np.any(out[heads[off]] == out[g.tail[off]])  # still proper
+    avg = math.ceil(g.num_vertices / nc)
+    f0 = np.bincount(col, minlength=nc)
+    f1 = np.bincount(out, minlength=nc)
+    moved = out != col
+    assert moves == int(moved.sum())
+    assert np.all(f0[col[moved]] > avg) and np.all(f0[out[moved]] < avg)
+    assert np.all(f1[f0 < avg] <= avg)
