@@ -490,7 +490,7 @@ static int upload_edges(cudaStream_t s, const glv_edge *host, int64_t n, DevScra
 static int open_stream(Call &c) {
   TRY(device_ready());
   if (!engine_pool()) return fail(GLV_ERR_CUDA, "could not create the device memory pool");
-  CK(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
+  CK(engine_stream(&c.s));
   return GLV_OK;
 }
 

@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include <mutex>
@@ -53,6 +54,57 @@ static cudaMemPool_t engine_pool() {
   }
   return g_pool[dev];
 }
+// One internal stream per device, created once.  Creating and destroying a
+// stream per call made the first pool allocation of the next call wait
+// (0.1-0.9 s) while the pool settled the blocks freed on the destroyed
+// stream.  Calls from several host threads on one device share the stream,
+// so their work is serialised (each call still waits only for its own
+// results).
+static std::mutex g_stream_mu;
+static cudaStream_t g_stream[128];
+static cudaError_t engine_stream(cudaStream_t *s) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= 128) return cudaErrorInvalidDevice;
+  std::lock_guard<std::mutex> lock(g_stream_mu);
+  if (!g_stream[dev]) {
+    e = cudaStreamCreateWithFlags(&g_stream[dev], cudaStreamNonBlocking);
+    if (e != cudaSuccess) return e;
+  }
+  *s = g_stream[dev];
+  return cudaSuccess;
+}
+
+// Blocks the engine freed, kept by device and size class and handed to later
+// allocations of the same class.  All engine work on a device runs on its one
+// internal stream, so a block reused here is ordered after its last use.  In
+// steady state (the same call repeated) no allocation reaches the driver: a
+// pool allocation after a call's frees sometimes waited 0.1-0.9 s.  A failed
+// pool allocation first returns the cached blocks; glv_release_cached_memory
+// returns them too.
+struct BlockCache {
+  std::mutex mu;
+  std::unordered_map<size_t, std::vector<void *>> free;
+  std::unordered_map<void *, size_t> live;
+};
+static BlockCache g_cache[128];
+
+static int current_device() {
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= 128) d = 0;
+  return d;
+}
+
+static void flush_block_cache(int dev, cudaStream_t s) {
+  if (dev < 0 || dev >= 128) return;
+  BlockCache &bc = g_cache[dev];
+  std::lock_guard<std::mutex> lock(bc.mu);
+  for (auto &kv : bc.free)
+    for (void *q : kv.second) cudaFreeAsync(q, s);
+  bc.free.clear();
+}
+
 static std::atomic<int> g_profile{0};  // 0 off, 1 per-class sweep, 2 per launch
 
 // Learned gate (process-wide): parameters and keep threshold.
@@ -251,6 +303,8 @@ class Engine {
   int32_t *cSize = nullptr, *dSize = nullptr;
   int32_t *C = nullptr, *Cpast = nullptr, *Ctgt = nullptr;
   int32_t *color_ = nullptr;
+  const bool debug_ = getenv("GRAPPOLO_B200_DEBUG") != nullptr;
+  int dev_ = current_device();
   double *cst = nullptr;  // {constant, 2m}
   long launches_ = 0;
   bool integral = false;
@@ -270,7 +324,7 @@ class Engine {
   bool learned() const { return mode_ == GLV_MODE_LEARNED; }
   int gate_init();
 
- private:
+ public:  // the allocator (the C ABI helpers allocate level-0 arrays through it)
   // Requests above 1 MiB are rounded up to quarter-octave size classes so that
   // repeated runs, whose level sizes differ slightly, reuse the pool's blocks.
   static size_t size_class(size_t bytes) {
@@ -290,20 +344,51 @@ class Engine {
               n * sizeof(T) * 1e-9, used * 1e-9);
     }
     const size_t bytes = size_class(std::max<size_t>(n, 1) * sizeof(T));
+    BlockCache &bc = g_cache[dev_];
+    {
+      std::lock_guard<std::mutex> lock(bc.mu);
+      auto it = bc.free.find(bytes);
+      if (it != bc.free.end() && !it->second.empty()) {
+        *p = static_cast<T *>(it->second.back());
+        it->second.pop_back();
+        bc.live[(void *)*p] = bytes;
+        return GLV_OK;
+      }
+    }
+    const double ta = debug_ ? now_s() : 0.0;
     cudaError_t e = cudaMallocFromPoolAsync((void **)p, bytes, pool_, s_);
     if (e == cudaErrorMemoryAllocation) {
-      // the pool keeps freed blocks; hand the unused ones back and retry once
+      // return the cached blocks and the pool's unused memory, retry once
       cudaGetLastError();
+      flush_block_cache(dev_, s_);
       cudaStreamSynchronize(s_);
       cudaMemPoolTrimTo(pool_, 0);
+      if (debug_) fprintf(stderr, "grappolo_b200: pool trimmed after a failed allocation\n");
       e = cudaMallocFromPoolAsync((void **)p, bytes, pool_, s_);
     }
+    if (debug_ && now_s() - ta > 2e-3)
+      fprintf(stderr, "grappolo_b200: slow allocation of %.3f GB: %.4f s\n", bytes * 1e-9,
+              now_s() - ta);
     CK(e);
+    std::lock_guard<std::mutex> lock(bc.mu);
+    bc.live[(void *)*p] = bytes;
     return GLV_OK;
   }
   template <class T>
   void dfree(T *&p) {
-    if (p) cudaFreeAsync(p, s_);
+    if (!p) return;
+    BlockCache &bc = g_cache[dev_];
+    {
+      std::lock_guard<std::mutex> lock(bc.mu);
+      auto it = bc.live.find((void *)p);
+      if (it != bc.live.end()) {
+        bc.free[it->second].push_back((void *)p);
+        bc.live.erase(it);
+        p = nullptr;
+        return;
+      }
+    }
+    cudaFreeAsync(p, s_);
     p = nullptr;
   }
   int temp(size_t bytes) {
@@ -680,30 +765,33 @@ int Engine::color_spec(const Level &L, int *ncolors) {
   const uint32_t seed = 0x5bd1e995u;
   LAUNCH(k_spec_init, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, L.ptr, L.tail,
          kSpecBlockDeg, color_, wl, cnt, bl, cnt + 1);
-  int32_t h[3];
-  CK(cudaMemcpyAsync(h, cnt, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
-  CK(cudaStreamSynchronize(s_));
+  // Rounds run in groups without a host read: the kernels take the list
+  // lengths from device counters, and a round after the last conflict is a
+  // set of empty launches.  The host reads the counters once per group.
+  constexpr int kSpecGroup = 8;
+  const int gw = nsm_ * 16, gb = nsm_ * 4;
   int rounds = 0;
-  while (h[0] + h[1] > 0) {
-    if (++rounds > 100000) return fail(GLV_ERR_CUDA, "speculative colouring did not settle");
-    const int64_t nw = h[0], nb = h[1];
-    if (nw) LAUNCH(k_spec_assign_warp, grid_for(nw * 32, 256, nsm_ * 16), 256, 0, s_, nw, wl,
-                   L.ptr, L.tail, color_, status);
-    if (nb) LAUNCH(k_spec_assign_block, (int)std::min<int64_t>(nb, nsm_ * 4), 512, 0, s_, nb, bl,
-                   L.ptr, L.tail, color_, status);
-    CK(cudaMemsetAsync(cnt + 2, 0, sizeof(int32_t), s_));
-    if (nw) LAUNCH(k_spec_conflicts, grid_for(nw * 32, 256, nsm_ * 16), 256, 0, s_, nw, wl,
-                   L.ptr, L.tail, seed, color_, nx, cnt + 2);
-    if (nb) LAUNCH(k_spec_conflicts_block, (int)std::min<int64_t>(nb, nsm_ * 4), 512, 0, s_, nb,
-                   bl, L.ptr, L.tail, seed, color_, nx, cnt + 2);
-    CK(cudaMemcpyAsync(&h[2], cnt + 2, sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
-    CK(cudaStreamSynchronize(s_));
-    if (h[2] == 0) break;
-    CK(cudaMemsetAsync(cnt, 0, 2 * sizeof(int32_t), s_));
-    LAUNCH(k_spec_split, grid_for(h[2], 256, nsm_ * 16), 256, 0, s_, (int64_t)h[2], nx, L.ptr,
-           kSpecBlockDeg, wl, cnt, bl, cnt + 1);
+  while (true) {
+    for (int r = 0; r < kSpecGroup; ++r, ++rounds) {
+      LAUNCH(k_spec_assign_warp, gw, 256, 0, s_, cnt, wl, L.ptr, L.tail, color_, status);
+      LAUNCH(k_spec_assign_block, gb, 512, 0, s_, cnt + 1, bl, L.ptr, L.tail, color_, status);
+      CK(cudaMemsetAsync(cnt + 2, 0, sizeof(int32_t), s_));
+      LAUNCH(k_spec_conflicts, gw, 256, 0, s_, cnt, wl, L.ptr, L.tail, seed, color_, nx, cnt + 2);
+      LAUNCH(k_spec_conflicts_block, gb, 512, 0, s_, cnt + 1, bl, L.ptr, L.tail, seed, color_,
+             nx, cnt + 2);
+      CK(cudaMemsetAsync(cnt, 0, 2 * sizeof(int32_t), s_));
+      LAUNCH(k_spec_split, gw, 256, 0, s_, cnt + 2, nx, L.ptr, kSpecBlockDeg, wl, cnt, bl,
+             cnt + 1);
+    }
+    int32_t h[2];
+    const double tw = debug_ ? now_s() : 0.0;
     CK(cudaMemcpyAsync(h, cnt, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
     CK(cudaStreamSynchronize(s_));
+    if (debug_)
+      fprintf(stderr, "grappolo_b200: spec rounds %d: wait %.4f s, lists %d + %d\n", rounds,
+              now_s() - tw, h[0], h[1]);
+    if (h[0] + h[1] == 0) break;
+    if (rounds > 100000) return fail(GLV_ERR_CUDA, "speculative colouring did not settle");
   }
   if (getenv("GRAPPOLO_B200_DEBUG"))
     fprintf(stderr, "grappolo_b200: speculative colouring nv=%ld rounds=%d\n", (long)L.nv, rounds);
@@ -2294,10 +2382,7 @@ struct Call {
       g_launches += eng->launches_;
       delete eng;
     }
-    if (s) {
-      cudaStreamSynchronize(s);
-      cudaStreamDestroy(s);
-    }
+    if (s) cudaStreamSynchronize(s);  // the stream is the device's, kept for the next call
   }
 };
 
@@ -2336,7 +2421,7 @@ static int open_call(Call &c, int mode, long nv, const long *ptr, const glv_edge
   if (mode < GLV_MODE_VERIFY || mode > GLV_MODE_LEARNED) return fail(GLV_ERR_ARG, "bad mode");
   const int64_t nnz = ptr[nv];
   if (nnz > 0 && !edges && !(tail64 && w)) return fail(GLV_ERR_ARG, "edge arrays are NULL");
-  CK(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
+  CK(engine_stream(&c.s));
   c.eng = new Engine(c.s, mode);
   TRY(c.eng->init(nv, nnz));
   const double t0 = now_s();
@@ -2344,13 +2429,10 @@ static int open_call(Call &c, int mode, long nv, const long *ptr, const glv_edge
   L.nv = nv;
   L.nnz = nnz;
   L.owned = true;
-  cudaMemPool_t pool = engine_pool();
-  if (!pool) return fail(GLV_ERR_CUDA, "could not create the device memory pool");
-  CK(cudaMallocFromPoolAsync((void **)&L.ptr, (nv + 1) * sizeof(int64_t), pool, c.s));
-  CK(cudaMallocFromPoolAsync((void **)&L.tail, std::max<int64_t>(nnz, 1) * sizeof(int32_t), pool,
-                             c.s));
-  CK(cudaMallocFromPoolAsync((void **)&L.w, std::max<int64_t>(nnz, 1) * sizeof(double), pool,
-                             c.s));
+  // through the engine's allocator: its block cache serves repeated calls
+  TRY(c.eng->alloc(&L.ptr, nv + 1));
+  TRY(c.eng->alloc(&L.tail, std::max<int64_t>(nnz, 1)));
+  TRY(c.eng->alloc(&L.w, std::max<int64_t>(nnz, 1)));
   CK(cudaMemcpyAsync(L.ptr, ptr, (nv + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c.s));
   // Edges move in chunks through one device staging buffer.
   const int64_t chunk = std::min<int64_t>(std::max<int64_t>(nnz, 1), 1 << 24);
@@ -2358,7 +2440,7 @@ static int open_call(Call &c, int mode, long nv, const long *ptr, const glv_edge
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, 0);
   if (edges) {
     glv_edge *stage;
-    CK(cudaMallocFromPoolAsync((void **)&stage, chunk * sizeof(glv_edge), engine_pool(), c.s));
+    TRY(c.eng->alloc(&stage, chunk));
     for (int64_t b = 0; b < nnz; b += chunk) {
       const int64_t n = std::min(chunk, nnz - b);
       CK(cudaMemcpyAsync(stage, edges + b, n * sizeof(glv_edge), cudaMemcpyHostToDevice, c.s));
@@ -2366,12 +2448,12 @@ static int open_call(Call &c, int mode, long nv, const long *ptr, const glv_edge
       ++c.launches;
       CK(cudaGetLastError());
     }
-    CK(cudaFreeAsync(stage, c.s));
+    c.eng->dfree(stage);
   } else if (nnz > 0) {
     int64_t *stage;
     int32_t *bad;
-    CK(cudaMallocFromPoolAsync((void **)&stage, chunk * sizeof(int64_t), engine_pool(), c.s));
-    CK(cudaMallocFromPoolAsync((void **)&bad, sizeof(int32_t), engine_pool(), c.s));
+    TRY(c.eng->alloc(&stage, chunk));
+    TRY(c.eng->alloc(&bad, 1));
     CK(cudaMemsetAsync(bad, 0, sizeof(int32_t), c.s));
     for (int64_t b = 0; b < nnz; b += chunk) {
       const int64_t n = std::min(chunk, nnz - b);
@@ -2381,8 +2463,8 @@ static int open_call(Call &c, int mode, long nv, const long *ptr, const glv_edge
       CK(cudaGetLastError());
     }
     CK(cudaMemcpyAsync(L.w, w, nnz * sizeof(double), cudaMemcpyHostToDevice, c.s));
-    CK(cudaFreeAsync(stage, c.s));
-    CK(cudaFreeAsync(bad, c.s));
+    c.eng->dfree(stage);
+    c.eng->dfree(bad);
   }
   CK(cudaStreamSynchronize(c.s));
   c.t_transfer += now_s() - t0;
@@ -2461,6 +2543,15 @@ const char *glv_version(void) { return "grappolo_b200 0.1 (sm_100a)"; }
 const char *glv_last_error(void) { return g_err.c_str(); }
 long glv_kernel_launch_count(void) { return g_launches.load(); }
 void glv_release_cached_memory(void) {
+  int cur = 0;
+  cudaGetDevice(&cur);
+  for (int d = 0; d < 128; ++d) {
+    if (!g_stream[d]) continue;
+    cudaSetDevice(d);
+    flush_block_cache(d, g_stream[d]);
+    cudaStreamSynchronize(g_stream[d]);
+  }
+  cudaSetDevice(cur);
   std::lock_guard<std::mutex> lock(g_pool_mu);
   for (auto &p : g_pool)
     if (p) cudaMemPoolTrimTo(p, 0);
@@ -2511,7 +2602,7 @@ int glv_dev_run_multiphase(long nv, const long *d_ptr, const int *d_tail, const 
   if (mode < GLV_MODE_VERIFY || mode > GLV_MODE_LEARNED) return fail(GLV_ERR_ARG, "bad mode");
   if (stats) memset(stats, 0, sizeof(*stats));
   Call c;
-  CK(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
+  CK(engine_stream(&c.s));
   if (stream) {
     cudaEvent_t ev;
     CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
@@ -2652,7 +2743,7 @@ int glv_dev_run_batch(int num_graphs, const long *vertex_offsets, const long *d_
   if (nv >= (1L << 31) - 1) return fail(GLV_ERR_TOO_LARGE, "nv >= 2^31");
   if (mode < GLV_MODE_VERIFY || mode > GLV_MODE_FAST) return fail(GLV_ERR_ARG, "bad mode");
   Call c;
-  CK(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
+  CK(engine_stream(&c.s));
   if (stream) {
     cudaEvent_t ev;
     CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
@@ -2793,7 +2884,7 @@ int glv_renumber_clusters(long *C, long size, long *numClusters) {
   if (size >= (1L << 31) - 1) return fail(GLV_ERR_TOO_LARGE, "size >= 2^31");
   TRY(device_ready());
   Call c;
-  CK(cudaStreamCreateWithFlags(&c.s, cudaStreamNonBlocking));
+  CK(engine_stream(&c.s));
   c.eng = new Engine(c.s, GLV_MODE_VERIFY);
   TRY(c.eng->init(size, 0));
   TRY(upload_ids(c, C, size, c.eng->C, size));

@@ -820,10 +820,14 @@ __device__ __forceinline__ int first_free_color(const int64_t *ptr, const int32_
 }
 
 // Warp per vertex (rows below kSpecBlockDeg entries).
-__global__ void __launch_bounds__(256) k_spec_assign_warp(int64_t n, const int32_t *list,
+// List lengths come from device counters, so rounds run back to back without
+// the host reading them.
+__global__ void __launch_bounds__(256) k_spec_assign_warp(const int32_t *count,
+                                                          const int32_t *list,
                                                           const int64_t *ptr, const int32_t *tail,
                                                           int32_t *color, int32_t *status) {
   __shared__ uint32_t bm[8][kMaxColors / 32];
+  const int64_t n = *count;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -845,12 +849,14 @@ __global__ void __launch_bounds__(256) k_spec_assign_warp(int64_t n, const int32
 }
 
 // Block per vertex (hubs).
-__global__ void __launch_bounds__(512) k_spec_assign_block(int64_t n, const int32_t *list,
+__global__ void __launch_bounds__(512) k_spec_assign_block(const int32_t *count,
+                                                           const int32_t *list,
                                                            const int64_t *ptr,
                                                            const int32_t *tail, int32_t *color,
                                                            int32_t *status) {
   __shared__ uint32_t bm[kMaxColors / 32];
   __shared__ int s_min[16];
+  const int64_t n = *count;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   for (int64_t k = blockIdx.x; k < n; k += gridDim.x) {
     const int32_t v = list[k];
@@ -884,11 +890,12 @@ __device__ __forceinline__ bool spec_wins(int32_t u, int32_t v, const int64_t *p
 
 // A vertex that shares its colour with a higher-priority neighbour resets
 // and goes to the next round's list.  Warp per vertex.
-__global__ void __launch_bounds__(256) k_spec_conflicts(int64_t n, const int32_t *list,
+__global__ void __launch_bounds__(256) k_spec_conflicts(const int32_t *count, const int32_t *list,
                                                         const int64_t *ptr, const int32_t *tail,
                                                         uint32_t seed, int32_t *color,
                                                         int32_t *next, int32_t *next_count) {
   const int lane = threadIdx.x & 31;
+  const int64_t n = *count;
   const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t k = wid; k < n; k += nw) {
@@ -907,12 +914,14 @@ __global__ void __launch_bounds__(256) k_spec_conflicts(int64_t n, const int32_t
 }
 
 // Same, one block per vertex (rows of at least kSpecBlockDeg entries).
-__global__ void __launch_bounds__(512) k_spec_conflicts_block(int64_t n, const int32_t *list,
+__global__ void __launch_bounds__(512) k_spec_conflicts_block(const int32_t *count,
+                                                              const int32_t *list,
                                                               const int64_t *ptr,
                                                               const int32_t *tail, uint32_t seed,
                                                               int32_t *color, int32_t *next,
                                                               int32_t *next_count) {
   __shared__ int s_lose;
+  const int64_t n = *count;
   for (int64_t k = blockIdx.x; k < n; k += gridDim.x) {
     const int32_t v = list[k];
     if (threadIdx.x == 0) s_lose = 0;
@@ -950,9 +959,10 @@ __global__ void k_spec_init(int64_t nv, const int64_t *ptr, const int32_t *tail,
 }
 
 // Split a list by degree (next round's lists).
-__global__ void k_spec_split(int64_t n, const int32_t *list, const int64_t *ptr,
+__global__ void k_spec_split(const int32_t *count, const int32_t *list, const int64_t *ptr,
                              int64_t block_deg, int32_t *wl, int32_t *wcount, int32_t *bl,
                              int32_t *bcount) {
+  const int64_t n = *count;
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
        k += (int64_t)gridDim.x * blockDim.x) {
     const int32_t v = list[k];
