@@ -751,7 +751,9 @@ def main():
     steps_timed = sum(s['sweep_steps'] for s in stats)
     roofline = {'bound': 'hbm',
                 'kernel': 'k_sweep_iteration (one Louvain iteration: every colour class and the '
-                          'modularity pass; 32 B per CSR entry + 48 B per vertex)',
+                          'modularity; 32 B per CSR entry + 48 B per vertex with a full '
+                          'modularity pass, 16 B per entry + 44 B per vertex when e_xx is '
+                          'carried from the moves)',
                 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                 'frac': (achieved / peak) if achieved else None, 'peak_kind': peak_kind,
                 'traffic': (ratio * sweep_b / steps_timed) if (ratio and steps_timed) else None,

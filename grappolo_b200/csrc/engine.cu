@@ -1623,6 +1623,15 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
   p.task_ctr = d_ctr;
   p.nnz = L.nnz;
   p.split_row = split_row_;
+  // Fast mode on non-integral weights (no exact result to keep): after the
+  // first sweep of a phase, e_xx is carried from the moves instead of a pass
+  // over every entry.  GRAPPOLO_B200_FULL_MODULARITY=1 keeps the full pass;
+  // GRAPPOLO_B200_CHECK_MODULARITY=1 runs both and fails when they differ.
+  const char *fm = getenv("GRAPPOLO_B200_FULL_MODULARITY");
+  const bool check_exx = getenv("GRAPPOLO_B200_CHECK_MODULARITY") != nullptr;
+  const bool carry_exx =
+      !jacobi && !bt && !ordered() && !integral && !(fm && fm[0] == '1') && L.nnz > 0;
+
   if (bt) {
     p.gid = bt->gid;
     p.gacc = bt->gacc;
@@ -1632,6 +1641,12 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
                                                    kPersistSmem));
   if (per_sm < 1) return fail(GLV_ERR_CUDA, "persistent sweep kernel does not fit on an SM");
   const int grid = per_sm * nsm_;
+  double *exx_buf = nullptr;
+  if (carry_exx) {
+    TRY(alloc(&exx_buf, (size_t)grid + 1));  // carried e_xx, then one slot per block
+    p.a.exx_delta = exx_buf + 1;
+    p.exx_state = exx_buf;
+  }
   void *args[] = {&p};
   const bool debug = getenv("GRAPPOLO_B200_DEBUG") != nullptr;
   uint64_t *d_trace = nullptr;
@@ -1716,6 +1731,7 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
       for (int g = 0; g < bt->G; ++g)
         if (bt->h_act[g]) batch_edges += (double)bt->gnnz[g];
     }
+    p.exx_mode = (carry_exx && n >= 2) ? (check_exx ? 2 : 1) : 0;
     cudaError_t e = cudaMemsetAsync(d_ctr, 0, steps.size() * sizeof(int64_t), s_);
     if (e == cudaSuccess) e = cudaMemsetAsync(step_big_, 0, steps.size() * sizeof(int32_t), s_);
     if (e0) cudaEventRecord(e0, s_);
@@ -1724,10 +1740,20 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
                                       kPersistSmem, s_);
     if (e1) cudaEventRecord(e1, s_);
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(h_mod_, mod_out_, 3 * sizeof(double), cudaMemcpyDeviceToHost, s_);
+      e = cudaMemcpyAsync(h_mod_, mod_out_, 4 * sizeof(double), cudaMemcpyDeviceToHost, s_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s_);
     t_sweep += now_s() - t0;
     if (e != cudaSuccess) { g_err = cudaGetErrorString(e); rc = GLV_ERR_CUDA; break; }
+    if (p.exx_mode == 2) {
+      const double carried = h_mod_[1], full = h_mod_[3];
+      if (debug)
+        fprintf(stderr, "grappolo_b200: e_xx carried %.17g full %.17g (rel %.3g)\n", carried,
+                full, fabs(carried - full) / std::max(1.0, fabs(full)));
+      if (!(fabs(carried - full) <= 1e-9 * std::max(1.0, fabs(full)))) {
+        rc = fail(GLV_ERR_CUDA, "carried e_xx differs from the full pass");
+        break;
+      }
+    }
     ++launches_;
     if (bt) {
       edges_swept += batch_edges;
@@ -1748,7 +1774,10 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
     if (e0) {
       float ms = 0;
       if (cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) sweep_kernel_s += ms * 1e-3;
-      sweep_bytes += 32.0 * (double)L.nnz + 48.0 * (double)L.nv;
+      // sweep: 16 B per entry + 36 B per vertex; modularity: a full pass 16 B
+      // per entry + 12 B per vertex, a carried e_xx 8 B per vertex (cDeg)
+      sweep_bytes += (p.exx_mode == 1) ? 16.0 * (double)L.nnz + 44.0 * (double)L.nv
+                                       : 32.0 * (double)L.nnz + 48.0 * (double)L.nv;
       ++sweep_steps;
     }
     if (debug) {
@@ -1838,6 +1867,7 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
   dfree(d_ctr);
   dfree(d_cls_b);
   dfree(d_kept);
+  dfree(exx_buf);
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
   dfree(d_steps);

@@ -54,6 +54,12 @@ struct IterArgs {
   // batches of graphs: per-graph modularity sums instead of one Q
   const int32_t *gid;
   double *gacc;
+  // The internal-weight term e_xx: 0 = a full pass over the level (stored in
+  // exx_state); 1 = exx_state plus this sweep's moves' changes (a.exx_delta),
+  // with only sum cDeg^2 taken in full; 2 = both, Q from the carried value
+  // and the full pass's e_xx in mod_out[3] (a self-check)
+  int exx_mode;
+  double *exx_state;
 };
 
 // Gated or batched sweeps: kept[c] = 1 when some member of colour class c is
@@ -113,16 +119,28 @@ __device__ __forceinline__ void apply_deltas_range(const IterArgs &p, int64_t b,
 
 // Q from the per-block partials (block 0, all threads).
 __device__ __forceinline__ void modularity_fold(const IterArgs &p, int64_t nparts, double *sh) {
-  double e = 0.0, a = 0.0;
+  double e = 0.0, a = 0.0, d = 0.0;
   const int64_t per = (nparts + blockDim.x - 1) / blockDim.x;
   const int64_t b = threadIdx.x * per, en = min(nparts, b + per);
-  for (int64_t i = b; i < en; ++i) { e = __dadd_rn(e, p.part_e[i]); a = __dadd_rn(a, p.part_a[i]); }
+  for (int64_t i = b; i < en; ++i) {
+    e = __dadd_rn(e, p.part_e[i]);
+    a = __dadd_rn(a, p.part_a[i]);
+    if (p.exx_mode == 2) d = __dadd_rn(d, p.a.exx_delta[i]);
+  }
   e = block_sum<kPersistThreads>(e, sh);
   a = block_sum<kPersistThreads>(a, sh);
+  if (p.exx_mode == 2) d = block_sum<kPersistThreads>(d, sh);
   if (threadIdx.x == 0) {
     const double c = p.cst[0];
-    p.mod_out[0] = __dsub_rn(__dmul_rn(e, c), __dmul_rn(__dmul_rn(a, c), c));
-    p.mod_out[1] = e;
+    double exx = e;  // mode 0: the full pass
+    if (p.exx_mode == 1) exx = __dadd_rn(p.exx_state[0], e);  // e holds the moves' changes
+    if (p.exx_mode == 2) {
+      exx = __dadd_rn(p.exx_state[0], d);
+      p.mod_out[3] = e;
+    }
+    if (p.exx_state) p.exx_state[0] = exx;
+    p.mod_out[0] = __dsub_rn(__dmul_rn(exx, c), __dmul_rn(__dmul_rn(a, c), c));
+    p.mod_out[1] = exx;
     p.mod_out[2] = a;
   }
 }
@@ -143,6 +161,8 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
   GLV_TRACE(4 * p.nsteps);
   __shared__ int64_t s_task;
   __shared__ int s_flag;
+  // this block's slot of the moves' e_xx changes (only this block writes it)
+  if (p.a.exx_delta && threadIdx.x == 0) p.a.exx_delta[blockIdx.x] = 0.0;
   for (int s = 0; s < p.nsteps; ++s) {
     const StepDesc &st = p.steps[s];
     // a class the gate emptied is skipped whole (no work, no barrier)
@@ -237,7 +257,11 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
     const int64_t ntiles = merge_tiles(p.nv, p.nnz);
     MergeSmem *msm = reinterpret_cast<MergeSmem *>(smem_raw);
     __syncthreads();  // stage-1 tables in the same shared memory are done
-    if (p.gid) {
+    if (p.exx_mode == 1) {
+      // e_xx is carried: only a2 = sum of cDeg^2 over the level
+      for (int64_t c = gt; c < p.nv; c += ngt) a2 = __dadd_rn(a2, __dmul_rn(p.cDeg[c], p.cDeg[c]));
+      if (threadIdx.x == 0) ex = p.a.exx_delta[blockIdx.x];
+    } else if (p.gid) {
       // contiguous tile ranges, so a thread's running pair changes graph rarely
       GraphAcc acc;
       const int64_t tb = ntiles * blockIdx.x / gridDim.x;

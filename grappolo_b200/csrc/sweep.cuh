@@ -46,6 +46,9 @@ struct SweepArgs {
   // batches of graphs (one level holds many graphs; nullptr = one graph)
   const int32_t *gid;      // per vertex: its graph
   const double *gcst;      // per graph: 1 / (2m) of that graph
+  // per block: sum over the moves of 2 (e_iy - e_ix), the change each move
+  // makes to the modularity's internal-weight term (nullptr = not tracked)
+  double *exx_delta;
 };
 
 __device__ __forceinline__ bool skipped(const SweepArgs &a, int32_t v) {
@@ -82,6 +85,14 @@ __device__ __forceinline__ void emit_decision(const SweepArgs &a, int64_t pos, i
   bool moved = (target != own) && (target != -1);
   a.move_old[pos] = moved ? own : -1;
   a.move_new[pos] = target;
+  if (moved && a.exx_delta) {
+    // the move's gain is t1 - t2 with t1 = 2 (e_iy - e_ix) (louvain_gain):
+    // recover t1 from it and t2, computed as the gain computed it
+    const double ax = __dsub_rn(a.cDeg[own], degree);
+    const double t2 = __dmul_rn(__dmul_rn(__dmul_rn(2.0, degree), __dsub_rn(a.cDeg[target], ax)),
+                                cst_of(a, v));
+    atomicAdd(&a.exx_delta[blockIdx.x], __dadd_rn(best_g, t2));
+  }
   if (moved && a.last_move) a.last_move[v] = a.iter;
   if (moved && a.atomic_deltas) {
     atomicAdd(&a.dDeg[target], degree);
@@ -394,7 +405,7 @@ __device__ __forceinline__ void block_vertex(const SweepArgs &a, int64_t pos, in
   if (threadIdx.x == 0) {
     for (int k = 1; k < nwb; ++k)
       if (better(s_g[k], s_c[k], g, bc)) { g = s_g[k]; bc = s_c[k]; }
-    emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), degree, own_w);
+    emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), degree, own_w, g);
   }
   __syncthreads();
 }

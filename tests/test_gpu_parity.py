@@ -300,3 +300,18 @@ def test_vertex_following(name, g, ref):
     assert ne == int(ref['ne'])
     assert np.array_equal(cg.ptr, ref['cptr']) and np.array_equal(cg.tail, ref['ctail'])
     assert np.array_equal(cg.weight, ref['cweight'])
+
+
+@pytest.mark.parametrize('name', ['pp100k_w', 'rmat16'])
+def test_carried_modularity_matches_full_pass(monkeypatch, oracle, name):
+    """Fast mode on non-integral weights carries the internal-weight term of Q
+    from the moves (2 (e_iy - e_ix) each) instead of a pass over every entry.
+    With GRAPPOLO_B200_CHECK_MODULARITY the engine also runs the full pass each
+    sweep and fails when the two differ by more than 1e-9 (relative)."""
+    monkeypatch.setenv('GRAPPOLO_B200_CHECK_MODULARITY', '1')
+    g = graphs.random_weights(graphs.planted_partition(), seed=8) if name == 'pp100k_w' \
+        else graphs.rmat(16, seed=6)
+    C, st = louvain.runMultiPhaseColoring(g, numThreads=8, stats=True)
+    assert st['total_iterations'] >= 3
+    _, so, _ = oracle.run_multiphase_coloring(g)
+    assert abs(st['final_modularity'] - so['final_mod']) <= FAST_Q_TOL
