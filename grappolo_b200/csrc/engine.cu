@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <map>
 #include <unordered_map>
 #include <vector>
 
@@ -85,10 +86,35 @@ static cudaError_t engine_stream(cudaStream_t *s) {
 // returns them too.
 struct BlockCache {
   std::mutex mu;
-  std::unordered_map<size_t, std::vector<void *>> free;
+  std::map<size_t, std::vector<void *>> free;  // by size class, ascending
   std::unordered_map<void *, size_t> live;
+  std::unordered_map<void *, uint64_t> last_use;  // call generation of the block's last use
+  uint64_t gen = 0;                                // calls finished on this device
 };
 static BlockCache g_cache[128];
+
+// End of a call: blocks the call did not use go back to the pool, so a
+// workload whose sizes change (the waves of a batch) does not hoard memory.
+static void end_call_block_cache(int dev, cudaStream_t s) {
+  if (dev < 0 || dev >= 128) return;
+  BlockCache &bc = g_cache[dev];
+  std::lock_guard<std::mutex> lock(bc.mu);
+  for (auto &kv : bc.free) {
+    auto &v = kv.second;
+    size_t keep = 0;
+    for (size_t i = 0; i < v.size(); ++i) {
+      auto it = bc.last_use.find(v[i]);
+      if (it != bc.last_use.end() && it->second >= bc.gen) {
+        v[keep++] = v[i];
+      } else {
+        if (it != bc.last_use.end()) bc.last_use.erase(it);
+        cudaFreeAsync(v[i], s);
+      }
+    }
+    v.resize(keep);
+  }
+  ++bc.gen;
+}
 
 static int current_device() {
   int d = 0;
@@ -101,7 +127,10 @@ static void flush_block_cache(int dev, cudaStream_t s) {
   BlockCache &bc = g_cache[dev];
   std::lock_guard<std::mutex> lock(bc.mu);
   for (auto &kv : bc.free)
-    for (void *q : kv.second) cudaFreeAsync(q, s);
+    for (void *q : kv.second) {
+      bc.last_use.erase(q);
+      cudaFreeAsync(q, s);
+    }
   bc.free.clear();
 }
 
@@ -346,25 +375,37 @@ class Engine {
     const size_t bytes = size_class(std::max<size_t>(n, 1) * sizeof(T));
     BlockCache &bc = g_cache[dev_];
     {
+      // the smallest cached block of at least this class and at most twice it
+      // (repeated calls whose sizes drift a little, like a batch's waves,
+      // reuse each other's blocks)
       std::lock_guard<std::mutex> lock(bc.mu);
-      auto it = bc.free.find(bytes);
-      if (it != bc.free.end() && !it->second.empty()) {
+      for (auto it = bc.free.lower_bound(bytes); it != bc.free.end() && it->first <= 2 * bytes;
+           ++it) {
+        if (it->second.empty()) continue;
         *p = static_cast<T *>(it->second.back());
         it->second.pop_back();
-        bc.live[(void *)*p] = bytes;
+        bc.live[(void *)*p] = it->first;
+        bc.last_use[(void *)*p] = bc.gen;
         return GLV_OK;
       }
     }
     const double ta = debug_ ? now_s() : 0.0;
     cudaError_t e = cudaMallocFromPoolAsync((void **)p, bytes, pool_, s_);
     if (e == cudaErrorMemoryAllocation) {
-      // return the cached blocks and the pool's unused memory, retry once
+      // hand the cached blocks to the pool and retry; then also return the
+      // pool's unused memory to the device and retry once more
       cudaGetLastError();
       flush_block_cache(dev_, s_);
       cudaStreamSynchronize(s_);
-      cudaMemPoolTrimTo(pool_, 0);
-      if (debug_) fprintf(stderr, "grappolo_b200: pool trimmed after a failed allocation\n");
       e = cudaMallocFromPoolAsync((void **)p, bytes, pool_, s_);
+      if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        cudaMemPoolTrimTo(pool_, 0);
+        if (debug_) fprintf(stderr, "grappolo_b200: pool trimmed after a failed allocation\n");
+        e = cudaMallocFromPoolAsync((void **)p, bytes, pool_, s_);
+      } else if (debug_) {
+        fprintf(stderr, "grappolo_b200: block cache returned after a failed allocation\n");
+      }
     }
     if (debug_ && now_s() - ta > 2e-3)
       fprintf(stderr, "grappolo_b200: slow allocation of %.3f GB: %.4f s\n", bytes * 1e-9,
@@ -372,6 +413,7 @@ class Engine {
     CK(e);
     std::lock_guard<std::mutex> lock(bc.mu);
     bc.live[(void *)*p] = bytes;
+    bc.last_use[(void *)*p] = bc.gen;
     return GLV_OK;
   }
   template <class T>
@@ -2411,6 +2453,7 @@ struct Call {
       launches += eng->launches_;
       g_launches += eng->launches_;
       delete eng;
+      if (s) end_call_block_cache(current_device(), s);
     }
     if (s) cudaStreamSynchronize(s);  // the stream is the device's, kept for the next call
   }
