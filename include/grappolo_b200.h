@@ -381,8 +381,13 @@ int glv_dev_modularity_static(long nv, const long *d_ptr, const int *d_tail,
                               double constant, double *d_out, void *stream);
 
 /* Device memory: the engine allocates from its own stream-ordered pool per
- * device and keeps freed blocks cached for later calls.  This returns the
- * cached blocks to the driver. */
+ * device, keeps the blocks a call frees for the next call (blocks a call does
+ * not reuse go back to the pool when it ends), and runs all its work on one
+ * internal stream per device (calls from several host threads on one device
+ * are serialised).  Between calls the engine therefore still holds up to one
+ * call's peak of device memory.  This returns the cached blocks and the
+ * pool's unused memory to the driver, e.g. before handing the device to
+ * another allocator. */
 void glv_release_cached_memory(void);
 
 /* ---- learned move gate (no counterpart in the reference) ---------------- */
