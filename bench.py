@@ -49,11 +49,16 @@ def parse_args():
     p.add_argument('--no-cpu-baseline', action='store_true')
     p.add_argument('--profile-level', type=int, default=1,
                    help='1: time each class sweep (roofline); 2: time every launch by kind')
-    p.add_argument('--workload', choices=['rmat', 'batch', 'csr', 'compare'], default='rmat',
+    p.add_argument('--workload', choices=['rmat', 'powerlaw', 'batch', 'csr', 'compare'],
+                   default='rmat',
                    help='rmat: one R-MAT graph (default); batch: 4,096 planted-partition '
                         'graphs run as batches; csr: edge list to CSR (removeEdges, both '
                         'directions, rows sorted) of a raw R-MAT edge list; compare: '
                         'community-comparison metrics of two labellings of 2^scale vertices')
+    p.add_argument('--powerlaw-vertices', type=int, default=4_000_000,
+                   help='powerlaw workload: vertices of the planted power-law graph')
+    p.add_argument('--gate-tau', type=float, default=None,
+                   help='learned mode: keep threshold of the move gate (default: the trained one)')
     p.add_argument('--csr-sample-scale', type=int, default=16,
                    help='csr workload: R-MAT scale of the reference\'s CPU sample')
     p.add_argument('--batch-graphs', type=int, default=4096)
@@ -64,6 +69,20 @@ def parse_args():
 
 def workload_config(args, nv, nnz, extra=None):
     kind = 'learned-gated' if args.mode == 'learned' else 'plain'
+    if args.workload == 'powerlaw':
+        cfg = {'workload': f'{kind} multiphase Louvain (coloring=1) on a planted power-law '
+                           f'community graph of {nv} vertices',
+               'graph': f'planted power-law, {nv} vertices, degree exponent 2.5 (mean 20, max '
+                        f'5000), community-size exponent 1.5 (20 to 20000), mu 0.3, unit FP64 '
+                        f'weights, seed 1 (host generator)',
+               'num_vertices': nv, 'nnz': nnz, 'threshold': 1e-6, 'C_threshold': 1e-4,
+               'minGraphSize': 1000, 'parallelism': f'replicas x{args.gpus}',
+               'l2': 'inputs larger than L2 (no flush)'}
+        if args.mode == 'learned':
+            cfg['gate_tau'] = args.gate_tau
+        if extra:
+            cfg.update(extra)
+        return cfg
     gen = ('bounded-scratch device builder, weights from an edge hash' if args.scale >= 26
            else 'device builder')
     cfg = {'workload': f'{kind} multiphase Louvain (coloring=1) on R-MAT scale {args.scale}',
@@ -163,9 +182,13 @@ def run_reference(args, rank):
     from grappolo_b200 import graphs
     from oracle import Reference
     dev = torch.device('cuda:0') if torch.cuda.is_available() else torch.device('cpu')
-    ptr, tail, w = graphs.rmat_device(args.scale, device=dev)
-    g = graphs.CSRGraph(ptr.cpu().numpy(), tail.cpu().numpy().astype(np.int64), w.cpu().numpy())
-    del ptr, tail, w
+    if args.workload == 'powerlaw':
+        g = graphs.planted_powerlaw(args.powerlaw_vertices, seed=1)
+    else:
+        ptr, tail, w = graphs.rmat_device(args.scale, device=dev)
+        g = graphs.CSRGraph(ptr.cpu().numpy(), tail.cpu().numpy().astype(np.int64),
+                            w.cpu().numpy())
+        del ptr, tail, w
     if dev.type == 'cuda':
         torch.cuda.empty_cache()
     cores = os.cpu_count() or 1
@@ -661,9 +684,18 @@ def main():
             'learned': _lib.GLV_MODE_LEARNED}[args.mode]
     if args.mode == 'learned':
         from grappolo_b200 import gate
-        gate.set_gate(*gate.load_default())
+        params, tau = gate.load_default()
+        if args.gate_tau is None:
+            args.gate_tau = tau
+        gate.set_gate(params, args.gate_tau)
 
-    if args.scale >= 26:  # edge lists of tens of GB: the bounded-scratch builder
+    if args.workload == 'powerlaw':
+        g = graphs.planted_powerlaw(args.powerlaw_vertices, seed=1)
+        ptr = torch.from_numpy(g.ptr).to(dev)
+        tail = torch.from_numpy(g.tail.astype(np.int32)).to(dev)
+        w = torch.from_numpy(g.weight).to(dev)
+        del g
+    elif args.scale >= 26:  # edge lists of tens of GB: the bounded-scratch builder
         ptr, tail, w = graphs.rmat_device_lean(args.scale, device=dev)
         torch.cuda.empty_cache()  # hand torch's freed scratch back for the engine's pool
     else:
