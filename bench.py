@@ -743,12 +743,17 @@ def main():
         if args.scale >= 26:  # the engine's cached blocks back to the device for torch
             L.glv_release_cached_memory()
             torch.cuda.empty_cache()
-        heads = torch.repeat_interleave(torch.arange(nv, device=dev, dtype=torch.int64),
-                                        ptr[1:] - ptr[:-1])
+        # the AoS edge records (head, tail, weight) in pinned host memory, built on the
+        # device a chunk of entries at a time (R-MAT 27 holds 101 GB of them)
         aos = torch.empty((nnz, 3), dtype=torch.int64, pin_memory=True)
-        dev_aos = torch.stack([heads, tail.to(torch.int64), w.view(torch.int64)], dim=1)
-        aos.copy_(dev_aos)
-        del dev_aos, heads
+        chunk = 1 << 27
+        for b in range(0, nnz, chunk):
+            e = min(nnz, b + chunk)
+            pos = torch.arange(b, e, device=dev, dtype=torch.int64)
+            heads = torch.searchsorted(ptr, pos, right=True) - 1
+            aos[b:e].copy_(torch.stack([heads, tail[b:e].to(torch.int64),
+                                        w[b:e].view(torch.int64)], dim=1))
+            del pos, heads
         hptr = ptr.cpu().pin_memory()
         hC = torch.empty(nv, dtype=torch.int64, pin_memory=True)
         import ctypes as ct
