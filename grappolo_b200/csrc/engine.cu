@@ -2002,7 +2002,31 @@ int Engine::coarsen_chunked(const Level &in, const int32_t *Cm, int64_t ncl, Lev
   av = nullptr;
   if (sliced) { TRY(alloc(&ak, cap)); TRY(alloc(&av, cap)); }
   CK(cudaMemsetAsync(rowc, 0, (ncl + 1) * sizeof(int64_t), s_));
-  TRY(merge_splits(in));
+  // The rows in community order (vertex id within a community), so that a
+  // chunk's rows are one run of merge tiles and each chunk reads only them.
+  const int64_t ntiles = merge_tiles(in.nv, in.nnz);
+  int32_t *perm, *oid;
+  uint32_t *ok1, *ok2;
+  int64_t *pdeg, *pptr, *split_perm, *ctile;
+  TRY(alloc(&ok1, in.nv)); TRY(alloc(&ok2, in.nv)); TRY(alloc(&oid, in.nv)); TRY(alloc(&perm, in.nv));
+  TRY(alloc(&pdeg, in.nv + 1)); TRY(alloc(&pptr, in.nv + 1)); TRY(alloc(&split_perm, ntiles + 1));
+  TRY(alloc(&ctile, K + 1));
+  LAUNCH(k_comm_order_keys, grid_for(in.nv, 256, nsm_ * 16), 256, 0, s_, in.nv, Cm, ok1, oid);
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, ok1, ok2, oid, perm, in.nv, 0, 32, s_));
+  TRY(temp(tb));
+  CK(cub::DeviceRadixSort::SortPairs(temp_, tb, ok1, ok2, oid, perm, in.nv, 0, 32, s_));
+  LAUNCH(k_perm_degrees, grid_for(in.nv, 256, nsm_ * 16), 256, 0, s_, in.nv, perm, in.ptr, pdeg);
+  CK(cudaMemsetAsync(pdeg + in.nv, 0, sizeof(int64_t), s_));
+  CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, pdeg, pptr, in.nv + 1, s_));
+  TRY(temp(tb));
+  CK(cub::DeviceScan::ExclusiveSum(temp_, tb, pdeg, pptr, in.nv + 1, s_));
+  LAUNCH(k_merge_splits, grid_for(ntiles + 1, 256, nsm_ * 8), 256, 0, s_, in.nv, in.nnz, pptr,
+         ntiles, split_perm);
+  LAUNCH(k_chunk_tiles, (K + 1 + 255) / 256, 256, 0, s_, K, bounds, in.nv, ok2, pptr, ctile);
+  std::vector<int64_t> hct(K + 1);
+  CK(cudaMemcpyAsync(hct.data(), ctile, (K + 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  dfree(ok1); dfree(oid); dfree(pdeg); dfree(ctile);
   // the coarse rows go straight to their place: `total` (records of all
   // chunks) bounds the coarse entries, and a copy of the chunks' outputs
   // would double the peak on levels of billions of entries
@@ -2010,7 +2034,6 @@ int Engine::coarsen_chunked(const Level &in, const int32_t *Cm, int64_t ncl, Lev
   o.nv = ncl;
   o.owned = true;
   int64_t at = 0;
-  const int64_t ntiles = merge_tiles(in.nv, in.nnz);
   const int grid = std::max(1, (int)std::min<int64_t>(ntiles, nsm_ * 8));
   // sort + reduce n records of (kin, vin) into (kout, vout); returns the pairs
   auto sort_reduce = [&](uint64_t *ka, uint64_t *kb, double *va, double *vb, int64_t n,
@@ -2033,9 +2056,9 @@ int Engine::coarsen_chunked(const Level &in, const int32_t *Cm, int64_t ncl, Lev
   auto records = [&](int64_t a0, int64_t a1, int64_t t0, int64_t t1, int seeds,
                      int64_t *n) -> int {
     CK(cudaMemsetAsync(counter, 0, sizeof(unsigned long long), s_));
-    LAUNCH(k_chunk_records, grid, 256, 0, s_, in.nv, in.nnz, in.ptr, in.tail, in.w, Cm,
-           split_row_, (int32_t)a0, (int32_t)a1, nb, t0, t1, vf ? 0 : seeds, vf ? 1 : 0,
-           (unsigned long long)cap, counter, k1, v1);
+    LAUNCH(k_chunk_records, grid, 256, sizeof(PermTileSmem), s_, in.nv, in.nnz, in.ptr,
+           in.tail, in.w, Cm, perm, pptr, split_perm, (int32_t)a0, (int32_t)a1, nb, t0, t1,
+           vf ? 0 : seeds, vf ? 1 : 0, (unsigned long long)cap, counter, k1, v1);
     unsigned long long hn = 0;
     CK(cudaMemcpyAsync(&hn, counter, sizeof(hn), cudaMemcpyDeviceToHost, s_));
     CK(cudaStreamSynchronize(s_));
@@ -2059,10 +2082,12 @@ int Engine::coarsen_chunked(const Level &in, const int32_t *Cm, int64_t ncl, Lev
       const int64_t a0 = hb[k], a1 = hb[k + 1];
       if (a1 <= a0) continue;
       const int end_bit = nb + bits_for(std::max<int64_t>(a1 - a0 - 1, 1));
+      // the chunk's tile run (one tile past the start of the next chunk's rows)
+      const int64_t tk0 = hct[k], tk1 = std::min<int64_t>(ntiles, hct[k + 1] + 1);
       int64_t np = 0;
       if (hp[k + 1] - hp[k] <= cap) {
         int64_t n = 0;
-        TRY(records(a0, a1, 0, ntiles, 1, &n));
+        TRY(records(a0, a1, tk0, tk1, 1, &n));
         TRY(sort_reduce(k1, k2, v1, v2, n, end_bit, uk, uv, &np));
       } else {
         // slices of tiles; a slice whose records overflow is cut in two
@@ -2070,7 +2095,7 @@ int Engine::coarsen_chunked(const Level &in, const int32_t *Cm, int64_t ncl, Lev
         std::vector<std::pair<int64_t, int64_t>> todo;
         const int64_t nsl = 2 * ((hp[k + 1] - hp[k] + cap - 1) / cap);
         for (int64_t q = nsl - 1; q >= 0; --q)
-          todo.push_back({ntiles * q / nsl, ntiles * (q + 1) / nsl});
+          todo.push_back({tk0 + (tk1 - tk0) * q / nsl, tk0 + (tk1 - tk0) * (q + 1) / nsl});
         bool first = true;
         while (!todo.empty()) {
           const auto sl = todo.back();
@@ -2112,6 +2137,7 @@ int Engine::coarsen_chunked(const Level &in, const int32_t *Cm, int64_t ncl, Lev
   }
   dfree(ak); dfree(av);
   dfree(k1); dfree(k2); dfree(uk); dfree(v1); dfree(v2); dfree(uv);
+  dfree(ok2); dfree(perm); dfree(pptr); dfree(split_perm);
   unsigned long long hdiag = 0;
   CK(cudaMemcpyAsync(&hdiag, ndiag, sizeof(hdiag), cudaMemcpyDeviceToHost, s_));
   dfree(counter); dfree(d_np); dfree(ndiag); dfree(bounds); dfree(pb); dfree(cnt); dfree(prefix);
@@ -2471,6 +2497,8 @@ static int device_ready() {
                          (int)kPersistSmem);
     cudaFuncSetAttribute(k_hub_accum, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          kHubStageCap * (int)(sizeof(double) + sizeof(int32_t)));
+    cudaFuncSetAttribute(k_chunk_records, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)sizeof(PermTileSmem));
     attrs = true;
   }
   return GLV_OK;

@@ -1011,16 +1011,31 @@ __global__ void k_chunk_bounds(int64_t ncl, const int64_t *prefix, int K, int64_
   bounds[k] = (k == K) ? ncl : lo;
 }
 
+// Shared memory of one tile of the community-ordered rows: row starts
+// relative to the tile's first entry, the rows' communities and their first
+// entries in the CSR.
+struct PermTileSmem {
+  int32_t off[kMergeTile + 2];
+  int32_t comm[kMergeTile + 1];
+  int64_t base[kMergeTile + 1];
+};
+
 // Records of the chunk [a0, a1) (merge-path tiles, warp-aggregated slots).
-// Only tiles [t0, t1) are read (a chunk too large for the buffer is done in
-// slices); seeds come with the slice that has `seeds` set; records past `cap`
-// are counted but not written (the caller then cuts the slice finer).
+// The tiles run over the level's rows in community order: row r of that
+// order is vertex perm[r], its entries start at pptr[r] in the order's
+// numbering and at ptr[perm[r]] in the CSR, so the rows of a chunk are a
+// contiguous run of tiles.  Only tiles [t0, t1) are read (the chunk's run, or
+// a slice of it when its records exceed the buffer); seeds come with the
+// slice that has `seeds` set; records past `cap` are counted but not written
+// (the caller then cuts the slice finer).  Dynamic shared memory:
+// sizeof(PermTileSmem).
 __global__ void __launch_bounds__(256) k_chunk_records(
     int64_t nv, int64_t nnz, const int64_t *ptr, const int32_t *tail, const double *w,
-    const int32_t *C, const int64_t *split_row, int32_t a0, int32_t a1, int nb, int64_t t0,
-    int64_t t1, int seeds, int trunc, unsigned long long cap, unsigned long long *counter,
-    uint64_t *keys, double *vals) {
-  __shared__ MergeSmem sm;
+    const int32_t *C, const int32_t *perm, const int64_t *pptr, const int64_t *split_row,
+    int32_t a0, int32_t a1, int nb, int64_t t0, int64_t t1, int seeds, int trunc,
+    unsigned long long cap, unsigned long long *counter, uint64_t *keys, double *vals) {
+  extern __shared__ unsigned char dsm_raw[];
+  PermTileSmem &sm = *reinterpret_cast<PermTileSmem *>(dsm_raw);
   const int lane = threadIdx.x & 31;
   if (seeds) {
     for (int64_t a = a0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < a1;
@@ -1042,10 +1057,14 @@ __global__ void __launch_bounds__(256) k_chunk_records(
     const int nr = (int)(ih - i0 + 1);
     __syncthreads();
     for (int k = threadIdx.x; k <= nr; k += blockDim.x) {
-      const int64_t r = ptr[i0 + k] - j0;
+      const int64_t r = pptr[i0 + k] - j0;
       sm.off[k] = (int32_t)max((int64_t)0, min(r, (int64_t)kMergeTile + 1));
     }
-    for (int k = threadIdx.x; k < nr; k += blockDim.x) sm.comm[k] = C[i0 + k];
+    for (int k = threadIdx.x; k < nr; k += blockDim.x) {
+      const int32_t v = perm[i0 + k];
+      sm.comm[k] = C[v];
+      sm.base[k] = ptr[v] - pptr[i0 + k];
+    }
     __syncthreads();
     const int ne = (int)(j1 - j0);
     // every lane of a warp runs the same trip count, so the ballot sees them all
@@ -1063,7 +1082,7 @@ __global__ void __launch_bounds__(256) k_chunk_records(
         }
         const int32_t a = sm.comm[lo];
         if (a >= a0 && a < a1) {
-          const int64_t e = j0 + q;
+          const int64_t e = j0 + q + sm.base[lo];  // the entry's place in the CSR
           const int32_t b = C[tail[e]];
           if (b >= 0) {
             take = true;
@@ -1086,6 +1105,45 @@ __global__ void __launch_bounds__(256) k_chunk_records(
       }
     }
   }
+}
+
+// Community order of the rows: degrees of the rows in that order (for the
+// order's row starts).
+__global__ void k_perm_degrees(int64_t nv, const int32_t *perm, const int64_t *ptr,
+                               int64_t *deg) {
+  for (int64_t r = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; r < nv;
+       r += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t v = perm[r];
+    deg[r] = ptr[v + 1] - ptr[v];
+  }
+}
+
+// Sort keys of the community order: C as unsigned (a vertex without a
+// community, -1, sorts last) and the vertex id.
+__global__ void k_comm_order_keys(int64_t nv, const int32_t *C, uint32_t *keys, int32_t *ids) {
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    keys[v] = (uint32_t)C[v];
+    ids[v] = (int32_t)v;
+  }
+}
+
+// Tile run of each chunk [bounds[k], bounds[k+1]): the first row of the
+// community order with C >= bounds[k] (binary search in the sorted keys),
+// turned into a merge-path coordinate and a tile index (first tile that
+// reaches it for a start, past it for an end).
+__global__ void k_chunk_tiles(int K, const int64_t *bounds, int64_t nv, const uint32_t *skeys,
+                              const int64_t *pptr, int64_t *tiles) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k > K) return;
+  const uint32_t a = (uint32_t)bounds[k];
+  int64_t lo = 0, hi = nv;  // first r with skeys[r] >= a
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (skeys[mid] >= a) hi = mid; else lo = mid + 1;
+  }
+  const int64_t d = pptr[lo] + lo;  // merge coordinate where the chunk's rows start
+  tiles[k] = (k == 0) ? 0 : d / kMergeTile;
 }
 
 // Row counts and the chunk's tails of its unique (a, b) pairs.
