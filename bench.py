@@ -797,8 +797,9 @@ def main():
                 'achieved': achieved, 'peak': peak, 'unit': 'GB/s',
                 'frac': (achieved / peak) if achieved else None, 'peak_kind': peak_kind,
                 'traffic': (ratio * sweep_b / steps_timed) if (ratio and steps_timed) else None,
-                'traffic_source': 'ncu DRAM bytes / algorithmic bytes of the R-MAT scale-22 capture '
-                                  '(profiles/sweep_iteration_rmat22.md) times this launch\'s bytes',
+                'traffic_source': 'ncu dram__bytes_read.sum + dram__bytes_write.sum over the '
+                                  'algorithmic bytes of one k_sweep_iteration launch on R-MAT '
+                                  'scale 22, times this launch\'s algorithmic bytes',
                 'algorithmic_bytes_per_launch': sweep_b / steps_timed if steps_timed else None,
                 'avg_launch_s': sweep_t / steps_timed if steps_timed else None}
     s0 = stats[-1]

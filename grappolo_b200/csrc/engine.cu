@@ -36,11 +36,12 @@ static std::atomic<long> g_launches{0};
 // of one run (and of the next run) do not go back to the driver at every
 // synchronisation; glv_release_cached_memory() returns them.
 static std::mutex g_pool_mu;
-static cudaMemPool_t g_pool[128];
+constexpr int kMaxDevices = 128;  // device ordinals the per-device tables cover
+static cudaMemPool_t g_pool[kMaxDevices];
 
 static cudaMemPool_t engine_pool() {
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128) return nullptr;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
   std::lock_guard<std::mutex> lock(g_pool_mu);
   if (!g_pool[dev]) {
     cudaMemPoolProps props = {};
@@ -62,12 +63,12 @@ static cudaMemPool_t engine_pool() {
 // so their work is serialised (each call still waits only for its own
 // results).
 static std::mutex g_stream_mu;
-static cudaStream_t g_stream[128];
+static cudaStream_t g_stream[kMaxDevices];
 static cudaError_t engine_stream(cudaStream_t *s) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
-  if (dev < 0 || dev >= 128) return cudaErrorInvalidDevice;
+  if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
   std::lock_guard<std::mutex> lock(g_stream_mu);
   if (!g_stream[dev]) {
     e = cudaStreamCreateWithFlags(&g_stream[dev], cudaStreamNonBlocking);
@@ -91,12 +92,12 @@ struct BlockCache {
   std::unordered_map<void *, uint64_t> last_use;  // call generation of the block's last use
   uint64_t gen = 0;                                // calls finished on this device
 };
-static BlockCache g_cache[128];
+static BlockCache g_cache[kMaxDevices];
 
 // End of a call: blocks the call did not use go back to the pool, so a
 // workload whose sizes change (the waves of a batch) does not hoard memory.
 static void end_call_block_cache(int dev, cudaStream_t s) {
-  if (dev < 0 || dev >= 128) return;
+  if (dev < 0 || dev >= kMaxDevices) return;
   BlockCache &bc = g_cache[dev];
   std::lock_guard<std::mutex> lock(bc.mu);
   for (auto &kv : bc.free) {
@@ -118,12 +119,12 @@ static void end_call_block_cache(int dev, cudaStream_t s) {
 
 static int current_device() {
   int d = 0;
-  if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= 128) d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess || d < 0 || d >= kMaxDevices) d = 0;
   return d;
 }
 
 static void flush_block_cache(int dev, cudaStream_t s) {
-  if (dev < 0 || dev >= 128) return;
+  if (dev < 0 || dev >= kMaxDevices) return;
   BlockCache &bc = g_cache[dev];
   std::lock_guard<std::mutex> lock(bc.mu);
   for (auto &kv : bc.free)
@@ -158,6 +159,7 @@ static int fail(int code, const char *msg) {
   g_err = msg;
   return code;
 }
+static int fail(int code, const std::string &msg) { return fail(code, msg.c_str()); }
 
 #define CK(expr)                                                                         \
   do {                                                                                   \
@@ -2485,21 +2487,38 @@ struct Call {
   }
 };
 
+// The dynamic shared-memory limits of the kernels that take more than 48 KB
+// are a per-device setting: they are raised once for each device, with that
+// device current, the first time an entry point runs on it.
+static int set_kernel_attributes() {
+  const struct { const void *fn; int bytes; } want[] = {
+      {(const void *)k_sweep_block, kBlockCap * (int)(sizeof(double) + sizeof(int32_t))},
+      {(const void *)k_sweep_iteration, (int)kPersistSmem},
+      {(const void *)k_hub_accum, kHubStageCap * (int)(sizeof(double) + sizeof(int32_t))},
+      {(const void *)k_chunk_records, (int)sizeof(PermTileSmem)},
+  };
+  for (const auto &k : want) {
+    const cudaError_t e =
+        cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, k.bytes);
+    if (e != cudaSuccess)
+      return fail(GLV_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
+  }
+  return GLV_OK;
+}
+
 static int device_ready() {
   int n = 0;
   if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0)
     return fail(GLV_ERR_NO_DEVICE, "no CUDA device");
-  static bool attrs = false;
-  if (!attrs) {
-    cudaFuncSetAttribute(k_sweep_block, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         kBlockCap * (int)(sizeof(double) + sizeof(int32_t)));
-    cudaFuncSetAttribute(k_sweep_iteration, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)kPersistSmem);
-    cudaFuncSetAttribute(k_hub_accum, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         kHubStageCap * (int)(sizeof(double) + sizeof(int32_t)));
-    cudaFuncSetAttribute(k_chunk_records, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)sizeof(PermTileSmem));
-    attrs = true;
+  int dev = 0;
+  CK(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= kMaxDevices) return fail(GLV_ERR_ARG, "device ordinal out of range");
+  static std::mutex mu;
+  static bool attrs[kMaxDevices] = {};
+  std::lock_guard<std::mutex> lock(mu);
+  if (!attrs[dev]) {
+    TRY(set_kernel_attributes());
+    attrs[dev] = true;
   }
   return GLV_OK;
 }
@@ -3167,7 +3186,7 @@ constexpr int64_t kStaticModMaxVertices = kStaticModParts * kModVB;
 static __device__ __align__(256) double g_mod_scratch[2 * kStaticModParts];
 
 static std::mutex g_mod_scratch_mu;
-static double *g_mod_scratch_addr[128];  // device address of g_mod_scratch, per device
+static double *g_mod_scratch_addr[kMaxDevices];  // device address of g_mod_scratch, per device
 
 // The fold of k_modularity_final with the constant passed by value, so the
 // call needs no device copy of it.
@@ -3202,13 +3221,18 @@ extern "C" int glv_dev_modularity_static(long nv, const long *d_ptr, const int *
                 "static scratch covers; use the allocating entry points");
   if (!d_ptr || !d_tail || !d_weight || !d_C || !d_cDeg || !d_out)
     return fail(GLV_ERR_ARG, "glv_dev_modularity_static: NULL pointer");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(GLV_ERR_NO_DEVICE, "glv_dev_modularity_static: no CUDA device");
   int dev = 0;
   CK(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 128) return fail(GLV_ERR_ARG, "glv_dev_modularity_static: device id");
+  if (dev < 0 || dev >= kMaxDevices) return fail(GLV_ERR_ARG, "glv_dev_modularity_static: device id");
   double *scratch = nullptr;
   {
     // First call on a device: look up the array's device address with that
-    // device current.
+    // device current.  The address is kept for the life of the process; it
+    // belongs to the device's primary context, so a caller that resets the
+    // device (cudaDeviceReset) must not call this entry again afterwards.
     std::lock_guard<std::mutex> lock(g_mod_scratch_mu);
     if (!g_mod_scratch_addr[dev]) {
       void *p = nullptr;

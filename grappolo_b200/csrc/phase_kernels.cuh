@@ -130,7 +130,8 @@ __global__ void __launch_bounds__(256) k_modularity_part(int64_t nv, const int64
     int h = 0;
     for (int64_t e = eb + threadIdx.x; e < ee; e += blockDim.x) {
       while (s_ptr[h + 1] <= e) ++h;
-      if (C[tail[e]] == s_c[h]) ex = __dadd_rn(ex, w[e]);
+      // a vertex labelled -1 belongs to no community: its entries add nothing
+      if (s_c[h] >= 0 && C[tail[e]] == s_c[h]) ex = __dadd_rn(ex, w[e]);
     }
   }
   ex = block_sum<256>(ex, sh);

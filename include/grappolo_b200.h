@@ -363,16 +363,20 @@ int glv_decide_batch(long nv, const long *ptr, const long *tail, const double *w
  * fragmented or full device and implicitly synchronises it), or code running
  * under a memory budget fixed at start-up.  Inputs and the output are the
  * caller's device buffers: d_ptr int64[nv+1], d_tail int32[nnz],
- * d_weight f64[nnz], d_C int32[nv] (-1 = none), d_cDeg f64[nv] (total weighted
- * degree of each community id), `constant` = 1 / (sum of all weighted degrees);
- * d_out f64[3] receives {Q, e_xx, a2_x} with Q = e_xx*constant -
- * a2_x*constant^2 (the formula of Coloring/parallelLouvainWithColoring.cpp:226-249).
+ * d_weight f64[nnz], d_C int32[nv] (-1 = in no community: such a vertex's
+ * entries add nothing to e_xx), d_cDeg f64[nv] (total weighted degree of each
+ * community id), `constant` = 1 / (sum of all weighted degrees).  d_out f64[3]
+ * receives {Q, e_xx, a2_x}: e_xx is the sum of w over entries (i, t) with
+ * C[t] == C[i] >= 0, a2_x the sum of d_cDeg[c]^2 over all ids c < nv, and
+ * Q = e_xx*constant - a2_x*constant^2.
  * Scratch is a 1 MiB static device array compiled into the library, which
  * bounds nv to 16,777,216 (larger nv returns GLV_ERR_LIMIT without touching the
  * GPU).  Every GPU that loads the library holds that array until the process
  * exits.  The first call on a device looks up the array's address (once per
  * device, with that device current); make that first call before any stream
- * capture.  The work is queued on `stream` (cudaStream_t, NULL = legacy
+ * capture.  The address is kept for the life of the process: after a
+ * cudaDeviceReset of that device the entry must not be called again.
+ * Without a GPU it returns GLV_ERR_NO_DEVICE.  The work is queued on `stream` (cudaStream_t, NULL = legacy
  * default stream) and is complete when the stream reaches it.  All calls on a
  * device share the one array: calls that overlap on the GPU (other streams,
  * other host threads) race and must be serialised by the caller. */

@@ -259,7 +259,7 @@ def make_compare(R, ref_root):
 
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 and not sys.argv[1].startswith('--') \
-        else '/root/reference'
+        else os.environ.get('GRAPPOLO_REFERENCE', '/root/reference')
     R = Reference()
     if '--vf' in sys.argv:
         make_vf(R, ref_root)

@@ -61,6 +61,32 @@ def test_static_modularity_matches_allocating_entry(weighted):
         assert _call(g, t, constant) == pytest.approx(expected, rel=MOD_REL_TOL)
 
 
+def _numpy_modularity(g, C, constant, cdeg):
+    heads = g.heads()
+    same = (C[heads] == C[g.tail]) & (C[heads] >= 0)
+    exx = float(np.sum(g.weight[same]))
+    a2 = float(np.sum(cdeg * cdeg))
+    return exx * constant - a2 * constant * constant
+
+
+def test_static_modularity_unlabelled_vertices_and_no_allocation():
+    """Vertices labelled -1 belong to no community, so their entries add
+    nothing to e_xx; and after its first call on a device the entry leaves the
+    device's free memory unchanged."""
+    import torch
+    g = graphs.planted_partition(num_blocks=50, block_size=40, seed=6)
+    C = louvain.runMultiPhaseColoring(g, numThreads=1).copy()
+    rng = np.random.default_rng(3)
+    C[rng.random(g.num_vertices) < 0.2] = -1  # edges between unlabelled vertices remain
+    t, constant = _device_inputs(g, C)
+    expected = _numpy_modularity(g, C, constant, t['cdeg'].cpu().numpy())
+    assert _call(g, t, constant) == pytest.approx(expected, rel=MOD_REL_TOL)
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info()[0]
+    assert _call(g, t, constant) == pytest.approx(expected, rel=MOD_REL_TOL)
+    assert torch.cuda.mem_get_info()[0] == free_before
+
+
 def test_static_modularity_rejects_oversize():
     L = _lib.lib()
     too_many = 16_777_216 + 1
