@@ -212,6 +212,7 @@ struct Step {
 
 struct ClassSched {
   int64_t begin = 0, end = 0;  // member positions of the whole class
+  int color = 0;               // the key (colour) the class was built from
   std::vector<Step> steps;
 };
 
@@ -300,7 +301,7 @@ class Engine {
 
   int init(int64_t nv0, int64_t nnz0);
   int upload_check(const Level &L);
-  int color(const Level &L, int *ncolors, double *secs);
+  int color(const Level &L, int *ncolors, double *secs, bool sweep = false);
   int coloring_phase(const Level &L, int ncolors, bool stale, double lower, double thresh,
                      double *mod, int *itr);
   int basic_phase(const Level &L, double lower, double thresh, double *mod, int *itr);
@@ -445,8 +446,9 @@ class Engine {
   int phase_init(const Level &L, bool need_past);
   int merge_splits(const Level &L);
   int build_schedule(const Level &L, const int32_t *color, int ncolors, const int32_t *sub,
-                     int nsub, std::vector<ClassSched> *sched);
+                     int nsub, std::vector<ClassSched> *sched, bool hubs = true);
   int hub_offsets(const Level &L, std::vector<ClassSched> &sched);
+  int group_classes(const Level &L, int ncolors, std::vector<ClassSched> *sched);
   int sublevels(const Level &L, int ncolors, int32_t **d_sub, int *nsub);
   int launch_sweep(const Level &L, const Step &st, SweepArgs a, bool ordered, Probes *pr);
   int launch_apply(const ClassSched &cs, bool ordered);
@@ -458,7 +460,7 @@ class Engine {
     const char *e = getenv("GRAPPOLO_B200_PERSISTENT");
     return !ordered() && !(e && e[0] == '0');
   }
-  int color_spec(const Level &L, int *ncolors);
+  int color_spec(const Level &L, int *ncolors, int64_t core_deg = INT64_MAX, int core_batches = 0);
   int recolor(const Level &L, int *ncolors, int passes);
   int grow_hub(size_t entries);
   bool ordered() const { return mode_ == GLV_MODE_VERIFY && !integral; }
@@ -499,6 +501,12 @@ class Engine {
   double *part_g_ = nullptr;
   size_t chunk_cap_ = 0, seg_cap_ = 0;
   bool hub_tables_clean_ = false;
+  // The current colour phase runs some colour classes together in one step
+  // (group_classes), so a step's members are not an independent set.
+  bool relaxed_ = false;
+  // Classes at and above this colour of colour_ are batches of the core (not
+  // independent sets); INT32_MAX = every class is an independent set.
+  int core_color_ = INT32_MAX;
   HubWork hub_work() const {
     return HubWork{hub_keys_, hub_vals_, hub_off_, hub_occ_, hub_occ_off_, hub_cnt_, hub_self_,
                    hub_ownw_, chunk_pos_, chunk_beg_, chunk_end_, seg_pos_, seg_beg_, seg_end_,
@@ -581,8 +589,8 @@ int Engine::init(int64_t nv0, int64_t nnz0) {
   // partials of the modularity pass (one per 256 vertices) and of the
   // constant's reduction (kConstParts blocks) share these buffers
   const size_t nparts = std::max<size_t>((n + kModVB - 1) / kModVB, kConstParts) + 1;
-  TRY(alloc(&part_e_, nparts)); TRY(alloc(&part_a_, nparts)); TRY(alloc(&mod_out_, 4));
-  CK(cudaMallocHost((void **)&h_mod_, 4 * sizeof(double)));
+  TRY(alloc(&part_e_, nparts)); TRY(alloc(&part_a_, nparts)); TRY(alloc(&mod_out_, 8));
+  CK(cudaMallocHost((void **)&h_mod_, 8 * sizeof(double)));
   CK(cudaMemsetAsync(dDeg, 0, n * sizeof(double), s_));
   CK(cudaMemsetAsync(dSize, 0, n * sizeof(int32_t), s_));
   return GLV_OK;
@@ -669,8 +677,24 @@ int Engine::phase_init(const Level &L, bool need_past) {
 }
 
 // ----------------------------------------------------------------- colouring
-int Engine::color(const Level &L, int *ncolors, double *secs) {
+// Fast-mode colour phases sweep the core (rows in degree bin
+// GRAPPOLO_B200_CORE_BIN and above, default the 128..511 bin) apart from the
+// colour classes: the colouring covers the rest of the graph, and the core
+// vertices run in GRAPPOLO_B200_CORE_BATCHES classes (default 32) that each
+// decide against one snapshot of their members' communities.  Skewed graphs
+// need hundreds of colours for their dense core, each a grid-wide step with a
+// few long rows; a core vertex has most of its weight outside its batch, so
+// deciding a batch together changes little of what each decision sees.
+static void core_settings(int *core_bin, int *batches) {
+  *core_bin = BIN_T128;
+  *batches = 32;
+  if (const char *e = getenv("GRAPPOLO_B200_CORE_BIN")) *core_bin = atoi(e);
+  if (const char *e = getenv("GRAPPOLO_B200_CORE_BATCHES")) *batches = atoi(e);
+}
+
+int Engine::color(const Level &L, int *ncolors, double *secs, bool sweep) {
   const double t0 = now_s();
+  core_color_ = INT32_MAX;
   if (L.nv == 0 && color_algo_ != 3) {
     *ncolors = 0;
     return GLV_OK;
@@ -689,7 +713,13 @@ int Engine::color(const Level &L, int *ncolors, double *secs) {
     if (secs) *secs = now_s() - t0;
     return GLV_OK;
   }
-  TRY(spec ? color_spec(L, ncolors) : color_jp(L, ncolors));
+  int core_bin = NBINS, nbatch = 0;
+  if (sweep && spec && color_algo_ == 1 && mode_ != GLV_MODE_VERIFY && !bt_)
+    core_settings(&core_bin, &nbatch);
+  const int64_t core_deg = (core_bin > BIN_G4 && core_bin < NBINS && nbatch > 0)
+                               ? first_degree_of_bin(core_bin, lim_)
+                               : INT64_MAX;
+  TRY(spec ? color_spec(L, ncolors, core_deg, nbatch) : color_jp(L, ncolors));
   if (dbg) {
     cudaStreamSynchronize(s_);
     fprintf(stderr, "grappolo_b200: colouring %.4f s (%d colours)\n", now_s() - td, *ncolors);
@@ -702,7 +732,7 @@ int Engine::color(const Level &L, int *ncolors, double *secs) {
   // one removes no colour (GRAPPOLO_B200_RECOLOR sets the maximum, 0 = off).
   // Only colourings with many classes are worth a pass, which costs about one
   // colouring (GRAPPOLO_B200_RECOLOR_MIN: the class count that triggers it).
-  if (mode_ != GLV_MODE_VERIFY) {
+  if (mode_ != GLV_MODE_VERIFY && core_color_ == INT32_MAX) {
     const char *rp = getenv("GRAPPOLO_B200_RECOLOR");
     const char *rm = getenv("GRAPPOLO_B200_RECOLOR_MIN");
     if (*ncolors > (rm ? atoi(rm) : 64)) TRY(recolor(L, ncolors, rp ? atoi(rp) : 2));
@@ -799,16 +829,19 @@ int Engine::color_jp(const Level &L, int *ncolors, const int32_t *key) {
 // Fast mode: speculative first-fit rounds with hashed-priority conflicts.
 constexpr int64_t kSpecBlockDeg = 2048;
 
-int Engine::color_spec(const Level &L, int *ncolors) {
+int Engine::color_spec(const Level &L, int *ncolors, int64_t core_deg, int core_batches) {
   int32_t *wl, *bl, *nx, *cnt, *status, *maxc;
+  unsigned long long *ncore;
   TRY(alloc(&wl, L.nv)); TRY(alloc(&bl, L.nv)); TRY(alloc(&nx, L.nv));
-  TRY(alloc(&cnt, 4)); TRY(alloc(&status, 1)); TRY(alloc(&maxc, 1));
+  TRY(alloc(&cnt, 4)); TRY(alloc(&status, 1)); TRY(alloc(&maxc, 1)); TRY(alloc(&ncore, 1));
   CK(cudaMemsetAsync(cnt, 0, 4 * sizeof(int32_t), s_));
   CK(cudaMemsetAsync(status, 0, sizeof(int32_t), s_));
   CK(cudaMemsetAsync(maxc, 0xff, sizeof(int32_t), s_));
+  CK(cudaMemsetAsync(ncore, 0, sizeof(unsigned long long), s_));
   const uint32_t seed = 0x5bd1e995u;
+  if (core_batches <= 0) core_deg = INT64_MAX;
   LAUNCH(k_spec_init, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, L.ptr, L.tail,
-         kSpecBlockDeg, color_, wl, cnt, bl, cnt + 1);
+         kSpecBlockDeg, core_deg, color_, wl, cnt, bl, cnt + 1, ncore);
   // Rounds run in groups without a host read: the kernels take the list
   // lengths from device counters, and a round after the last conflict is a
   // set of empty launches.  The host reads the counters once per group.
@@ -841,12 +874,31 @@ int Engine::color_spec(const Level &L, int *ncolors) {
     fprintf(stderr, "grappolo_b200: speculative colouring nv=%ld rounds=%d\n", (long)L.nv, rounds);
   LAUNCH(k_max_color, grid_for(L.nv, 256, nsm_ * 8), 256, 0, s_, L.nv, color_, maxc);
   int32_t hs, hm;
+  unsigned long long hcore = 0;
   CK(cudaMemcpyAsync(&hs, status, sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
   CK(cudaMemcpyAsync(&hm, maxc, sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaMemcpyAsync(&hcore, ncore, sizeof(hcore), cudaMemcpyDeviceToHost, s_));
   CK(cudaStreamSynchronize(s_));
-  dfree(wl); dfree(bl); dfree(nx); dfree(cnt); dfree(status); dfree(maxc);
-  if (hs) return fail(GLV_ERR_COLORS, "colouring needs more than 4096 colours");
+  if (hs) {
+    dfree(wl); dfree(bl); dfree(nx); dfree(cnt); dfree(status); dfree(maxc); dfree(ncore);
+    return fail(GLV_ERR_COLORS, "colouring needs more than 4096 colours");
+  }
   *ncolors = hm + 1;
+  if (hcore > 0) {
+    const int nb = (int)std::min<unsigned long long>(hcore, (unsigned long long)core_batches);
+    if (*ncolors + nb > kMaxColors) {
+      dfree(wl); dfree(bl); dfree(nx); dfree(cnt); dfree(status); dfree(maxc); dfree(ncore);
+      return fail(GLV_ERR_COLORS, "colouring needs more than 4096 colours");
+    }
+    LAUNCH(k_core_batches, grid_for(L.nv, 256, nsm_ * 8), 256, 0, s_, L.nv, (int32_t)*ncolors,
+           (int32_t)nb, color_);
+    core_color_ = *ncolors;
+    *ncolors += nb;
+    if (debug_)
+      fprintf(stderr, "grappolo_b200: %d colours + %d batches of %llu core vertices\n",
+              core_color_, nb, hcore);
+  }
+  dfree(wl); dfree(bl); dfree(nx); dfree(cnt); dfree(status); dfree(maxc); dfree(ncore);
   return GLV_OK;
 }
 
@@ -935,8 +987,10 @@ int Engine::sublevels(const Level &L, int ncolors, int32_t **d_sub, int *nsub) {
 }
 
 // ------------------------------------------------------------------ schedule
+// `hubs`: also lay out the block-path hub tables and work lists (every path but
+// the persistent sweep, which plans its long rows itself).
 int Engine::build_schedule(const Level &L, const int32_t *color, int ncolors, const int32_t *sub,
-                           int nsub, std::vector<ClassSched> *sched) {
+                           int nsub, std::vector<ClassSched> *sched, bool hubs) {
   const bool debug = getenv("GRAPPOLO_B200_DEBUG") != nullptr;
   const double tsd = now_s();
   const int64_t nkeys = (int64_t)ncolors * nsub * NBINS;
@@ -964,6 +1018,7 @@ int Engine::build_schedule(const Level &L, const int32_t *color, int ncolors, co
   for (int c = 0; c < ncolors; ++c) {
     ClassSched cs;
     cs.begin = pos;
+    cs.color = c;
     for (int sl = 0; sl < nsub; ++sl) {
       Step st;
       int64_t cnt = 0;
@@ -982,7 +1037,61 @@ int Engine::build_schedule(const Level &L, const int32_t *color, int ncolors, co
     }
   }
   if (debug) fprintf(stderr, "grappolo_b200: schedule sort+hist %.4f s\n", now_s() - tsd);
-  return hub_offsets(L, *sched);
+  return hubs ? hub_offsets(L, *sched) : GLV_OK;
+}
+
+// Fast mode: colour classes whose members all have long rows (degree bin at
+// least GRAPPOLO_B200_MERGE_BIN, default the hub bin) run in steps of up to
+// GRAPPOLO_B200_MERGE_CLASSES classes (default 16; 0 or 1 = every class its
+// own step).  Skewed graphs colour their dense core of high-degree vertices
+// with hundreds of classes of a few vertices each, and every class is a
+// grid-wide step; a vertex of such a class has almost all of its weight on
+// vertices outside the core, so deciding a few core classes against one
+// snapshot changes little of what each decision sees.  A group takes the
+// place of its first class; the other classes keep their order.  Returns the
+// schedule rebuilt over the groups (relaxed_ set) or leaves it unchanged.
+int Engine::group_classes(const Level &L, int ncolors, std::vector<ClassSched> *sched) {
+  relaxed_ = false;
+  if (mode_ == GLV_MODE_VERIFY || bt_ || sched->size() < 2) return GLV_OK;
+  int gmax = 16, min_bin = BIN_HUB;
+  if (const char *e = getenv("GRAPPOLO_B200_MERGE_CLASSES")) gmax = atoi(e);
+  if (const char *e = getenv("GRAPPOLO_B200_MERGE_BIN")) min_bin = atoi(e);
+  if (gmax <= 1 || min_bin < 0 || min_bin >= NBINS) return GLV_OK;
+  std::vector<int32_t> map(ncolors, 0);
+  int ngroups = 0, open = -1, in_open = 0, merged = 0;
+  for (const ClassSched &cs : *sched) {
+    bool long_rows = cs.steps.size() == 1;
+    for (const Step &st : cs.steps) long_rows = long_rows && st.seg[min_bin] == st.seg[0];
+    if (!long_rows) {
+      map[cs.color] = ngroups++;
+      continue;
+    }
+    if (open < 0 || in_open >= gmax) {
+      open = ngroups++;
+      in_open = 0;
+    } else {
+      ++merged;
+    }
+    map[cs.color] = open;
+    ++in_open;
+  }
+  if (merged == 0) return GLV_OK;
+  // colours with no member keep a slot that no vertex uses
+  int32_t *d_map, *key;
+  TRY(alloc(&d_map, ncolors));
+  TRY(alloc(&key, L.nv));
+  TRY(upload(s_, d_map, map));
+  LAUNCH(k_remap_colors, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, color_, d_map, key);
+  const int rc = build_schedule(L, key, ngroups, nullptr, 1, sched);
+  CK(cudaStreamSynchronize(s_));
+  dfree(d_map);
+  dfree(key);
+  TRY(rc);
+  relaxed_ = true;
+  if (getenv("GRAPPOLO_B200_DEBUG"))
+    fprintf(stderr, "grappolo_b200: %d colour classes run in %zu steps (%d merged)\n",
+            ngroups + merged, sched->size(), merged);
+  return GLV_OK;
 }
 
 int Engine::grow_hub(size_t entries) {
@@ -1378,6 +1487,9 @@ int Engine::coloring_phase(const Level &L, int ncolors, bool stale, double lower
   if (debug) { cudaStreamSynchronize(s_); fprintf(stderr, "grappolo_b200: phase init %.4f s\n", now_s() - td); td = now_s(); }
   std::vector<ClassSched> sched;
   TRY(build_schedule(L, color_, ncolors, d_sub, nsub, &sched));
+  relaxed_ = false;
+  if (nsub == 1 && core_color_ < ncolors) relaxed_ = true;  // core batches
+  else if (nsub == 1 && persistent()) TRY(group_classes(L, ncolors, &sched));
   if (debug) { cudaStreamSynchronize(s_); fprintf(stderr, "grappolo_b200: schedule %.4f s\n", now_s() - td); }
   dfree(d_sub);
   const bool ord = ordered();
@@ -1673,8 +1785,10 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
   // GRAPPOLO_B200_CHECK_MODULARITY=1 runs both and fails when they differ.
   const char *fm = getenv("GRAPPOLO_B200_FULL_MODULARITY");
   const bool check_exx = getenv("GRAPPOLO_B200_CHECK_MODULARITY") != nullptr;
-  const bool carry_exx =
-      !jacobi && !bt && !ordered() && !integral && !(fm && fm[0] == '1') && L.nnz > 0;
+  // (a step that runs several classes moves neighbours together, and the
+  // carried change of each move assumes its neighbours stay put)
+  const bool carry_exx = !jacobi && !bt && !ordered() && !integral && !relaxed_ &&
+                         !(fm && fm[0] == '1') && L.nnz > 0;
 
   if (bt) {
     p.gid = bt->gid;
@@ -1851,6 +1965,27 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
         last = t;
       }
       const double tm = h_trace[4 * ns + 1] > last ? (h_trace[4 * ns + 1] - last) * 1e-9 : 0.0;
+      if (const char *tf = getenv("GRAPPOLO_B200_TRACE_FILE")) {
+        // one line per step: level size, iteration, step, members per degree
+        // bin, hub chunks, then the stage times in microseconds
+        if (FILE *f = fopen(tf, "a")) {
+          uint64_t t = h_trace[4 * ns];
+          for (size_t k = 0; k < ns; ++k) {
+            const StepDesc &d = steps[k];
+            fprintf(f, "%ld %d %zu", (long)L.nv, n, k);
+            for (int b = 0; b < NBINS; ++b) fprintf(f, " %ld", (long)(d.seg[b + 1] - d.seg[b]));
+            fprintf(f, " %ld", (long)(d.hub_chunk[1] - d.hub_chunk[0]));
+            for (int q = 0; q < 4; ++q) {
+              const uint64_t x = h_trace[4 * k + q];
+              if (x == 0 || x < t) { fprintf(f, " 0"); continue; }
+              fprintf(f, " %.2f", (x - t) * 1e-3);
+              t = x;
+            }
+            fprintf(f, "\n");
+          }
+          fclose(f);
+        }
+      }
       std::vector<double> sorted = per;
       std::sort(sorted.begin(), sorted.end());
       fprintf(stderr,
@@ -2333,7 +2468,7 @@ int Engine::run_multiphase(const Level &L0, int32_t *d_C_orig, bool coloring,
   bool recolored = false;
   double tcol = 0;
   if (coloring) {
-    TRY(color(L, &ncolors, &tcol));
+    TRY(color(L, &ncolors, &tcol, true));
     t_color += tcol;
     recolored = true;
   }
@@ -2383,7 +2518,7 @@ int Engine::run_multiphase(const Level &L0, int32_t *d_C_orig, bool coloring,
         ++phase;
         recolored = false;
         if (coloring && L.nv > min_graph_size && !non_color) {
-          TRY(color(L, &ncolors, &tcol));
+          TRY(color(L, &ncolors, &tcol, true));
           t_color += tcol;
           recolored = true;
         }

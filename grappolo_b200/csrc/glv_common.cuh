@@ -44,6 +44,21 @@ __host__ __device__ inline int degree_bin(int64_t deg, BinLimits lim) {
   return BIN_BLOCK;
 }
 
+// Smallest degree whose bin is `bin` (bins above BIN_G4).
+__host__ __device__ inline int64_t first_degree_of_bin(int bin, BinLimits lim) {
+  switch (bin) {
+    case BIN_G8: return 5;
+    case BIN_G16: return 9;
+    case BIN_G32: return 17;
+    case BIN_WARP: return 33;
+    case BIN_T128: return (int64_t)lim.warp_max + 1;
+    case BIN_T256: return 512;
+    case BIN_BLOCK: return 1024;
+    case BIN_HUB: return (int64_t)lim.block_max + 1;
+    default: return 0;
+  }
+}
+
 __host__ __device__ inline uint32_t next_pow2(uint32_t x) {
   uint32_t p = 1;
   while (p < x) p <<= 1;

@@ -454,6 +454,15 @@ __global__ void k_reverse_class_key(int64_t nv, const int32_t *color, int32_t nc
     key[v] = ncolors - 1 - color[v];
 }
 
+// key[v] = map[color[v]]: colour classes relabelled as the sweep steps that
+// run them (several classes may share a step).
+__global__ void k_remap_colors(int64_t nv, const int32_t *color, const int32_t *map,
+                               int32_t *key) {
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
+       v += (int64_t)gridDim.x * blockDim.x)
+    key[v] = map[color[v]];
+}
+
 __global__ void k_max_color(int64_t nv, const int32_t *color, int32_t *out) {
   int32_t m = -1;
   for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
@@ -943,13 +952,23 @@ __global__ void __launch_bounds__(512) k_spec_conflicts_block(const int32_t *cou
 }
 
 // Initial lists: rows with no neighbour but themselves take colour 0; the
-// rest go to the warp or block list by degree.
+// rest go to the warp or block list by degree.  Rows of at least `core_deg`
+// entries (the core, swept in batches) take kCoreColor and stay out of the
+// lists: no other vertex sees them (their colour is negative), so the
+// colouring covers only the graph without the core.
+constexpr int32_t kCoreColor = -2;
 __global__ void k_spec_init(int64_t nv, const int64_t *ptr, const int32_t *tail,
-                            int64_t block_deg, int32_t *color, int32_t *wl, int32_t *wcount,
-                            int32_t *bl, int32_t *bcount) {
+                            int64_t block_deg, int64_t core_deg, int32_t *color, int32_t *wl,
+                            int32_t *wcount, int32_t *bl, int32_t *bcount,
+                            unsigned long long *ncore) {
   for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
        v += (int64_t)gridDim.x * blockDim.x) {
     const int64_t rb = ptr[v], re = ptr[v + 1];
+    if (re - rb >= core_deg) {
+      color[v] = kCoreColor;
+      atomicAdd(ncore, 1ull);
+      continue;
+    }
     bool any = false;
     for (int64_t j = rb; j < re && !any; ++j) any = tail[j] != (int32_t)v;
     color[v] = any ? -1 : 0;
@@ -957,6 +976,14 @@ __global__ void k_spec_init(int64_t nv, const int64_t *ptr, const int32_t *tail,
     if (re - rb >= block_deg) bl[atomicAdd(bcount, 1)] = (int32_t)v;
     else wl[atomicAdd(wcount, 1)] = (int32_t)v;
   }
+}
+
+// Core vertices join one of `nbatch` classes after the `base` colours of the
+// rest, by a hash of the id (balanced in expectation, the same on every run).
+__global__ void k_core_batches(int64_t nv, int32_t base, int32_t nbatch, int32_t *color) {
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
+       v += (int64_t)gridDim.x * blockDim.x)
+    if (color[v] == kCoreColor) color[v] = base + (int32_t)(mix32((uint32_t)v) % (uint32_t)nbatch);
 }
 
 // Split a list by degree (next round's lists).
