@@ -1743,7 +1743,7 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
   StepDesc *d_steps = nullptr;
   int64_t *d_ctr = nullptr;
   TRY(alloc(&d_steps, steps.size()));
-  TRY(alloc(&d_ctr, steps.size()));
+  TRY(alloc(&d_ctr, 2 * steps.size()));  // block and team queues of every step
   dfree(step_big_);
   TRY(alloc(&step_big_, steps.size()));
   TRY(upload(s_, d_steps, steps));
@@ -1890,7 +1890,7 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
         if (bt->h_act[g]) batch_edges += (double)bt->gnnz[g];
     }
     p.exx_mode = (carry_exx && n >= 2) ? (check_exx ? 2 : 1) : 0;
-    cudaError_t e = cudaMemsetAsync(d_ctr, 0, steps.size() * sizeof(int64_t), s_);
+    cudaError_t e = cudaMemsetAsync(d_ctr, 0, 2 * steps.size() * sizeof(int64_t), s_);
     if (e == cudaSuccess) e = cudaMemsetAsync(step_big_, 0, steps.size() * sizeof(int32_t), s_);
     if (e0) cudaEventRecord(e0, s_);
     if (e == cudaSuccess)

@@ -6,10 +6,10 @@
 // vertices.  Launching a few kernels per class leaves the GPU waiting on
 // launches and on the single largest row of each class.  Here every block of
 // a persistent grid takes part in every class:
-//   stage 1  hub chunks (global tables); rows of 1024..2047 entries per
-//            block, 512..1023 per 256-thread team, 128..511 per 128-thread
-//            team (shared tables); then warp items (rows <= 32 entries, and
-//            33..127-entry rows with a per-warp shared table)  -> grid barrier
+//   stage 1  hub chunks (global tables) and rows of 1024..4095 entries per
+//            block; rows of 128..1023 entries per 128-thread team (shared
+//            tables); then warp items (rows <= 32 entries, and 33..127-entry
+//            rows with a per-warp shared table)                  -> grid barrier
 //   stage 2  hub table segments -> partial arg-maxes            -> grid barrier
 //   stage 3  one warp per hub folds its partials                -> grid barrier
 //   stage 4  community totals += the class's deltas             -> grid barrier
@@ -47,7 +47,7 @@ struct IterArgs {
   double *cDeg;
   int32_t *cSize;
   uint64_t *trace;         // optional: globaltimer at each barrier, 4 per step + 2
-  int64_t *task_ctr;       // per step: next stage-1 task (zero at launch)
+  int64_t *task_ctr;       // per step: next block task, next team task (zero at launch)
   const int32_t *class_kept;  // gated sweeps: vertices the gate kept per class (NULL = all)
   int64_t nnz;
   const int64_t *split_row;   // merge-path tile boundaries of the level
@@ -93,7 +93,13 @@ __device__ __forceinline__ uint64_t global_ns() {
 constexpr int kPersistThreads = 512;
 constexpr int kPersistTableCap = 8192;  // BIN_BLOCK rows: degree <= 4095
 constexpr int kPersistWarpCap = 256;    // warp-table rows: degree <= 127
+constexpr int kTeamThreads = 128;      // team of the 128..1023-entry rows
+constexpr int kTeamCap = 2048;         // its table: table_cap(1023)
 constexpr size_t kPersistSmem = (size_t)kPersistTableCap * (sizeof(double) + sizeof(int32_t));
+static_assert(kPersistThreads / kTeamThreads * kTeamCap == kPersistTableCap,
+              "team tables tile the block table");
+static_assert(kTeamThreads / 32 * kPersistWarpCap <= kTeamCap,
+              "warp tables tile their team's table");
 static_assert(kPersistSmem >= sizeof(MergeSmem), "merge tiles must fit");
 static_assert(kPersistSmem >= (size_t)(kPersistThreads / 32) * kPersistWarpCap *
                                   (sizeof(double) + sizeof(int32_t)),
@@ -152,14 +158,22 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
   __shared__ int32_t s_c[32];
   const int warp = threadIdx.x >> 5, nwb = blockDim.x >> 5;
   const int64_t gw = (int64_t)blockIdx.x * nwb + warp, ngw = (int64_t)gridDim.x * nwb;
+  // warps numbered across blocks first: a step with few warp items spreads over SMs
+  const int64_t gwi = (int64_t)warp * gridDim.x + blockIdx.x;
   const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   const int64_t ngt = (int64_t)gridDim.x * blockDim.x;
+  // shared table region: one 8192-slot table (block tasks), four 2048-slot
+  // team tables, or a 256-slot table per warp inside its team's table
+  const int team = threadIdx.x / kTeamThreads, tt = threadIdx.x % kTeamThreads;
   double *tvals = reinterpret_cast<double *>(smem_raw);
-  double *wvals = tvals + (size_t)warp * kPersistWarpCap;
-  int32_t *wkeys = reinterpret_cast<int32_t *>(tvals + (size_t)nwb * kPersistWarpCap) +
-                   (size_t)warp * kPersistWarpCap;
+  int32_t *tkeys = reinterpret_cast<int32_t *>(tvals + kPersistTableCap);
+  double *team_vals = tvals + (size_t)team * kTeamCap;
+  int32_t *team_keys = tkeys + (size_t)team * kTeamCap;
+  double *wvals = team_vals + (size_t)(tt >> 5) * kPersistWarpCap;
+  int32_t *wkeys = team_keys + (size_t)(tt >> 5) * kPersistWarpCap;
   GLV_TRACE(4 * p.nsteps);
   __shared__ int64_t s_task;
+  __shared__ int64_t s_team_task[kPersistThreads / kTeamThreads];
   __shared__ int s_flag;
   // this block's slot of the moves' e_xx changes (only this block writes it)
   if (p.a.exx_delta && threadIdx.x == 0) p.a.exx_delta[blockIdx.x] = 0.0;
@@ -167,8 +181,13 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
     const StepDesc &st = p.steps[s];
     // a class the gate emptied is skipped whole (no work, no barrier)
     if (p.class_kept && p.class_kept[st.cls] == 0) continue;
-    // Stage 1 as a task queue: blocks take the next task of any kind, the
-    // heaviest kinds first, so no block serialises several kinds.
+    // Stage 1 in three parts, each from its own queue: (A) hub chunks and
+    // rows of 1024..4095 entries, whole blocks with an 8192-slot table;
+    // (B) rows of 128..1023 entries, 128-thread teams (four per block, each
+    // fetching its own rows, 2048-slot tables); (C) warp items (rows of up to
+    // 32 entries, several per warp; rows of 33..127 entries, one per warp),
+    // item t to warp t mod (warps of the grid), in the warp's slice of its
+    // team's table region.
     const int64_t n4 = st.seg[1] - st.seg[0], n8 = st.seg[2] - st.seg[1];
     const int64_t n16 = st.seg[3] - st.seg[2], n32 = st.seg[4] - st.seg[3];
     const int64_t nw = st.seg[5] - st.seg[4];
@@ -176,62 +195,51 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
     const int64_t witems = i4 + i8 + i16 + n32 + nw;
     const int64_t t_hub = st.hub_chunk[1] - st.hub_chunk[0];
     const int64_t t_blk = st.seg[BIN_BLOCK + 1] - st.seg[BIN_BLOCK];
-    const int64_t t_256 = (st.seg[BIN_T256 + 1] - st.seg[BIN_T256] + 1) / 2;
-    const int64_t t_128 = (st.seg[BIN_T128 + 1] - st.seg[BIN_T128] + 3) / 4;
-    const int64_t t_w = (witems + nwb - 1) / nwb;
-    const int64_t ntask = t_hub + t_blk + t_256 + t_128 + t_w;
-    while (true) {
-      if (threadIdx.x == 0) s_task = atomicAdd((unsigned long long *)&p.task_ctr[s], 1ull);
-      __syncthreads();
-      int64_t t = s_task;
-      __syncthreads();
-      if (t >= ntask) break;
-      if (t < t_hub) {
-        hub_accum_chunk(p.a, p.h, st.hub_chunk[0] + t, reinterpret_cast<int32_t *>(tvals + kPersistTableCap),
-                        tvals, s_self, s_g, s_c, &s_flag, s);
-        continue;
+    const int64_t n256 = st.seg[BIN_T256 + 1] - st.seg[BIN_T256];
+    const int64_t n128 = st.seg[BIN_T128 + 1] - st.seg[BIN_T128];
+    if (t_hub + t_blk > 0) {
+      while (true) {
+        if (threadIdx.x == 0)
+          s_task = atomicAdd((unsigned long long *)&p.task_ctr[2 * s], 1ull);
+        __syncthreads();
+        int64_t t = s_task;
+        __syncthreads();
+        if (t >= t_hub + t_blk) break;
+        if (t < t_hub) {
+          hub_accum_chunk(p.a, p.h, st.hub_chunk[0] + t,
+                          reinterpret_cast<int32_t *>(tvals + kPersistTableCap), tvals, s_self,
+                          s_g, s_c, &s_flag, s);
+        } else {
+          team_vertex<512>(p.a, st.seg[BIN_BLOCK] + (t - t_hub),
+                           reinterpret_cast<int32_t *>(tvals + kPersistTableCap), tvals, 0, s_self,
+                           s_g, s_c);
+        }
       }
-      t -= t_hub;
-      if (t < t_blk) {
-        team_vertex<512>(p.a, st.seg[BIN_BLOCK] + t, reinterpret_cast<int32_t *>(tvals + kPersistTableCap),
-                         tvals, 0, s_self, s_g, s_c);
-        continue;
+    }
+    if (n256 + n128 > 0) {
+      while (true) {
+        if (tt == 0)
+          s_team_task[team] = atomicAdd((unsigned long long *)&p.task_ctr[2 * s + 1], 1ull);
+        team_sync<128>(team);
+        const int64_t t = s_team_task[team];
+        team_sync<128>(team);
+        if (t >= n256 + n128) break;
+        const int64_t pos = (t < n256) ? st.seg[BIN_T256] + t : st.seg[BIN_T128] + (t - n256);
+        team_vertex<128>(p.a, pos, team_keys, team_vals, team, s_self + 4 * team,
+                         s_g + 4 * team, s_c + 4 * team);
       }
-      t -= t_blk;
-      if (t < t_256) {
-        // two 256-thread teams, tables of 2048 slots
-        const int team = threadIdx.x / 256;
-        const int64_t pos = st.seg[BIN_T256] + 2 * t + team;
-        if (pos < st.seg[BIN_T256 + 1])
-          team_vertex<256>(p.a, pos, reinterpret_cast<int32_t *>(tvals + kPersistTableCap) + team * 2048,
-                           tvals + team * 2048, team, s_self + 8 * team, s_g + 8 * team,
-                           s_c + 8 * team);
-        continue;
-      }
-      t -= t_256;
-      if (t < t_128) {
-        // four 128-thread teams, tables of 1024 slots
-        const int team = threadIdx.x / 128;
-        const int64_t pos = st.seg[BIN_T128] + 4 * t + team;
-        if (pos < st.seg[BIN_T128 + 1])
-          team_vertex<128>(p.a, pos, reinterpret_cast<int32_t *>(tvals + kPersistTableCap) + team * 1024,
-                           tvals + team * 1024, team, s_self + 4 * team, s_g + 4 * team,
-                           s_c + 4 * team);
-        continue;
-      }
-      t -= t_128;
-      // one warp item per warp of the block (per-warp shared tables)
-      int64_t k = t * nwb + warp;
-      if (k >= witems) continue;
-      if (k < i4) { small_item<4>(p.a, st.seg[0] + 8 * k, st.seg[1]); continue; }
-      k -= i4;
-      if (k < i8) { small_item<8>(p.a, st.seg[1] + 4 * k, st.seg[2]); continue; }
-      k -= i8;
-      if (k < i16) { small_item<16>(p.a, st.seg[2] + 2 * k, st.seg[3]); continue; }
-      k -= i16;
-      if (k < n32) { small_item<32>(p.a, st.seg[3] + k, st.seg[4]); continue; }
-      k -= n32;
-      warp_table_vertex(p.a, st.seg[4] + k, wkeys, wvals);
+    }
+    for (int64_t k = gwi; k < witems; k += ngw) {
+      int64_t q = k;
+      if (q < i4) { small_item<4>(p.a, st.seg[0] + 8 * q, st.seg[1]); continue; }
+      q -= i4;
+      if (q < i8) { small_item<8>(p.a, st.seg[1] + 4 * q, st.seg[2]); continue; }
+      q -= i8;
+      if (q < i16) { small_item<16>(p.a, st.seg[2] + 2 * q, st.seg[3]); continue; }
+      q -= i16;
+      if (q < n32) { small_item<32>(p.a, st.seg[3] + q, st.seg[4]); continue; }
+      q -= n32;
+      warp_table_vertex(p.a, st.seg[4] + q, wkeys, wvals);
     }
     grid.sync();
     GLV_TRACE(4 * s);
