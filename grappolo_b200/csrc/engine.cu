@@ -213,6 +213,7 @@ struct Step {
 struct ClassSched {
   int64_t begin = 0, end = 0;  // member positions of the whole class
   int color = 0;               // the key (colour) the class was built from
+  bool relaxed = false;        // not an independent set (a core batch or merged classes)
   std::vector<Step> steps;
 };
 
@@ -493,6 +494,9 @@ class Engine {
   // parallel hub path (per member slot arrays, work lists, filled-slot lists)
   int64_t *hub_occ_off_ = nullptr, *hub_seg_beg_ = nullptr, *hub_seg_end_ = nullptr;
   int32_t *hub_cnt_ = nullptr, *hub_left_ = nullptr, *hub_big_ = nullptr, *step_big_ = nullptr;
+  int32_t *hub_segs_left_ = nullptr, *hub_err_ = nullptr;
+  uint32_t *hub_state_ = nullptr;
+  uint32_t epoch_ = 0;  // persistent launches of this engine (hub states compare against it)
   double *hub_self_ = nullptr, *hub_ownw_ = nullptr;
   int32_t *hub_occ_ = nullptr;
   size_t hub_occ_cap_ = 0;
@@ -510,7 +514,8 @@ class Engine {
   HubWork hub_work() const {
     return HubWork{hub_keys_, hub_vals_, hub_off_, hub_occ_, hub_occ_off_, hub_cnt_, hub_self_,
                    hub_ownw_, chunk_pos_, chunk_beg_, chunk_end_, seg_pos_, seg_beg_, seg_end_,
-                   part_g_, part_c_, hub_seg_beg_, hub_seg_end_, hub_left_, hub_big_, step_big_};
+                   part_g_, part_c_, hub_seg_beg_, hub_seg_end_, hub_left_, hub_big_, step_big_,
+                   hub_segs_left_, hub_state_, 0u, hub_err_};
   }
   int hist_cap_ = 0;
   // ordered-delta buffers
@@ -547,6 +552,7 @@ void Engine::release() {
   dfree(hub_off_);
   dfree(hub_occ_off_); dfree(hub_seg_beg_); dfree(hub_seg_end_); dfree(hub_cnt_);
   dfree(hub_self_); dfree(hub_ownw_); dfree(hub_occ_); dfree(hub_left_); dfree(hub_big_);
+  dfree(hub_segs_left_); dfree(hub_state_); dfree(hub_err_);
   dfree(step_big_); dfree(chunk_pos_); dfree(seg_pos_);
   dfree(part_c_); dfree(chunk_beg_); dfree(chunk_end_); dfree(seg_beg_); dfree(seg_end_);
   dfree(part_g_);
@@ -577,6 +583,9 @@ int Engine::init(int64_t nv0, int64_t nnz0) {
   TRY(alloc(&hub_occ_off_, n)); TRY(alloc(&hub_seg_beg_, n)); TRY(alloc(&hub_seg_end_, n));
   TRY(alloc(&hub_cnt_, n)); TRY(alloc(&hub_self_, n)); TRY(alloc(&hub_ownw_, n));
   TRY(alloc(&hub_left_, n)); TRY(alloc(&hub_big_, n));
+  TRY(alloc(&hub_segs_left_, n)); TRY(alloc(&hub_state_, n)); TRY(alloc(&hub_err_, 1));
+  CK(cudaMemsetAsync(hub_state_, 0, n * sizeof(uint32_t), s_));
+  CK(cudaMemsetAsync(hub_err_, 0, sizeof(int32_t), s_));
   CK(cudaMemsetAsync(hub_cnt_, 0, n * sizeof(int32_t), s_));
   CK(cudaMemsetAsync(hub_big_, 0, n * sizeof(int32_t), s_));
   CK(cudaMemsetAsync(hub_self_, 0, n * sizeof(double), s_));
@@ -1088,6 +1097,11 @@ int Engine::group_classes(const Level &L, int ncolors, std::vector<ClassSched> *
   dfree(key);
   TRY(rc);
   relaxed_ = true;
+  {
+    std::vector<int> members_per_group(ngroups, 0);
+    for (int c = 0; c < ncolors; ++c) ++members_per_group[map[c]];
+    for (ClassSched &cs : *sched) cs.relaxed = cs.color < ngroups && members_per_group[cs.color] > 1;
+  }
   if (getenv("GRAPPOLO_B200_DEBUG"))
     fprintf(stderr, "grappolo_b200: %d colour classes run in %zu steps (%d merged)\n",
             ngroups + merged, sched->size(), merged);
@@ -1111,11 +1125,13 @@ __global__ void k_scatter_i64(int64_t n, const int32_t *pos, const int64_t *val,
 }
 
 __global__ void k_hub_chunk_counts(int64_t n, const int32_t *pos, const int32_t *members,
-                                   const int64_t *ptr, int32_t *left) {
+                                   const int64_t *ptr, const int64_t *seg_beg,
+                                   const int64_t *seg_end, int32_t *left, int32_t *segs_left) {
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
        k += (int64_t)gridDim.x * blockDim.x) {
     const int32_t v = members[pos[k]];
     left[pos[k]] = (int32_t)((ptr[v + 1] - ptr[v] + kHubChunk - 1) / kHubChunk);
+    segs_left[pos[k]] = (int32_t)(seg_end[pos[k]] - seg_beg[pos[k]]);
   }
 }
 
@@ -1298,7 +1314,7 @@ int Engine::hub_offsets(const Level &L, std::vector<ClassSched> &sched) {
     LAUNCH(k_scatter_i64, grid_for(nh, 256, nsm_ * 4), 256, 0, s_, nh, d_pos, d_vals + 3 * nh,
            hub_seg_end_);
     LAUNCH(k_hub_chunk_counts, grid_for(nh, 256, nsm_ * 4), 256, 0, s_, nh, d_pos, members_, L.ptr,
-           hub_left_);
+           hub_seg_beg_, hub_seg_end_, hub_left_, hub_segs_left_);
   }
   CK(cudaStreamSynchronize(s_));
   dfree(d_pos);
@@ -1488,8 +1504,12 @@ int Engine::coloring_phase(const Level &L, int ncolors, bool stale, double lower
   std::vector<ClassSched> sched;
   TRY(build_schedule(L, color_, ncolors, d_sub, nsub, &sched));
   relaxed_ = false;
-  if (nsub == 1 && core_color_ < ncolors) relaxed_ = true;  // core batches
-  else if (nsub == 1 && persistent()) TRY(group_classes(L, ncolors, &sched));
+  if (nsub == 1 && core_color_ < ncolors) {  // core batches
+    relaxed_ = true;
+    for (ClassSched &cs : sched) cs.relaxed = cs.color >= core_color_;
+  } else if (nsub == 1 && persistent()) {
+    TRY(group_classes(L, ncolors, &sched));
+  }
   if (debug) { cudaStreamSynchronize(s_); fprintf(stderr, "grappolo_b200: schedule %.4f s\n", now_s() - td); }
   dfree(d_sub);
   const bool ord = ordered();
@@ -1511,6 +1531,7 @@ int Engine::coloring_phase(const Level &L, int ncolors, bool stale, double lower
   a.hub_keys = hub_keys_; a.hub_vals = hub_vals_; a.hub_off = hub_off_;
   CK(cudaMemcpyAsync(&a.constant, cst, sizeof(double), cudaMemcpyDeviceToHost, s_));
   CK(cudaStreamSynchronize(s_));
+  a.defer_c = (relaxed_ && persistent()) ? 1 : 0;
   if (persistent()) return run_persistent(L, sched, a, false, lower, thresh, mod, itr);
   cudaGraphExec_t exec = nullptr;
   long nodes = 0;
@@ -1744,8 +1765,6 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
   int64_t *d_ctr = nullptr;
   TRY(alloc(&d_steps, steps.size()));
   TRY(alloc(&d_ctr, 2 * steps.size()));  // block and team queues of every step
-  dfree(step_big_);
-  TRY(alloc(&step_big_, steps.size()));
   TRY(upload(s_, d_steps, steps));
   int64_t *d_cls_b = nullptr;
   int32_t *d_kept = nullptr;
@@ -1763,7 +1782,7 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
   }
   IterArgs p{};
   p.a = a;
-  p.h = hub_work();  // after step_big_ exists
+  p.h = hub_work();
   p.steps = d_steps;
   p.nsteps = (int)steps.size();
   p.jacobi = jacobi ? 1 : 0;
@@ -1785,10 +1804,51 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
   // GRAPPOLO_B200_CHECK_MODULARITY=1 runs both and fails when they differ.
   const char *fm = getenv("GRAPPOLO_B200_FULL_MODULARITY");
   const bool check_exx = getenv("GRAPPOLO_B200_CHECK_MODULARITY") != nullptr;
-  // (a step that runs several classes moves neighbours together, and the
-  // carried change of each move assumes its neighbours stay put)
-  const bool carry_exx = !jacobi && !bt && !ordered() && !integral && !relaxed_ &&
-                         !(fm && fm[0] == '1') && L.nnz > 0;
+  bool carry_exx = !jacobi && !bt && !ordered() && !integral && !(fm && fm[0] == '1') &&
+                   L.nnz > 0;
+  // A step that runs several classes (a core batch) moves neighbours together,
+  // and the carried change of each move assumes its neighbours stay put: the
+  // entries whose two ends share such a step correct the carried sum.  When
+  // they are too many to list, the phase takes the full pass instead.
+  int32_t *step_of = nullptr, *pos_of = nullptr, *pair_u = nullptr, *pair_t = nullptr;
+  double *pair_w = nullptr;
+  int64_t npairs = 0;
+  if (carry_exx && relaxed_) {
+    std::vector<uint8_t> rel(sched.size());
+    for (size_t k = 0; k < sched.size(); ++k) rel[k] = sched[k].relaxed ? 1 : 0;
+    uint8_t *d_rel;
+    int64_t *d_cb;
+    unsigned long long *d_cnt;
+    const int64_t cap = std::max<int64_t>(int64_t(1) << 20, L.nnz / 16);
+    TRY(alloc(&step_of, L.nv)); TRY(alloc(&pos_of, L.nv));
+    TRY(alloc(&d_rel, sched.size())); TRY(alloc(&d_cb, sched.size())); TRY(alloc(&d_cnt, 1));
+    TRY(alloc(&pair_u, cap)); TRY(alloc(&pair_t, cap)); TRY(alloc(&pair_w, cap));
+    TRY(upload(s_, d_rel, rel));
+    TRY(upload(s_, d_cb, cls_b));
+    CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), s_));
+    LAUNCH(k_member_steps, grid_for(nmem, 256, nsm_ * 16), 256, 0, s_, nmem, members_,
+           (int)sched.size(), d_cb, step_of, pos_of);
+    LAUNCH(k_step_pairs, std::max(1, (int)std::min<int64_t>(merge_tiles(L.nv, L.nnz), nsm_ * 8)),
+           256, 0, s_, L.nv, L.nnz, L.ptr, L.tail, L.w, step_of, d_rel, pos_of, split_row_, cap,
+           pair_u, pair_t, pair_w, d_cnt);
+    unsigned long long hc = 0;
+    CK(cudaMemcpyAsync(&hc, d_cnt, sizeof(hc), cudaMemcpyDeviceToHost, s_));
+    CK(cudaStreamSynchronize(s_));
+    dfree(d_rel); dfree(d_cb); dfree(d_cnt); dfree(step_of); dfree(pos_of);
+    if ((int64_t)hc <= cap) {
+      npairs = (int64_t)hc;
+    } else {
+      carry_exx = false;
+      dfree(pair_u); dfree(pair_t); dfree(pair_w);
+    }
+    if (getenv("GRAPPOLO_B200_DEBUG"))
+      fprintf(stderr, "grappolo_b200: %llu same-step entries (cap %ld)%s\n", hc, (long)cap,
+              carry_exx ? "" : ": full modularity passes");
+  }
+  p.pair_u = pair_u;
+  p.pair_t = pair_t;
+  p.pair_w = pair_w;
+  p.npairs = npairs;
 
   if (bt) {
     p.gid = bt->gid;
@@ -1891,17 +1951,21 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
     }
     p.exx_mode = (carry_exx && n >= 2) ? (check_exx ? 2 : 1) : 0;
     cudaError_t e = cudaMemsetAsync(d_ctr, 0, 2 * steps.size() * sizeof(int64_t), s_);
-    if (e == cudaSuccess) e = cudaMemsetAsync(step_big_, 0, steps.size() * sizeof(int32_t), s_);
+    p.h.epoch = ++epoch_;
     if (e0) cudaEventRecord(e0, s_);
     if (e == cudaSuccess)
       e = cudaLaunchCooperativeKernel((void *)k_sweep_iteration, grid, kPersistThreads, args,
                                       kPersistSmem, s_);
     if (e1) cudaEventRecord(e1, s_);
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(h_mod_, mod_out_, 4 * sizeof(double), cudaMemcpyDeviceToHost, s_);
+      e = cudaMemcpyAsync(h_mod_, mod_out_, 5 * sizeof(double), cudaMemcpyDeviceToHost, s_);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s_);
     t_sweep += now_s() - t0;
     if (e != cudaSuccess) { g_err = cudaGetErrorString(e); rc = GLV_ERR_CUDA; break; }
+    if (h_mod_[4] != 0.0) {
+      rc = fail(GLV_ERR_CUDA, "sweep: a hub's table scan gave up waiting for its chunks");
+      break;
+    }
     if (p.exx_mode == 2) {
       const double carried = h_mod_[1], full = h_mod_[3];
       if (debug)
@@ -2044,6 +2108,7 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
   }
   dfree(d_trace);
   dfree(d_ctr);
+  dfree(pair_u); dfree(pair_t); dfree(pair_w);
   dfree(d_cls_b);
   dfree(d_kept);
   dfree(exx_buf);

@@ -10,11 +10,11 @@
 //            block; rows of 128..1023 entries per 128-thread team (shared
 //            tables); then warp items (rows <= 32 entries, and 33..127-entry
 //            rows with a per-warp shared table)                  -> grid barrier
-//   stage 2  hub table segments -> partial arg-maxes            -> grid barrier
-//   stage 3  one warp per hub folds its partials                -> grid barrier
-//   stage 4  community totals += the class's deltas             -> grid barrier
-// (stages 2-3 only for classes with hubs; stage 4 after the class's last
-// sublevel), then the modularity pass of the iteration.
+//            (a hub with more filled slots than its last chunk's block
+//            scans is decided by scan-segment tasks of the same queue)
+//   stage 2  community totals += the class's deltas             -> grid barrier
+// (stage 2 after the class's last sublevel), then the modularity pass of the
+// iteration.
 #pragma once
 
 #include <cooperative_groups.h>
@@ -60,6 +60,14 @@ struct IterArgs {
   // and the full pass's e_xx in mod_out[3] (a self-check)
   int exx_mode;
   double *exx_state;
+  // Carried e_xx with classes that are not independent sets (core batches):
+  // the CSR entries (member slot of u, member slot of t, w) whose two ends
+  // run in the same step.  Each move's change 2 (e_iy - e_ix) assumes its
+  // neighbours stay; for such an entry whose two ends both moved the carried
+  // sum is corrected by w ([y_u == y_t] + [x_u == x_t] - [y_u == x_t] - [x_u == y_t]).
+  const int32_t *pair_u, *pair_t;
+  const double *pair_w;
+  int64_t npairs;
 };
 
 // Gated or batched sweeps: kept[c] = 1 when some member of colour class c is
@@ -110,6 +118,11 @@ __device__ __forceinline__ void apply_deltas_range(const IterArgs &p, int64_t b,
                                                    int64_t gt, int64_t ngt) {
   for (int64_t pos = b + gt; pos < e; pos += ngt) {
     const int32_t o = p.a.move_old[pos];
+    if (p.a.defer_c) {
+      // deferred decisions: moves, and isolated vertices leaving every community
+      const int32_t n = p.a.move_new[pos];
+      if (o >= 0 || n < 0) p.a.C[p.a.members[pos]] = n;
+    }
     if (o < 0) continue;
     const int32_t cs[2] = {p.a.move_new[pos], o};
 #pragma unroll
@@ -157,7 +170,7 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
   __shared__ double s_self[32], s_g[32], sh[32];
   __shared__ int32_t s_c[32];
   const int warp = threadIdx.x >> 5, nwb = blockDim.x >> 5;
-  const int64_t gw = (int64_t)blockIdx.x * nwb + warp, ngw = (int64_t)gridDim.x * nwb;
+  const int64_t ngw = (int64_t)gridDim.x * nwb;
   // warps numbered across blocks first: a step with few warp items spreads over SMs
   const int64_t gwi = (int64_t)warp * gridDim.x + blockIdx.x;
   const int64_t gt = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -175,6 +188,7 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
   __shared__ int64_t s_task;
   __shared__ int64_t s_team_task[kPersistThreads / kTeamThreads];
   __shared__ int s_flag;
+  __shared__ uint32_t s_word;
   // this block's slot of the moves' e_xx changes (only this block writes it)
   if (p.a.exx_delta && threadIdx.x == 0) p.a.exx_delta[blockIdx.x] = 0.0;
   for (int s = 0; s < p.nsteps; ++s) {
@@ -195,24 +209,29 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
     const int64_t witems = i4 + i8 + i16 + n32 + nw;
     const int64_t t_hub = st.hub_chunk[1] - st.hub_chunk[0];
     const int64_t t_blk = st.seg[BIN_BLOCK + 1] - st.seg[BIN_BLOCK];
+    const int64_t t_seg = st.hub_segs[1] - st.hub_segs[0];
     const int64_t n256 = st.seg[BIN_T256 + 1] - st.seg[BIN_T256];
     const int64_t n128 = st.seg[BIN_T128 + 1] - st.seg[BIN_T128];
-    if (t_hub + t_blk > 0) {
+    if (t_hub + t_blk + t_seg > 0) {
+      // hub chunks, then block rows, then hub scan segments (which wait for
+      // their hub's chunks: every chunk is handed out before any segment)
       while (true) {
         if (threadIdx.x == 0)
           s_task = atomicAdd((unsigned long long *)&p.task_ctr[2 * s], 1ull);
         __syncthreads();
         int64_t t = s_task;
         __syncthreads();
-        if (t >= t_hub + t_blk) break;
+        if (t >= t_hub + t_blk + t_seg) break;
         if (t < t_hub) {
           hub_accum_chunk(p.a, p.h, st.hub_chunk[0] + t,
                           reinterpret_cast<int32_t *>(tvals + kPersistTableCap), tvals, s_self,
                           s_g, s_c, &s_flag, s);
-        } else {
+        } else if (t < t_hub + t_blk) {
           team_vertex<512>(p.a, st.seg[BIN_BLOCK] + (t - t_hub),
                            reinterpret_cast<int32_t *>(tvals + kPersistTableCap), tvals, 0, s_self,
                            s_g, s_c);
+        } else {
+          hub_segment_task(p.a, p.h, st.hub_segs[0] + (t - t_hub - t_blk), s_g, s_c, &s_word);
         }
       }
     }
@@ -243,16 +262,6 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
     }
     grid.sync();
     GLV_TRACE(4 * s);
-    if (st.hub_segs[1] > st.hub_segs[0] && __ldcg(&p.h.step_big[s])) {
-      for (int64_t si = st.hub_segs[0] + blockIdx.x; si < st.hub_segs[1]; si += gridDim.x)
-        hub_scan_segment(p.a, p.h, si, s_g, s_c);
-      grid.sync();
-      GLV_TRACE(4 * s + 1);
-      for (int64_t pos = st.seg[BIN_HUB] + gw; pos < st.seg[BIN_HUB + 1]; pos += ngw)
-        hub_final(p.a, p.h, pos);
-      grid.sync();
-      GLV_TRACE(4 * s + 2);
-    }
     if (!p.jacobi && st.apply[1] > st.apply[0]) {
       apply_deltas_range(p, st.apply[0], st.apply[1], gt, ngt);
       grid.sync();
@@ -265,6 +274,21 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
     const int64_t ntiles = merge_tiles(p.nv, p.nnz);
     MergeSmem *msm = reinterpret_cast<MergeSmem *>(smem_raw);
     __syncthreads();  // stage-1 tables in the same shared memory are done
+    if (p.exx_mode >= 1 && p.npairs > 0) {
+      // same-step entries whose two ends both moved (see IterArgs::pair_u)
+      double corr = 0.0;
+      for (int64_t k = gt; k < p.npairs; k += ngt) {
+        const int32_t pu = p.pair_u[k], pt = p.pair_t[k];
+        const int32_t xu = p.a.move_old[pu], xt = p.a.move_old[pt];
+        if (xu < 0 || xt < 0) continue;
+        const int32_t yu = p.a.move_new[pu], yt = p.a.move_new[pt];
+        const int f = (yu == yt) + (xu == xt) - (yu == xt) - (xu == yt);
+        if (f != 0) corr = __dadd_rn(corr, __dmul_rn((double)f, p.pair_w[k]));
+      }
+      corr = block_sum<kPersistThreads>(corr, sh);
+      if (threadIdx.x == 0 && corr != 0.0) p.a.exx_delta[blockIdx.x] += corr;
+      __syncthreads();
+    }
     if (p.exx_mode == 1) {
       // e_xx is carried: only a2 = sum of cDeg^2 over the level
       for (int64_t c = gt; c < p.nv; c += ngt) a2 = __dadd_rn(a2, __dmul_rn(p.cDeg[c], p.cDeg[c]));
@@ -291,7 +315,10 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
   }
   grid.sync();
   GLV_TRACE(4 * p.nsteps + 1);
-  if (blockIdx.x == 0 && !p.gid) modularity_fold(p, gridDim.x, sh);
+  if (blockIdx.x == 0) {
+    if (!p.gid) modularity_fold(p, gridDim.x, sh);
+    if (threadIdx.x == 0) p.mod_out[4] = (double)__ldcg(p.h.err);
+  }
   if (p.jacobi && p.nsteps > 0) {
     // Q above used the totals before the moves; now take the moves' deltas.
     apply_deltas_range(p, p.steps[0].apply[0], p.steps[p.nsteps - 1].apply[1], gt, ngt);

@@ -298,6 +298,79 @@ __global__ void __launch_bounds__(256) k_modularity_merge(int64_t nv, int64_t nn
   if (threadIdx.x == 0) { part_e[blockIdx.x] = ex; part_a[blockIdx.x] = a2; }
 }
 
+// The CSR entries (i -> t, i != t) whose two ends run in the same relaxed
+// sweep step (step_of[i] == step_of[t] and relaxed[step_of[i]]), as member
+// slots (pos_of) and weight, appended at *count up to `cap` (count keeps
+// growing past cap, so the caller sees an overflow).  Merge-path tiles: hub
+// rows spread over many blocks.
+__global__ void __launch_bounds__(256) k_step_pairs(int64_t nv, int64_t nnz, const int64_t *ptr,
+                                                    const int32_t *tail, const double *w,
+                                                    const int32_t *step_of,
+                                                    const uint8_t *relaxed,
+                                                    const int32_t *pos_of,
+                                                    const int64_t *split_row, int64_t cap,
+                                                    int32_t *pu, int32_t *pt, double *pw,
+                                                    unsigned long long *count) {
+  __shared__ MergeSmem sm;
+  const int64_t ntiles = merge_tiles(nv, nnz);
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t d0 = tile * (int64_t)kMergeTile;
+    const int64_t d1 = min(d0 + (int64_t)kMergeTile, nv + nnz);
+    const int64_t i0 = split_row[tile], i1 = split_row[tile + 1];
+    const int64_t j0 = d0 - i0, j1 = d1 - i1;
+    if (j1 <= j0) continue;  // tile-uniform
+    const int64_t ih = min(i1, nv - 1);
+    const int nr = (int)(ih - i0 + 1);
+    __syncthreads();
+    for (int k = threadIdx.x; k <= nr; k += blockDim.x) {
+      const int64_t r = ptr[i0 + k] - j0;
+      sm.off[k] = (int32_t)max((int64_t)0, min(r, (int64_t)kMergeTile + 1));
+    }
+    // the row's step, or -1 when the step is an independent set
+    for (int k = threadIdx.x; k < nr; k += blockDim.x) {
+      const int32_t st = step_of[i0 + k];
+      sm.comm[k] = (st >= 0 && relaxed[st]) ? st : -1;
+    }
+    __syncthreads();
+    const int ne = (int)(j1 - j0);
+    for (int q = threadIdx.x; q < ne; q += blockDim.x) {
+      int lo = 0, hi = nr - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (sm.off[mid] <= q) lo = mid; else hi = mid - 1;
+      }
+      const int32_t st = sm.comm[lo];
+      if (st < 0) continue;
+      const int64_t e = j0 + q;
+      const int32_t t = tail[e];
+      const int64_t i = i0 + lo;
+      if (t == (int32_t)i || step_of[t] != st) continue;
+      const unsigned long long k = atomicAdd(count, 1ull);
+      if ((int64_t)k < cap) {
+        pu[k] = pos_of[i];
+        pt[k] = pos_of[t];
+        pw[k] = w[e];
+      }
+    }
+  }
+}
+
+// step_of[members[pos]] = the step (class) holding pos, pos_of[members[pos]] = pos.
+__global__ void k_member_steps(int64_t nmem, const int32_t *members, int nclass,
+                               const int64_t *cls_begin, int32_t *step_of, int32_t *pos_of) {
+  for (int64_t pos = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; pos < nmem;
+       pos += (int64_t)gridDim.x * blockDim.x) {
+    int lo = 0, hi = nclass - 1;  // last class starting at or before pos
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (cls_begin[mid] <= pos) lo = mid; else hi = mid - 1;
+    }
+    const int32_t v = members[pos];
+    step_of[v] = lo;
+    pos_of[v] = (int32_t)pos;
+  }
+}
+
 // out[0] = Q, out[1] = e_xx, out[2] = a2_x.  `cst` = {constant, 2m}.
 __global__ void __launch_bounds__(256) k_modularity_final(int nparts, const double *part_e,
                                                           const double *part_a, const double *cst,

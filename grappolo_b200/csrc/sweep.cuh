@@ -49,6 +49,10 @@ struct SweepArgs {
   // per block: sum over the moves of 2 (e_iy - e_ix), the change each move
   // makes to the modularity's internal-weight term (nullptr = not tracked)
   double *exx_delta;
+  // colour phases whose classes include batches of the core: decisions reach
+  // C only after their step (the apply stage), so every member of a step
+  // decides against the communities its step started from
+  int defer_c;
 };
 
 __device__ __forceinline__ bool skipped(const SweepArgs &a, int32_t v) {
@@ -79,7 +83,7 @@ __device__ __forceinline__ void emit_decision(const SweepArgs &a, int64_t pos, i
   if (a.target) {
     a.target[v] = target;
     if (a.own_w) a.own_w[v] = own_w;
-  } else {
+  } else if (!a.defer_c) {
     a.C[v] = target;
   }
   bool moved = (target != own) && (target != -1);
@@ -510,7 +514,13 @@ struct HubWork {
   const int64_t *hub_seg_beg, *hub_seg_end;  // per member slot: its segments
   int32_t *chunks_left;     // per member slot: chunks still accumulating
   int32_t *big;             // per member slot: 1 = decided by the segment scan
-  int32_t *step_big;        // per step: some hub of the step is big (persistent kernel)
+  int32_t *step_big;        // per step: some hub of the step is big (unused by the persistent kernel)
+  // persistent kernel: segments are tasks of their step that wait for the
+  // hub's chunks; the last segment to finish decides the hub
+  int32_t *segs_left;       // per member slot: segments not yet scanned
+  uint32_t *state;          // per member slot: 4 * epoch + 1 decided, + 2 segments needed
+  uint32_t epoch;           // this launch (0: the launch-per-kernel path, big[] instead)
+  int32_t *err;             // set when a segment's wait gives up
 };
 
 constexpr int kHubChunk = 2048;      // CSR entries per accumulation work item
@@ -651,6 +661,10 @@ __device__ __forceinline__ void hub_accum_chunk(const SweepArgs &a, const HubWor
     if (threadIdx.x == 0) {
       emit_stay(a, pos, v, a.C[v]);
       h.chunks_left[pos] = (int32_t)((a.ptr[v + 1] - a.ptr[v] + kHubChunk - 1) / kHubChunk);
+      if (h.epoch) {
+        __threadfence();
+        atomicExch(&h.state[pos], 4u * h.epoch + 1u);
+      }
     }
     __syncthreads();
     return;
@@ -663,8 +677,12 @@ __device__ __forceinline__ void hub_accum_chunk(const SweepArgs &a, const HubWor
   const int32_t nfill = __ldcg(&h.cnt[pos]);
   if (nfill > kHubInlineCap) {
     if (threadIdx.x == 0) {
-      h.big[pos] = 1;
-      if (step >= 0) atomicOr(&h.step_big[step], 1);
+      if (h.epoch) {
+        atomicExch(&h.state[pos], 4u * h.epoch + 2u);  // its segment tasks decide it
+      } else {
+        h.big[pos] = 1;
+        if (step >= 0) atomicOr(&h.step_big[step], 1);
+      }
     }
     __syncthreads();
     return;
@@ -687,8 +705,93 @@ __device__ __forceinline__ void hub_accum_chunk(const SweepArgs &a, const HubWor
     h.self_w[pos] = 0.0;
     h.own_w[pos] = 0.0;
     h.chunks_left[pos] = (int32_t)((a.ptr[v + 1] - a.ptr[v] + kHubChunk - 1) / kHubChunk);
+    if (h.epoch) {
+      __threadfence();
+      atomicExch(&h.state[pos], 4u * h.epoch + 1u);
+    }
   }
   __syncthreads();
+}
+
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+constexpr uint32_t kSpinLimit = 1u << 22;  // polls of a segment's wait (x >= 128 ns)
+
+// Persistent kernel: one scan segment of a hub as a block task (all threads
+// call).  Segments are queued after every chunk of their step and a chunk
+// never waits, so the wait ends once the hub's chunks are folded.  The last
+// segment to finish folds the partial arg-maxes and decides the hub.
+__device__ __forceinline__ void hub_segment_task(const SweepArgs &a, const HubWork &h, int64_t si,
+                                                 double *s_g, int32_t *s_c, uint32_t *s_word) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwb = blockDim.x >> 5;
+  const int32_t pos = h.seg_pos[si];
+  const uint32_t decided = 4u * h.epoch + 1u;
+  if (threadIdx.x == 0) {
+    uint32_t st, it = 0;
+    while ((st = ld_acquire(&h.state[pos])) < decided) {
+      if (++it > kSpinLimit) {
+        atomicExch(h.err, 1);
+        st = 0;
+        break;
+      }
+      __nanosleep(128);
+    }
+    s_word[0] = st;
+  }
+  __syncthreads();
+  const uint32_t st = s_word[0];
+  __syncthreads();
+  if (st != decided + 1u) return;  // decided by its last chunk (block-uniform)
+  const int32_t v = a.members[pos];
+  const int32_t own = a.C[v];
+  const double degree = a.vDeg[v];
+  const double own_w = __ldcg(&h.own_w[pos]);
+  const double eix = __dsub_rn(own_w, __ldcg(&h.self_w[pos]));
+  const double ax = __dsub_rn(a.cDeg[own], degree);
+  int32_t *keys = h.keys + h.tab_off[pos];
+  double *vals = h.vals + h.tab_off[pos];
+  const int32_t *occ = h.occ + h.occ_off[pos];
+  const int64_t ob = h.seg_beg[si];
+  const int64_t oe = min(h.seg_end[si], (int64_t)__ldcg(&h.cnt[pos]));
+  double g = 0.0;
+  int32_t bc = INT32_MAX;
+  if (ob < oe) hub_scan_slots(a, keys, vals, occ, ob, oe, own, eix, ax, degree, cst_of(a, v), g, bc);
+  warp_argmax(g, bc);
+  if (lane == 0) { s_g[warp] = g; s_c[warp] = bc; }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int k = 1; k < nwb; ++k)
+      if (better(s_g[k], s_c[k], g, bc)) { g = s_g[k]; bc = s_c[k]; }
+    h.part_g[si] = g;
+    h.part_c[si] = bc;
+    __threadfence();
+    s_word[0] = (atomicSub(&h.segs_left[pos], 1) == 1) ? 1u : 0u;
+  }
+  __syncthreads();
+  const bool last = s_word[0] != 0;
+  __syncthreads();
+  if (!last || warp != 0) return;
+  __threadfence();
+  g = 0.0;
+  bc = INT32_MAX;
+  for (int64_t k = h.hub_seg_beg[pos] + lane; k < h.hub_seg_end[pos]; k += 32) {
+    const double pg = __ldcg(&h.part_g[k]);
+    const int32_t pc = __ldcg(&h.part_c[k]);
+    if (better(pg, pc, g, bc)) { g = pg; bc = pc; }
+  }
+  warp_argmax(g, bc);
+  if (lane == 0) {
+    emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), degree, own_w, g);
+    h.cnt[pos] = 0;
+    h.self_w[pos] = 0.0;
+    h.own_w[pos] = 0.0;
+    h.chunks_left[pos] = (int32_t)((a.ptr[v + 1] - a.ptr[v] + kHubChunk - 1) / kHubChunk);
+    h.segs_left[pos] = (int32_t)(h.hub_seg_end[pos] - h.hub_seg_beg[pos]);
+  }
 }
 
 // All threads of the block call; s_g/s_c are 32-entry block scratch.

@@ -69,6 +69,9 @@ def test_final_modularity_within_reference_range(name, mode, oracle):
     lo, hi = pin['printed_range']
     q = st['final_modularity']
     assert _within(q, lo, hi), (name, mode, q, lo, hi)
+    # isolated vertices belong to no community (Coloring/runMultiPhaseColoring.cpp:141)
+    deg = np.diff(g.ptr)
+    assert np.all(C[deg == 0] == -1) and np.all(C[deg > 0] >= 0)
     # the modularity of the returned community array over the input graph,
     # against the same quantity of the reference's runs
     q_c = oracle.modularity(g, C)
