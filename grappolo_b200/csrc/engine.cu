@@ -894,6 +894,8 @@ int Engine::color_spec(const Level &L, int *ncolors, int64_t core_deg, int core_
   }
   *ncolors = hm + 1;
   if (hcore > 0) {
+    // (fewer batches for small cores cost modularity on planted power-law
+    // graphs and saved no time: every core keeps core_batches steps)
     const int nb = (int)std::min<unsigned long long>(hcore, (unsigned long long)core_batches);
     if (*ncolors + nb > kMaxColors) {
       dfree(wl); dfree(bl); dfree(nx); dfree(cnt); dfree(status); dfree(maxc); dfree(ncore);

@@ -524,7 +524,7 @@ struct HubWork {
 };
 
 constexpr int kHubChunk = 2048;      // CSR entries per accumulation work item
-constexpr int kHubSeg = 2048;        // filled slots per scan work item
+constexpr int kHubSeg = 8192;        // filled slots per scan work item
 constexpr int kHubStageCap = 4096;   // block-local staging table of one chunk
 constexpr int kHubInlineCap = 4096;  // filled slots the last chunk's block scans itself
 constexpr int kHubBatch = 4;         // table slots a thread has in flight at once
