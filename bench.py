@@ -47,6 +47,10 @@ def parse_args():
     p.add_argument('--mode', choices=['fast', 'verify', 'learned'], default='fast')
     p.add_argument('--no-e2e', action='store_true')
     p.add_argument('--no-cpu-baseline', action='store_true')
+    p.add_argument('--no-learned', action='store_true',
+                   help='rmat workload: skip the learned-gate comparison runs')
+    p.add_argument('--full-run-scale', type=int, default=20,
+                   help='R-MAT scale of the reference full-run sample in cpu_baseline')
     p.add_argument('--profile-level', type=int, default=1,
                    help='1: time each class sweep (roofline); 2: time every launch by kind')
     p.add_argument('--workload', choices=['rmat', 'powerlaw', 'batch', 'csr', 'compare'],
@@ -781,9 +785,17 @@ def main():
                'transfer_s_per_step': statistics.mean(s['time_transfer'] for s in est)}
         del aos, hptr, hC
 
+    # time-to-modularity, learned gate vs plain, on the same graph
+    learned_cmp = None
+    if args.mode == 'fast' and args.workload == 'rmat' and not args.no_learned:
+        learned_cmp = learned_vs_plain(L, nv, ptr, tail, w, C, stats, t / args.steps,
+                                       args.steps, dev)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(ptr, tail, w)
+        if args.workload == 'rmat':
+            cpu['full_run'] = reference_full_run(args.full_run_scale)
 
     peak, peak_kind = measured_peak()
     achieved = (sweep_b / sweep_t) / 1e9 if sweep_t > 0 else None
@@ -818,6 +830,7 @@ def main():
                               'renumber+coarsen': s0['time_building'],
                               'other': s0['time_total'] - s0['time_clustering']
                               - s0['time_coloring'] - s0['time_building']},
+             'learned': learned_cmp,
              'step_totals_s': [round(s['time_total'], 4) for s in stats],
              'step_splits_s': [[round(s[k], 4) for k in ('time_clustering', 'time_coloring',
                                                          'time_building')] for s in stats]}
@@ -832,6 +845,69 @@ def main():
     if dist:
         dist.destroy_process_group()
     return 0
+
+
+def learned_vs_plain(L, nv, ptr, tail, w, C, plain_stats, plain_s, steps, dev):
+    """The learned gate (shipped parameters) on the same graph as the plain
+    timed runs: device time per full run, final Q and entries evaluated."""
+    import torch
+    from grappolo_b200 import _lib, gate, louvain
+    params, tau = gate.load_default()
+    gate.set_gate(params, tau)
+
+    def run():
+        return louvain.run_multiphase_device(nv, ptr.data_ptr(), tail.data_ptr(), w.data_ptr(),
+                                             C.data_ptr(), coloring=True,
+                                             mode=_lib.GLV_MODE_LEARNED,
+                                             stream=torch.cuda.current_stream().cuda_stream)
+    run()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    st = [run() for _ in range(steps)]
+    ev1.record()
+    torch.cuda.synchronize()
+    lt = ev0.elapsed_time(ev1) * 1e-3 / steps
+    q_plain = statistics.median(s['final_modularity'] for s in plain_stats)
+    q_learned = statistics.median(s['final_modularity'] for s in st)
+    return {'gate_tau': tau, 'plain_s_per_run': plain_s, 'learned_s_per_run': lt,
+            'time_ratio_learned_over_plain': lt / plain_s,
+            'q_plain_median': q_plain, 'q_learned_median': q_learned,
+            'dq': q_learned - q_plain,
+            'entries_plain_per_run': statistics.mean(s['edges_swept'] for s in plain_stats),
+            'entries_learned_per_run': statistics.mean(s['edges_swept'] for s in st),
+            'iterations_plain': plain_stats[-1]['total_iterations'],
+            'iterations_learned': st[-1]['total_iterations']}
+
+
+def reference_full_run(scale):
+    """Time to modularity of the reference itself: Grappolo's
+    runMultiPhaseColoring (oracle/_ref, shipped -Ofast flags, all host cores;
+    Coloring/runMultiPhaseColoring.cpp:51-238) on the seeded numpy R-MAT graph
+    of the given scale, beside this engine's fast mode on the same graph."""
+    from grappolo_b200 import _lib, graphs, louvain
+    from oracle import Reference
+    g = graphs.rmat(scale, seed=1)
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    _, s, _ = Reference(fast=True).run_multiphase_coloring(g, nthreads=cores)
+    ref_wall = time.perf_counter() - t0
+    louvain.run_multiphase_csr(g, coloring=True, mode=_lib.GLV_MODE_FAST)  # warm
+    t0 = time.perf_counter()
+    _, st = louvain.run_multiphase_csr(g, coloring=True, mode=_lib.GLV_MODE_FAST)
+    gpu_wall = time.perf_counter() - t0
+    return {'graph': f'R-MAT scale {scale}, edge factor 16, a=0.57 b=0.19 c=0.19, FP64 '
+                     f'weights U(0,1], numpy seed 1 ({g.num_vertices} vertices, {g.nnz} '
+                     f'CSR entries)',
+            'reference': {'threads': cores, 'total_time_s': s.get('total_time'),
+                          'wall_s': ref_wall, 'final_modularity': s.get('final_mod'),
+                          'phases': s.get('phases'),
+                          'iterations': s.get('total_iterations')},
+            'gpu_fast': {'wall_s_host_csr_in': gpu_wall,
+                         'engine_total_s': st['time_total'],
+                         'final_modularity': st['final_modularity'],
+                         'phases': st['phases'], 'iterations': st['total_iterations']},
+            'time_ratio_reference_over_gpu': (s.get('total_time') or ref_wall) / gpu_wall}
 
 
 def cpu_baseline(ptr, tail, w):
