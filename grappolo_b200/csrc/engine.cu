@@ -2382,23 +2382,37 @@ int Engine::coarsen(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
   const int nb = bits_for(std::max<int64_t>(ncl - 1, 1));
   const uint64_t sentinel = 1ull << (2 * nb);
   const int end_bit = 2 * nb + 1;
-  const int64_t n = ncl + in.nnz;
-  const int g = grid_for(n, 256, nsm_ * 16);
-  if (n > crec_cap_) {
+  const int64_t n_all = ncl + in.nnz;
+  if (n_all > crec_cap_) {
     dfree(ck1_); dfree(ck2_); dfree(cv1_); dfree(cv2_);
     // sized for level 0 when that is modest, so every level reuses them
     const int64_t lvl0 = nnz0_ + nv0_;
-    crec_cap_ = lvl0 <= (int64_t(1) << 30) ? std::max<int64_t>(n, lvl0) : n;
+    crec_cap_ = lvl0 <= (int64_t(1) << 30) ? std::max<int64_t>(n_all, lvl0) : n_all;
     TRY(alloc(&ck1_, crec_cap_)); TRY(alloc(&ck2_, crec_cap_));
     TRY(alloc(&cv1_, crec_cap_)); TRY(alloc(&cv2_, crec_cap_));
   }
   uint64_t *k1 = ck1_, *k2 = ck2_;
   double *v1 = cv1_, *v2 = cv2_;
   TRY(merge_splits(in));
-  LAUNCH(k_coarse_records, std::max(1, (int)std::min<int64_t>(merge_tiles(in.nv, in.nnz),
-                                                               nsm_ * 8)),
-         256, 0, s_, in.nv, in.nnz, in.ptr, in.tail, in.w, Cm, ncl, nb, sentinel, split_row_, k1,
-         v1);
+  const int rgrid = std::max(1, (int)std::min<int64_t>(merge_tiles(in.nv, in.nnz), nsm_ * 8));
+  int64_t n = n_all;
+  if (ordered()) {
+    // every entry keeps its slot (a sentinel when it makes no record): the
+    // stable sort then leaves each pair's records in (i, j) order
+    LAUNCH(k_coarse_records, rgrid, 256, 0, s_, in.nv, in.nnz, in.ptr, in.tail, in.w, Cm, ncl, nb,
+           sentinel, split_row_, k1, v1);
+  } else {
+    unsigned long long *d_cnt;
+    TRY(alloc(&d_cnt, 1));
+    CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), s_));
+    LAUNCH(k_coarse_records_compact, rgrid, 256, 0, s_, in.nv, in.nnz, in.ptr, in.tail, in.w, Cm,
+           ncl, nb, split_row_, k1, v1, d_cnt);
+    unsigned long long hc = 0;
+    CK(cudaMemcpyAsync(&hc, d_cnt, sizeof(hc), cudaMemcpyDeviceToHost, s_));
+    CK(cudaStreamSynchronize(s_));
+    dfree(d_cnt);
+    n = ncl + (int64_t)hc;
+  }
   size_t tb = 0;
   CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, k1, k2, v1, v2, n, 0, end_bit, s_));
   TRY(temp(tb));
@@ -2408,6 +2422,7 @@ int Engine::coarsen(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
   uint64_t *ukeys;
   double *uvals;
   int64_t np = 0;
+  const int g = grid_for(n, 256, nsm_ * 16);
   if (ordered()) {
     // one thread folds each pair's records in (i, j) order
     int32_t *flag;

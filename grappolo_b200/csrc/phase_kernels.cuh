@@ -748,6 +748,69 @@ __global__ void __launch_bounds__(256) k_coarse_records(
   }
 }
 
+// The same records, only those that exist (a >= b >= 0), appended after the
+// seeds at ncl + *count in no particular order (warp-aggregated appends): for
+// the parallel folds, where the order of additions is free, the sort then
+// moves half as many records.
+__global__ void __launch_bounds__(256) k_coarse_records_compact(
+    int64_t nv, int64_t nnz, const int64_t *ptr, const int32_t *tail, const double *w,
+    const int32_t *C, int64_t ncl, int nb, const int64_t *split_row, uint64_t *keys,
+    double *vals, unsigned long long *count) {
+  for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < ncl;
+       a += (int64_t)gridDim.x * blockDim.x) {
+    keys[a] = ((uint64_t)a << nb) | (uint64_t)a;
+    vals[a] = 0.0;
+  }
+  __shared__ MergeSmem sm;
+  const int lane = threadIdx.x & 31;
+  const int64_t ntiles = merge_tiles(nv, nnz);
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t d0 = tile * (int64_t)kMergeTile;
+    const int64_t d1 = min(d0 + (int64_t)kMergeTile, nv + nnz);
+    const int64_t i0 = split_row[tile], i1 = split_row[tile + 1];
+    const int64_t j0 = d0 - i0, j1 = d1 - i1;
+    if (j1 <= j0) continue;  // tile-uniform
+    const int64_t ih = min(i1, nv - 1);
+    const int nr = (int)(ih - i0 + 1);
+    __syncthreads();
+    for (int k = threadIdx.x; k <= nr; k += blockDim.x) {
+      const int64_t r = ptr[i0 + k] - j0;
+      sm.off[k] = (int32_t)max((int64_t)0, min(r, (int64_t)kMergeTile + 1));
+    }
+    for (int k = threadIdx.x; k < nr; k += blockDim.x) sm.comm[k] = C[i0 + k];
+    __syncthreads();
+    const int ne = (int)(j1 - j0);
+    for (int q0 = 0; q0 < ne; q0 += blockDim.x) {  // every lane of a warp takes each round
+      const int q = q0 + (int)threadIdx.x;
+      bool keep = false;
+      uint64_t key = 0;
+      double val = 0.0;
+      if (q < ne) {
+        int lo = 0, hi = nr - 1;
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (sm.off[mid] <= q) lo = mid; else hi = mid - 1;
+        }
+        const int64_t e = j0 + q;
+        const int32_t a = sm.comm[lo];
+        const int32_t b = C[tail[e]];
+        keep = a >= b && b >= 0;
+        key = ((uint64_t)a << nb) | (uint64_t)(uint32_t)b;
+        val = w[e];
+      }
+      const unsigned m = __ballot_sync(FULL, keep);
+      unsigned long long base = 0;
+      if (lane == 0 && m) base = atomicAdd(count, (unsigned long long)__popc(m));
+      base = __shfl_sync(FULL, base, 0);
+      if (keep) {
+        const int64_t at = ncl + (int64_t)base + __popc(m & ((1u << lane) - 1u));
+        keys[at] = key;
+        vals[at] = val;
+      }
+    }
+  }
+}
+
 // Segment heads of the sorted records -> flags (1 at the first record of each
 // distinct key, sentinel excluded).
 __global__ void k_segment_heads(int64_t n, const uint64_t *keys, uint64_t sentinel,
@@ -796,15 +859,21 @@ __global__ void k_scatter_pairs(int64_t n, const uint64_t *keys, const double *v
 __global__ void k_row_counts(int64_t np, const uint64_t *ukeys, int nb, int64_t *lower_cnt,
                              int64_t *upper_cnt, int64_t *ne_off) {
   const uint64_t mask = (1ull << nb) - 1;
+  const int lane = threadIdx.x & 31;
+  unsigned long long off_diag = 0;  // this thread's pairs with a > b
   for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < np;
        p += (int64_t)gridDim.x * blockDim.x) {
     const int64_t a = (int64_t)(ukeys[p] >> nb), b = (int64_t)(ukeys[p] & mask);
     atomicAdd((unsigned long long *)&lower_cnt[a], 1ull);
     if (a > b) {
       atomicAdd((unsigned long long *)&upper_cnt[b], 1ull);
-      atomicAdd((unsigned long long *)ne_off, 1ull);
+      ++off_diag;
     }
   }
+  // one counter update per warp (a single counter for every pair serialised them)
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) off_diag += __shfl_xor_sync(FULL, off_diag, off);
+  if (lane == 0 && off_diag) atomicAdd((unsigned long long *)ne_off, off_diag);
 }
 
 // Lower part of each row: pairs (a, b <= a) in ascending b.  Pairs are sorted
