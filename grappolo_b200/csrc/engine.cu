@@ -2395,24 +2395,27 @@ int Engine::coarsen(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
   double *v1 = cv1_, *v2 = cv2_;
   TRY(merge_splits(in));
   const int rgrid = std::max(1, (int)std::min<int64_t>(merge_tiles(in.nv, in.nnz), nsm_ * 8));
-  int64_t n = n_all;
-  if (ordered()) {
-    // every entry keeps its slot (a sentinel when it makes no record): the
-    // stable sort then leaves each pair's records in (i, j) order
-    LAUNCH(k_coarse_records, rgrid, 256, 0, s_, in.nv, in.nnz, in.ptr, in.tail, in.w, Cm, ncl, nb,
-           sentinel, split_row_, k1, v1);
-  } else {
-    unsigned long long *d_cnt;
-    TRY(alloc(&d_cnt, 1));
-    CK(cudaMemsetAsync(d_cnt, 0, sizeof(unsigned long long), s_));
-    LAUNCH(k_coarse_records_compact, rgrid, 256, 0, s_, in.nv, in.nnz, in.ptr, in.tail, in.w, Cm,
-           ncl, nb, split_row_, k1, v1, d_cnt);
-    unsigned long long hc = 0;
-    CK(cudaMemcpyAsync(&hc, d_cnt, sizeof(hc), cudaMemcpyDeviceToHost, s_));
-    CK(cudaStreamSynchronize(s_));
-    dfree(d_cnt);
-    n = ncl + (int64_t)hc;
+  // records of the pairs that exist, in entry order (two passes over the tiles)
+  const int64_t ntiles = merge_tiles(in.nv, in.nnz);
+  int64_t *tile_cnt, *tile_off;
+  TRY(alloc(&tile_cnt, ntiles + 1)); TRY(alloc(&tile_off, ntiles + 1));
+  CK(cudaMemsetAsync(tile_cnt + ntiles, 0, sizeof(int64_t), s_));
+  LAUNCH(k_coarse_tile_counts, rgrid, 256, 0, s_, in.nv, in.nnz, in.ptr, in.tail, Cm, nb,
+         split_row_, tile_cnt);
+  {
+    size_t sb = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, sb, tile_cnt, tile_off, ntiles + 1, s_));
+    TRY(temp(sb));
+    CK(cub::DeviceScan::ExclusiveSum(temp_, sb, tile_cnt, tile_off, ntiles + 1, s_));
   }
+  LAUNCH(k_coarse_records_compact, rgrid, 256, 0, s_, in.nv, in.nnz, in.ptr, in.tail, in.w, Cm,
+         ncl, nb, split_row_, tile_off, k1, v1);
+  int64_t nrec = 0;
+  CK(cudaMemcpyAsync(&nrec, tile_off + ntiles, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  dfree(tile_cnt);
+  dfree(tile_off);
+  const int64_t n = ncl + nrec;
   size_t tb = 0;
   CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, k1, k2, v1, v2, n, 0, end_bit, s_));
   TRY(temp(tb));
@@ -2494,9 +2497,11 @@ int Engine::coarsen(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
   LAUNCH(k_emit_lower, gp, 256, 0, s_, np, ukeys, uvals, nb, o.ptr, lower_first, o.tail, o.w, tk1,
          tv1, sentinel);
   mark("emit lower");
-  CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, tk1, tk2, tv1, tv2, np, 0, end_bit, s_));
+  // stable on the b bits (and the sentinel bit) only: each b's keys already
+  // come in ascending a
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, tk1, tk2, tv1, tv2, np, nb, end_bit, s_));
   TRY(temp(tb));
-  CK(cub::DeviceRadixSort::SortPairs(temp_, tb, tk1, tk2, tv1, tv2, np, 0, end_bit, s_));
+  CK(cub::DeviceRadixSort::SortPairs(temp_, tb, tk1, tk2, tv1, tv2, np, nb, end_bit, s_));
   mark("emit sort");
   LAUNCH(k_run_first, gp, 256, 0, s_, np, tk2, nb, sentinel, upper_first);
   LAUNCH(k_emit_upper, gp, 256, 0, s_, np, tk2, tv2, nb, o.ptr, lower_cnt, upper_first, o.tail,

@@ -694,121 +694,117 @@ __global__ void k_compose(int64_t n, int32_t *C_orig, const int32_t *C, int firs
 
 // ---------------------------------------------------------------------------
 // Coarsening (Utility/buildNextPhase.cpp:83-255).  Records: one seed (a, a,
-// 0.0) per cluster, then one per CSR entry i->t with a = C[i] >= b = C[t], in
-// (i, j) order; others get the sentinel key.  A stable radix sort by
-// (a << nb) | b groups each pair with its entries still in (i, j) order.
-__global__ void __launch_bounds__(256) k_coarse_records(
-    int64_t nv, int64_t nnz, const int64_t *ptr, const int32_t *tail, const double *w,
-    const int32_t *C, int64_t ncl, int nb, uint64_t sentinel, const int64_t *split_row,
-    uint64_t *keys, double *vals) {
-  // seeds
-  for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < ncl;
-       a += (int64_t)gridDim.x * blockDim.x) {
-    keys[a] = ((uint64_t)a << nb) | (uint64_t)a;
-    vals[a] = 0.0;
-  }
-  // entries: merge-path tiles, so hub rows spread over many blocks
-  __shared__ MergeSmem sm;
-  const int64_t ntiles = merge_tiles(nv, nnz);
-  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int64_t d0 = tile * (int64_t)kMergeTile;
-    const int64_t d1 = min(d0 + (int64_t)kMergeTile, nv + nnz);
-    const int64_t i0 = split_row[tile], i1 = split_row[tile + 1];
-    const int64_t j0 = d0 - i0, j1 = d1 - i1;
-    if (j1 <= j0) continue;  // tile-uniform
+// 0.0) per cluster, then one per CSR entry i->t with a = C[i] >= b = C[t] >= 0,
+// in (i, j) order.  A stable radix sort by (a << nb) | b groups each pair with
+// its entries still in (i, j) order.  The records are written in two passes
+// over the merge tiles: k_coarse_tile_counts counts each tile's records, an
+// exclusive scan places the tiles, and k_coarse_records_compact writes each
+// tile's records at its place in entry order (the sort then moves about half
+// as many records as one slot per entry would).
+template <bool WRITE>
+__device__ __forceinline__ void coarse_tile(int64_t tile, int64_t nv, int64_t nnz,
+                                            const int64_t *ptr, const int32_t *tail,
+                                            const double *w, const int32_t *C, int nb,
+                                            const int64_t *split_row, MergeSmem *sm,
+                                            int32_t *s_warp, uint64_t *keys, double *vals,
+                                            int64_t base, int64_t *count) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwb = blockDim.x >> 5;
+  const int64_t d0 = tile * (int64_t)kMergeTile;
+  const int64_t d1 = min(d0 + (int64_t)kMergeTile, nv + nnz);
+  const int64_t i0 = split_row[tile], i1 = split_row[tile + 1];
+  const int64_t j0 = d0 - i0, j1 = d1 - i1;
+  int64_t kept = 0;
+  if (j1 > j0) {  // tile-uniform
     const int64_t ih = min(i1, nv - 1);
     const int nr = (int)(ih - i0 + 1);
     __syncthreads();
     for (int k = threadIdx.x; k <= nr; k += blockDim.x) {
       const int64_t r = ptr[i0 + k] - j0;
-      sm.off[k] = (int32_t)max((int64_t)0, min(r, (int64_t)kMergeTile + 1));
+      sm->off[k] = (int32_t)max((int64_t)0, min(r, (int64_t)kMergeTile + 1));
     }
-    for (int k = threadIdx.x; k < nr; k += blockDim.x) sm.comm[k] = C[i0 + k];
+    for (int k = threadIdx.x; k < nr; k += blockDim.x) sm->comm[k] = C[i0 + k];
     __syncthreads();
     const int ne = (int)(j1 - j0);
-    for (int q = threadIdx.x; q < ne; q += blockDim.x) {
-      int lo = 0, hi = nr - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (sm.off[mid] <= q) lo = mid; else hi = mid - 1;
-      }
-      const int64_t e = j0 + q;
-      const int32_t a = sm.comm[lo];
-      const int32_t b = C[tail[e]];
-      // b < 0: an endpoint in no community (an isolated vertex, or a graph of a
-      // batch that has finished) contributes no record
-      if (a >= b && b >= 0) {
-        keys[ncl + e] = ((uint64_t)a << nb) | (uint64_t)b;
-        vals[ncl + e] = w[e];
-      } else {
-        keys[ncl + e] = sentinel;
-        vals[ncl + e] = 0.0;
-      }
-    }
-  }
-}
-
-// The same records, only those that exist (a >= b >= 0), appended after the
-// seeds at ncl + *count in no particular order (warp-aggregated appends): for
-// the parallel folds, where the order of additions is free, the sort then
-// moves half as many records.
-__global__ void __launch_bounds__(256) k_coarse_records_compact(
-    int64_t nv, int64_t nnz, const int64_t *ptr, const int32_t *tail, const double *w,
-    const int32_t *C, int64_t ncl, int nb, const int64_t *split_row, uint64_t *keys,
-    double *vals, unsigned long long *count) {
-  for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < ncl;
-       a += (int64_t)gridDim.x * blockDim.x) {
-    keys[a] = ((uint64_t)a << nb) | (uint64_t)a;
-    vals[a] = 0.0;
-  }
-  __shared__ MergeSmem sm;
-  const int lane = threadIdx.x & 31;
-  const int64_t ntiles = merge_tiles(nv, nnz);
-  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int64_t d0 = tile * (int64_t)kMergeTile;
-    const int64_t d1 = min(d0 + (int64_t)kMergeTile, nv + nnz);
-    const int64_t i0 = split_row[tile], i1 = split_row[tile + 1];
-    const int64_t j0 = d0 - i0, j1 = d1 - i1;
-    if (j1 <= j0) continue;  // tile-uniform
-    const int64_t ih = min(i1, nv - 1);
-    const int nr = (int)(ih - i0 + 1);
-    __syncthreads();
-    for (int k = threadIdx.x; k <= nr; k += blockDim.x) {
-      const int64_t r = ptr[i0 + k] - j0;
-      sm.off[k] = (int32_t)max((int64_t)0, min(r, (int64_t)kMergeTile + 1));
-    }
-    for (int k = threadIdx.x; k < nr; k += blockDim.x) sm.comm[k] = C[i0 + k];
-    __syncthreads();
-    const int ne = (int)(j1 - j0);
-    for (int q0 = 0; q0 < ne; q0 += blockDim.x) {  // every lane of a warp takes each round
+    for (int q0 = 0; q0 < ne; q0 += blockDim.x) {  // block-uniform rounds
       const int q = q0 + (int)threadIdx.x;
       bool keep = false;
       uint64_t key = 0;
-      double val = 0.0;
+      int64_t e = 0;
       if (q < ne) {
         int lo = 0, hi = nr - 1;
         while (lo < hi) {
           const int mid = (lo + hi + 1) >> 1;
-          if (sm.off[mid] <= q) lo = mid; else hi = mid - 1;
+          if (sm->off[mid] <= q) lo = mid; else hi = mid - 1;
         }
-        const int64_t e = j0 + q;
-        const int32_t a = sm.comm[lo];
+        e = j0 + q;
+        const int32_t a = sm->comm[lo];
         const int32_t b = C[tail[e]];
         keep = a >= b && b >= 0;
         key = ((uint64_t)a << nb) | (uint64_t)(uint32_t)b;
-        val = w[e];
       }
       const unsigned m = __ballot_sync(FULL, keep);
-      unsigned long long base = 0;
-      if (lane == 0 && m) base = atomicAdd(count, (unsigned long long)__popc(m));
-      base = __shfl_sync(FULL, base, 0);
-      if (keep) {
-        const int64_t at = ncl + (int64_t)base + __popc(m & ((1u << lane) - 1u));
-        keys[at] = key;
-        vals[at] = val;
+      if (WRITE) {
+        // place of this round's records: warps in order, lanes in order
+        if (lane == 0) s_warp[warp] = __popc(m);
+        __syncthreads();
+        int before = 0, total = 0;
+        for (int k = 0; k < nwb; ++k) {
+          const int c = s_warp[k];
+          if (k < warp) before += c;
+          total += c;
+        }
+        if (keep) {
+          const int64_t at = base + kept + before + __popc(m & ((1u << lane) - 1u));
+          keys[at] = key;
+          vals[at] = w[e];
+        }
+        kept += total;
+        __syncthreads();
+      } else {
+        kept += __popc(m);  // per warp; summed over warps below
       }
     }
   }
+  if (!WRITE) {
+    if (lane == 0) s_warp[warp] = (int32_t)kept;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int64_t t = 0;
+      for (int k = 0; k < nwb; ++k) t += s_warp[k];
+      count[tile] = t;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) k_coarse_tile_counts(
+    int64_t nv, int64_t nnz, const int64_t *ptr, const int32_t *tail, const int32_t *C, int nb,
+    const int64_t *split_row, int64_t *count) {
+  __shared__ MergeSmem sm;
+  __shared__ int32_t s_warp[32];
+  const int64_t ntiles = merge_tiles(nv, nnz);
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+    coarse_tile<false>(tile, nv, nnz, ptr, tail, nullptr, C, nb, split_row, &sm, s_warp, nullptr,
+                       nullptr, 0, count);
+}
+
+// Seeds (a, a, 0.0) in slots 0..ncl-1, then every tile's records from
+// ncl + tile_off[tile].
+__global__ void __launch_bounds__(256) k_coarse_records_compact(
+    int64_t nv, int64_t nnz, const int64_t *ptr, const int32_t *tail, const double *w,
+    const int32_t *C, int64_t ncl, int nb, const int64_t *split_row, const int64_t *tile_off,
+    uint64_t *keys, double *vals) {
+  for (int64_t a = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; a < ncl;
+       a += (int64_t)gridDim.x * blockDim.x) {
+    keys[a] = ((uint64_t)a << nb) | (uint64_t)a;
+    vals[a] = 0.0;
+  }
+  __shared__ MergeSmem sm;
+  __shared__ int32_t s_warp[32];
+  const int64_t ntiles = merge_tiles(nv, nnz);
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+    coarse_tile<true>(tile, nv, nnz, ptr, tail, w, C, nb, split_row, &sm, s_warp, keys, vals,
+                      ncl + tile_off[tile], nullptr);
 }
 
 // Segment heads of the sorted records -> flags (1 at the first record of each
@@ -879,6 +875,8 @@ __global__ void k_row_counts(int64_t np, const uint64_t *ukeys, int nb, int64_t 
 // Lower part of each row: pairs (a, b <= a) in ascending b.  Pairs are sorted
 // by (a, b), so a pair's rank inside row a is p - first pair of a; also emits
 // the transposed key (b << nb) | a of every off-diagonal pair for the mirror.
+// The transposed keys come in ascending a for each b, so a stable sort of
+// their b bits alone orders them by (b, a).
 __global__ void k_emit_lower(int64_t np, const uint64_t *ukeys, const double *uvals, int nb,
                              const int64_t *row_ptr, const int64_t *lower_first,
                              int32_t *otail, double *ow, uint64_t *tkeys, double *tvals,
