@@ -66,6 +66,8 @@ def parse_args():
     p.add_argument('--csr-sample-scale', type=int, default=16,
                    help='csr workload: R-MAT scale of the reference\'s CPU sample')
     p.add_argument('--batch-graphs', type=int, default=4096)
+    p.add_argument('--batch-sample', type=int, default=24,
+                   help='batch workload: graphs the reference runs for cpu_baseline')
     p.add_argument('--wave-pairs', type=float, default=3.5e8,
                    help='batch workload: expected undirected pairs per batched run')
     return p.parse_args()
@@ -570,8 +572,10 @@ def run_batch_workload(args, world, rank, local):
     Graphs are split into consecutive waves of about --wave-pairs expected
     pairs; each wave is one batched run.  A step runs every wave once; the
     metric is graphs/s over the whole set, with per-graph finishing times
-    (from the start of its wave) as p50/p99.  Replicas on N GPUs each run the
-    whole set (weak scaling)."""
+    (from the start of its wave) as p50/p99.  On N GPUs the set is split into
+    N shards of about equal expected entries (grappolo_b200.sharding), each
+    rank runs its shard and the per-graph results are gathered on the host
+    (strong scaling: the whole set is the job)."""
     import numpy as np
     import torch
     from grappolo_b200 import graphs, louvain, _lib
@@ -584,7 +588,10 @@ def run_batch_workload(args, world, rank, local):
         dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=900),
                                 device_id=dev)
     mode = _lib.GLV_MODE_FAST if args.mode == 'fast' else _lib.GLV_MODE_VERIFY
-    specs = graphs.batch_specs(args.batch_graphs, seed=3)
+    from grappolo_b200 import sharding
+    all_specs = graphs.batch_specs(args.batch_graphs, seed=3)
+    mine = sharding.shard_by_work(all_specs[:, 0] * all_specs[:, 3], world)[rank]
+    specs = all_specs[mine]
     pairs = specs[:, 0] * specs[:, 3] / 2.0
     waves, g0 = [], 0
     while g0 < len(specs):
@@ -596,7 +603,8 @@ def run_batch_workload(args, world, rank, local):
         g0 = g1
     data = []
     for k, (a, b) in enumerate(waves):
-        voff, ptr, tail, w = graphs.planted_batch_device(specs[a:b], seed=1000 + k, device=dev)
+        voff, ptr, tail, w = graphs.planted_batch_device(specs[a:b], seed=1000 + 7919 * rank + k,
+                                                         device=dev)
         C = torch.empty(ptr.numel() - 1, dtype=torch.int32, device=dev)
         data.append((voff, ptr, tail, w, C))
     torch.cuda.synchronize()
@@ -630,8 +638,15 @@ def run_batch_workload(args, world, rank, local):
     graphs_done = args.steps * len(specs)
     t_max, g_all = aggregate(t, graphs_done, dist, dev)
     last = runs[-1]
-    done = np.concatenate([r['done_seconds'] for r in last])
-    q = np.concatenate([r['final_modularity'] for r in last])
+    # per-graph results of every shard, in the batch's graph order
+    per = sharding.gather_results(
+        mine, np.stack([np.concatenate([r['done_seconds'] for r in last]),
+                        np.concatenate([r['final_modularity'] for r in last])], axis=1),
+        len(all_specs), dist)
+    done, q = per[:, 0], per[:, 1]
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = batch_cpu_baseline(data[0], args.batch_sample)
     edges = sum(r['edges_swept'] for run in runs for r in run)
     launches = sum(r['kernel_launches'] for run in runs for r in run)
     line = {'metric': 'batched Louvain graphs/s', 'value': g_all / t_max, 'unit': 'graphs/s',
@@ -640,8 +655,9 @@ def run_batch_workload(args, world, rank, local):
             'vs_baseline': None, 'dtype': 'f64',
             'data': 'synthetic (seeded planted-partition graphs generated on the device)',
             'config': {'workload': f'batched plain multiphase Louvain (coloring=1) on '
-                                   f'{len(specs)} planted-partition graphs',
-                       'graphs': len(specs), 'num_vertices': int(nv_total), 'nnz': int(nnz_total),
+                                   f'{len(all_specs)} planted-partition graphs',
+                       'graphs': len(all_specs), 'graphs_this_rank': len(specs),
+                       'num_vertices_this_rank': int(nv_total), 'nnz_this_rank': int(nnz_total),
                        'waves': len(waves), 'wave_pairs': args.wave_pairs, 'mode': args.mode,
                        'threshold': 1e-6, 'C_threshold': 1e-4, 'minGraphSize': 1000,
                        'per_graph_done_s_p50': float(np.percentile(done, 50)),
@@ -649,14 +665,45 @@ def run_batch_workload(args, world, rank, local):
                        'modularity_mean': float(q.mean()), 'modularity_min': float(q.min()),
                        'local_move_edges_per_s': edges / t,
                        'rounds_per_wave': [r['rounds'] for r in last],
-                       'parallelism': f'replicas x{world}',
+                       'parallelism': (f'{world} shards of about equal expected entries, '
+                                       f'per-graph results gathered on the host')
+                       if world > 1 else 'one GPU',
                        'l2': 'inputs larger than L2 (no flush)'},
-            'gpu_launches': launches, 'clocks': clk, 'cpu_baseline': None, 'e2e': None}
+            'gpu_launches': launches, 'clocks': clk, 'cpu_baseline': cpu, 'e2e': None}
+    if world > 1:
+        line['scaling'] = 'strong'
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
     return 0
+
+
+def batch_cpu_baseline(wave, sample):
+    """The reference's runMultiPhaseColoring (oracle/_ref, shipped -Ofast flags,
+    all host cores) on the first `sample` graphs of the first wave, one call per
+    graph: graphs/s on that subset."""
+    import numpy as np
+    from grappolo_b200 import graphs
+    from oracle import Reference
+    voff, ptr, tail, w, _ = wave
+    hptr, htail, hw = ptr.cpu().numpy(), tail.cpu().numpy(), w.cpu().numpy()
+    cores = os.cpu_count() or 1
+    R = Reference(fast=True)
+    n = min(sample, len(voff) - 1)
+    secs, ents = 0.0, 0
+    for k in range(n):
+        v0, v1 = int(voff[k]), int(voff[k + 1])
+        e0, e1 = int(hptr[v0]), int(hptr[v1])
+        g = graphs.CSRGraph(hptr[v0:v1 + 1] - e0, htail[e0:e1].astype(np.int64) - v0, hw[e0:e1])
+        t0 = time.perf_counter()
+        R.run_multiphase_coloring(g, nthreads=cores)
+        secs += time.perf_counter() - t0
+        ents += g.nnz
+    return {'value': n / secs, 'unit': 'graphs/s', 'cores': cores, 'kind': 'reference',
+            'sample': f'reference runMultiPhaseColoring (-Ofast build, {cores} OpenMP threads) '
+                      f'on the first {n} graphs of the first wave, one call per graph '
+                      f'({ents} CSR entries, {secs:.1f} s)'}
 
 
 def main():
