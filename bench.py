@@ -152,7 +152,7 @@ def measured_peak():
 
 def profiled_traffic_ratio():
     """DRAM bytes per algorithmic byte of the sweep kernels, from the committed ncu summary."""
-    path = os.path.join(ROOT, 'profiles', 'sweep_iteration_rmat22.txt')
+    path = os.path.join(ROOT, 'profiles', 'sweep_iteration_rmat24.txt')
     try:
         with open(path) as f:
             for line in f:
@@ -857,8 +857,9 @@ def main():
                 'frac': (achieved / peak) if achieved else None, 'peak_kind': peak_kind,
                 'traffic': (ratio * sweep_b / steps_timed) if (ratio and steps_timed) else None,
                 'traffic_source': 'ncu dram__bytes_read.sum + dram__bytes_write.sum over the '
-                                  'algorithmic bytes of one k_sweep_iteration launch on R-MAT '
-                                  'scale 22, times this launch\'s algorithmic bytes',
+                                  'algorithmic bytes of one k_sweep_iteration launch on this '
+                                  'R-MAT scale 24 graph (phase 1, iteration 2), times the '
+                                  'average launch\'s algorithmic bytes',
                 'algorithmic_bytes_per_launch': sweep_b / steps_timed if steps_timed else None,
                 'avg_launch_s': sweep_t / steps_timed if steps_timed else None}
     s0 = stats[-1]
