@@ -611,15 +611,24 @@ int Engine::init(int64_t nv0, int64_t nnz0) {
 __global__ void k_check_weights(int64_t nnz, const double *w, const int32_t *tail, int64_t nv,
                                 int32_t *flags, double *total) {
   double s = 0.0;
+  bool frac = false, bad = false;  // flags kept per thread: one update per warp at the end
   for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < nnz;
        j += (int64_t)gridDim.x * blockDim.x) {
     const double x = w[j];
-    if (!(x >= 0.0 && x == floor(x))) atomicOr(&flags[0], 1);
+    frac = frac || !(x >= 0.0 && x == floor(x));
     const int32_t t = tail[j];
-    if (t < 0 || t >= nv) atomicOr(&flags[1], 1);
+    bad = bad || t < 0 || t >= nv;
     s += x;
   }
-  atomicAdd(total, s);
+  frac = __any_sync(FULL, frac);
+  bad = __any_sync(FULL, bad);
+#pragma unroll
+  for (int off = 16; off >= 1; off >>= 1) s += __shfl_xor_sync(FULL, s, off);
+  if ((threadIdx.x & 31) == 0) {
+    if (frac) atomicOr(&flags[0], 1);
+    if (bad) atomicOr(&flags[1], 1);
+    atomicAdd(total, s);
+  }
 }
 
 int Engine::upload_check(const Level &L) {
@@ -1910,6 +1919,12 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
     p.a.last_move = last_move_;
   }
   bool force_full = true;  // the first sweep of a phase is always a full one
+  // Gated sweeps only in the phase's tail: once a full sweep gains less than
+  // GRAPPOLO_B200_GATE_TAIL (default 16) times the threshold.  Early sweeps
+  // move many vertices, and a gate that misses some of them costs iterations.
+  double gate_tail = 16.0;
+  if (const char *e = getenv("GRAPPOLO_B200_GATE_TAIL")) gate_tail = atof(e);
+  double last_full_gain = INFINITY;
   float tau = 0.5f;
   {
     std::lock_guard<std::mutex> lock(g_gate_mu);
@@ -1921,10 +1936,11 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
     p.a.iter = n;
     bool gated_now = false;
     if (gating || tracing) {
-      if (n >= 2)
+      gated_now = gating && !force_full && n >= 2 &&
+                  (gate_tail <= 0.0 || last_full_gain < gate_tail * thresh);
+      if (n >= 2 && (gated_now || tracing))
         LAUNCH(k_gate_features, grid_for(L.nv, 256, nsm_ * 8), 256, 0, s_, L.nv, L.ptr, vDeg,
                rec_own_, rec_gain_, last_move_, n, phase_index_, feat_);
-      gated_now = gating && !force_full && n >= 2;
       p.a.skip = nullptr;
       if (gated_now) {
         CK(cudaMemsetAsync(evald_, 0, sizeof(unsigned long long), s_));
@@ -2094,6 +2110,7 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
     if (debug)
       fprintf(stderr, "grappolo_b200: iter %d gated %d q %.9f gain %.3e edges %.0f time %.5f\n", n,
               (int)gated_now, q, q - prev, edges_swept, now_s() - t0);
+    if (!gated_now) last_full_gain = q - prev;
     if (q - prev < thresh) {
       // A phase ends only after a full (ungated) sweep gains less than thresh.
       if (!gated_now) break;

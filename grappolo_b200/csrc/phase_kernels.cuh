@@ -551,15 +551,23 @@ __global__ void k_max_color(int64_t nv, const int32_t *color, int32_t *out) {
 __global__ void k_schedule_keys(int64_t nv, const int64_t *ptr, const int32_t *color,
                                 const int32_t *sub, int nsub, BinLimits lim, int32_t *keys,
                                 int32_t *vals, int32_t *hist) {
-  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
-       v += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t deg = ptr[v + 1] - ptr[v];
-    const int c = color ? color[v] : 0;
-    const int s = sub ? sub[v] : 0;
-    const int k = (c * nsub + s) * NBINS + degree_bin(deg, lim);
-    keys[v] = k;
-    vals[v] = (int32_t)v;
-    atomicAdd(&hist[k], 1);
+  // every lane of a warp takes each round, so equal keys of a round share one
+  // histogram update (a few keys take most vertices)
+  const int lane = threadIdx.x & 31;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t v0 = (int64_t)blockIdx.x * blockDim.x; v0 < nv; v0 += stride) {
+    const int64_t v = v0 + threadIdx.x;
+    int k = -1;
+    if (v < nv) {
+      const int64_t deg = ptr[v + 1] - ptr[v];
+      const int c = color ? color[v] : 0;
+      const int s = sub ? sub[v] : 0;
+      k = (c * nsub + s) * NBINS + degree_bin(deg, lim);
+      keys[v] = k;
+      vals[v] = (int32_t)v;
+    }
+    const unsigned m = __match_any_sync(FULL, k);
+    if (k >= 0 && lane == __ffs(m) - 1) atomicAdd(&hist[k], __popc(m));
   }
 }
 
