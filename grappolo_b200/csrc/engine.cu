@@ -13,6 +13,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include <functional>
 #include <mutex>
 #include <thread>
 
@@ -497,6 +498,16 @@ class Engine {
   int32_t *hub_segs_left_ = nullptr, *hub_err_ = nullptr;
   uint32_t *hub_state_ = nullptr;
   uint32_t epoch_ = 0;  // persistent launches of this engine (hub states compare against it)
+  int hub_chunk_ = kHubChunk;  // CSR entries per hub chunk (the autotuner may lower it)
+  // trial launches of the autotuner: stop after this many iterations (0 = the
+  // phase's own test) and keep the last launch's device time
+  int max_iters_ = 0;
+  double last_launch_s_ = 0.0;
+  bool tune_cached_ = false;
+  int tune_choice_[2] = {0, 0};  // block_max, hub chunk chosen for this run (0 = not tuned)
+  int autotune(const Level &L, int ncolors, std::vector<ClassSched> *sched,
+               const std::function<int(std::vector<ClassSched> *)> &make_sched, SweepArgs a,
+               double lower, double thresh);
   double *hub_self_ = nullptr, *hub_ownw_ = nullptr;
   int32_t *hub_occ_ = nullptr;
   size_t hub_occ_cap_ = 0;
@@ -515,7 +526,7 @@ class Engine {
     return HubWork{hub_keys_, hub_vals_, hub_off_, hub_occ_, hub_occ_off_, hub_cnt_, hub_self_,
                    hub_ownw_, chunk_pos_, chunk_beg_, chunk_end_, seg_pos_, seg_beg_, seg_end_,
                    part_g_, part_c_, hub_seg_beg_, hub_seg_end_, hub_left_, hub_big_, step_big_,
-                   hub_segs_left_, hub_state_, 0u, hub_err_};
+                   hub_segs_left_, hub_state_, 0u, hub_err_, hub_chunk_};
   }
   int hist_cap_ = 0;
   // ordered-delta buffers
@@ -1137,11 +1148,12 @@ __global__ void k_scatter_i64(int64_t n, const int32_t *pos, const int64_t *val,
 
 __global__ void k_hub_chunk_counts(int64_t n, const int32_t *pos, const int32_t *members,
                                    const int64_t *ptr, const int64_t *seg_beg,
-                                   const int64_t *seg_end, int32_t *left, int32_t *segs_left) {
+                                   const int64_t *seg_end, int chunk, int32_t *left,
+                                   int32_t *segs_left) {
   for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
        k += (int64_t)gridDim.x * blockDim.x) {
     const int32_t v = members[pos[k]];
-    left[pos[k]] = (int32_t)((ptr[v + 1] - ptr[v] + kHubChunk - 1) / kHubChunk);
+    left[pos[k]] = (int32_t)((ptr[v + 1] - ptr[v] + chunk - 1) / chunk);
     segs_left[pos[k]] = (int32_t)(seg_end[pos[k]] - seg_beg[pos[k]]);
   }
 }
@@ -1254,10 +1266,10 @@ int Engine::hub_offsets(const Level &L, std::vector<ClassSched> &sched) {
         if (!parallel) continue;
         occ_off.push_back((int64_t)step_occ);
         step_occ += (size_t)deg + 1;
-        for (int64_t x = rb; x < re; x += kHubChunk) {
+        for (int64_t x = rb; x < re; x += hub_chunk_) {
           c_pos.push_back((int32_t)pos);
           c_beg.push_back(x);
-          c_end.push_back(std::min<int64_t>(re, x + kHubChunk));
+          c_end.push_back(std::min<int64_t>(re, x + hub_chunk_));
         }
         seg_b.push_back((int64_t)s_pos.size());
         for (int64_t x = 0; x < deg + 1; x += kHubSeg) {
@@ -1325,7 +1337,7 @@ int Engine::hub_offsets(const Level &L, std::vector<ClassSched> &sched) {
     LAUNCH(k_scatter_i64, grid_for(nh, 256, nsm_ * 4), 256, 0, s_, nh, d_pos, d_vals + 3 * nh,
            hub_seg_end_);
     LAUNCH(k_hub_chunk_counts, grid_for(nh, 256, nsm_ * 4), 256, 0, s_, nh, d_pos, members_, L.ptr,
-           hub_seg_beg_, hub_seg_end_, hub_left_, hub_segs_left_);
+           hub_seg_beg_, hub_seg_end_, hub_chunk_, hub_left_, hub_segs_left_);
   }
   CK(cudaStreamSynchronize(s_));
   dfree(d_pos);
@@ -1366,7 +1378,7 @@ int Engine::recolor(const Level &L, int *ncolors, int passes) {
     CK(cudaMemsetAsync(d_ctr, 0, steps.size() * sizeof(int64_t), s_));
     CK(cudaMemsetAsync(newc, 0xff, L.nv * sizeof(int32_t), s_));
     RecolorArgs r{L.ptr, L.tail, members_, newc, d_steps, (int)steps.size(), d_ctr,
-                  chunk_pos_, chunk_beg_, chunk_end_, hub_off_, hub_keys_, hub_left_};
+                  chunk_pos_, chunk_beg_, chunk_end_, hub_off_, hub_keys_, hub_left_, hub_chunk_};
     void *args[] = {&r};
     CK(cudaLaunchCooperativeKernel((void *)k_recolor_pass, grid, kRecolorThreads, args, 0, s_));
     ++launches_;
@@ -1513,14 +1525,18 @@ int Engine::coloring_phase(const Level &L, int ncolors, bool stale, double lower
   }
   if (debug) { cudaStreamSynchronize(s_); fprintf(stderr, "grappolo_b200: phase init %.4f s\n", now_s() - td); td = now_s(); }
   std::vector<ClassSched> sched;
-  TRY(build_schedule(L, color_, ncolors, d_sub, nsub, &sched));
-  relaxed_ = false;
-  if (nsub == 1 && core_color_ < ncolors) {  // core batches
-    relaxed_ = true;
-    for (ClassSched &cs : sched) cs.relaxed = cs.color >= core_color_;
-  } else if (nsub == 1 && persistent()) {
-    TRY(group_classes(L, ncolors, &sched));
-  }
+  auto make_sched = [&](std::vector<ClassSched> *out) -> int {
+    TRY(build_schedule(L, color_, ncolors, d_sub, nsub, out));
+    relaxed_ = false;
+    if (nsub == 1 && core_color_ < ncolors) {  // core batches
+      relaxed_ = true;
+      for (ClassSched &cs : *out) cs.relaxed = cs.color >= core_color_;
+    } else if (nsub == 1 && persistent()) {
+      TRY(group_classes(L, ncolors, out));
+    }
+    return GLV_OK;
+  };
+  TRY(make_sched(&sched));
   if (debug) { cudaStreamSynchronize(s_); fprintf(stderr, "grappolo_b200: schedule %.4f s\n", now_s() - td); }
   dfree(d_sub);
   const bool ord = ordered();
@@ -1543,6 +1559,10 @@ int Engine::coloring_phase(const Level &L, int ncolors, bool stale, double lower
   CK(cudaMemcpyAsync(&a.constant, cst, sizeof(double), cudaMemcpyDeviceToHost, s_));
   CK(cudaStreamSynchronize(s_));
   a.defer_c = (relaxed_ && persistent()) ? 1 : 0;
+  if (persistent() && phase_index_ == 0 && !bt_) {
+    TRY(autotune(L, ncolors, &sched, make_sched, a, lower, thresh));
+    a.hub_keys = hub_keys_; a.hub_vals = hub_vals_; a.hub_off = hub_off_;
+  }
   if (persistent()) return run_persistent(L, sched, a, false, lower, thresh, mod, itr);
   cudaGraphExec_t exec = nullptr;
   long nodes = 0;
@@ -1593,6 +1613,138 @@ __global__ void k_rotate(int64_t n, int32_t *past, int32_t *curr, const int32_t 
     past[i] = curr[i];
     curr[i] = tgt[i];
   }
+}
+
+// ------------------------------------------------------------- autotuner
+// Speed-only knobs of the persistent sweep, picked per graph: the degree above
+// which a row is a hub (global table, chunks over many blocks) instead of a
+// block row (8192-slot shared table), and the entries per hub chunk.  Neither
+// changes a decision: every candidate folds the same per-community sums
+// (exactly, on integral weights) and takes the same arg-max.  On the first
+// colour phase of a level with at least GRAPPOLO_B200_AUTOTUNE_MIN entries
+// (default 2^24; GRAPPOLO_B200_AUTOTUNE=0 switches it off) each candidate runs
+// one sweep iteration of the actual level from the phase's start state, which
+// is restored after every trial; the fastest (device time of the launch)
+// wins and is cached for the process under the graph's signature (vertex and
+// entry counts and the row-degree histogram in powers of two), so repeated
+// runs on the same graph pay once.
+struct TuneChoice {
+  int block_max;
+  int hub_chunk;
+  double seconds;
+};
+static std::mutex g_tune_mu;
+static std::map<std::string, TuneChoice> g_tune_cache;
+
+__global__ void k_degree_log_hist(int64_t nv, const int64_t *ptr, unsigned long long *hist) {
+  __shared__ unsigned int sh[64];
+  for (int k = threadIdx.x; k < 64; k += blockDim.x) sh[k] = 0;
+  __syncthreads();
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    const uint64_t d = (uint64_t)(ptr[v + 1] - ptr[v]);
+    atomicAdd(&sh[d ? 64 - __clzll((long long)d) : 0], 1u);
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < 64; k += blockDim.x)
+    if (sh[k]) atomicAdd(&hist[k], (unsigned long long)sh[k]);
+}
+
+int Engine::autotune(const Level &L, int ncolors, std::vector<ClassSched> *sched,
+                     const std::function<int(std::vector<ClassSched> *)> &make_sched,
+                     SweepArgs a, double lower, double thresh) {
+  const char *on = getenv("GRAPPOLO_B200_AUTOTUNE");
+  if (on && on[0] == '0') return GLV_OK;
+  const char *mn = getenv("GRAPPOLO_B200_AUTOTUNE_MIN");
+  if (L.nnz < (mn ? atoll(mn) : (int64_t(1) << 24))) return GLV_OK;
+  (void)ncolors;
+  // signature
+  unsigned long long *d_hist;
+  TRY(alloc(&d_hist, 64));
+  CK(cudaMemsetAsync(d_hist, 0, 64 * sizeof(unsigned long long), s_));
+  LAUNCH(k_degree_log_hist, grid_for(L.nv, 256, nsm_ * 4), 256, 0, s_, L.nv, L.ptr, d_hist);
+  unsigned long long hist[64];
+  CK(cudaMemcpyAsync(hist, d_hist, sizeof(hist), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  dfree(d_hist);
+  std::string sig = std::to_string(L.nv) + ":" + std::to_string(L.nnz) + ":" +
+                    std::to_string(mode_);
+  for (int k = 0; k < 64; ++k)
+    if (hist[k]) sig += ":" + std::to_string(k) + "=" + std::to_string(hist[k]);
+  const bool debug = getenv("GRAPPOLO_B200_DEBUG") != nullptr;
+  const BinLimits lim0 = lim_;
+  const int chunk0 = hub_chunk_;
+  auto apply = [&](int block_max, int chunk) -> int {
+    if (block_max == lim_.block_max && chunk == hub_chunk_) return GLV_OK;
+    lim_.block_max = block_max;
+    hub_chunk_ = chunk;
+    return make_sched(sched);
+  };
+  bool hit = false;
+  TuneChoice cached{};
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune_cache.find(sig);
+    if (it != g_tune_cache.end()) {
+      hit = true;
+      cached = it->second;
+    }
+  }
+  if (hit) {
+    tune_cached_ = true;
+    tune_choice_[0] = cached.block_max;
+    tune_choice_[1] = cached.hub_chunk;
+    return apply(cached.block_max, cached.hub_chunk);
+  }
+  // the phase's start state, restored after every trial
+  int32_t *C0, *S0;
+  double *D0;
+  TRY(alloc(&C0, L.nv)); TRY(alloc(&S0, L.nv)); TRY(alloc(&D0, L.nv));
+  CK(cudaMemcpyAsync(C0, C, L.nv * sizeof(int32_t), cudaMemcpyDeviceToDevice, s_));
+  CK(cudaMemcpyAsync(S0, cSize, L.nv * sizeof(int32_t), cudaMemcpyDeviceToDevice, s_));
+  CK(cudaMemcpyAsync(D0, cDeg, L.nv * sizeof(double), cudaMemcpyDeviceToDevice, s_));
+  // statistics the trials must not touch
+  const double s_t = t_sweep, s_e = edges_swept, s_k = sweep_kernel_s, s_b = sweep_bytes;
+  const long s_l = launches_, s_s = sweep_steps, s_g = gated_iterations_;
+  const int bms[3] = {lim0.block_max, 2047, 1023};
+  const int chunks[2] = {kHubChunk, kHubChunk / 2};
+  TuneChoice best{lim0.block_max, chunk0, INFINITY};
+  int rc = GLV_OK;
+  for (int bi = 0; bi < 3 && rc == GLV_OK; ++bi) {
+    if (bms[bi] > lim0.block_max || (bi > 0 && bms[bi] == lim0.block_max)) continue;
+    for (int ci = 0; ci < 2 && rc == GLV_OK; ++ci) {
+      rc = apply(bms[bi], chunks[ci]);
+      if (rc != GLV_OK) break;
+      SweepArgs ta = a;
+      ta.hub_keys = hub_keys_; ta.hub_vals = hub_vals_; ta.hub_off = hub_off_;
+      max_iters_ = 1;
+      double q = 0;
+      int it = 0;
+      rc = run_persistent(L, *sched, ta, false, lower, thresh, &q, &it);
+      max_iters_ = 0;
+      if (rc != GLV_OK) break;
+      if (debug)
+        fprintf(stderr, "grappolo_b200: autotune block_max %d chunk %d: %.3f ms\n", bms[bi],
+                chunks[ci], last_launch_s_ * 1e3);
+      if (last_launch_s_ < best.seconds) best = TuneChoice{bms[bi], chunks[ci], last_launch_s_};
+      cudaMemcpyAsync(C, C0, L.nv * sizeof(int32_t), cudaMemcpyDeviceToDevice, s_);
+      cudaMemcpyAsync(cSize, S0, L.nv * sizeof(int32_t), cudaMemcpyDeviceToDevice, s_);
+      cudaMemcpyAsync(cDeg, D0, L.nv * sizeof(double), cudaMemcpyDeviceToDevice, s_);
+    }
+  }
+  CK(cudaStreamSynchronize(s_));
+  dfree(C0); dfree(S0); dfree(D0);
+  t_sweep = s_t; edges_swept = s_e; sweep_kernel_s = s_k; sweep_bytes = s_b;
+  launches_ = s_l; sweep_steps = s_s; gated_iterations_ = s_g;
+  if (rc != GLV_OK) return rc;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune_cache[sig] = best;
+  }
+  tune_cached_ = false;
+  tune_choice_[0] = best.block_max;
+  tune_choice_[1] = best.hub_chunk;
+  return apply(best.block_max, best.hub_chunk);
 }
 
 int Engine::basic_phase(const Level &L, double lower, double thresh, double *mod, int *itr) {
@@ -1888,7 +2040,7 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
   }
   const int level = g_profile.load();
   cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (level > 0) {
+  if (level > 0 || max_iters_ > 0) {
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
   }
@@ -2014,6 +2166,7 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
     if (e0) {
       float ms = 0;
       if (cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess) sweep_kernel_s += ms * 1e-3;
+      last_launch_s_ = ms * 1e-3;
       // sweep: 16 B per entry + 36 B per vertex; modularity: a full pass 16 B
       // per entry + 12 B per vertex, a carried e_xx 8 B per vertex (cDeg)
       sweep_bytes += (p.exx_mode == 1) ? 16.0 * (double)L.nnz + 44.0 * (double)L.nv
@@ -2110,6 +2263,10 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
     if (debug)
       fprintf(stderr, "grappolo_b200: iter %d gated %d q %.9f gain %.3e edges %.0f time %.5f\n", n,
               (int)gated_now, q, q - prev, edges_swept, now_s() - t0);
+    if (max_iters_ > 0 && n >= max_iters_) {
+      prev = q;
+      break;
+    }
     if (!gated_now) last_full_gain = q - prev;
     if (q - prev < thresh) {
       // A phase ends only after a full (ungated) sweep gains less than thresh.
@@ -2652,6 +2809,9 @@ int Engine::run_multiphase(const Level &L0, int32_t *d_C_orig, bool coloring,
     st->sweep_bytes = sweep_bytes;
     st->sweep_steps = sweep_steps;
     for (int k = 0; k < kSlots; ++k) st->kernel_time[k] = slot_s[k];
+    st->tuned_block_max = tune_choice_[0];
+    st->tuned_hub_chunk = tune_choice_[1];
+    st->tuned_from_cache = tune_cached_ ? 1 : 0;
   }
   return GLV_OK;
 }

@@ -28,6 +28,7 @@ struct RecolorArgs {
   const int64_t *hub_off;      // per member slot: offset of its hub table region
   int32_t *hub_words;          // hub table regions, used as all-ones bitmaps here
   int32_t *chunks_left;        // per member slot: chunks not yet folded
+  int chunk;                   // CSR entries per hub chunk
 };
 
 constexpr int kRecolorThreads = 512;
@@ -144,8 +145,7 @@ __device__ __forceinline__ void recolor_hub_chunk(const RecolorArgs &r, int64_t 
     for (int q = lane; q < kColorWords; q += 32) gw[q] = 0xffffffffu;
     if (lane == 0) {
       r.newc[v] = (first == INT32_MAX) ? kMaxColors - 1 : first;
-      r.chunks_left[pos] =
-          (int32_t)((r.ptr[v + 1] - r.ptr[v] + kHubChunk - 1) / kHubChunk);
+      r.chunks_left[pos] = (int32_t)((r.ptr[v + 1] - r.ptr[v] + r.chunk - 1) / r.chunk);
     }
   }
   __syncthreads();

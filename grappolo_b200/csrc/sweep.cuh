@@ -521,9 +521,10 @@ struct HubWork {
   uint32_t *state;          // per member slot: 4 * epoch + 1 decided, + 2 segments needed
   uint32_t epoch;           // this launch (0: the launch-per-kernel path, big[] instead)
   int32_t *err;             // set when a segment's wait gives up
+  int chunk;                // CSR entries per accumulation chunk (<= kHubChunk)
 };
 
-constexpr int kHubChunk = 2048;      // CSR entries per accumulation work item
+constexpr int kHubChunk = 2048;      // most CSR entries per accumulation work item
 constexpr int kHubSeg = 8192;        // filled slots per scan work item
 constexpr int kHubStageCap = 4096;   // block-local staging table of one chunk
 constexpr int kHubInlineCap = 4096;  // filled slots the last chunk's block scans itself
@@ -660,7 +661,7 @@ __device__ __forceinline__ void hub_accum_chunk(const SweepArgs &a, const HubWor
   if (skip) {
     if (threadIdx.x == 0) {
       emit_stay(a, pos, v, a.C[v]);
-      h.chunks_left[pos] = (int32_t)((a.ptr[v + 1] - a.ptr[v] + kHubChunk - 1) / kHubChunk);
+      h.chunks_left[pos] = (int32_t)((a.ptr[v + 1] - a.ptr[v] + h.chunk - 1) / h.chunk);
       if (h.epoch) {
         __threadfence();
         atomicExch(&h.state[pos], 4u * h.epoch + 1u);
@@ -704,7 +705,7 @@ __device__ __forceinline__ void hub_accum_chunk(const SweepArgs &a, const HubWor
     h.cnt[pos] = 0;
     h.self_w[pos] = 0.0;
     h.own_w[pos] = 0.0;
-    h.chunks_left[pos] = (int32_t)((a.ptr[v + 1] - a.ptr[v] + kHubChunk - 1) / kHubChunk);
+    h.chunks_left[pos] = (int32_t)((a.ptr[v + 1] - a.ptr[v] + h.chunk - 1) / h.chunk);
     if (h.epoch) {
       __threadfence();
       atomicExch(&h.state[pos], 4u * h.epoch + 1u);
@@ -789,7 +790,7 @@ __device__ __forceinline__ void hub_segment_task(const SweepArgs &a, const HubWo
     h.cnt[pos] = 0;
     h.self_w[pos] = 0.0;
     h.own_w[pos] = 0.0;
-    h.chunks_left[pos] = (int32_t)((a.ptr[v + 1] - a.ptr[v] + kHubChunk - 1) / kHubChunk);
+    h.chunks_left[pos] = (int32_t)((a.ptr[v + 1] - a.ptr[v] + h.chunk - 1) / h.chunk);
     h.segs_left[pos] = (int32_t)(h.hub_seg_end[pos] - h.hub_seg_beg[pos]);
   }
 }
@@ -842,7 +843,7 @@ __device__ __forceinline__ void hub_final(const SweepArgs &a, const HubWork &h, 
     h.self_w[pos] = 0.0;
     h.own_w[pos] = 0.0;
     h.big[pos] = 0;
-    h.chunks_left[pos] = (int32_t)((a.ptr[v + 1] - a.ptr[v] + kHubChunk - 1) / kHubChunk);
+    h.chunks_left[pos] = (int32_t)((a.ptr[v + 1] - a.ptr[v] + h.chunk - 1) / h.chunk);
   }
 }
 

@@ -110,6 +110,13 @@ typedef struct glv_run_stats {
   double kernel_time[GLV_KERNEL_SLOTS]; /* s */
   int nphase;               /* entries filled in phase[] */
   glv_phase_stats phase[GLV_MAX_PHASES];
+  /* The autotuner's choice for this run's first colour phase (0 = not tuned:
+   * small level, Jacobi-only run, or GRAPPOLO_B200_AUTOTUNE=0): the degree
+   * above which rows are hubs, the entries per hub chunk, and 1 when the
+   * choice came from the process's cache of earlier runs on the same graph. */
+  int tuned_block_max;
+  int tuned_hub_chunk;
+  int tuned_from_cache;
 } glv_run_stats;
 
 /* ---- graph construction and files ---------------------------------------- */
