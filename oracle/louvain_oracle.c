@@ -886,6 +886,12 @@ static void free_graph(long *ptr, long *tail, double *w, int owned) {
  * with the previous colour count (:61-66,113-115).  The first colour phase
  * that fails to gain switches to Jacobi phases on the same graph (:199-206).
  * C_orig is composed after every phase, before the gain test (:128-144).     */
+/* Vertices of the last multiphase run for which no colour qualified in a
+ * coloring = 2 recolouring (where type 0 of the reference is undefined). */
+static long vbase_stuck_total = 0;
+
+long lvo_last_vbase_stuck(void) { return vbase_stuck_total; }
+
 static int color_for(int coloring, int numColors, long nv, const long *ptr, const long *tail,
                      int *colors) {
     if (coloring == 3) {
@@ -896,7 +902,7 @@ static int color_for(int coloring, int numColors, long nv, const long *ptr, cons
     for (long i = 0; i < nv; i++) colors[i] = -1;
     int mc = lvo_color_greedy(nv, ptr, tail, colors);
     /* coloring = 2 balances the colouring (runMultiPhaseColoring.cpp:67-73) */
-    if (coloring == 2 && mc >= 0) lvo_vbase(nv, ptr, tail, colors, mc + 1, 0, NULL);
+    if (coloring == 2 && mc >= 0) lvo_vbase(nv, ptr, tail, colors, mc + 1, 0, &vbase_stuck_total);
     return mc;
 }
 
@@ -908,6 +914,7 @@ int lvo_run_multiphase_coloring(long nv, const long *ptr0, const long *tail0,
     double *w = (double *)w0;
     int owned = 0;
     long NV = nv, gnv = nv;
+    vbase_stuck_total = 0;
     int *colors = (int *)malloc(sizeof(int) * (nv ? nv : 1));
     int nColors = color_for(coloring, numColors, gnv, ptr, tail, colors);
     if (nColors == -2) { free(colors); return -1; }

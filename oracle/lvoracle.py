@@ -77,6 +77,7 @@ class COracle:
         L.lvo_color_greedy.restype = ct.c_int
         L.lvo_color_mhash.restype = ct.c_int
         L.lvo_vbase.restype = ct.c_long
+        L.lvo_last_vbase_stuck.restype = ct.c_long
         L.lvo_gini.restype = ct.c_double
         L.lvo_compare_communities.restype = ct.c_int
         L.lvo_remove_edges.restype = ct.c_long
@@ -267,7 +268,8 @@ class COracle:
         if rc != 0:
             raise RuntimeError('oracle: colour count reached the 4096 cap')
         return C, dict(phases=s.phases, total_iterations=s.total_iterations,
-                       final_clusters=s.final_clusters, final_mod=s.final_mod), \
+                       final_clusters=s.final_clusters, final_mod=s.final_mod,
+                       vbase_stuck=self.L.lvo_last_vbase_stuck()), \
             self._records(recs, min(s.nrec, 256))
 
     def run_multiphase_basic(self, g, threshold=1e-6):
@@ -329,8 +331,13 @@ def parse_comparison_log(text: str) -> dict:
 class Reference:
     """Grappolo's own functions, compiled from its sources (oracle/_ref)."""
 
-    def __init__(self, fast: bool = False, quiet: bool = True):
+    def __init__(self, fast: bool = False, quiet: bool = True, patched_vbase: bool = False):
+        """patched_vbase loads the build whose vBaseRedistribution gains its missing
+        return (oracle/ref_vbase.cpp), so coloring = 2 runs; its type 0 is defined
+        only where the oracle reports no stuck vertex."""
         name = 'libgrappolo_ref_fast.so' if fast else 'libgrappolo_ref.so'
+        if patched_vbase:
+            name = 'libgrappolo_ref_vbase.so'
         path = os.path.join(HERE, '_ref', name)
         if not os.path.exists(path):
             build()
@@ -552,6 +559,21 @@ class Reference:
                                         ct.c_int(nthreads), buf, ct.c_long(1 << 22))
         text = buf.value.decode(errors='replace')
         return C, parse_reference_log(text), text
+
+    def vbase(self, g, color, ncolors, vtype=0):
+        """vBaseRedistribution (Coloring/vBase.cpp:6-168) from the copy with its missing
+        return added (oracle/ref_vbase.cpp); one thread.  Type 0 reads past its
+        frequency array when no colour qualifies: callers keep only cases the
+        oracle reports as never stuck."""
+        path = os.path.join(HERE, '_ref', 'libgrappolo_ref_vbase.so')
+        if not os.path.exists(path):
+            build()
+        L = self.L if self.L._name == path else ct.CDLL(path)
+        p, t, w = _csr(g)
+        col = np.ascontiguousarray(color, dtype=np.int32).copy()
+        L.ref_vbase(ct.c_long(g.num_vertices), _lp(p), _lp(t), _dp(w), _ip(col),
+                    ct.c_int(ncolors), ct.c_int(vtype))
+        return col
 
     def graph(self, g):
         """A persistent reference `graph` (AoS) for repeated calls; free with free_graph."""

@@ -86,3 +86,25 @@ def gini_cases():
 
 COMPARE_INTS = ('same_same', 'same_diff', 'diff_same', 'num_communities1', 'num_communities2')
 COMPARE_FLOATS = ('precision', 'recall', 'f_score', 'gini1', 'gini2')
+
+
+def vbase_cases():
+    """(name, graph, input colouring, colour count, {type: expected colours},
+    expected multiphase run or None) for every case of vbase.npz: the
+    reference's vBaseRedistribution and its coloring = 2 multiphase run, one
+    thread, built with the function's missing return added."""
+    z = np.load(os.path.join(GOLDEN, 'vbase.npz'))
+    out = []
+    for name in map(str, z['names']):
+        tail = z[f'{name}_tail'].astype(np.int64)
+        w = z[f'{name}_weight'] if f'{name}_weight' in z.files else np.ones(len(tail))
+        g = CSRGraph(z[f'{name}_ptr'], tail, w)
+        exp = {int(t): z[f'{name}_t{t}'] for t in z[f'{name}_types']}
+        mp = None
+        if f'{name}_mp_C' in z.files:
+            mp = dict(C=z[f'{name}_mp_C'], phases=int(z[f'{name}_mp_phases']),
+                      total_iterations=int(z[f'{name}_mp_itr']),
+                      final_clusters=int(z[f'{name}_mp_clusters']),
+                      final_mod=float(z[f'{name}_mp_mod']))
+        out.append((name, g, z[f'{name}_color'], int(z[f'{name}_ncolors']), exp, mp))
+    return out

@@ -7,6 +7,7 @@ Run from the repository root after ``make -C oracle``:
     python tests/golden/make_golden.py --mhash  # only mhash.npz (coloring = 3)
     python tests/golden/make_golden.py --csr    # only csr_build.npz and karate.bin
     python tests/golden/make_golden.py --compare  # only compare.npz
+    python tests/golden/make_golden.py --vbase    # only vbase.npz (coloring = 2)
 
 Each fixture ``<case>.npz`` holds an input CSR and what the reference's
 functions return for it at OMP_NUM_THREADS=1: the distance-1 colouring, one
@@ -257,6 +258,85 @@ def make_compare(R, ref_root):
     print('wrote compare', list(cases))
 
 
+def stars_and_clique(nv, nstars, clique, seed, paths=0, weighted=False):
+    """Stars of 2-11 leaves and paths of 3-7 vertices on randomly permuted ids,
+    isolated vertices, and a clique on the `clique` highest ids.  The clique
+    sets the colour count; only colour 0 (the isolated vertices) is
+    oversized, and the clique's colour-0 member comes last in vertex order, so
+    a colour qualifies for every vertex vBaseRedistribution moves and its
+    first-fit scan (Coloring/vBase.cpp:113-116) stays inside its arrays."""
+    rng = np.random.default_rng(seed)
+    e, v = [], 0
+    for _ in range(nstars):
+        k = int(rng.integers(2, 12))
+        e += [(v, v + j) for j in range(1, k + 1)]
+        v += k + 1
+    for _ in range(paths):
+        k = int(rng.integers(3, 8))
+        e += [(v + j, v + j + 1) for j in range(k - 1)]
+        v += k
+    assert v <= nv - clique
+    perm = rng.permutation(nv - clique)
+    e = [(int(perm[a]), int(perm[b])) for a, b in e]
+    c0 = nv - clique
+    e += [(c0 + a, c0 + b) for a in range(clique) for b in range(a + 1, clique)]
+    g = graphs.from_edges(nv, e)
+    return graphs.random_weights(g, seed=seed) if weighted else g
+
+
+def vbase_cases(ref_root):
+    """(graph, types stored for the single call, multiphase stored) per case."""
+    cases = {
+        'pp1000': (all_cases(ref_root)['pp1000'], (1,), False),
+        'rmat12': (graphs.rmat(12, seed=4), (1,), False),
+        'star': (graphs.from_edges(60, [(0, i) for i in range(1, 60)] + [(1, 2), (3, 4)]),
+                 (1,), False),
+    }
+    for nv, ns, kc, paths, seed in [(3000, 60, 10, 0, 0), (6000, 200, 12, 20, 1),
+                                    (12000, 400, 16, 50, 2), (30000, 800, 20, 100, 1)]:
+        cases[f'sc{nv}'] = (stars_and_clique(nv, ns, kc, seed, paths, weighted=seed == 1),
+                            (0, 1), True)
+    return cases
+
+
+def make_vbase(ref_root):
+    """vbase.npz: vBaseRedistribution (Coloring/vBase.cpp:6-168) and the
+    coloring = 2 multiphase run (runMultiPhaseColoring.cpp:67-74,180-186) of
+    the reference built with the function's missing return added
+    (oracle/ref_vbase.cpp), one thread.  The input colouring is the
+    reference's distance-1 colouring.  Type 0 and the multiphase run (which
+    calls type 0) are stored only where the oracle finds a qualifying colour
+    for every vertex that moves: elsewhere the reference reads past its
+    frequency array and its result is not defined."""
+    from oracle import COracle
+    R = Reference(patched_vbase=True)
+    O = COracle()
+    out, names = {}, []
+    for name, (g, types, mp) in vbase_cases(ref_root).items():
+        col, mc, _ = R.color(g)
+        nc = mc + 1
+        out.update({f'{name}_ptr': g.ptr, f'{name}_tail': g.tail.astype(np.int32),
+                    f'{name}_color': col.astype(np.int32), f'{name}_ncolors': nc})
+        if mp:  # the single call reads no weights
+            out[f'{name}_weight'] = g.weight
+        for t in types:
+            if t == 0:
+                assert O.vbase(g, col, nc, 0)[2] == 0, name
+            out[f'{name}_t{t}'] = R.vbase(g, col, nc, t)
+        out[f'{name}_types'] = np.array(types)
+        if mp:
+            _, so, _ = O.run_multiphase_coloring(g, coloring=2)
+            assert so['vbase_stuck'] == 0, name
+            C, s, _ = R.run_multiphase_coloring(g, coloring=2)
+            out.update({f'{name}_mp_C': C, f'{name}_mp_phases': s['phases'],
+                        f'{name}_mp_itr': s['total_iterations'],
+                        f'{name}_mp_clusters': s['final_clusters'],
+                        f'{name}_mp_mod': s['final_mod']})
+        names.append(name)
+        print('vbase', name, g.num_vertices, g.nnz, 'colours', nc, 'types', types, 'multiphase', mp)
+    np.savez_compressed(os.path.join(HERE, 'vbase.npz'), names=np.array(names), **out)
+
+
 def main():
     ref_root = sys.argv[1] if len(sys.argv) > 1 and not sys.argv[1].startswith('--') \
         else os.environ.get('GRAPPOLO_REFERENCE', '/root/reference')
@@ -272,6 +352,9 @@ def main():
         return
     if '--compare' in sys.argv:
         make_compare(R, ref_root)
+        return
+    if '--vbase' in sys.argv:
+        make_vbase(ref_root)
         return
     rng = np.random.default_rng(2024)
     for name, g in all_cases(ref_root).items():

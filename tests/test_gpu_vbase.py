@@ -1,11 +1,15 @@
 """Balanced recolouring (coloring = 2, vBaseRedistribution) on the GPU against
-the oracle restatement (the reference's own function cannot run here; see
-tests/test_vbase_oracle.py).  Colourings and, in verify mode, whole
-multiphase runs must equal the oracle's exactly."""
+the reference's own function (tests/golden/vbase.npz, from a copy with its
+missing return added) and against the oracle restatement on larger graphs.
+Colourings and, in verify mode, whole multiphase runs must be equal exactly.
+Type 0 and the multiphase runs are pinned to the reference only on graphs
+where its first-fit scan finds a colour for every vertex it moves
+(tests/test_vbase_oracle.py); elsewhere the oracle is the checker."""
 import numpy as np
 import pytest
 
 from grappolo_b200 import _lib, graphs, louvain
+from _golden import vbase_cases
 
 pytestmark = pytest.mark.gpu
 
@@ -29,6 +33,29 @@ def test_vbase_vs_oracle(oracle, name, g, vtype):
     out, n = louvain.vBaseRedistribution(g, col, mc + 1, vtype)
     assert n == moves
     assert np.array_equal(out, exp)
+
+
+VBASE = vbase_cases()
+
+
+@pytest.mark.parametrize('case', VBASE, ids=[c[0] for c in VBASE])
+def test_vbase_golden(case):
+    name, g, col, nc, exp, _ = case
+    for vtype, want in exp.items():
+        out, n = louvain.vBaseRedistribution(g, col, nc, vtype)
+        assert np.array_equal(out, want), (name, vtype)
+        assert n == int((want != col).sum())
+
+
+@pytest.mark.parametrize('case', [c for c in VBASE if c[5] is not None],
+                         ids=[c[0] for c in VBASE if c[5] is not None])
+def test_multiphase_coloring2_golden(case):
+    name, g, _, _, _, mp = case
+    C, st = louvain.runMultiPhaseColoring(g, coloring=2, numThreads=1, stats=True)
+    assert np.array_equal(C, mp['C'])
+    assert (st['phases'], st['total_iterations'], st['final_clusters']) == \
+        (mp['phases'], mp['total_iterations'], mp['final_clusters'])
+    assert abs(st['final_modularity'] - mp['final_mod']) <= 5e-7  # printed with %lf
 
 
 @pytest.mark.parametrize('name', ['pp1000', 'rmat12', 'pp100k'])

@@ -1,15 +1,23 @@
 """The oracle's balanced recolouring (vBaseRedistribution, Coloring/vBase.cpp)
-against a second, pure-Python restatement of the same rule, and its
-invariants.  The reference's own function cannot serve as the checker here:
-it is declared int but returns nothing (the call traps when built by g++),
-and its first-fit scan reads past its frequency array when no colour
-qualifies, after which it need not terminate."""
+against the reference's own function (tests/golden/vbase.npz), against a
+second, pure-Python restatement of the same rule, and its invariants.
+
+The reference's function is declared int but returns nothing, so the call
+traps when g++ builds it as it is; the golden vectors come from a copy with
+that one `return` added (oracle/ref_vbase.cpp).  Its first-fit scan (type 0,
+which the multiphase driver uses) reads past its frequency array when no
+colour qualifies for a vertex, after which its result is not defined: type 0
+and the coloring = 2 multiphase runs are pinned on graphs where the oracle
+finds a colour for every vertex it moves (the oracle's stuck count is 0)."""
 import math
 
 import numpy as np
 import pytest
 
 from grappolo_b200 import graphs
+from _golden import vbase_cases
+
+VBASE = vbase_cases()
 
 
 def vbase_py(g, color, ncolors, vtype):
@@ -59,3 +67,27 @@ def test_vbase_oracle(oracle, name, g, vtype):
     assert moves == int(moved.sum())
     assert np.all(f0[col[moved]] > avg) and np.all(f0[out[moved]] < avg)
     assert np.all(f1[f0 < avg] <= avg)
+
+
+@pytest.mark.parametrize('case', VBASE, ids=[c[0] for c in VBASE])
+def test_vbase_oracle_golden(oracle, case):
+    name, g, col, nc, exp, _ = case
+    assert np.array_equal(oracle.color_greedy(g)[0], col)  # the reference's input colouring
+    for vtype, want in exp.items():
+        out, moves, stuck = oracle.vbase(g, col, nc, vtype)
+        assert np.array_equal(out, want), (name, vtype)
+        assert moves == int((want != col).sum())
+        if vtype == 0:
+            assert stuck == 0
+
+
+@pytest.mark.parametrize('case', [c for c in VBASE if c[5] is not None],
+                         ids=[c[0] for c in VBASE if c[5] is not None])
+def test_multiphase_coloring2_oracle_golden(oracle, case):
+    name, g, _, _, _, mp = case
+    C, s, _ = oracle.run_multiphase_coloring(g, coloring=2)
+    assert s['vbase_stuck'] == 0
+    assert np.array_equal(C, mp['C'])
+    assert (s['phases'], s['total_iterations'], s['final_clusters']) == \
+        (mp['phases'], mp['total_iterations'], mp['final_clusters'])
+    assert abs(s['final_mod'] - mp['final_mod']) <= 5e-7  # the reference prints %lf
