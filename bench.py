@@ -880,6 +880,7 @@ def main():
                               - s0['time_coloring'] - s0['time_building']},
              'learned': learned_cmp,
              'autotune': {'block_max': s0['tuned_block_max'], 'hub_chunk': s0['tuned_hub_chunk'],
+                          'hub_cluster': s0['hub_cluster'],
                           'from_cache': bool(s0['tuned_from_cache'])},
              'step_totals_s': [round(s['time_total'], 4) for s in stats],
              'step_splits_s': [[round(s[k], 4) for k in ('time_clustering', 'time_coloring',

@@ -68,7 +68,8 @@ class GlvRunStats(ct.Structure):
                 ('sweep_bytes', ct.c_double), ('sweep_steps', ct.c_long),
                 ('kernel_time', ct.c_double * GLV_KERNEL_SLOTS), ('nphase', ct.c_int),
                 ('phase', GlvPhaseStats * GLV_MAX_PHASES), ('tuned_block_max', ct.c_int),
-                ('tuned_hub_chunk', ct.c_int), ('tuned_from_cache', ct.c_int)]
+                ('tuned_hub_chunk', ct.c_int), ('tuned_from_cache', ct.c_int),
+                ('hub_cluster', ct.c_int)]
 
     def to_dict(self) -> dict:
         d = {k: getattr(self, k) for k, _ in self._fields_ if k not in ('phase', 'kernel_time')}

@@ -505,6 +505,7 @@ class Engine {
   double last_launch_s_ = 0.0;
   bool tune_cached_ = false;
   int tune_choice_[2] = {0, 0};  // block_max, hub chunk chosen for this run (0 = not tuned)
+  int first_cluster_ = -1;       // cluster size of the run's first colour phase (-1 = none yet)
   int autotune(const Level &L, int ncolors, std::vector<ClassSched> *sched,
                const std::function<int(std::vector<ClassSched> *)> &make_sched, SweepArgs a,
                double lower, double thresh);
@@ -515,6 +516,22 @@ class Engine {
   int64_t *chunk_beg_ = nullptr, *chunk_end_ = nullptr, *seg_beg_ = nullptr, *seg_end_ = nullptr;
   double *part_g_ = nullptr;
   size_t chunk_cap_ = 0, seg_cap_ = 0;
+  // Hub rows of the persistent kernel on thread-block clusters of cluster_
+  // blocks (0: all hubs as chunks over global tables).  A hub whose table
+  // needs at most cluster_parts_ cluster-sized partitions is a cluster row
+  // when the schedule is built for the persistent sweep (sweep_rows_);
+  // hub_pos_h_/hub_deg_h_ are the cluster rows' member slots (ascending) and
+  // row lengths.
+  int cluster_ = 0;
+  int cluster_parts_ = kClusterMaxParts;
+  bool sweep_rows_ = false;
+  int32_t *ct_pos_ = nullptr, *ct_part_ = nullptr, *ct_nparts_ = nullptr, *ct_c_ = nullptr;
+  double *ct_g_ = nullptr;
+  size_t ct_cap_ = 0;
+  std::vector<int32_t> hub_pos_h_;
+  std::vector<int64_t> hub_deg_h_;
+  int cluster_grid(int cl);  // blocks of a cooperative launch with cl-block clusters
+  int cluster_grid_[kClusterMax + 1] = {};
   bool hub_tables_clean_ = false;
   // The current colour phase runs some colour classes together in one step
   // (group_classes), so a step's members are not an independent set.
@@ -526,7 +543,8 @@ class Engine {
     return HubWork{hub_keys_, hub_vals_, hub_off_, hub_occ_, hub_occ_off_, hub_cnt_, hub_self_,
                    hub_ownw_, chunk_pos_, chunk_beg_, chunk_end_, seg_pos_, seg_beg_, seg_end_,
                    part_g_, part_c_, hub_seg_beg_, hub_seg_end_, hub_left_, hub_big_, step_big_,
-                   hub_segs_left_, hub_state_, 0u, hub_err_, hub_chunk_};
+                   hub_segs_left_, hub_state_, 0u, hub_err_, hub_chunk_, ct_pos_, ct_part_,
+                   ct_nparts_, ct_g_, ct_c_};
   }
   int hist_cap_ = 0;
   // ordered-delta buffers
@@ -565,6 +583,7 @@ void Engine::release() {
   dfree(hub_self_); dfree(hub_ownw_); dfree(hub_occ_); dfree(hub_left_); dfree(hub_big_);
   dfree(hub_segs_left_); dfree(hub_state_); dfree(hub_err_);
   dfree(step_big_); dfree(chunk_pos_); dfree(seg_pos_);
+  dfree(ct_pos_); dfree(ct_part_); dfree(ct_nparts_); dfree(ct_g_); dfree(ct_c_);
   dfree(part_c_); dfree(chunk_beg_); dfree(chunk_end_); dfree(seg_beg_); dfree(seg_end_);
   dfree(part_g_);
   dfree(dkeys_); dfree(dkeys2_); dfree(drecs_); dfree(drecs2_);
@@ -604,6 +623,21 @@ int Engine::init(int64_t nv0, int64_t nnz0) {
   if (const char *bm = getenv("GRAPPOLO_B200_BLOCK_MAX")) {
     const int v = atoi(bm);
     if (v >= lim_.warp_max && v <= 4095) lim_.block_max = v;
+  }
+  // hub rows on clusters of this many blocks (1, 2, 4, 8 or 16; 0 = global
+  // tables, the default); the autotuner may change it
+  cluster_ = 0;
+  if (const char *cl = getenv("GRAPPOLO_B200_CLUSTER")) {
+    const int v = atoi(cl);
+    if (v == 0 || (v <= kClusterMax && (v & (v - 1)) == 0)) cluster_ = v;
+  }
+  if (cluster_ > 0 && cluster_grid(cluster_) < cluster_) cluster_ = 0;
+  if (getenv("GRAPPOLO_B200_DEBUG"))
+    fprintf(stderr, "grappolo_b200: hub clusters of %d blocks (grid %d)\n", cluster_,
+            cluster_ > 0 ? cluster_grid(cluster_) : 0);
+  if (const char *cp = getenv("GRAPPOLO_B200_CLUSTER_PARTS")) {
+    const int v = atoi(cp);
+    if (v >= 1 && (v & (v - 1)) == 0) cluster_parts_ = v;
   }
   TRY(alloc(&cst, 4));
   // partials of the modularity pass (one per 256 vertices) and of the
@@ -1195,6 +1229,9 @@ int Engine::hub_offsets(const Level &L, std::vector<ClassSched> &sched) {
     for (auto &st : cs.steps)
       for (int64_t k = st.seg[BIN_HUB]; k < st.seg[BIN_HUB + 1]; ++k) hpos.push_back((int32_t)k);
   std::vector<int64_t> hb_all(2 * hpos.size());
+  hub_pos_h_.clear();
+  hub_deg_h_.clear();
+  const bool cl_rows = parallel && sweep_rows_ && cluster_ > 0;
   if (!hpos.empty()) {
     int32_t *d_pos;
     int64_t *bounds;
@@ -1261,6 +1298,18 @@ int Engine::hub_offsets(const Level &L, std::vector<ClassSched> &sched) {
       for (int64_t k = 0; k < e - b; ++k) {
         const int64_t rb = hb[2 * k], re = hb[2 * k + 1], deg = re - rb;
         const int64_t pos = b + k;
+        uint32_t np = 0, cap = 0;
+        if (cl_rows) cluster_row_shape(deg, cluster_, &np, &cap);
+        if (cl_rows && np <= (uint32_t)cluster_parts_) {
+          // a cluster row: no global table, chunks or segments
+          hub_pos_h_.push_back((int32_t)pos);
+          hub_deg_h_.push_back(deg);
+          tab_off.push_back(0);
+          occ_off.push_back(0);
+          seg_b.push_back((int64_t)s_pos.size());
+          seg_e.push_back((int64_t)s_pos.size());
+          continue;
+        }
         tab_off.push_back((int64_t)step_tab);
         step_tab += table_cap(deg);
         if (!parallel) continue;
@@ -1526,15 +1575,17 @@ int Engine::coloring_phase(const Level &L, int ncolors, bool stale, double lower
   if (debug) { cudaStreamSynchronize(s_); fprintf(stderr, "grappolo_b200: phase init %.4f s\n", now_s() - td); td = now_s(); }
   std::vector<ClassSched> sched;
   auto make_sched = [&](std::vector<ClassSched> *out) -> int {
-    TRY(build_schedule(L, color_, ncolors, d_sub, nsub, out));
+    sweep_rows_ = persistent();
+    int rc = build_schedule(L, color_, ncolors, d_sub, nsub, out);
     relaxed_ = false;
-    if (nsub == 1 && core_color_ < ncolors) {  // core batches
+    if (rc == GLV_OK && nsub == 1 && core_color_ < ncolors) {  // core batches
       relaxed_ = true;
       for (ClassSched &cs : *out) cs.relaxed = cs.color >= core_color_;
-    } else if (nsub == 1 && persistent()) {
-      TRY(group_classes(L, ncolors, out));
+    } else if (rc == GLV_OK && nsub == 1 && persistent()) {
+      rc = group_classes(L, ncolors, out);
     }
-    return GLV_OK;
+    sweep_rows_ = false;
+    return rc;
   };
   TRY(make_sched(&sched));
   if (debug) { cudaStreamSynchronize(s_); fprintf(stderr, "grappolo_b200: schedule %.4f s\n", now_s() - td); }
@@ -1563,6 +1614,10 @@ int Engine::coloring_phase(const Level &L, int ncolors, bool stale, double lower
     TRY(autotune(L, ncolors, &sched, make_sched, a, lower, thresh));
     a.hub_keys = hub_keys_; a.hub_vals = hub_vals_; a.hub_off = hub_off_;
   }
+  if (first_cluster_ < 0) first_cluster_ = persistent() ? cluster_ : 0;
+  if (debug)
+    fprintf(stderr, "grappolo_b200: colour phase: persistent %d ordered %d cluster %d rows %zu\n",
+            persistent() ? 1 : 0, ordered() ? 1 : 0, cluster_, hub_pos_h_.size());
   if (persistent()) return run_persistent(L, sched, a, false, lower, thresh, mod, itr);
   cudaGraphExec_t exec = nullptr;
   long nodes = 0;
@@ -1631,6 +1686,7 @@ __global__ void k_rotate(int64_t n, int32_t *past, int32_t *curr, const int32_t 
 struct TuneChoice {
   int block_max;
   int hub_chunk;
+  int cluster;
   double seconds;
 };
 static std::mutex g_tune_mu;
@@ -1674,10 +1730,12 @@ int Engine::autotune(const Level &L, int ncolors, std::vector<ClassSched> *sched
   const bool debug = getenv("GRAPPOLO_B200_DEBUG") != nullptr;
   const BinLimits lim0 = lim_;
   const int chunk0 = hub_chunk_;
-  auto apply = [&](int block_max, int chunk) -> int {
-    if (block_max == lim_.block_max && chunk == hub_chunk_) return GLV_OK;
+  const int cluster0 = cluster_;
+  auto apply = [&](int block_max, int chunk, int cl) -> int {
+    if (block_max == lim_.block_max && chunk == hub_chunk_ && cl == cluster_) return GLV_OK;
     lim_.block_max = block_max;
     hub_chunk_ = chunk;
+    cluster_ = cl;
     return make_sched(sched);
   };
   bool hit = false;
@@ -1694,7 +1752,7 @@ int Engine::autotune(const Level &L, int ncolors, std::vector<ClassSched> *sched
     tune_cached_ = true;
     tune_choice_[0] = cached.block_max;
     tune_choice_[1] = cached.hub_chunk;
-    return apply(cached.block_max, cached.hub_chunk);
+    return apply(cached.block_max, cached.hub_chunk, cached.cluster);
   }
   // the phase's start state, restored after every trial
   int32_t *C0, *S0;
@@ -1706,14 +1764,22 @@ int Engine::autotune(const Level &L, int ncolors, std::vector<ClassSched> *sched
   // statistics the trials must not touch
   const double s_t = t_sweep, s_e = edges_swept, s_k = sweep_kernel_s, s_b = sweep_bytes;
   const long s_l = launches_, s_s = sweep_steps, s_g = gated_iterations_;
+  // Candidates: hub thresholds 4095 and 2047 with every hub on global tables
+  // in 2048-entry chunks, 1024-entry chunks, and the hub rows that fit on
+  // 2-block clusters (the larger hubs keep their chunks).
+  std::vector<TuneChoice> cands;
   const int bms[3] = {lim0.block_max, 2047, 1023};
-  const int chunks[2] = {kHubChunk, kHubChunk / 2};
-  TuneChoice best{lim0.block_max, chunk0, INFINITY};
-  int rc = GLV_OK;
-  for (int bi = 0; bi < 3 && rc == GLV_OK; ++bi) {
+  for (int bi = 0; bi < 3; ++bi) {
     if (bms[bi] > lim0.block_max || (bi > 0 && bms[bi] == lim0.block_max)) continue;
-    for (int ci = 0; ci < 2 && rc == GLV_OK; ++ci) {
-      rc = apply(bms[bi], chunks[ci]);
+    if (bi < 2) cands.push_back(TuneChoice{bms[bi], kHubChunk, 0, INFINITY});
+    if (bi == 0) cands.push_back(TuneChoice{bms[bi], kHubChunk / 2, 0, INFINITY});
+    if (bi == 0 && cluster_grid(2) > 0) cands.push_back(TuneChoice{bms[bi], kHubChunk, 2, INFINITY});
+  }
+  TuneChoice best{lim0.block_max, chunk0, cluster0, INFINITY};
+  int rc = GLV_OK;
+  for (const TuneChoice &cand : cands) {
+    {
+      rc = apply(cand.block_max, cand.hub_chunk, cand.cluster);
       if (rc != GLV_OK) break;
       SweepArgs ta = a;
       ta.hub_keys = hub_keys_; ta.hub_vals = hub_vals_; ta.hub_off = hub_off_;
@@ -1724,9 +1790,10 @@ int Engine::autotune(const Level &L, int ncolors, std::vector<ClassSched> *sched
       max_iters_ = 0;
       if (rc != GLV_OK) break;
       if (debug)
-        fprintf(stderr, "grappolo_b200: autotune block_max %d chunk %d: %.3f ms\n", bms[bi],
-                chunks[ci], last_launch_s_ * 1e3);
-      if (last_launch_s_ < best.seconds) best = TuneChoice{bms[bi], chunks[ci], last_launch_s_};
+        fprintf(stderr, "grappolo_b200: autotune block_max %d chunk %d cluster %d: %.3f ms\n",
+                cand.block_max, cand.hub_chunk, cand.cluster, last_launch_s_ * 1e3);
+      if (last_launch_s_ < best.seconds)
+        best = TuneChoice{cand.block_max, cand.hub_chunk, cand.cluster, last_launch_s_};
       cudaMemcpyAsync(C, C0, L.nv * sizeof(int32_t), cudaMemcpyDeviceToDevice, s_);
       cudaMemcpyAsync(cSize, S0, L.nv * sizeof(int32_t), cudaMemcpyDeviceToDevice, s_);
       cudaMemcpyAsync(cDeg, D0, L.nv * sizeof(double), cudaMemcpyDeviceToDevice, s_);
@@ -1744,13 +1811,16 @@ int Engine::autotune(const Level &L, int ncolors, std::vector<ClassSched> *sched
   tune_cached_ = false;
   tune_choice_[0] = best.block_max;
   tune_choice_[1] = best.hub_chunk;
-  return apply(best.block_max, best.hub_chunk);
+  return apply(best.block_max, best.hub_chunk, best.cluster);
 }
 
 int Engine::basic_phase(const Level &L, double lower, double thresh, double *mod, int *itr) {
   TRY(phase_init(L, true));
   std::vector<ClassSched> sched;
-  TRY(build_schedule(L, nullptr, 1, nullptr, 1, &sched));
+  sweep_rows_ = persistent();
+  const int rc_sched = build_schedule(L, nullptr, 1, nullptr, 1, &sched);
+  sweep_rows_ = false;
+  TRY(rc_sched);
   const bool ord = ordered();
   if (ord) {
     if (!dkeys_) {
@@ -1900,6 +1970,50 @@ int Engine::gate_init() {
   return GLV_OK;
 }
 
+__global__ void k_scatter_i32(int64_t n, const int32_t *pos, const int32_t *val, int32_t *out) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n;
+       k += (int64_t)gridDim.x * blockDim.x)
+    out[pos[k]] = val[k];
+}
+
+// Blocks of the persistent sweep kernel that a cooperative launch with
+// clusters of cl blocks keeps resident at once (whole clusters only); 0 when
+// none fits.
+int Engine::cluster_grid(int cl) {
+  if (cl < 1 || cl > kClusterMax) return 0;
+  if (cluster_grid_[cl] > 0) return cluster_grid_[cl];
+  if (cl == 1) {  // every block is a cluster of its own
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_iteration<true>,
+                                                      kPersistThreads, kPersistSmem) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    cluster_grid_[1] = per_sm * nsm_;
+    return cluster_grid_[1];
+  }
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)cl;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(cl * nsm_));
+  cfg.blockDim = dim3(kPersistThreads);
+  cfg.dynamicSmemBytes = kPersistSmem;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  int nclusters = 0;
+  if (cudaOccupancyMaxActiveClusters(&nclusters, (const void *)k_sweep_iteration<true>, &cfg) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  cluster_grid_[cl] = nclusters * cl;
+  return cluster_grid_[cl];
+}
+
 // One cooperative launch per iteration (persist.cuh).  Colour phases: C is
 // updated in place and Q is taken after the sweep; Jacobi phases: targets go
 // to Ctgt, Q is taken on the state before the moves, and the loop rotates
@@ -1913,7 +2027,7 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
     cls_e.push_back(cs.end);
     for (size_t k = 0; k < cs.steps.size(); ++k) {
       const Step &st = cs.steps[k];
-      StepDesc d;
+      StepDesc d{};
       d.cls = (int64_t)cls_b.size() - 1;
       for (int b = 0; b <= NBINS; ++b) d.seg[b] = st.seg[b];
       d.hub_chunk[0] = st.hub_chunk[0]; d.hub_chunk[1] = st.hub_chunk[1];
@@ -1924,10 +2038,52 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
       steps.push_back(d);
     }
   }
+  // Hub rows as cluster tasks: one per (row, community partition), in the
+  // step's hub order; their chunk and segment lists are not used.
+  const int cl = (cluster_ > 0 && !hub_pos_h_.empty()) ? cluster_ : 0;
+  if (cl > 0) {
+    std::vector<int32_t> t_pos, t_part, t_np, p_pos, p_np;
+    size_t hk = 0;
+    for (auto &d : steps) {
+      d.ctask[0] = d.ctask[1] = (int64_t)t_pos.size();
+      while (hk < hub_pos_h_.size() && hub_pos_h_[hk] < d.seg[BIN_HUB]) ++hk;
+      for (; hk < hub_pos_h_.size() && hub_pos_h_[hk] < d.seg[BIN_HUB + 1]; ++hk) {
+        const int32_t pos = hub_pos_h_[hk];
+        uint32_t np, cap;
+        cluster_row_shape(hub_deg_h_[hk], cl, &np, &cap);
+        for (uint32_t q = 0; q < np; ++q) {
+          t_pos.push_back((int32_t)pos);
+          t_part.push_back((int32_t)q);
+          t_np.push_back((int32_t)np);
+        }
+        if (np > 1) { p_pos.push_back((int32_t)pos); p_np.push_back((int32_t)np); }
+      }
+      d.ctask[1] = (int64_t)t_pos.size();
+    }
+    if (t_pos.size() > ct_cap_) {  // task lists and the partitioned rows' partials
+      dfree(ct_pos_); dfree(ct_part_); dfree(ct_nparts_); dfree(ct_g_); dfree(ct_c_); dfree(ct_g_); dfree(ct_c_);
+      ct_cap_ = t_pos.size();
+      TRY(alloc(&ct_pos_, ct_cap_)); TRY(alloc(&ct_part_, ct_cap_)); TRY(alloc(&ct_nparts_, ct_cap_));
+      TRY(alloc(&ct_g_, ct_cap_)); TRY(alloc(&ct_c_, ct_cap_));
+    }
+    TRY(upload(s_, ct_pos_, t_pos)); TRY(upload(s_, ct_part_, t_part));
+    TRY(upload(s_, ct_nparts_, t_np));
+    if (!p_pos.empty()) {  // partitions still to finish, per partitioned row
+      int32_t *d_pp;
+      TRY(alloc(&d_pp, 2 * p_pos.size()));
+      TRY(upload(s_, d_pp, p_pos));
+      CK(cudaMemcpyAsync(d_pp + p_pos.size(), p_np.data(), p_np.size() * sizeof(int32_t),
+                         cudaMemcpyHostToDevice, s_));
+      LAUNCH(k_scatter_i32, grid_for((int64_t)p_pos.size(), 256, nsm_ * 4), 256, 0, s_,
+             (int64_t)p_pos.size(), d_pp, d_pp + p_pos.size(), hub_segs_left_);
+      CK(cudaStreamSynchronize(s_));
+      dfree(d_pp);
+    }
+  }
   StepDesc *d_steps = nullptr;
   int64_t *d_ctr = nullptr;
   TRY(alloc(&d_steps, steps.size()));
-  TRY(alloc(&d_ctr, 2 * steps.size()));  // block and team queues of every step
+  TRY(alloc(&d_ctr, 3 * steps.size()));  // block, team and cluster queues of every step
   TRY(upload(s_, d_steps, steps));
   int64_t *d_cls_b = nullptr;
   int32_t *d_kept = nullptr;
@@ -2018,10 +2174,11 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
     p.gacc = bt->gacc;
   }
   int per_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_iteration, kPersistThreads,
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_sweep_iteration<false>, kPersistThreads,
                                                    kPersistSmem));
   if (per_sm < 1) return fail(GLV_ERR_CUDA, "persistent sweep kernel does not fit on an SM");
-  const int grid = per_sm * nsm_;
+  const int grid = cl > 0 ? cluster_grid(cl) : per_sm * nsm_;
+  if (grid < 1) return fail(GLV_ERR_CUDA, "no cluster of the persistent sweep kernel fits");
   double *exx_buf = nullptr;
   if (carry_exx) {
     TRY(alloc(&exx_buf, (size_t)grid + 1));  // carried e_xx, then one slot per block
@@ -2033,9 +2190,9 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
   uint64_t *d_trace = nullptr;
   std::vector<uint64_t> h_trace;
   if (debug) {
-    TRY(alloc(&d_trace, 4 * steps.size() + 2));
-    CK(cudaMemsetAsync(d_trace, 0, (4 * steps.size() + 2) * sizeof(uint64_t), s_));
-    h_trace.resize(4 * steps.size() + 2);
+    TRY(alloc(&d_trace, 8 * steps.size() + 2));
+    CK(cudaMemsetAsync(d_trace, 0, (8 * steps.size() + 2) * sizeof(uint64_t), s_));
+    h_trace.resize(8 * steps.size() + 2);
     p.trace = d_trace;
   }
   const int level = g_profile.load();
@@ -2120,12 +2277,29 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
         if (bt->h_act[g]) batch_edges += (double)bt->gnnz[g];
     }
     p.exx_mode = (carry_exx && n >= 2) ? (check_exx ? 2 : 1) : 0;
-    cudaError_t e = cudaMemsetAsync(d_ctr, 0, 2 * steps.size() * sizeof(int64_t), s_);
+    cudaError_t e = cudaMemsetAsync(d_ctr, 0, 3 * steps.size() * sizeof(int64_t), s_);
     p.h.epoch = ++epoch_;
     if (e0) cudaEventRecord(e0, s_);
-    if (e == cudaSuccess)
-      e = cudaLaunchCooperativeKernel((void *)k_sweep_iteration, grid, kPersistThreads, args,
+    if (e == cudaSuccess && cl > 0) {
+      cudaLaunchAttribute at[2];
+      at[0].id = cudaLaunchAttributeCooperative;
+      at[0].val.cooperative = 1;
+      at[1].id = cudaLaunchAttributeClusterDimension;
+      at[1].val.clusterDim.x = (unsigned)cl;
+      at[1].val.clusterDim.y = 1;
+      at[1].val.clusterDim.z = 1;
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3((unsigned)grid);
+      cfg.blockDim = dim3(kPersistThreads);
+      cfg.dynamicSmemBytes = kPersistSmem;
+      cfg.stream = s_;
+      cfg.attrs = at;
+      cfg.numAttrs = 2;
+      e = cudaLaunchKernelEx(&cfg, k_sweep_iteration<true>, p);
+    } else if (e == cudaSuccess) {
+      e = cudaLaunchCooperativeKernel((void *)k_sweep_iteration<false>, grid, kPersistThreads, args,
                                       kPersistSmem, s_);
+    }
     if (e1) cudaEventRecord(e1, s_);
     if (e == cudaSuccess)
       e = cudaMemcpyAsync(h_mod_, mod_out_, 5 * sizeof(double), cudaMemcpyDeviceToHost, s_);
@@ -2133,7 +2307,9 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
     t_sweep += now_s() - t0;
     if (e != cudaSuccess) { g_err = cudaGetErrorString(e); rc = GLV_ERR_CUDA; break; }
     if (h_mod_[4] != 0.0) {
-      rc = fail(GLV_ERR_CUDA, "sweep: a hub's table scan gave up waiting for its chunks");
+      rc = fail(GLV_ERR_CUDA, h_mod_[4] == 2.0
+                                  ? "sweep: a hub partition's cluster table overflowed"
+                                  : "sweep: a hub's table scan gave up waiting for its chunks");
       break;
     }
     if (p.exx_mode == 2) {
@@ -2209,12 +2385,19 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
             const StepDesc &d = steps[k];
             fprintf(f, "%ld %d %zu", (long)L.nv, n, k);
             for (int b = 0; b < NBINS; ++b) fprintf(f, " %ld", (long)(d.seg[b + 1] - d.seg[b]));
-            fprintf(f, " %ld", (long)(d.hub_chunk[1] - d.hub_chunk[0]));
+            fprintf(f, " %ld", (long)(d.hub_chunk[1] - d.hub_chunk[0] + d.ctask[1] - d.ctask[0]));
+            const uint64_t t0 = t;
             for (int q = 0; q < 4; ++q) {
               const uint64_t x = h_trace[4 * k + q];
               if (x == 0 || x < t) { fprintf(f, " 0"); continue; }
               fprintf(f, " %.2f", (x - t) * 1e-3);
               t = x;
+            }
+            // when the block queue, the team queue, the warp items and the
+            // cluster tasks ran dry
+            for (int q = 0; q < 4; ++q) {
+              const uint64_t x = h_trace[4 * ns + 2 + 4 * k + q];
+              fprintf(f, " %.2f", (x > t0) ? (x - t0) * 1e-3 : 0.0);
             }
             fprintf(f, "\n");
           }
@@ -2812,6 +2995,7 @@ int Engine::run_multiphase(const Level &L0, int32_t *d_C_orig, bool coloring,
     st->tuned_block_max = tune_choice_[0];
     st->tuned_hub_chunk = tune_choice_[1];
     st->tuned_from_cache = tune_cached_ ? 1 : 0;
+    st->hub_cluster = first_cluster_ < 0 ? 0 : first_cluster_;
   }
   return GLV_OK;
 }
@@ -2892,7 +3076,8 @@ struct Call {
 static int set_kernel_attributes() {
   const struct { const void *fn; int bytes; } want[] = {
       {(const void *)k_sweep_block, kBlockCap * (int)(sizeof(double) + sizeof(int32_t))},
-      {(const void *)k_sweep_iteration, (int)kPersistSmem},
+      {(const void *)k_sweep_iteration<false>, (int)kPersistSmem},
+      {(const void *)k_sweep_iteration<true>, (int)kPersistSmem},
       {(const void *)k_hub_accum, kHubStageCap * (int)(sizeof(double) + sizeof(int32_t))},
       {(const void *)k_chunk_records, (int)sizeof(PermTileSmem)},
   };
@@ -2902,6 +3087,11 @@ static int set_kernel_attributes() {
     if (e != cudaSuccess)
       return fail(GLV_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
   }
+  // clusters of 16 blocks are beyond the portable size of 8
+  const cudaError_t e = cudaFuncSetAttribute((const void *)k_sweep_iteration<true>,
+                                             cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+  if (e != cudaSuccess)
+    return fail(GLV_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
   return GLV_OK;
 }
 

@@ -6,7 +6,9 @@
 // vertices.  Launching a few kernels per class leaves the GPU waiting on
 // launches and on the single largest row of each class.  Here every block of
 // a persistent grid takes part in every class:
-//   stage 1  hub chunks (global tables) and rows of 1024..4095 entries per
+//   stage 1  hub rows on thread-block clusters (one table over the shared
+//            memory of a cluster's blocks) or, without clusters, hub chunks
+//            (global tables); rows of 1024..4095 entries per
 //            block; rows of 128..1023 entries per 128-thread team (shared
 //            tables); then warp items (rows <= 32 entries, and 33..127-entry
 //            rows with a per-warp shared table)                  -> grid barrier
@@ -30,6 +32,7 @@ struct StepDesc {
   int64_t hub_segs[2];     // hub scan work items
   int64_t apply[2];        // member range whose deltas are applied after this step
   int64_t cls;             // colour class of the step
+  int64_t ctask[2];        // hub tasks on thread-block clusters (cluster_row_tasks)
 };
 
 struct IterArgs {
@@ -47,7 +50,7 @@ struct IterArgs {
   double *cDeg;
   int32_t *cSize;
   uint64_t *trace;         // optional: globaltimer at each barrier, 4 per step + 2
-  int64_t *task_ctr;       // per step: next block task, next team task (zero at launch)
+  int64_t *task_ctr;       // per step: next block, team and cluster task (zero at launch)
   const int32_t *class_kept;  // gated sweeps: vertices the gate kept per class (NULL = all)
   int64_t nnz;
   const int64_t *split_row;   // merge-path tile boundaries of the level
@@ -98,6 +101,16 @@ __device__ __forceinline__ uint64_t global_ns() {
     if (p.trace && blockIdx.x == 0 && threadIdx.x == 0) p.trace[slot] = global_ns(); \
   } while (0)
 
+// Debug traces, 4 slots per step after the 4 per step + 2: the latest time
+// over the grid at which a queue of step s ran dry (q = 0 block queue, 1 team
+// queue, 2 warp items, 3 cluster tasks).
+#define GLV_QTRACE(s, q, cond)                                                       \
+  do {                                                                               \
+    if (p.trace && (cond))                                                           \
+      atomicMax((unsigned long long *)&p.trace[4 * p.nsteps + 2 + 4 * (s) + (q)],    \
+                (unsigned long long)global_ns());                                    \
+  } while (0)
+
 constexpr int kPersistThreads = 512;
 constexpr int kPersistTableCap = 8192;  // BIN_BLOCK rows: degree <= 4095
 constexpr int kPersistWarpCap = 256;    // warp-table rows: degree <= 127
@@ -109,6 +122,7 @@ static_assert(kPersistThreads / kTeamThreads * kTeamCap == kPersistTableCap,
 static_assert(kTeamThreads / 32 * kPersistWarpCap <= kTeamCap,
               "warp tables tile their team's table");
 static_assert(kPersistSmem >= sizeof(MergeSmem), "merge tiles must fit");
+static_assert(kPersistTableCap >= kClusterBlockSlots, "a cluster table part must fit");
 static_assert(kPersistSmem >= (size_t)(kPersistThreads / 32) * kPersistWarpCap *
                                   (sizeof(double) + sizeof(int32_t)),
               "warp tables must fit in the block-table region");
@@ -164,6 +178,10 @@ __device__ __forceinline__ void modularity_fold(const IterArgs &p, int64_t npart
   }
 }
 
+// kClusters: the instantiation launched with a cluster dimension, which runs
+// the steps' cluster tasks; the other one leaves that code out entirely (its
+// registers go to the other paths).
+template <bool kClusters>
 __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs p) {
   cg::grid_group grid = cg::this_grid();
   extern __shared__ unsigned char smem_raw[];
@@ -185,10 +203,13 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
   double *wvals = team_vals + (size_t)(tt >> 5) * kPersistWarpCap;
   int32_t *wkeys = team_keys + (size_t)(tt >> 5) * kPersistWarpCap;
   GLV_TRACE(4 * p.nsteps);
-  __shared__ int64_t s_task;
-  __shared__ int64_t s_team_task[kPersistThreads / kTeamThreads];
+  // next task of the block and team queues, by task parity: the following
+  // task is fetched when a task starts and published after it ends
+  __shared__ int64_t s_task[2];
+  __shared__ int64_t s_team_task[kPersistThreads / kTeamThreads][2];
   __shared__ int s_flag;
   __shared__ uint32_t s_word;
+  __shared__ ClusterShared s_cluster;
   // this block's slot of the moves' e_xx changes (only this block writes it)
   if (p.a.exx_delta && threadIdx.x == 0) p.a.exx_delta[blockIdx.x] = 0.0;
   for (int s = 0; s < p.nsteps; ++s) {
@@ -212,16 +233,25 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
     const int64_t t_seg = st.hub_segs[1] - st.hub_segs[0];
     const int64_t n256 = st.seg[BIN_T256 + 1] - st.seg[BIN_T256];
     const int64_t n128 = st.seg[BIN_T128 + 1] - st.seg[BIN_T128];
+    const int64_t t_ct = kClusters ? st.ctask[1] - st.ctask[0] : 0;
+    if constexpr (kClusters) if (t_ct > 0) {
+      // hub rows on clusters (launches with a cluster dimension): every block
+      // of a cluster takes part in every task of its cluster
+      cluster_row_tasks(p.a, p.h, st.ctask[0], t_ct, &p.task_ctr[3 * s + 2],
+                        reinterpret_cast<int32_t *>(tvals + kPersistTableCap), tvals, &s_cluster,
+                        s_g, s_c);
+      GLV_QTRACE(s, 3, threadIdx.x == 0);
+    }
     if (t_hub + t_blk + t_seg > 0) {
       // hub chunks, then block rows, then hub scan segments (which wait for
       // their hub's chunks: every chunk is handed out before any segment)
-      while (true) {
-        if (threadIdx.x == 0)
-          s_task = atomicAdd((unsigned long long *)&p.task_ctr[2 * s], 1ull);
-        __syncthreads();
-        int64_t t = s_task;
-        __syncthreads();
+      unsigned long long *ctr = (unsigned long long *)&p.task_ctr[3 * s];
+      if (threadIdx.x == 0) s_task[0] = (int64_t)atomicAdd(ctr, 1ull);
+      __syncthreads();
+      for (unsigned it = 0;; ++it) {
+        const int64_t t = s_task[it & 1];
         if (t >= t_hub + t_blk + t_seg) break;
+        const int64_t nxt = (threadIdx.x == 0) ? (int64_t)atomicAdd(ctr, 1ull) : 0;
         if (t < t_hub) {
           hub_accum_chunk(p.a, p.h, st.hub_chunk[0] + t,
                           reinterpret_cast<int32_t *>(tvals + kPersistTableCap), tvals, s_self,
@@ -233,20 +263,26 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
         } else {
           hub_segment_task(p.a, p.h, st.hub_segs[0] + (t - t_hub - t_blk), s_g, s_c, &s_word);
         }
+        if (threadIdx.x == 0) s_task[(it + 1) & 1] = nxt;
+        __syncthreads();
       }
+      GLV_QTRACE(s, 0, threadIdx.x == 0);
     }
     if (n256 + n128 > 0) {
-      while (true) {
-        if (tt == 0)
-          s_team_task[team] = atomicAdd((unsigned long long *)&p.task_ctr[2 * s + 1], 1ull);
-        team_sync<128>(team);
-        const int64_t t = s_team_task[team];
-        team_sync<128>(team);
+      unsigned long long *ctr = (unsigned long long *)&p.task_ctr[3 * s + 1];
+      if (tt == 0) s_team_task[team][0] = (int64_t)atomicAdd(ctr, 1ull);
+      team_sync<128>(team);
+      for (unsigned it = 0;; ++it) {
+        const int64_t t = s_team_task[team][it & 1];
         if (t >= n256 + n128) break;
+        const int64_t nxt = (tt == 0) ? (int64_t)atomicAdd(ctr, 1ull) : 0;
         const int64_t pos = (t < n256) ? st.seg[BIN_T256] + t : st.seg[BIN_T128] + (t - n256);
         team_vertex<128>(p.a, pos, team_keys, team_vals, team, s_self + 4 * team,
                          s_g + 4 * team, s_c + 4 * team);
+        if (tt == 0) s_team_task[team][(it + 1) & 1] = nxt;
+        team_sync<128>(team);
       }
+      GLV_QTRACE(s, 1, tt == 0);
     }
     for (int64_t k = gwi; k < witems; k += ngw) {
       int64_t q = k;
@@ -260,6 +296,7 @@ __global__ void __launch_bounds__(kPersistThreads, 2) k_sweep_iteration(IterArgs
       q -= n32;
       warp_table_vertex(p.a, st.seg[4] + q, wkeys, wvals);
     }
+    GLV_QTRACE(s, 2, (threadIdx.x & 31) == 0 && gwi < witems);
     grid.sync();
     GLV_TRACE(4 * s);
     if (!p.jacobi && st.apply[1] > st.apply[0]) {

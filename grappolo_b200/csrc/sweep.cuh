@@ -13,6 +13,8 @@
 // chunks in row order), so the sums are bit-identical to the reference's.
 #pragma once
 
+#include <cooperative_groups.h>
+
 #include "glv_common.cuh"
 
 namespace glv {
@@ -115,6 +117,15 @@ __device__ __forceinline__ int32_t finish_choice(const SweepArgs &a, int32_t own
   return t;
 }
 
+// The same with cSize[own] loaded by the caller ahead of time: only a move
+// out of a singleton reads the target's size.
+__device__ __forceinline__ int32_t finish_choice(const SweepArgs &a, int32_t own, int32_t own_size,
+                                                 double best_g, int32_t best_c) {
+  int32_t t = (best_g > 0.0) ? best_c : own;
+  if (t != own && own_size == 1 && t > own && a.cSize[t] == 1) t = own;
+  return t;
+}
+
 // ---------------------------------------------------------------------------
 // Rows of at most G entries: G lanes per vertex, one entry per lane, no table.
 // One warp handles the 32/G member slots starting at `base` (all lanes call).
@@ -132,8 +143,8 @@ __device__ __forceinline__ void small_item(const SweepArgs &a, int64_t base, int
   const int32_t own = (valid && deg > 0) ? a.C[v] : -1;
   const bool skip = valid && deg > 0 && skipped(a, v);
   const bool has = !skip && gl < deg;
-  const int32_t t = has ? a.tail[rb + gl] : -1;
-  const double wt = has ? a.w[rb + gl] : 0.0;
+  const int32_t t = has ? __ldcs(&a.tail[rb + gl]) : -1;
+  const double wt = has ? __ldcs(&a.w[rb + gl]) : 0.0;
   const int32_t c = has ? a.C[t] : -1;
   const unsigned long long key =
       has ? (((unsigned long long)grp << 32) | (uint32_t)c) : (0xFFFFFFFF00000000ull | lane);
@@ -231,12 +242,14 @@ __device__ __forceinline__ double warp_accumulate(const SweepArgs &a, int32_t v,
   double self_loop = 0.0;
   // Software pipeline, two rounds deep: while this round is folded, the next
   // round's communities are gathered and the round after's entries load.
-  // Neighbours' communities do not change during the sweep of one step.
+  // Neighbours' communities do not change during the sweep of one step.  The
+  // row's entries are read once per sweep: streaming loads (evict-first in
+  // L1 and L2) keep them from pushing the gathered per-vertex arrays out of L2.
   const int64_t j0 = rb + lane, j1 = j0 + stride;
-  int32_t t_cur = (j0 < re) ? a.tail[j0] : -1;
-  double w_cur = (j0 < re) ? a.w[j0] : 0.0;
-  int32_t t_next = (j1 < re) ? a.tail[j1] : -1;
-  double w_next = (j1 < re) ? a.w[j1] : 0.0;
+  int32_t t_cur = (j0 < re) ? __ldcs(&a.tail[j0]) : -1;
+  double w_cur = (j0 < re) ? __ldcs(&a.w[j0]) : 0.0;
+  int32_t t_next = (j1 < re) ? __ldcs(&a.tail[j1]) : -1;
+  double w_next = (j1 < re) ? __ldcs(&a.w[j1]) : 0.0;
   int32_t c_cur = (j0 < re) ? a.C[t_cur] : -1;
   for (int64_t base = rb; base < re; base += stride) {
     const int64_t j = base + lane;
@@ -248,8 +261,8 @@ __device__ __forceinline__ double warp_accumulate(const SweepArgs &a, int32_t v,
     c_cur = (jn < re) ? a.C[t_next] : -1;
     t_cur = t_next;
     w_cur = w_next;
-    t_next = (jnn < re) ? a.tail[jnn] : -1;
-    w_next = (jnn < re) ? a.w[jnn] : 0.0;
+    t_next = (jnn < re) ? __ldcs(&a.tail[jnn]) : -1;
+    w_next = (jnn < re) ? __ldcs(&a.w[jnn]) : 0.0;
     const uint32_t key = has ? (uint32_t)c : (0x80000000u | lane);
     const unsigned m = __match_any_sync(FULL, key);
     const bool leader = has && (lane == __ffs(m) - 1);
@@ -328,23 +341,26 @@ __device__ __forceinline__ void warp_table_vertex(const SweepArgs &a, int64_t po
     return;
   }
   const int64_t rb = a.ptr[v], re = a.ptr[v + 1];
+  const int32_t own = a.C[v];
+  const double degree = a.vDeg[v];
+  const double cdeg_own = a.cDeg[own];
+  const int32_t own_size = (lane == 0) ? a.cSize[own] : 0;
   const uint32_t cap = table_cap(re - rb);
   const uint32_t mask = cap - 1;
   for (uint32_t s = lane; s < cap; s += 32) { keys[s] = -1; vals[s] = 0.0; }
   __syncwarp();
-  const int32_t own = a.C[v];
   if (lane == 0) keys[hash_slot(own, mask)] = own;
   __syncwarp();
   const double self_loop = warp_accumulate(a, v, rb, re, 32, keys, vals, mask, false);
-  const double degree = a.vDeg[v];
   const double own_w = vals[hash_slot(own, mask)];
   const double eix = __dsub_rn(own_w, self_loop);
-  const double ax = __dsub_rn(a.cDeg[own], degree);
+  const double ax = __dsub_rn(cdeg_own, degree);
   double g = 0.0;
   int32_t bc = INT32_MAX;
   scan_table(a, keys, vals, lane, cap, 32, own, eix, ax, degree, cst_of(a, v), g, bc);
   warp_argmax(g, bc);
-  if (lane == 0) emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), degree, own_w, g);
+  if (lane == 0)
+    emit_decision(a, pos, v, own, finish_choice(a, own, own_size, g, bc), degree, own_w, g);
   __syncwarp();
 }
 
@@ -435,12 +451,18 @@ __device__ __forceinline__ void team_vertex(const SweepArgs &a, int64_t pos, int
     if (tt == 0) emit_stay(a, pos, v, a.C[v]);
     return;
   }
+  // the row's bounds and the vertex's own values load together, and the
+  // community totals of its own community right after: they arrive while
+  // the table is cleared and the row accumulates
   const int64_t rb = a.ptr[v], re = a.ptr[v + 1];
+  const int32_t own = a.C[v];
+  const double degree = a.vDeg[v];
+  const double cdeg_own = a.cDeg[own];
+  const int32_t own_size = (tt == 0) ? a.cSize[own] : 0;
   const uint32_t cap = table_cap(re - rb);
   const uint32_t mask = cap - 1;
   for (uint32_t s = tt; s < cap; s += T) { keys[s] = -1; vals[s] = 0.0; }
   team_sync<T>(team);
-  const int32_t own = a.C[v];
   if (tt == 0) keys[hash_slot(own, mask)] = own;
   team_sync<T>(team);
   const double sl = warp_accumulate(a, v, rb + 32 * tw, re, 32 * NW, keys, vals, mask, true);
@@ -448,10 +470,9 @@ __device__ __forceinline__ void team_vertex(const SweepArgs &a, int64_t pos, int
   team_sync<T>(team);
   double self_loop = 0.0;
   for (int k = 0; k < NW; ++k) self_loop = __dadd_rn(self_loop, s_self[k]);
-  const double degree = a.vDeg[v];
   const double own_w = vals[hash_slot(own, mask)];
   const double eix = __dsub_rn(own_w, self_loop);
-  const double ax = __dsub_rn(a.cDeg[own], degree);
+  const double ax = __dsub_rn(cdeg_own, degree);
   double g = 0.0;
   int32_t bc = INT32_MAX;
   scan_table(a, keys, vals, tt, cap, T, own, eix, ax, degree, cst_of(a, v), g, bc);
@@ -461,7 +482,7 @@ __device__ __forceinline__ void team_vertex(const SweepArgs &a, int64_t pos, int
   if (tt == 0) {
     for (int k = 1; k < NW; ++k)
       if (better(s_g[k], s_c[k], g, bc)) { g = s_g[k]; bc = s_c[k]; }
-    emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), degree, own_w, g);
+    emit_decision(a, pos, v, own, finish_choice(a, own, own_size, g, bc), degree, own_w, g);
   }
   team_sync<T>(team);
 }
@@ -522,6 +543,15 @@ struct HubWork {
   uint32_t epoch;           // this launch (0: the launch-per-kernel path, big[] instead)
   int32_t *err;             // set when a segment's wait gives up
   int chunk;                // CSR entries per accumulation chunk (<= kHubChunk)
+  // persistent kernel on thread-block clusters (cluster_row_tasks): the hub
+  // rows' tasks, one per (row, community partition); a partitioned row's
+  // partial bests are ct_g/ct_c[task] and segs_left[member slot] counts its
+  // partitions not yet done
+  const int32_t *ct_pos;    // task -> member slot
+  const int32_t *ct_part;   // task -> partition index
+  const int32_t *ct_nparts; // task -> partitions of its row (a power of two)
+  double *ct_g;             // task -> best gain of its partition
+  int32_t *ct_c;            //         and its community
 };
 
 constexpr int kHubChunk = 2048;      // most CSR entries per accumulation work item
@@ -844,6 +874,226 @@ __device__ __forceinline__ void hub_final(const SweepArgs &a, const HubWork &h, 
     h.own_w[pos] = 0.0;
     h.big[pos] = 0;
     h.chunks_left[pos] = (int32_t)((a.ptr[v + 1] - a.ptr[v] + h.chunk - 1) / h.chunk);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Hub rows on thread-block clusters (persistent kernel, parallel modes).  The
+// CL blocks of a cluster hold one open-addressing table in their shared
+// memory, reached through distributed shared memory: slot s lives in block
+// s mod CL at local slot s / CL, up to CL x kClusterBlockSlots slots.  A row
+// whose table would need more is split by community: partition p of P takes
+// the neighbours whose community c has mix32(c) mod P = p, each partition a
+// separate task that reads the whole row; the partitions' best moves are
+// folded by the last one to finish.  Nothing of a hub table touches HBM.
+
+constexpr int kClusterBlockSlots = 8192;  // table slots in one block's shared region
+constexpr int kClusterMax = 16;           // largest cluster the tasks support
+constexpr int kClusterMaxParts = 2;       // most partitions of a cluster row (each reads the row)
+
+// Per-block scratch of the cluster tasks; rank 0's copy is the one read.
+struct ClusterShared {
+  double acc[2][2];              // by task parity: the row's self-loop weight, Counter[own]
+  double g[kClusterMax];         // per block: best gain
+  int32_t c[kClusterMax];        //            and its community
+  int64_t next;                  // next task of the step (set by rank 0)
+};
+
+// Partitions of a row of `deg` entries on a cluster of `cl` blocks, and the
+// slots of each partition's table (both powers of two).
+__host__ __device__ inline void cluster_row_shape(int64_t deg, int cl, uint32_t *nparts,
+                                                  uint32_t *cap) {
+  const uint32_t need = table_cap(deg);
+  const uint32_t full = (uint32_t)cl * kClusterBlockSlots;
+  *nparts = need > full ? need / full : 1u;
+  *cap = need / *nparts;
+}
+
+// Find or insert `key` in the cluster table; returns the slot, or UINT32_MAX
+// when every slot holds another key (a partition far above its expected
+// load; the caller raises the error flag).
+__device__ __forceinline__ uint32_t cluster_table_slot(cooperative_groups::cluster_group &cl,
+                                                       int32_t *keys, uint32_t mask,
+                                                       unsigned cl_bits, int32_t key) {
+  uint32_t s = hash_slot(key, mask);
+  const uint32_t rank_mask = (1u << cl_bits) - 1u;
+  for (uint32_t probe = 0; probe <= mask; ++probe) {
+    int32_t *k = cl.map_shared_rank(keys, s & rank_mask) + (s >> cl_bits);
+    const int32_t old = atomicCAS(k, -1, key);
+    if (old == -1 || old == key) return s;
+    s = (s + 1) & mask;
+  }
+  return UINT32_MAX;
+}
+
+// Warp gw of the cluster's nw warps adds its entries of row [rb, rb + deg) that
+// fall in partition `part` to the cluster table, and sums (per lane) the row's
+// self-loop weight and the weight to the row's own community.
+__device__ __forceinline__ void cluster_accumulate(const SweepArgs &a,
+                                                   cooperative_groups::cluster_group &cl,
+                                                   int32_t v, int32_t own, int64_t rb, int64_t re,
+                                                   int64_t gw, int64_t nw, int32_t *keys,
+                                                   double *vals, uint32_t mask, unsigned cl_bits,
+                                                   uint32_t part, uint32_t part_mask,
+                                                   double &self_w, double &own_w, bool &overflow) {
+  const int lane = threadIdx.x & 31;
+  const int64_t stride = 32 * nw;
+  const uint32_t rank_mask = (1u << cl_bits) - 1u;
+  // two rounds in flight, as in warp_accumulate
+  const int64_t j0 = rb + 32 * gw + lane, j1 = j0 + stride;
+  int32_t t_cur = (j0 < re) ? __ldcs(&a.tail[j0]) : -1;
+  double w_cur = (j0 < re) ? __ldcs(&a.w[j0]) : 0.0;
+  int32_t t_next = (j1 < re) ? __ldcs(&a.tail[j1]) : -1;
+  double w_next = (j1 < re) ? __ldcs(&a.w[j1]) : 0.0;
+  int32_t c_cur = (j0 < re) ? a.C[t_cur] : -1;
+  for (int64_t base = rb + 32 * gw; base < re; base += stride) {
+    const int64_t j = base + lane;
+    const bool has = j < re;
+    const int32_t t = t_cur;
+    const double wt = w_cur;
+    const int32_t c = c_cur;
+    const int64_t jn = j + stride, jnn = j + 2 * stride;
+    c_cur = (jn < re) ? a.C[t_next] : -1;
+    t_cur = t_next;
+    w_cur = w_next;
+    t_next = (jnn < re) ? __ldcs(&a.tail[jnn]) : -1;
+    w_next = (jnn < re) ? __ldcs(&a.w[jnn]) : 0.0;
+    if (has && t == v) self_w += wt;
+    if (has && c == own) own_w += wt;
+    const bool mine = has && (mix32((uint32_t)c) & part_mask) == part;
+    const uint32_t key = mine ? (uint32_t)c : (0x80000000u | lane);
+    const unsigned m = __match_any_sync(FULL, key);
+    const bool leader = mine && (lane == __ffs(m) - 1);
+    double acc = 0.0;
+    unsigned rem = leader ? m : 0u;
+    const int rounds = __reduce_max_sync(FULL, (unsigned)__popc(rem));
+    for (int it = 0; it < rounds; ++it) {
+      const int src = rem ? __ffs(rem) - 1 : lane;
+      const double x = __shfl_sync(FULL, wt, src);
+      if (rem) { acc += x; rem &= rem - 1; }
+    }
+    if (leader) {
+      const uint32_t s = cluster_table_slot(cl, keys, mask, cl_bits, c);
+      if (s == UINT32_MAX) overflow = true;
+      else atomicAdd(cl.map_shared_rank(vals, s & rank_mask) + (s >> cl_bits), acc);
+    }
+  }
+}
+
+// The hub tasks [tb, tb + ntask) of one step, run by every thread of every
+// block of the cluster.  `keys`/`vals` are this block's table region (at
+// least kClusterBlockSlots slots), `cs` its ClusterShared, `red` 32 doubles
+// and `redc` 32 ints of block scratch (every block of the cluster calls with
+// the same tb, ntask and ctr).  Two cluster barriers per task: after
+// the inserts (row sums complete), and after the scan (every block's best in
+// rank 0, its own slots cleared again, the next task published).  The row
+// sums alternate between two slots by task parity, so rank 0 clears one pair
+// while the blocks may already add to the other.
+__device__ __forceinline__ void cluster_row_tasks(const SweepArgs &a, const HubWork &h, int64_t tb,
+                                               int64_t ntask, int64_t *ctr, int32_t *keys,
+                                               double *vals, ClusterShared *cs, double *red,
+                                               int32_t *redc) {
+  namespace cgx = cooperative_groups;
+  cgx::cluster_group cl = cgx::this_cluster();
+  const unsigned ncl = cl.num_blocks(), rank = cl.block_rank();
+  const unsigned cl_bits = __ffs(ncl) - 1;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwb = blockDim.x >> 5;
+  ClusterShared *cs0 = cl.map_shared_rank(cs, 0);
+  for (uint32_t q = threadIdx.x; q < kClusterBlockSlots; q += blockDim.x) {
+    keys[q] = -1;
+    vals[q] = 0.0;
+  }
+  if (rank == 0 && threadIdx.x == 0) {
+    cs->next = (int64_t)atomicAdd((unsigned long long *)ctr, 1ull);
+    cs->acc[0][0] = cs->acc[0][1] = cs->acc[1][0] = cs->acc[1][1] = 0.0;
+  }
+  cl.sync();
+  for (unsigned it = 0;; ++it) {
+    const int64_t t = cs0->next;
+    if (t >= ntask) break;
+    const int64_t ti = tb + t;
+    const int32_t pos = h.ct_pos[ti];
+    const uint32_t part = (uint32_t)h.ct_part[ti], nparts = (uint32_t)h.ct_nparts[ti];
+    const int32_t v = a.members[pos];
+    const int32_t own = a.C[v];
+    if (skipped(a, v)) {  // cluster-uniform
+      if (rank == 0 && threadIdx.x == 0 && part == 0) emit_stay(a, pos, v, own);
+      cl.sync();  // every block has read `next`
+      if (rank == 0 && threadIdx.x == 0)
+        cs->next = (int64_t)atomicAdd((unsigned long long *)ctr, 1ull);
+      cl.sync();
+      continue;
+    }
+    double *acc = cs0->acc[it & 1];
+    const int64_t rb = a.ptr[v], re = a.ptr[v + 1];
+    uint32_t np, cap;
+    cluster_row_shape(re - rb, (int)ncl, &np, &cap);
+    const uint32_t local = cap >> cl_bits;  // this block's slots of the table
+    double self_w = 0.0, own_w = 0.0;
+    bool overflow = false;
+    cluster_accumulate(a, cl, v, own, rb, re, (int64_t)rank * nwb + warp, (int64_t)ncl * nwb, keys,
+                       vals, cap - 1, cl_bits, part, nparts - 1, self_w, own_w, overflow);
+    if (overflow) atomicExch(h.err, 2);
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1) {
+      self_w += __shfl_xor_sync(FULL, self_w, off);
+      own_w += __shfl_xor_sync(FULL, own_w, off);
+    }
+    if (lane == 0) {
+      if (self_w != 0.0) atomicAdd(&acc[0], self_w);
+      if (own_w != 0.0) atomicAdd(&acc[1], own_w);
+    }
+    cl.sync();  // every entry is in the table, the row sums are complete
+    const double degree = a.vDeg[v];
+    const double row_own = acc[1];
+    const double eix = __dsub_rn(row_own, acc[0]);
+    const double ax = __dsub_rn(a.cDeg[own], degree);
+    double g = 0.0;
+    int32_t bc = INT32_MAX;
+    scan_table(a, keys, vals, threadIdx.x, local, blockDim.x, own, eix, ax, degree, cst_of(a, v),
+               g, bc);
+    warp_argmax(g, bc);
+    if (lane == 0) { red[warp] = g; redc[warp] = bc; }
+    __syncthreads();  // the block's scan is done: its slots are cleared below
+    if (threadIdx.x == 0) {
+      for (int k = 1; k < nwb; ++k)
+        if (better(red[k], redc[k], g, bc)) { g = red[k]; bc = redc[k]; }
+      cs0->g[rank] = g;
+      cs0->c[rank] = bc;
+      if (rank == 0) cs->next = (int64_t)atomicAdd((unsigned long long *)ctr, 1ull);
+    }
+    for (uint32_t q = threadIdx.x; q < local; q += blockDim.x) {
+      keys[q] = -1;
+      vals[q] = 0.0;
+    }
+    cl.sync();  // bests in rank 0, tables clear, next task published
+    if (rank == 0 && threadIdx.x == 0) {
+      g = cs->g[0];
+      bc = cs->c[0];
+      for (unsigned k = 1; k < ncl; ++k)
+        if (better(cs->g[k], cs->c[k], g, bc)) { g = cs->g[k]; bc = cs->c[k]; }
+      cs->acc[it & 1][0] = 0.0;  // read by every block before the barrier above
+      cs->acc[it & 1][1] = 0.0;
+      bool decide = true;
+      if (nparts > 1) {
+        // the last partition of the row to finish folds the others' bests
+        h.ct_g[ti] = g;
+        h.ct_c[ti] = bc;
+        __threadfence();
+        decide = atomicSub(&h.segs_left[pos], 1) == 1;
+        if (decide) {
+          __threadfence();
+          const int64_t t0 = ti - part;
+          for (uint32_t k = 0; k < nparts; ++k) {
+            const double pg = __ldcg(&h.ct_g[t0 + k]);
+            const int32_t pc = __ldcg(&h.ct_c[t0 + k]);
+            if (better(pg, pc, g, bc)) { g = pg; bc = pc; }
+          }
+          h.segs_left[pos] = (int32_t)nparts;
+        }
+      }
+      if (decide) emit_decision(a, pos, v, own, finish_choice(a, own, g, bc), degree, row_own, g);
+    }
   }
 }
 

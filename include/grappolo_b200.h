@@ -117,6 +117,9 @@ typedef struct glv_run_stats {
   int tuned_block_max;
   int tuned_hub_chunk;
   int tuned_from_cache;
+  /* Blocks per thread-block cluster of the hub rows in the first colour
+   * phase (0: every hub row as chunks over global tables). */
+  int hub_cluster;
 } glv_run_stats;
 
 /* ---- graph construction and files ---------------------------------------- */
