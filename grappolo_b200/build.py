@@ -13,7 +13,8 @@ NVCC = os.environ.get('NVCC', '/usr/local/cuda/bin/nvcc')
 
 SOURCES = ['engine.cu', 'compat.cpp']
 HEADERS = ['glv_common.cuh', 'sweep.cuh', 'phase_kernels.cuh', 'persist.cuh', 'recolor.cuh',
-           'batch.cuh', 'batch_kernels.cuh', 'gate.cuh', 'csr_build.cuh', 'compare.cuh']
+           'batch.cuh', 'batch_kernels.cuh', 'gate.cuh', 'csr_build.cuh', 'compare.cuh',
+           'coarsen_hash.cuh']
 FLAGS = ['-gencode', 'arch=compute_100a,code=sm_100a', '-O3', '-lineinfo', '--fmad=false',
          '-std=c++17', '-Xcompiler', '-fPIC', '-cudart', 'static',
          f'-I{os.path.join(ROOT, "include")}', f'-I{CSRC}']

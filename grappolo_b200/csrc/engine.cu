@@ -25,6 +25,7 @@
 #include "persist.cuh"
 #include "recolor.cuh"
 #include "vbase.cuh"
+#include "coarsen_hash.cuh"
 #include "phase_kernels.cuh"
 #include "sweep.cuh"
 
@@ -309,6 +310,8 @@ class Engine {
   int basic_phase(const Level &L, double lower, double thresh, double *mod, int *itr);
   int renumber(int32_t *C, int64_t n, int64_t *ncl);
   int coarsen(const Level &in, const int32_t *C, int64_t ncl, Level *out, int64_t *num_edges);
+  int coarsen_hash(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
+                   int64_t *num_edges, bool dense);
   int coarsen_chunked(const Level &in, const int32_t *C, int64_t ncl, Level *out,
                       int64_t *num_edges, int64_t budget, bool vf = false);
   int modularity_of(const Level &L, const int32_t *C, double *q);
@@ -2727,6 +2730,17 @@ int Engine::coarsen(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
     if (!ordered() && ncl > 0 && (cc || ncl + in.nnz > (int64_t(1) << 30)))
       return coarsen_chunked(in, Cm, ncl, out, num_edges, budget);
   }
+  // Fast and learned modes (no entry order to keep): a level with few
+  // communities folds its entries into a dense ncl x ncl matrix; the others
+  // keep the sorts.  GRAPPOLO_B200_COARSEN=sort|hash forces the sorts or the
+  // per-community hash tables on every level.
+  if (mode_ != GLV_MODE_VERIFY && ncl > 0) {
+    const char *cv = getenv("GRAPPOLO_B200_COARSEN");
+    const std::string want = cv ? cv : "";
+    if (want == "hash") return coarsen_hash(in, Cm, ncl, out, num_edges, false);
+    if (want != "sort" && ncl <= kDenseCoarseMax)
+      return coarsen_hash(in, Cm, ncl, out, num_edges, true);
+  }
   const bool debug = getenv("GRAPPOLO_B200_DEBUG") != nullptr;
   double tdbg = now_s();
   auto mark = [&](const char *what) {
@@ -2871,6 +2885,179 @@ int Engine::coarsen(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
   dfree(upper_first);
   *out = o;
   *num_edges = hne + ncl;
+  return GLV_OK;
+}
+
+// The next level without sorts (coarsen_hash.cuh): per-community hash
+// tables, or with `dense` an ncl x ncl matrix of sums (ncl <= kDenseCoarseMax).
+int Engine::coarsen_hash(const Level &in, const int32_t *Cm, int64_t ncl, Level *out,
+                         int64_t *num_edges, bool dense) {
+  const bool debug = getenv("GRAPPOLO_B200_DEBUG") != nullptr;
+  double tdbg = now_s();
+  auto mark = [&](const char *what) {
+    if (!debug) return;
+    cudaStreamSynchronize(s_);
+    const double t = now_s();
+    fprintf(stderr, "grappolo_b200: coarsen %s %.4f s\n", what, t - tdbg);
+    tdbg = t;
+  };
+  const int64_t nv = in.nv;
+  const int g_nv = grid_for(nv, 256, nsm_ * 16), g_cl = grid_for(ncl + 1, 256, nsm_ * 16);
+  // 1. members in community order and their entry offsets
+  uint32_t *mk1, *mk2;
+  int32_t *mv1, *mv2;
+  int64_t *mdeg, *mptr, *d_nmem;
+  TRY(alloc(&mk1, nv)); TRY(alloc(&mk2, nv)); TRY(alloc(&mv1, nv)); TRY(alloc(&mv2, nv));
+  TRY(alloc(&mdeg, nv + 1)); TRY(alloc(&mptr, nv + 1)); TRY(alloc(&d_nmem, 1));
+  CK(cudaMemsetAsync(d_nmem, 0, sizeof(int64_t), s_));
+  CK(cudaMemsetAsync(mdeg + nv, 0, sizeof(int64_t), s_));
+  LAUNCH(k_hc_member_keys, g_nv, 256, 0, s_, nv, Cm, in.ptr, ncl, mk1, mv1);
+  size_t tb = 0;
+  const int kbits = bits_for(ncl);
+  CK(cub::DeviceRadixSort::SortPairs(nullptr, tb, mk1, mk2, mv1, mv2, nv, 0, kbits, s_));
+  TRY(temp(tb));
+  CK(cub::DeviceRadixSort::SortPairs(temp_, tb, mk1, mk2, mv1, mv2, nv, 0, kbits, s_));
+  LAUNCH(k_hc_member_degrees, g_nv, 256, 0, s_, nv, mk2, mv2, in.ptr, ncl, mdeg, d_nmem);
+  CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, mdeg, mptr, nv + 1, s_));
+  TRY(temp(tb));
+  CK(cub::DeviceScan::ExclusiveSum(temp_, tb, mdeg, mptr, nv + 1, s_));
+  int64_t nmem = 0;
+  CK(cudaMemcpyAsync(&nmem, d_nmem, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  int64_t E = 0;
+  CK(cudaMemcpyAsync(&E, mptr + nmem, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
+  dfree(mk1); dfree(mv1); dfree(mdeg);
+  // 2. community entry ranges; big-community tables or the dense matrix
+  int64_t *cE0, *cE1, *capA, *gtoff, *nch, *nchoff, *cnt;
+  uint8_t *has_self;
+  int32_t *err;
+  TRY(alloc(&cE0, ncl + 1)); TRY(alloc(&cE1, ncl + 1)); TRY(alloc(&capA, ncl + 1));
+  TRY(alloc(&gtoff, ncl + 1)); TRY(alloc(&nch, ncl + 1)); TRY(alloc(&nchoff, ncl + 1));
+  TRY(alloc(&cnt, ncl + 1)); TRY(alloc(&has_self, ncl + 1)); TRY(alloc(&err, 1));
+  CK(cudaMemsetAsync(cE0, 0, (ncl + 1) * sizeof(int64_t), s_));
+  CK(cudaMemsetAsync(cE1, 0, (ncl + 1) * sizeof(int64_t), s_));
+  CK(cudaMemsetAsync(cnt, 0, (ncl + 1) * sizeof(int64_t), s_));
+  CK(cudaMemsetAsync(has_self, 0, (ncl + 1) * sizeof(uint8_t), s_));
+  CK(cudaMemsetAsync(err, 0, sizeof(int32_t), s_));
+  CK(cudaMemsetAsync(capA + ncl, 0, sizeof(int64_t), s_));
+  CK(cudaMemsetAsync(nch + ncl, 0, sizeof(int64_t), s_));
+  if (nmem > 0)
+    LAUNCH(k_hc_community_ranges, grid_for(nmem, 256, nsm_ * 16), 256, 0, s_, nmem, mk2, mptr, cE0,
+           cE1);
+  int64_t G = 0, nchunks = 0;
+  if (!dense) {
+    LAUNCH(k_hc_big_caps, g_cl, 256, 0, s_, ncl, cE0, cE1, capA, nch);
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, capA, gtoff, ncl + 1, s_));
+    TRY(temp(tb));
+    CK(cub::DeviceScan::ExclusiveSum(temp_, tb, capA, gtoff, ncl + 1, s_));
+    CK(cub::DeviceScan::ExclusiveSum(temp_, tb, nch, nchoff, ncl + 1, s_));
+    CK(cudaMemcpyAsync(&G, gtoff + ncl, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
+    CK(cudaMemcpyAsync(&nchunks, nchoff + ncl, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
+  }
+  CK(cudaStreamSynchronize(s_));
+  int32_t *gkeys = nullptr, *chunk_comm = nullptr, *out_b = nullptr;
+  double *gvals = nullptr, *dmat = nullptr, *out_w = nullptr;
+  uint32_t *dbits = nullptr;
+  if (dense) {
+    const int64_t cells = ncl * ncl;
+    TRY(alloc(&dmat, cells)); TRY(alloc(&dbits, (cells + 31) / 32));
+    CK(cudaMemsetAsync(dmat, 0, cells * sizeof(double), s_));
+    CK(cudaMemsetAsync(dbits, 0, ((cells + 31) / 32) * sizeof(uint32_t), s_));
+  } else {
+    TRY(alloc(&out_b, std::max<int64_t>(E, 1))); TRY(alloc(&out_w, std::max<int64_t>(E, 1)));
+    if (G > 0) {
+      TRY(alloc(&gkeys, G)); TRY(alloc(&gvals, G)); TRY(alloc(&chunk_comm, nchunks));
+      CK(cudaMemsetAsync(gkeys, 0xff, G * sizeof(int32_t), s_));
+      CK(cudaMemsetAsync(gvals, 0, G * sizeof(double), s_));
+      LAUNCH(k_hc_chunk_list, g_cl, 256, 0, s_, ncl, nchoff, chunk_comm);
+    }
+  }
+  dfree(capA); dfree(nch);
+  mark("hash members");
+  // 3. tasks: one window of kHashWindow entries' small communities each, then
+  // the big communities' chunks
+  if (E > 0) {
+    const int64_t nwin = (E + kHashWindow - 1) / kHashWindow;
+    int64_t *nbch, *nbch_off;
+    TRY(alloc(&nbch, ncl + 1)); TRY(alloc(&nbch_off, ncl + 1));
+    CK(cudaMemsetAsync(nbch + ncl, 0, sizeof(int64_t), s_));
+    unsigned long long *wE0, *wE1;
+    TRY(alloc(&wE0, nwin)); TRY(alloc(&wE1, nwin));
+    CK(cudaMemsetAsync(wE0, 0xff, nwin * sizeof(unsigned long long), s_));
+    CK(cudaMemsetAsync(wE1, 0, nwin * sizeof(unsigned long long), s_));
+    LAUNCH(k_hc_windows, g_cl, 256, 0, s_, ncl, cE0, cE1, wE0, wE1, nbch);
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, nbch, nbch_off, ncl + 1, s_));
+    TRY(temp(tb));
+    CK(cub::DeviceScan::ExclusiveSum(temp_, tb, nbch, nbch_off, ncl + 1, s_));
+    int64_t nbig = 0;
+    CK(cudaMemcpyAsync(&nbig, nbch_off + ncl, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
+    CK(cudaStreamSynchronize(s_));
+    const int64_t ntask = nwin + nbig;
+    unsigned long long *tE0, *tE1;
+    int64_t *mlo, *mhi;
+    TRY(alloc(&tE0, ntask)); TRY(alloc(&tE1, ntask)); TRY(alloc(&mlo, ntask)); TRY(alloc(&mhi, ntask));
+    CK(cudaMemcpyAsync(tE0, wE0, nwin * sizeof(unsigned long long), cudaMemcpyDeviceToDevice, s_));
+    CK(cudaMemcpyAsync(tE1, wE1, nwin * sizeof(unsigned long long), cudaMemcpyDeviceToDevice, s_));
+    dfree(wE0); dfree(wE1);
+    if (nbig > 0)
+      LAUNCH(k_hc_big_tasks, g_cl, 256, 0, s_, ncl, nwin, cE0, cE1, nbch_off, tE0, tE1);
+    LAUNCH(k_hc_tile_members, grid_for(ntask, 256, nsm_ * 16), 256, 0, s_, ntask, tE0, tE1, mptr,
+           nmem, mlo, mhi);
+    HashTileArgs ha{ntask, nwin, nmem, ncl, mptr, tE0, tE1, mlo, mhi, mk2, mv2, in.ptr, in.tail,
+                    in.w, Cm, cE0, gtoff, gkeys, gvals, out_b, out_w, cnt, has_self, err, dmat,
+                    dbits};
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_hc_tiles, kHashThreads,
+                                                     sizeof(HashTileSmem)));
+    if (per_sm < 1) return fail(GLV_ERR_CUDA, "coarsening task kernel does not fit on an SM");
+    const int grid = (int)std::min<int64_t>(ntask, (int64_t)per_sm * nsm_);
+    LAUNCH(k_hc_tiles, grid, kHashThreads, sizeof(HashTileSmem), s_, ha);
+    dfree(nbch); dfree(nbch_off); dfree(tE0); dfree(tE1); dfree(mlo); dfree(mhi);
+    mark("hash tasks");
+    if (nchunks > 0)
+      LAUNCH(k_hc_big_emit, (int)std::min<int64_t>(nchunks, nsm_ * 8), 256, 0, s_, nchunks,
+             chunk_comm, nchoff, gtoff, gkeys, gvals, cE0, out_b, out_w, cnt, has_self);
+    mark("hash big");
+  }
+  int32_t herr = 0;
+  CK(cudaMemcpyAsync(&herr, err, sizeof(int32_t), cudaMemcpyDeviceToHost, s_));
+  // 4. rows
+  int64_t *rowc;
+  TRY(alloc(&rowc, ncl + 1));
+  const int g_rows = grid_for(ncl * 32, 256, nsm_ * 16);
+  if (dense) LAUNCH(k_hc_dense_counts, g_rows, 256, 0, s_, ncl, dbits, rowc);
+  else LAUNCH(k_hc_row_lengths, g_cl, 256, 0, s_, ncl, cnt, has_self, rowc);
+  Level o;
+  o.nv = ncl;
+  o.owned = true;
+  TRY(alloc(&o.ptr, ncl + 1));
+  CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, rowc, o.ptr, ncl + 1, s_));
+  TRY(temp(tb));
+  CK(cub::DeviceScan::ExclusiveSum(temp_, tb, rowc, o.ptr, ncl + 1, s_));
+  CK(cudaMemcpyAsync(&o.nnz, o.ptr + ncl, sizeof(int64_t), cudaMemcpyDeviceToHost, s_));
+  CK(cudaStreamSynchronize(s_));
+  if (herr) return fail(GLV_ERR_CUDA, "coarsening: a community's table filled up");
+  TRY(alloc(&o.tail, o.nnz)); TRY(alloc(&o.w, o.nnz));
+  if (dense) {
+    LAUNCH(k_hc_dense_emit, g_rows, 256, 0, s_, ncl, dbits, dmat, o.ptr, o.tail, o.w);
+  } else {
+    const int64_t nct = (o.nnz + kCopyTile - 1) / kCopyTile;
+    int64_t *alo, *ahi;
+    TRY(alloc(&alo, nct)); TRY(alloc(&ahi, nct));
+    LAUNCH(k_hc_copy_rows, grid_for(nct, 256, nsm_ * 16), 256, 0, s_, nct, ncl, o.ptr, alo, ahi);
+    LAUNCH(k_hc_compact, (int)std::max<int64_t>(1, std::min<int64_t>(nct, nsm_ * 8)), 256, 0, s_,
+           ncl, o.ptr, alo, ahi, cE0, has_self, out_b, out_w, o.tail, o.w);
+    dfree(alo); dfree(ahi);
+  }
+  CK(cudaStreamSynchronize(s_));
+  mark("hash rows");
+  dfree(mk2); dfree(mv2); dfree(mptr); dfree(d_nmem); dfree(cE0); dfree(cE1); dfree(gtoff);
+  dfree(nchoff); dfree(cnt); dfree(has_self); dfree(err); dfree(rowc);
+  if (out_b) { dfree(out_b); dfree(out_w); }
+  if (gkeys) { dfree(gkeys); dfree(gvals); dfree(chunk_comm); }
+  if (dmat) { dfree(dmat); dfree(dbits); }
+  *out = o;
+  *num_edges = (o.nnz - ncl) / 2 + ncl;  // one (a, a) entry per row, the rest in mirrored pairs
   return GLV_OK;
 }
 
@@ -3080,6 +3267,7 @@ static int set_kernel_attributes() {
       {(const void *)k_sweep_iteration<true>, (int)kPersistSmem},
       {(const void *)k_hub_accum, kHubStageCap * (int)(sizeof(double) + sizeof(int32_t))},
       {(const void *)k_chunk_records, (int)sizeof(PermTileSmem)},
+      {(const void *)k_hc_tiles, (int)sizeof(HashTileSmem)},
   };
   for (const auto &k : want) {
     const cudaError_t e =
