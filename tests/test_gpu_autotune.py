@@ -6,8 +6,11 @@ after each trial) and caches the choice by the graph's signature.
   graph the community array still equals the reference's one-thread run
   (the pinned digest of tests/golden/pins.json);
 * a second run on the same graph takes the cached choice;
-* tuned runs are not slower than the default knobs (device sweep time), and
-  fast-mode modularity stays within the reference's range.
+* tuned runs are not slower than the default knobs (device sweep time per
+  sweep, under the deterministic id-order colouring: with the speculative
+  colouring's races the iteration count of R-MAT 20 varies about threefold
+  from run to run), and fast-mode modularity stays within the reference's
+  range.
 """
 import hashlib
 import json
@@ -41,6 +44,7 @@ def test_tuned_not_slower_and_cached(monkeypatch, name):
     with open(os.path.join(HERE, 'golden', 'fast_pins.json')) as f:
         lo, hi = json.load(f)[name]['printed_range']
     g = make_graph(name)
+    monkeypatch.setenv('GRAPPOLO_B200_COLORING', 'id')
     _lib.lib().glv_set_profiling(1)  # device time of the sweep launches
     try:
         monkeypatch.setenv('GRAPPOLO_B200_AUTOTUNE', '0')
@@ -57,7 +61,7 @@ def test_tuned_not_slower_and_cached(monkeypatch, name):
         assert (st['tuned_block_max'], st['tuned_hub_chunk']) == \
             (first['tuned_block_max'], first['tuned_hub_chunk'])
         assert lo - 1e-3 <= st['final_modularity'] <= hi + 1e-3
-    t_base = sorted(s['sweep_kernel_time'] for s in base)[1]
-    t_tuned = sorted(s['sweep_kernel_time'] for s in tuned)[1]
+    t_base = sorted(s['sweep_kernel_time'] / s['total_iterations'] for s in base)[1]
+    t_tuned = sorted(s['sweep_kernel_time'] / s['total_iterations'] for s in tuned)[1]
     assert t_tuned <= 1.10 * t_base, (t_tuned, t_base, first['tuned_block_max'],
                                       first['tuned_hub_chunk'])

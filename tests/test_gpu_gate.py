@@ -63,9 +63,13 @@ def _trained():
 RUNS = 5  # fast-mode runs differ (atomic order): compare medians
 
 
-def test_learned_gate_gains_over_plain():
+def test_learned_gate_gains_over_plain(monkeypatch):
     """Planted power-law graph: the gated runs evaluate fewer CSR entries and
-    their median modularity is within 1e-3 of the plain runs' median."""
+    their median modularity is within 1e-3 of the plain runs' median.  The
+    deterministic id-order colouring is used: with the speculative colouring's
+    races the iteration count of this graph ranges from 11 to 24 from run to
+    run, which buries the gate's saving in the spread of the plain runs."""
+    monkeypatch.setenv('GRAPPOLO_B200_COLORING', 'id')
     p, tau = _trained()
     gate.set_gate(p, tau)
     g = graphs.planted_powerlaw(150000, seed=21)
