@@ -1497,7 +1497,7 @@ int Engine::launch_sweep(const Level &L, const Step &st, SweepArgs a, bool order
           const int64_t nc = st.hub_chunk[1] - st.hub_chunk[0];
           const int64_t ns = st.hub_segs[1] - st.hub_segs[0];
           LAUNCH(k_hub_accum, (int)std::min<int64_t>(nc, nsm_ * 4), 512,
-                 kHubStageCap * (sizeof(double) + sizeof(int32_t)), s_, a, hw, st.hub_chunk[0],
+                 kHubStageSmem, s_, a, hw, st.hub_chunk[0],
                  st.hub_chunk[1]);
           LAUNCH(k_hub_scan, (int)std::min<int64_t>(ns, nsm_ * 8), 256, 0, s_, a, hw,
                  st.hub_segs[0], st.hub_segs[1]);
@@ -3265,7 +3265,7 @@ static int set_kernel_attributes() {
       {(const void *)k_sweep_block, kBlockCap * (int)(sizeof(double) + sizeof(int32_t))},
       {(const void *)k_sweep_iteration<false>, (int)kPersistSmem},
       {(const void *)k_sweep_iteration<true>, (int)kPersistSmem},
-      {(const void *)k_hub_accum, kHubStageCap * (int)(sizeof(double) + sizeof(int32_t))},
+      {(const void *)k_hub_accum, kHubStageSmem},
       {(const void *)k_chunk_records, (int)sizeof(PermTileSmem)},
       {(const void *)k_hc_tiles, (int)sizeof(HashTileSmem)},
   };

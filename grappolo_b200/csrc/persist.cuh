@@ -123,6 +123,9 @@ static_assert(kTeamThreads / 32 * kPersistWarpCap <= kTeamCap,
               "warp tables tile their team's table");
 static_assert(kPersistSmem >= sizeof(MergeSmem), "merge tiles must fit");
 static_assert(kPersistTableCap >= kClusterBlockSlots, "a cluster table part must fit");
+static_assert(kHubStageCap * (sizeof(double) + sizeof(int32_t)) <=
+                  (size_t)kPersistTableCap * sizeof(double),
+              "a hub chunk's staging values and filled-slot list sit below the table keys");
 static_assert(kPersistSmem >= (size_t)(kPersistThreads / 32) * kPersistWarpCap *
                                   (sizeof(double) + sizeof(int32_t)),
               "warp tables must fit in the block-table region");

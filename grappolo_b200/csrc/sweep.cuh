@@ -224,6 +224,23 @@ __device__ __forceinline__ uint32_t table_slot(int32_t *keys, uint32_t mask, int
   }
 }
 
+// table_slot that also tells whether this call inserted the key.
+__device__ __forceinline__ uint32_t table_slot_new(int32_t *keys, uint32_t mask, int32_t key,
+                                                   bool &fresh) {
+  uint32_t s = hash_slot(key, mask);
+  fresh = false;
+  while (true) {
+    int32_t k = keys[s];
+    if (k == key) return s;
+    if (k == -1) {
+      int32_t old = atomicCAS(&keys[s], -1, key);
+      if (old == -1) { fresh = true; return s; }
+      if (old == key) return s;
+    }
+    s = (s + 1) & mask;
+  }
+}
+
 __device__ __forceinline__ uint32_t table_find(const int32_t *keys, uint32_t mask, int32_t key) {
   uint32_t s = hash_slot(key, mask);
   while (keys[s] != key) s = (s + 1) & mask;
@@ -234,10 +251,12 @@ __device__ __forceinline__ uint32_t table_find(const int32_t *keys, uint32_t mas
 // fold their group's weights starting from the table value, so each
 // community's sum is the sequential CSR-order sum.  Returns the self-loop sum
 // (same value in every lane).  With `atomic_add` the group sums are added with
-// atomics instead (used when several warps share one table).
+// atomics instead (used when several warps share one table).  With `fill`
+// every slot this call fills first is appended to fill[] (count in *nfill).
 __device__ __forceinline__ double warp_accumulate(const SweepArgs &a, int32_t v, int64_t rb,
                                                   int64_t re, int64_t stride, int32_t *keys,
-                                                  double *vals, uint32_t mask, bool atomic_add) {
+                                                  double *vals, uint32_t mask, bool atomic_add,
+                                                  int32_t *fill = nullptr, int *nfill = nullptr) {
   const int lane = threadIdx.x & 31;
   double self_loop = 0.0;
   // Software pipeline, two rounds deep: while this round is folded, the next
@@ -269,7 +288,13 @@ __device__ __forceinline__ double warp_accumulate(const SweepArgs &a, int32_t v,
     uint32_t slot = 0;
     double acc = 0.0;
     if (leader) {
-      slot = table_slot(keys, mask, c);
+      if (fill) {
+        bool fresh;
+        slot = table_slot_new(keys, mask, c, fresh);
+        if (fresh) fill[atomicAdd(nfill, 1)] = (int32_t)slot;
+      } else {
+        slot = table_slot(keys, mask, c);
+      }
       if (!atomic_add) acc = vals[slot];
     }
     unsigned rem = leader ? m : 0u;
@@ -560,6 +585,8 @@ constexpr int kHubStageCap = 4096;   // block-local staging table of one chunk
 constexpr int kHubInlineCap = 4096;  // filled slots the last chunk's block scans itself
 constexpr int kHubBatch = 4;         // table slots a thread has in flight at once
 static_assert(kHubChunk < kHubStageCap, "a chunk's distinct keys must fit the staging table");
+// staging values, the filled-slot list and staging keys of one chunk
+constexpr int kHubStageSmem = kHubStageCap * (int)(sizeof(double) + 2 * sizeof(int32_t));
 
 // Best (gain, id) over the filled slots occ[k0..k1) of a hub table; the slots
 // are emptied for the table's next use.  kHubBatch slots per thread are
@@ -610,31 +637,37 @@ __device__ __forceinline__ void hub_accum_chunk(const SweepArgs &a, const HubWor
   const int32_t v = a.members[pos];
   const bool skip = skipped(a, v);  // block-uniform
   const uint32_t smask = kHubStageCap - 1;
+  // the staging slots in the order they were first filled (s_flag[0] of them)
+  int32_t *sfill = reinterpret_cast<int32_t *>(svals + kHubStageCap);
   if (!skip) {
   for (uint32_t q = threadIdx.x; q < kHubStageCap; q += blockDim.x) { skeys[q] = -1; svals[q] = 0.0; }
-  if (threadIdx.x == 0) s_self[0] = 0.0;
+  if (threadIdx.x == 0) { s_self[0] = 0.0; s_flag[0] = 0; }
   __syncthreads();
-  double sl = warp_accumulate(a, v, eb + 32 * warp, ee, 32 * nwb, skeys, svals, smask, true);
+  double sl = warp_accumulate(a, v, eb + 32 * warp, ee, 32 * nwb, skeys, svals, smask, true, sfill,
+                              s_flag);
   if (lane == 0 && sl != 0.0) atomicAdd(&s_self[0], sl);
   __syncthreads();
+  const int nfill = s_flag[0];
   const uint32_t mask = table_cap(a.ptr[v + 1] - a.ptr[v]) - 1;
   int32_t *keys = h.keys + h.tab_off[pos];
   double *vals = h.vals + h.tab_off[pos];
   int32_t *occ = h.occ + h.occ_off[pos];
   const int32_t own = a.C[v];
   // Each thread inserts kHubBatch staged keys at once: the probes of one
-  // round are independent CASes in flight together.
-  for (uint32_t q0 = 0; q0 < kHubStageCap; q0 += kHubBatch * blockDim.x) {
-    // blockDim * kHubBatch divides kHubStageCap: warp-uniform loop
+  // round are independent CASes in flight together.  Only the filled staging
+  // slots are visited (at most kHubChunk: one round of 4 x 512 keys).
+  for (int q0 = 0; q0 < nfill; q0 += kHubBatch * (int)blockDim.x) {
+    // nfill is the block's: a block-uniform loop
     int32_t c[kHubBatch];
     double val[kHubBatch];
     uint32_t s[kHubBatch];
     bool pend[kHubBatch], ins[kHubBatch];
 #pragma unroll
     for (int j = 0; j < kHubBatch; ++j) {
-      const uint32_t q = q0 + j * blockDim.x + threadIdx.x;
-      c[j] = skeys[q];
-      val[j] = svals[q];
+      const int q = q0 + j * (int)blockDim.x + (int)threadIdx.x;
+      const int32_t sl = (q < nfill) ? sfill[q] : -1;
+      c[j] = (sl >= 0) ? skeys[sl] : -1;
+      val[j] = (sl >= 0) ? svals[sl] : 0.0;
       pend[j] = c[j] >= 0;
       ins[j] = false;
       s[j] = pend[j] ? hash_slot(c[j], mask) : 0u;
@@ -1103,8 +1136,9 @@ __global__ void __launch_bounds__(512) k_hub_accum(SweepArgs a, HubWork h, int64
   __shared__ double s_self[1], s_g[32];
   __shared__ int32_t s_c[32];
   __shared__ int s_flag[1];
+  // staging values, the filled-slot list, staging keys (kHubStageSmem bytes)
   double *svals = reinterpret_cast<double *>(smem_raw);
-  int32_t *skeys = reinterpret_cast<int32_t *>(svals + kHubStageCap);
+  int32_t *skeys = reinterpret_cast<int32_t *>(svals + kHubStageCap) + kHubStageCap;
   for (int64_t ci = cb + blockIdx.x; ci < ce; ci += gridDim.x)
     hub_accum_chunk(a, h, ci, skeys, svals, s_self, s_g, s_c, s_flag, -1);
 }
