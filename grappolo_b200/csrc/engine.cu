@@ -719,8 +719,18 @@ int Engine::phase_init(const Level &L, bool need_past) {
     LAUNCH(k_init_phase, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, L.ptr, L.w, vDeg, cDeg,
            cSize, C, need_past ? Cpast : (int32_t *)nullptr);
   } else {
-    LAUNCH(k_init_phase_warp, grid_for(L.nv * 32, 256, nsm_ * 16), 256, 0, s_, L.nv, L.ptr, L.w,
-           vDeg, cDeg, cSize, C, need_past ? Cpast : (int32_t *)nullptr);
+    if (L.nnz >= 64 * L.nv) {  // long rows: a warp per row reads them coalesced
+      LAUNCH(k_init_phase_warp, grid_for(L.nv * 32, 256, nsm_ * 16), 256, 0, s_, L.nv, L.ptr,
+             L.w, vDeg, cDeg, cSize, C, need_past ? Cpast : (int32_t *)nullptr);
+    } else {  // short rows: merge-path tiles (split_row_ from merge_splits above)
+      CK(cudaMemsetAsync(vDeg, 0, L.nv * sizeof(double), s_));
+      const int64_t nt = merge_tiles(L.nv, L.nnz);
+      if (L.nnz > 0)
+        LAUNCH(k_row_sums_tiles, (int)std::max<int64_t>(1, std::min<int64_t>(nt, nsm_ * 8)),
+               kRowSumThreads, sizeof(RowSumSmem), s_, L.nv, L.nnz, L.ptr, L.w, split_row_, vDeg);
+      LAUNCH(k_init_phase_fill, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, vDeg, cDeg,
+             cSize, C, need_past ? Cpast : (int32_t *)nullptr);
+    }
   }
   if (ordered()) {
     LAUNCH(k_constant_sequential, 1, 1, 0, s_, L.nv, vDeg, cst);
@@ -3268,6 +3278,7 @@ static int set_kernel_attributes() {
       {(const void *)k_hub_accum, kHubStageSmem},
       {(const void *)k_chunk_records, (int)sizeof(PermTileSmem)},
       {(const void *)k_hc_tiles, (int)sizeof(HashTileSmem)},
+      {(const void *)k_row_sums_tiles, (int)sizeof(RowSumSmem)},
   };
   for (const auto &k : want) {
     const cudaError_t e =

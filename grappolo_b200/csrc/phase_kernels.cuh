@@ -30,7 +30,8 @@ __global__ void k_init_phase(int64_t nv, const int64_t *ptr, const double *w, do
 }
 
 // Same results when every summation order is exact (integral weights) or when
-// bit-exactness is not asked for: one warp per row.
+// bit-exactness is not asked for: one warp per row (levels of long rows; see
+// k_row_sums_tiles for levels of short ones).
 __global__ void k_init_phase_warp(int64_t nv, const int64_t *ptr, const double *w, double *vDeg,
                                   double *cDeg, int32_t *cSize, int32_t *C, int32_t *C2) {
   const int lane = threadIdx.x & 31;
@@ -172,6 +173,92 @@ struct MergeSmem {
   int32_t off[kMergeTile + 2];
   int32_t comm[kMergeTile + 1];
 };
+
+// Row sums of w (vertex degrees) over merge-path tiles, for the parallel
+// modes (any order of a row's additions): every entry is read once, with
+// coalesced loads, instead of a warp walking each row.  A tile sums its
+// entries per row (a segmented scan over each warp's entries, then one
+// shared add per row and warp); a row wholly inside the tile is stored, a row that
+// spans tiles gets each tile's part with an atomic add (vDeg must be zero on
+// entry).  Launched with kRowSumThreads threads and sizeof(RowSumSmem) bytes.
+constexpr int kRowSumThreads = 256;
+struct RowSumSmem {
+  double acc[kMergeTile + 1];
+  int32_t off[kMergeTile + 2];
+};
+
+__global__ void __launch_bounds__(kRowSumThreads) k_row_sums_tiles(int64_t nv, int64_t nnz,
+                                                                   const int64_t *ptr,
+                                                                   const double *w,
+                                                                   const int64_t *split_row,
+                                                                   double *vDeg) {
+  extern __shared__ unsigned char smem_raw[];
+  RowSumSmem &sm = *reinterpret_cast<RowSumSmem *>(smem_raw);
+  const int lane = threadIdx.x & 31;
+  const int64_t ntiles = merge_tiles(nv, nnz);
+  for (int64_t tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int64_t d0 = tile * (int64_t)kMergeTile;
+    const int64_t d1 = min(d0 + (int64_t)kMergeTile, nv + nnz);
+    const int64_t i0 = split_row[tile], i1 = split_row[tile + 1];
+    const int64_t j0 = d0 - i0, j1 = d1 - i1;
+    if (j1 <= j0) continue;  // only row ends: those rows are complete or zero (tile-uniform)
+    // rows holding entries j0..j1-1: i0 .. ih
+    const int64_t ih = min(i1, nv - 1);
+    const int nr = (int)(ih - i0 + 1);
+    for (int k = threadIdx.x; k <= nr; k += kRowSumThreads) {
+      const int64_t r = ptr[i0 + k] - j0;
+      sm.off[k] = (int32_t)max((int64_t)0, min(r, (int64_t)kMergeTile + 1));
+      if (k < nr) sm.acc[k] = 0.0;
+    }
+    __syncthreads();
+    const int ne = (int)(j1 - j0);
+    for (int q0 = 0; q0 < ne; q0 += kRowSumThreads) {  // ne is the tile's: warp-uniform
+      const int q = q0 + (int)threadIdx.x;
+      const bool has = q < ne;
+      int lo = 0;
+      double x = 0.0;
+      if (has) {
+        int hi = nr - 1;  // the last row starting at or before q
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (sm.off[mid] <= q) lo = mid; else hi = mid - 1;
+        }
+        x = w[j0 + q];
+      }
+      // the warp's entries come in row order: a segmented inclusive scan
+      // leaves each row's warp sum in its last lane
+      const int key = has ? lo : -1 - lane;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const double y = __shfl_up_sync(FULL, x, off);
+        const int ky = __shfl_up_sync(FULL, key, off);
+        if (lane >= off && ky == key) x += y;
+      }
+      const int knext = __shfl_down_sync(FULL, key, 1);
+      if (has && (lane == 31 || knext != key)) atomicAdd(&sm.acc[lo], x);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < nr; k += kRowSumThreads) {
+      const int64_t i = i0 + k;
+      const bool whole = ptr[i] >= j0 && i < i1;  // starts and ends in this tile
+      if (whole) vDeg[i] = sm.acc[k];
+      else if (sm.acc[k] != 0.0) atomicAdd(&vDeg[i], sm.acc[k]);
+    }
+    __syncthreads();  // the next tile reuses the shared arrays
+  }
+}
+
+// The singleton state of a phase from the degrees in vDeg.
+__global__ void k_init_phase_fill(int64_t nv, const double *vDeg, double *cDeg, int32_t *cSize,
+                                  int32_t *C, int32_t *C2) {
+  for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    cDeg[v] = vDeg[v];
+    cSize[v] = 1;
+    C[v] = (int32_t)v;
+    if (C2) C2[v] = (int32_t)v;
+  }
+}
 
 // Modularity partials of merge tile `tile` added to (ex, a2): a2 over the rows
 // that end in the tile, ex over its entries whose two ends share a community
