@@ -359,7 +359,8 @@ class Engine {
   unsigned long long *evald_ = nullptr;
   int phase_index_ = 0;
   bool learned() const { return mode_ == GLV_MODE_LEARNED; }
-  int gate_init();
+  int gate_init(int64_t nv, bool tracing);
+  void gate_release();
 
  public:  // the allocator (the C ABI helpers allocate level-0 arrays through it)
   // Requests above 1 MiB are rounded up to quarter-octave size classes so that
@@ -1966,11 +1967,15 @@ __global__ void k_trace_append(int64_t nv, const int64_t *ptr, const float *feat
   }
 }
 
-int Engine::gate_init() {
+// The gate's per-vertex state lives for one phase's sweeps: sized for the
+// phase's level and released after its last sweep, so the coarsening that
+// follows (the run's memory peak on large graphs) has that memory back.
+int Engine::gate_init(int64_t nv, bool tracing) {
   if (rec_own_) return GLV_OK;
-  const size_t n = (size_t)nv0_ + 1;
+  const size_t n = (size_t)nv + 1;
   TRY(alloc(&rec_own_, n)); TRY(alloc(&rec_gain_, n)); TRY(alloc(&last_move_, n));
-  TRY(alloc(&skip_, n)); TRY(alloc(&feat_, n * kGateIn)); TRY(alloc(&gate_p_, kGateParams));
+  TRY(alloc(&skip_, n)); TRY(alloc(&gate_p_, kGateParams));
+  if (tracing) TRY(alloc(&feat_, n * kGateIn));  // feature rows only for trace capture
   TRY(alloc(&evald_, 1));
   if (learned()) {
     std::lock_guard<std::mutex> lock(g_gate_mu);
@@ -1981,6 +1986,11 @@ int Engine::gate_init() {
     CK(cudaStreamSynchronize(s_));
   }
   return GLV_OK;
+}
+
+void Engine::gate_release() {
+  dfree(rec_own_); dfree(rec_gain_); dfree(last_move_); dfree(skip_); dfree(feat_);
+  dfree(gate_p_); dfree(evald_);
 }
 
 __global__ void k_scatter_i32(int64_t n, const int32_t *pos, const int32_t *val, int32_t *out) {
@@ -2232,7 +2242,7 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
     CK(cudaMemcpyAsync(bt->act, bt->h_act.data(), bt->G, cudaMemcpyHostToDevice, s_));
   }
   if (gating || tracing) {
-    TRY(gate_init());
+    TRY(gate_init(L.nv, tracing));
     CK(cudaMemsetAsync(last_move_, 0, L.nv * sizeof(int32_t), s_));
     CK(cudaMemsetAsync(rec_own_, 0, L.nv * sizeof(double), s_));
     CK(cudaMemsetAsync(rec_gain_, 0, L.nv * sizeof(float), s_));
@@ -2260,14 +2270,17 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
     if (gating || tracing) {
       gated_now = gating && !force_full && n >= 2 &&
                   (gate_tail <= 0.0 || last_full_gain < gate_tail * thresh);
-      if (n >= 2 && (gated_now || tracing))
-        LAUNCH(k_gate_features, grid_for(L.nv, 256, nsm_ * 8), 256, 0, s_, L.nv, L.ptr, vDeg,
-               rec_own_, rec_gain_, last_move_, n, phase_index_, feat_);
+      const GateFeatSrc fsrc{L.ptr, vDeg, rec_own_, rec_gain_, last_move_, n, phase_index_};
+      if (n >= 2 && tracing)
+        LAUNCH(k_gate_features, grid_for(L.nv, 256, nsm_ * 8), 256, 0, s_, L.nv, fsrc, feat_);
       p.a.skip = nullptr;
       if (gated_now) {
+        // the features are computed inside the inference kernel unless a
+        // trace capture has just written them
         CK(cudaMemsetAsync(evald_, 0, sizeof(unsigned long long), s_));
         LAUNCH(k_gate_infer, std::max(1, (int)std::min<int64_t>((L.nv + 127) / 128, nsm_ * 8)), 256, 0,
-               s_, L.nv, feat_, gate_p_, tau, L.ptr, (float *)nullptr, skip_, evald_);
+               s_, L.nv, tracing ? (const float *)feat_ : nullptr, fsrc, gate_p_, tau, L.ptr,
+               (float *)nullptr, skip_, evald_);
         CK(cudaMemsetAsync(d_kept, 0, nclass * sizeof(int32_t), s_));
         LAUNCH(k_class_kept, grid_for(nmem, 256, nsm_ * 8), 256, 0, s_, nclass, d_cls_b, nmem,
                members_, skip_, d_kept);
@@ -2478,6 +2491,7 @@ int Engine::run_persistent(const Level &L, const std::vector<ClassSched> &sched,
       LAUNCH(k_rotate, grid_for(L.nv, 256, nsm_ * 16), 256, 0, s_, L.nv, Cpast, C, Ctgt);
     }
   }
+  if (gating || tracing) gate_release();
   dfree(d_trace);
   dfree(d_ctr);
   dfree(pair_u); dfree(pair_t); dfree(pair_w);
@@ -4115,7 +4129,7 @@ int glv_gate_infer(long n, const float *d_feat, float *d_prob, void *stream) {
   cudaStream_t s = (cudaStream_t)stream;
   if (n > 0) {
     k_gate_infer<<<(int)std::max<long>(1, std::min<long>((n + 127) / 128, 148 * 8)), 256, 0, s>>>(
-        n, d_feat, (const float *)dp.p, 0.5f, nullptr, d_prob, nullptr, nullptr);
+        n, d_feat, GateFeatSrc{}, (const float *)dp.p, 0.5f, nullptr, d_prob, nullptr, nullptr);
     ++g_launches;
     CK(cudaGetLastError());
   }

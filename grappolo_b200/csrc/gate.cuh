@@ -29,32 +29,50 @@ __device__ __forceinline__ float bf16r(float x) {
   return __bfloat162float(__float2bfloat16_rn(x));
 }
 
-__global__ void k_gate_features(int64_t nv, const int64_t *ptr, const double *vDeg,
-                                const double *rec_own, const float *rec_gain,
-                                const int32_t *last_move, int32_t iter, int32_t phase,
-                                float *feat) {
+// What the features of a vertex are computed from (the sweep's state after
+// iteration iter - 1 of phase `phase`).
+struct GateFeatSrc {
+  const int64_t *ptr;
+  const double *vDeg;
+  const double *rec_own;
+  const float *rec_gain;
+  const int32_t *last_move;
+  int32_t iter, phase;
+};
+
+__device__ __forceinline__ void gate_features(int64_t v, const GateFeatSrc &s, float f[kGateIn]) {
+  const double deg = (double)(s.ptr[v + 1] - s.ptr[v]);
+  const double wd = s.vDeg[v];
+  const double inv = wd > 0.0 ? 1.0 / wd : 0.0;
+  f[0] = (float)(log1p(deg) * 0.125);
+  f[1] = (float)(log1p(wd) * 0.125);
+  f[2] = (float)(s.rec_own[v] * inv);
+  f[3] = (float)((double)s.rec_gain[v] * inv);
+  f[4] = (float)(log1p((double)(s.iter - s.last_move[v])) * 0.25);
+  f[5] = (float)s.phase * 0.125f;
+}
+
+// The feature rows, for trace capture (the gated sweeps compute them inside
+// k_gate_infer instead).
+__global__ void k_gate_features(int64_t nv, GateFeatSrc src, float *feat) {
   for (int64_t v = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; v < nv;
        v += (int64_t)gridDim.x * blockDim.x) {
-    const double deg = (double)(ptr[v + 1] - ptr[v]);
-    const double wd = vDeg[v];
-    const double inv = wd > 0.0 ? 1.0 / wd : 0.0;
-    float *f = feat + (size_t)v * kGateIn;
-    f[0] = (float)(log1p(deg) * 0.125);
-    f[1] = (float)(log1p(wd) * 0.125);
-    f[2] = (float)(rec_own[v] * inv);
-    f[3] = (float)((double)rec_gain[v] * inv);
-    f[4] = (float)(log1p((double)(iter - last_move[v])) * 0.25);
-    f[5] = (float)phase * 0.125f;
+    float f[kGateIn];
+    gate_features(v, src, f);
+#pragma unroll
+    for (int i = 0; i < kGateIn; ++i) feat[(size_t)v * kGateIn + i] = f[i];
   }
 }
 
 // Inference: one warp per 16 vertices.  Layer 1 on the CUDA cores into a
 // per-warp BF16 tile, layer 2 with mma.sync (8 column tiles x 4 k-steps),
-// layer 3 as a 4-lane reduction.  prob may be NULL; skip[v] = (p < tau);
-// *evaluated += row lengths of the kept vertices.
+// layer 3 as a 4-lane reduction.  The features come from `feat` (rows of
+// kGateIn floats) or, when feat is NULL, from `src`: lane r computes those of
+// the tile's row r and the warp reads them by shuffles.  prob may be NULL;
+// skip[v] = (p < tau); *evaluated += row lengths of the kept vertices.
 __global__ void __launch_bounds__(256) k_gate_infer(int64_t nv, const float *feat,
-                                                    const float *params, float tau,
-                                                    const int64_t *ptr, float *prob,
+                                                    GateFeatSrc src, const float *params,
+                                                    float tau, const int64_t *ptr, float *prob,
                                                     uint8_t *skip,
                                                     unsigned long long *evaluated) {
   __shared__ float s_w1[kGateHid * kGateIn], s_b1[kGateHid], s_b2[kGateHid], s_w3[kGateHid];
@@ -78,12 +96,16 @@ __global__ void __launch_bounds__(256) k_gate_infer(int64_t nv, const float *fea
   unsigned long long local_eval = 0;
   for (int64_t tile = (int64_t)blockIdx.x * 8 + warp; tile < ntile; tile += (int64_t)gridDim.x * 8) {
     const int64_t v0 = tile * 16;
+    float mine[kGateIn] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // row `lane`'s features
+    if (!feat && lane < 16 && v0 + lane < nv) gate_features(v0 + lane, src, mine);
     // layer 1: lane handles hidden units lane and lane+32 for the 16 rows
     for (int r = 0; r < 16; ++r) {
       const int64_t v = v0 + r;
       float x[kGateIn];
 #pragma unroll
-      for (int i = 0; i < kGateIn; ++i) x[i] = (v < nv) ? feat[(size_t)v * kGateIn + i] : 0.0f;
+      for (int i = 0; i < kGateIn; ++i)
+        x[i] = feat ? ((v < nv) ? feat[(size_t)v * kGateIn + i] : 0.0f)
+                    : __shfl_sync(FULL, mine[i], r);
 #pragma unroll
       for (int q = 0; q < 2; ++q) {
         const int j = lane + 32 * q;

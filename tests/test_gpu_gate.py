@@ -83,3 +83,27 @@ def test_learned_gate_gains_over_plain(monkeypatch):
     e_plain = np.median([s['edges_swept'] for s in plain])
     e_gated = np.median([s['edges_swept'] for s in gated])
     assert e_gated < 0.9 * e_plain
+
+
+def test_fused_features_match_stored_rows(monkeypatch):
+    """Gated sweeps compute the gate's features inside the inference kernel;
+    with trace capture on they are written as rows first and read back.  On a
+    unit-weight graph with the id-order colouring every sum is exact, so the
+    two runs are the same run: equal communities, modularity and entries
+    evaluated."""
+    monkeypatch.setenv('GRAPPOLO_B200_COLORING', 'id')
+    p, tau = _trained()
+    gate.set_gate(p, tau)
+    g = graphs.planted_powerlaw(40000, seed=5)
+    C1, s1 = louvain.run_multiphase_csr(g, coloring=True, mode=_lib.GLV_MODE_LEARNED)
+    L = _lib.lib()
+    _lib.check(L.glv_trace_begin(1 << 20, 0.25))
+    try:
+        C2, s2 = louvain.run_multiphase_csr(g, coloring=True, mode=_lib.GLV_MODE_LEARNED)
+    finally:
+        L.glv_trace_end()
+    _, s0 = louvain.run_multiphase_csr(g, coloring=True, mode=_lib.GLV_MODE_FAST)
+    assert s1['edges_swept'] < s0['edges_swept']  # some sweeps were gated
+    assert np.array_equal(C1, C2)
+    assert s1['final_modularity'] == s2['final_modularity']
+    assert s1['edges_swept'] == s2['edges_swept']
