@@ -719,6 +719,12 @@ def main():
         return run_csr_workload(args, world, rank, local)
     if args.workload == 'compare':
         return run_compare_workload(args, world, rank, local)
+    if args.workload == 'rmat' and args.scale >= 26:
+        # graphs of tens of GB: torch's allocator maps pages as needed and
+        # unmaps the builder's freed scratch on empty_cache(), so none of it
+        # stays reserved beside the graph (the engine allocates from its own
+        # pool; with whole segments ~33 GB stayed reserved at scale 27)
+        os.environ.setdefault('PYTORCH_CUDA_ALLOC_CONF', 'expandable_segments:True')
     import numpy as np
     import torch
     from grappolo_b200 import graphs, louvain, _lib

@@ -361,6 +361,7 @@ class Engine {
   bool learned() const { return mode_ == GLV_MODE_LEARNED; }
   int gate_init(int64_t nv, bool tracing);
   void gate_release();
+  int64_t avail_bytes();
 
  public:  // the allocator (the C ABI helpers allocate level-0 arrays through it)
   // Requests above 1 MiB are rounded up to quarter-octave size classes so that
@@ -1988,6 +1989,29 @@ int Engine::gate_init(int64_t nv, bool tracing) {
   return GLV_OK;
 }
 
+// Device memory an allocation could still get: free on the device, unused in
+// the pool, and the blocks in this device's cache (a failed allocation hands
+// them back to the pool).
+int64_t Engine::avail_bytes() {
+  size_t fr = 0, tot = 0;
+  if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  uint64_t rc = 0, uc = 0;
+  if (pool_) {
+    cudaMemPoolGetAttribute(pool_, cudaMemPoolAttrReservedMemCurrent, &rc);
+    cudaMemPoolGetAttribute(pool_, cudaMemPoolAttrUsedMemCurrent, &uc);
+  }
+  size_t cached = 0;
+  {
+    BlockCache &bc = g_cache[dev_];
+    std::lock_guard<std::mutex> lock(bc.mu);
+    for (const auto &kv : bc.free) cached += kv.first * kv.second.size();
+  }
+  return (int64_t)fr + (int64_t)(rc > uc ? rc - uc : 0) + (int64_t)cached;
+}
+
 void Engine::gate_release() {
   dfree(rec_own_); dfree(rec_gain_); dfree(last_move_); dfree(skip_); dfree(feat_);
   dfree(gate_p_); dfree(evald_);
@@ -2654,10 +2678,27 @@ int Engine::coarsen_chunked(const Level &in, const int32_t *Cm, int64_t ncl, Lev
     return GLV_OK;
   };
   // The coarse rows go straight to their place.  `total` (records of all
-  // chunks) bounds the coarse entries; when that bound is large the chunks
-  // are run twice, first only to count, so the level gets its exact size.
-  const bool two_pass = total * (int64_t)(sizeof(int32_t) + sizeof(double)) > (int64_t(16) << 30) ||
-                        getenv("GRAPPOLO_B200_COARSEN_EXACT") != nullptr;
+  // chunks) bounds the coarse entries.  A level of that bound is allocated
+  // unless it is large and the device could not hold it beside a margin for
+  // the next phase (a tenth of the device, at least 8 GB); then the chunks
+  // run twice, first only to count, so the level gets its exact size (the
+  // counting pass repeats every chunk's records and sorts).
+  const int64_t bound_bytes = total * (int64_t)(sizeof(int32_t) + sizeof(double));
+  // GRAPPOLO_B200_COARSEN_PASSES=1|2 forces one way.
+  const char *cp = getenv("GRAPPOLO_B200_COARSEN_PASSES");
+  bool two_pass = getenv("GRAPPOLO_B200_COARSEN_EXACT") != nullptr || (cp && atoi(cp) == 2);
+  int64_t avail = -1;
+  if (!two_pass && !(cp && atoi(cp) == 1) && bound_bytes > (int64_t(16) << 30)) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) cudaGetLastError();
+    const int64_t margin = std::max<int64_t>(int64_t(8) << 30, (int64_t)tot / 10);
+    avail = avail_bytes();
+    two_pass = bound_bytes + margin > avail;
+  }
+  if (debug_)
+    fprintf(stderr, "grappolo_b200: chunked coarsening, %d chunks, bound %.2f GB, available "
+            "%.2f GB, %s\n", K, bound_bytes * 1e-9, avail * 1e-9,
+            two_pass ? "counting pass first" : "one pass");
   for (int pass = two_pass ? 0 : 1; pass < 2; ++pass) {
     const bool counting = pass == 0;
     if (!counting) {
