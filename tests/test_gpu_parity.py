@@ -109,16 +109,19 @@ def test_coarsen(name):
     assert np.array_equal(cg.weight, z['coarse_weight'])
 
 
-@pytest.mark.parametrize('exact', [False, True])
+@pytest.mark.parametrize('passes', [None, 'exact', '1', '2'])
 @pytest.mark.parametrize('name', CASES)
-def test_coarsen_chunked(name, exact, monkeypatch):
+def test_coarsen_chunked(name, passes, monkeypatch):
     """The chunked coarsening (forced, 7-record chunks, so communities are
     spread over many chunks; with and without the counting pass that sizes
-    the level exactly) builds the same coarse graph: bit for bit on integral
-    weights, to rounding on others (it adds in another order)."""
+    the level exactly, by its own choice or forced either way) builds the
+    same coarse graph: bit for bit on integral weights, to rounding on others
+    (it adds in another order)."""
     monkeypatch.setenv('GRAPPOLO_B200_COARSEN_CHUNK', '7')
-    if exact:
+    if passes == 'exact':
         monkeypatch.setenv('GRAPPOLO_B200_COARSEN_EXACT', '1')
+    elif passes:
+        monkeypatch.setenv('GRAPPOLO_B200_COARSEN_PASSES', passes)
     g, z = load(name)
     cg, ne = louvain.buildNextLevelGraphOpt(g, z['renum_C'], int(z['renum_n']), nThreads=8)
     assert ne == z['coarse_ne']
