@@ -107,6 +107,11 @@ class COracle:
         p, t, w = _csr(g)
         C = np.zeros(g.num_vertices, dtype=np.int64)
         col = np.ascontiguousarray(colors, dtype=np.int32)
+        # the C routine sizes its per-colour arrays by num_colors (one more
+        # than the largest colour, as color_greedy's second result is the
+        # largest colour): check before it writes past them
+        if col.size and (col.min() < 0 or col.max() >= num_colors):
+            raise ValueError('colours must lie in [0, num_colors)')
         itr = ct.c_int(0)
         tq = np.zeros(trace_cap)
         q = self.L.lvo_coloring_phase(ct.c_long(g.num_vertices), _lp(p), _lp(t), _dp(w), _lp(C),
@@ -219,6 +224,8 @@ class COracle:
         no colour qualified -- where type 0 of the reference is undefined)."""
         p, t, _ = _csr(g)
         col = np.array(color, dtype=np.int32)
+        if col.size and (col.min() < 0 or col.max() >= ncolors):
+            raise ValueError('colours must lie in [0, ncolors)')
         stuck = ct.c_long(0)
         n = self.L.lvo_vbase(ct.c_long(g.num_vertices), _lp(p), _lp(t), _ip(col),
                              ct.c_int(ncolors), ct.c_int(vtype), ct.byref(stuck))

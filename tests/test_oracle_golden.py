@@ -182,3 +182,17 @@ def test_gini_golden(oracle, k):
     sizes, value, srt = gini_cases()[k]
     g, s = oracle.gini(sizes)
     assert g == value and np.array_equal(s, srt)
+
+
+def test_colour_count_is_checked(oracle):
+    """color_greedy returns the largest colour; a colouring phase or a
+    redistribution given that as the colour count is refused before the C
+    routines index their per-colour arrays with it."""
+    g, _ = load('karate')
+    col, mc = oracle.color_greedy(g)
+    with pytest.raises(ValueError):
+        oracle.coloring_phase(g, col, mc)
+    with pytest.raises(ValueError):
+        oracle.vbase(g, col, mc)
+    q, C, itr, _ = oracle.coloring_phase(g, col, mc + 1)
+    assert itr >= 1 and C.shape == (g.num_vertices,)
