@@ -949,10 +949,20 @@ def reference_full_run(scale):
     t0 = time.perf_counter()
     _, s, _ = Reference(fast=True).run_multiphase_coloring(g, nthreads=cores)
     ref_wall = time.perf_counter() - t0
+    # the heuristic the learned gate stands in for, run by the reference
+    # itself beside the plain method it modifies: runMultiPhaseBasic and
+    # runMultiPhaseSyncType(3), the early-termination Louvain
+    # (FullSyncOptimization/parallelLouvainMethodEarlyTerminate.cpp:116-195)
+    _, sb, _ = Reference(fast=True).run_multiphase_basic(g, nthreads=cores)
+    _, se, _ = Reference(fast=True).run_multiphase_sync(g, 3, nthreads=cores)
     louvain.run_multiphase_csr(g, coloring=True, mode=_lib.GLV_MODE_FAST)  # warm
     t0 = time.perf_counter()
     _, st = louvain.run_multiphase_csr(g, coloring=True, mode=_lib.GLV_MODE_FAST)
     gpu_wall = time.perf_counter() - t0
+
+    def arm(x):
+        return {'total_time_s': x.get('total_time'), 'final_modularity': x.get('final_mod'),
+                'phases': x.get('phases'), 'iterations': x.get('total_iterations')}
     return {'graph': f'R-MAT scale {scale}, edge factor 16, a=0.57 b=0.19 c=0.19, FP64 '
                      f'weights U(0,1], numpy seed 1 ({g.num_vertices} vertices, {g.nnz} '
                      f'CSR entries)',
@@ -964,7 +974,12 @@ def reference_full_run(scale):
                          'engine_total_s': st['time_total'],
                          'final_modularity': st['final_modularity'],
                          'phases': st['phases'], 'iterations': st['total_iterations']},
-            'time_ratio_reference_over_gpu': (s.get('total_time') or ref_wall) / gpu_wall}
+            'time_ratio_reference_over_gpu': (s.get('total_time') or ref_wall) / gpu_wall,
+            'reference_basic': arm(sb),
+            'reference_early_termination': arm(se),
+            'early_termination_time_over_basic':
+                (se['total_time'] / sb['total_time'])
+                if se.get('total_time') and sb.get('total_time') else None}
 
 
 def cpu_baseline(ptr, tail, w):

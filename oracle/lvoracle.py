@@ -567,6 +567,21 @@ class Reference:
         text = buf.value.decode(errors='replace')
         return C, parse_reference_log(text), text
 
+    def run_multiphase_sync(self, g, sync_type=3, threshold=1e-6, nthreads=1,
+                            min_graph_size=1000, c_threshold=1e-4):
+        """runMultiPhaseSyncType (FullSyncOptimization/runMultiPhaseSyncType.cpp:48);
+        sync_type 3 is the early-termination Louvain
+        (parallelLouvainMethodEarlyTerminate.cpp:116-195)."""
+        p, t, w = _csr(g)
+        C = np.full(g.num_vertices, -1, dtype=np.int64)
+        buf = ct.create_string_buffer(1 << 22)
+        self.L.ref_run_multiphase_sync(ct.c_long(g.num_vertices), _lp(p), _lp(t), _dp(w), _lp(C),
+                                       ct.c_int(sync_type), ct.c_long(min_graph_size),
+                                       ct.c_double(threshold), ct.c_double(c_threshold),
+                                       ct.c_int(nthreads), buf, ct.c_long(1 << 22))
+        text = buf.value.decode(errors='replace')
+        return C, parse_reference_log(text), text
+
     def vbase(self, g, color, ncolors, vtype=0):
         """vBaseRedistribution (Coloring/vBase.cpp:6-168) from the copy with its missing
         return added (oracle/ref_vbase.cpp); one thread.  Type 0 reads past its

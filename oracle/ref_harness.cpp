@@ -2,7 +2,7 @@
 //
 // TEST INFRASTRUCTURE ONLY.  oracle/Makefile compiles this file together with
 // the reference's unmodified sources (Utility/, Coloring/,
-// BasicCommunitiesDetection/, InputsOutput/loadMetis.cpp) into
+// BasicCommunitiesDetection/, FullSyncOptimization/, InputsOutput/) into
 // oracle/_ref/libgrappolo_ref.so.  It converts the SoA CSR that the tests use
 // into the reference's `graph`/`edge` structs (DefineStructure/defs.h:78-92),
 // calls the reference function named in each wrapper, and copies results
@@ -22,6 +22,7 @@
 #include "color_comm.h"
 #include "coloring.h"
 #include "input_output.h"
+#include "sync_comm.h"
 #include "utilityClusteringFunctions.h"
 
 static int g_quiet = 0;
@@ -332,6 +333,26 @@ long ref_run_multiphase_coloring(long nv, const long *ptr, const long *tail, con
     a.threshold = threshold; a.C_threshold = C_threshold; a.nthreads = nthreads;
     for (long i = 0; i < nv; i++) C_orig[i] = -1;
     return run_captured(log, cap, call_coloring, &a);
+}
+
+// FullSyncOptimization/runMultiPhaseSyncType.cpp:48 (syncType 3: the
+// early-termination Louvain of parallelLouvainMethodEarlyTerminate.cpp).
+static void call_sync(void *p) {
+    mp_args *a = (mp_args *)p;
+    runMultiPhaseSyncType(a->G, a->C_orig, a->basicOpt, a->minGraphSize, a->threshold,
+                          a->C_threshold, a->nthreads, 1);
+}
+
+long ref_run_multiphase_sync(long nv, const long *ptr, const long *tail, const double *w,
+                             long *C_orig, int syncType, long minGraphSize, double threshold,
+                             double C_threshold, int nthreads, char *log, long cap) {
+    mp_args a;
+    a.G = make_graph(nv, ptr, tail, w);  // freed by the reference
+    a.C_orig = C_orig; a.coloring = 0; a.numColors = 0; a.replaceMap = 0;
+    a.basicOpt = syncType; a.minGraphSize = minGraphSize; a.threshold = threshold;
+    a.C_threshold = C_threshold; a.nthreads = nthreads;
+    for (long i = 0; i < nv; i++) C_orig[i] = -1;
+    return run_captured(log, cap, call_sync, &a);
 }
 
 long ref_run_multiphase_basic(long nv, const long *ptr, const long *tail, const double *w,

@@ -148,3 +148,19 @@ def test_community_comparison_matches_reference(oracle, reference, seed):
     assert np.array_equal(a1, b1) and np.array_equal(a2, b2)
     sz = rng.integers(0, 10000, int(rng.integers(1, 3000)))
     assert oracle.gini(sz)[0] == reference.gini(sz)[0]
+
+
+def test_early_termination_arm_runs(reference):
+    """The reference's early-termination Louvain (runMultiPhaseSyncType with
+    syncType 3), the heuristic the learned gate stands in for, runs through
+    the harness beside the plain Jacobi method it modifies: both print their
+    summaries, label every vertex and reach a positive modularity.  (It
+    terminates vertices for good, so its Q may differ from the plain one's.)"""
+    g = graphs.planted_partition(num_blocks=30, block_size=60, intra_degree=9,
+                                 inter_degree=3, seed=11)
+    Cb, sb, _ = reference.run_multiphase_basic(g, nthreads=2)
+    Ce, se, _ = reference.run_multiphase_sync(g, 3, nthreads=2)
+    for C, s in ((Cb, sb), (Ce, se)):
+        assert C.min() >= 0
+        assert s['final_mod'] > 0.3 and s['total_iterations'] >= 1 and s['total_time'] >= 0
+    assert abs(se['final_mod'] - sb['final_mod']) < 0.05
