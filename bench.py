@@ -937,6 +937,19 @@ def learned_vs_plain(L, nv, ptr, tail, w, C, plain_stats, plain_s, steps, dev):
             'iterations_learned': st[-1]['total_iterations']}
 
 
+def _reference_basic_and_early_termination(path, cores):
+    """Child process of reference_full_run: the reference's plain Jacobi
+    multiphase run and its early-termination run on the graph saved at path."""
+    import numpy as np
+    from grappolo_b200 import graphs
+    from oracle import Reference
+    z = np.load(path)
+    g = graphs.CSRGraph(z['ptr'], z['tail'], z['weight'])
+    _, sb, _ = Reference(fast=True).run_multiphase_basic(g, nthreads=cores)
+    _, se, _ = Reference(fast=True).run_multiphase_sync(g, 3, nthreads=cores)
+    return sb, se
+
+
 def reference_full_run(scale):
     """Time to modularity of the reference itself: Grappolo's
     runMultiPhaseColoring (oracle/_ref, shipped -Ofast flags, all host cores;
@@ -952,15 +965,27 @@ def reference_full_run(scale):
     # the heuristic the learned gate stands in for, run by the reference
     # itself beside the plain method it modifies: runMultiPhaseBasic and
     # runMultiPhaseSyncType(3), the early-termination Louvain
-    # (FullSyncOptimization/parallelLouvainMethodEarlyTerminate.cpp:116-195)
-    _, sb, _ = Reference(fast=True).run_multiphase_basic(g, nthreads=cores)
-    _, se, _ = Reference(fast=True).run_multiphase_sync(g, 3, nthreads=cores)
+    # (FullSyncOptimization/parallelLouvainMethodEarlyTerminate.cpp:116-195),
+    # in a child process, so that a failure of that code costs only its record
+    import numpy as np
+    from concurrent.futures import ProcessPoolExecutor
+    import multiprocessing as mp
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, 'graph.npz')
+        np.savez(path, ptr=g.ptr, tail=g.tail, weight=g.weight)
+        try:
+            with ProcessPoolExecutor(1, mp_context=mp.get_context('spawn')) as ex:
+                sb, se = ex.submit(_reference_basic_and_early_termination, path, cores).result()
+        except Exception as e:  # noqa: BLE001 - the record says what happened
+            sb = se = {'error': f'{type(e).__name__}: {e}'}
     louvain.run_multiphase_csr(g, coloring=True, mode=_lib.GLV_MODE_FAST)  # warm
     t0 = time.perf_counter()
     _, st = louvain.run_multiphase_csr(g, coloring=True, mode=_lib.GLV_MODE_FAST)
     gpu_wall = time.perf_counter() - t0
 
     def arm(x):
+        if 'error' in x:
+            return {'error': x['error']}
         return {'total_time_s': x.get('total_time'), 'final_modularity': x.get('final_mod'),
                 'phases': x.get('phases'), 'iterations': x.get('total_iterations')}
     return {'graph': f'R-MAT scale {scale}, edge factor 16, a=0.57 b=0.19 c=0.19, FP64 '
